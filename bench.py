@@ -1,0 +1,337 @@
+"""Benchmark: particle-substeps/s of the 2D MLS-MPM substep on B200.
+
+Workload (default): the 1,000,000-particle two-phase water/oil dam break on a
+1024x2048 grid (cellSize 10, gravity 90, 1/240 s macrosteps split by CFL 0.3),
+gather P2G, FP32.  One step = one macrostep: a CFL-certified batch of
+microsteps submitted through the reference-facing API
+(`step_cfl_batch_adaptive`, the host loop of stepCflBatchAdaptive) with its
+compact readback.
+
+* value: particles x committed substeps / summed device time of the batches
+  (CUDA events recorded on the solver's stream around each batch);
+* e2e: the same count / wall time of the API calls (host CFL planning, the
+  parameter upload from pinned memory, the graph launches and the 40-byte
+  compact readback of each batch);
+* roofline: the dominant kernel, from a kernel-by-kernel event-timed run of
+  real substeps right after the timed region;
+* cpu_baseline: the FP64 C restatement of the reference CPU step on a bounded
+  sample of the same scene, single-threaded like the reference's worker.
+
+`--impl reference` times that CPU restatement alone (the reference is
+TypeScript; no JavaScript runtime exists on this image).  Multi-GPU runs are
+replicas: each rank steps its own copy of the scene (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(ROOT, "powder-play_b200"), os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "particle-substeps/s on 1 B200, plain vs batched; adjoint/forward time ratio"
+UNIT = "particle-substeps/s"
+MACRO_DT = 1 / 240
+MAX_MICROSTEPS = 256
+L2_FLUSH_BYTES = 512 * 1024 * 1024
+
+
+def _rank_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for name, value in zip(names[1:], r[5:9]):
+                if value.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            data = json.load(f)
+        return float(data["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def build_workload(name: str):
+    from mpm_b200.scenes import (DAM_BREAK_GRAVITY, create_dam_break_scene, create_si_tank_scene, SI_TANK_GRAVITY)
+    if name == "dam-break-1m":
+        p, config = create_dam_break_scene()
+        return p, config, DAM_BREAK_GRAVITY, {
+            "workload": "two-phase water/oil dam break, 1,000,000 particles (500k water + 500k oil, 2x2 per "
+                        "cell), 1024x2048 grid, cellSize 10, gravity 90, macrostep 1/240 s, CFL 0.3",
+            "particles": len(p), "grid": "1024x2048", "macro_dt": MACRO_DT, "courant": 0.3}
+    if name == "si-tank":
+        p, config = create_si_tank_scene(seed=1)
+        return p, config, SI_TANK_GRAVITY, {
+            "workload": "SI Tait water tank, 1,600 particles, 80x80 grid (dx 2.5 mm), macrostep 1/120 s",
+            "particles": len(p), "grid": "80x80", "macro_dt": 1 / 120, "courant": 0.3}
+    raise SystemExit(f"unknown workload {name}")
+
+
+def plan_macrostep(solver, config, velocity, macro_dt, gravity):
+    from mpm_b200 import calculate_mpm_cfl_microsteps
+    from mpm_b200.cfl_bounds import calculate_mpm_cfl_velocity_bound
+    gmag = math.hypot(gravity["x"], gravity["y"])
+    bound = calculate_mpm_cfl_velocity_bound(velocity, macro_dt, gmag, 0, 0, 0, 0)
+    bound = max(bound, solver._last_scheduled_velocity_bound or 0.0)
+    plan = calculate_mpm_cfl_microsteps(macro_dt, config["grid"]["cellSize"], solver.cfl_bounds["waveSpeedBound"],
+                                        bound, MAX_MICROSTEPS)
+    return plan, bound
+
+
+def cpu_baseline(particles, config, gravity, micro_dt, substeps: int) -> dict:
+    """The FP64 C restatement of the reference CPU step (oracle/), timed on a
+    bounded sample: `substeps` substeps of the full scene, one thread."""
+    from oracle import OracleState
+    state = OracleState(particles, dict(config, dt=micro_dt, gravity=gravity))
+    cfg = dict(config, dt=micro_dt, gravity=gravity)
+    t0 = time.perf_counter()
+    state.run(cfg, substeps)
+    elapsed = time.perf_counter() - t0
+    n = len(particles)
+    return {"value": n * substeps / elapsed, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{substeps} substeps of the full {n}-particle scene at dt {micro_dt:.3e} s "
+                      f"({elapsed:.1f} s, C FP64 restatement of stepMpm, single thread)"}
+
+
+def kernel_bytes(name: str, n: int, active: tuple) -> float:
+    """Algorithmic bytes per launch of the substep kernels (the per-kernel
+    split of 104 B per particle + 64 B per active channel-node)."""
+    channel_nodes = float(sum(active))
+    table = {
+        "k_g2p": n * 104.0 + channel_nodes * 16.0,
+        "k_p2g_gather": n * 40.0 + channel_nodes * 16.0,
+        "k_grid_update": channel_nodes * 32.0,
+        "k_rank_prepare": n * (56.0 + 40.0 + 12.0),
+        "k_prepare_scatter": n * 56.0 + channel_nodes * 16.0,
+        "k_fixed_decode": channel_nodes * 16.0,
+        "k_count": n * 16.0,
+        "k_scatter": n * 16.0,
+    }
+    return table.get(name, 0.0)
+
+
+def run_reference(args):
+    rank, _, world = _rank_info()
+    if rank != 0:
+        return
+    particles, config, gravity, meta = build_workload(args.workload)
+    from mpm_b200 import calculate_mpm_cfl_microsteps, derive_mpm_mls_gpu_cfl_bounds
+    bounds = derive_mpm_mls_gpu_cfl_bounds(particles, config)
+    plan = calculate_mpm_cfl_microsteps(meta["macro_dt"], config["grid"]["cellSize"], bounds["waveSpeedBound"],
+                                        max(bounds["velocityBound"], 5.0), MAX_MICROSTEPS)
+    micro = float(np.float32(plan["microDt"]))
+    total_sub, total_s, samples = 0, 0.0, []
+    for step in range(args.warmup + args.steps):
+        res = cpu_baseline(particles, config, gravity, micro, args.reference_substeps)
+        if step >= args.warmup:
+            total_sub += args.reference_substeps
+            total_s += len(particles) * args.reference_substeps / res["value"]
+            samples.append(res["sample"])
+    value = len(particles) * total_sub / total_s
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scene)",
+            "impl": "reference", "config": dict(meta, p2g="CPU scatter (stepMpm restatement)"),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                             "sample": f"{args.reference_substeps} substeps per step; {samples[0] if samples else ''}"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args):
+    rank, local_rank, world = _rank_info()
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local_rank)
+    from mpm_b200 import create_experimental_mpm_mls_atomic_gpu_solver, create_mpm_mls_gpu_solver
+
+    particles, config, gravity, meta = build_workload(args.workload)
+    if args.p2g == "fixed":
+        solver = create_experimental_mpm_mls_atomic_gpu_solver(particles, config, device=local_rank,
+                                                               fixed_point_shift=args.fixed_shift)
+    else:
+        solver = create_mpm_mls_gpu_solver(particles, config, device=local_rank)
+    n = len(particles)
+    macro_dt = meta["macro_dt"]
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
+    velocity = solver.cfl_bounds["velocityBound"]
+
+    def one_step():
+        nonlocal velocity
+        plan, bound = plan_macrostep(solver, config, velocity, macro_dt, gravity)
+        m = solver.step_cfl_batch_adaptive(1, macro_dt, plan, bound, MAX_MICROSTEPS, gravity)
+        velocity = m["recommendedVelocityBound"]
+        return m
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    solver.device_ms_total = 0.0
+    solver.committed_microsteps_total = 0
+    wall = 0.0
+    retries = 0
+    h2d = d2h = 0
+    for _ in range(args.steps):
+        flush.zero_()  # L2 flush between timed steps (outside the timed batches)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m = one_step()
+        wall += time.perf_counter() - t0
+        retries += m["retryCount"]
+        batches = 1 + m["retryCount"]
+        h2d += batches * 160  # StepParams upload per batch
+        d2h += batches * 40   # compact speed / progress / status readback
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    device_s = solver.device_ms_total / 1e3
+    substeps = solver.committed_microsteps_total
+    times = torch.tensor([device_s, wall], dtype=torch.float64, device=f"cuda:{local_rank}")
+    if dist:
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    device_s, wall = float(times[0]), float(times[1])
+    value = world * n * substeps / device_s
+    e2e_value = world * n * substeps / wall
+
+    # roofline: kernel-by-kernel timing of real substeps right after the timed region
+    plan, bound = plan_macrostep(solver, config, velocity, macro_dt, gravity)
+    from mpm_b200.cfl import calculate_mpm_cfl_velocity_limit
+    limit = calculate_mpm_cfl_velocity_limit(config["grid"]["cellSize"], solver.cfl_bounds["waveSpeedBound"],
+                                             plan["microDt"])
+    prof = solver.profile_substeps(plan["stepCount"], plan["microDt"], gravity, velocity_limit=limit)
+    active = solver.count_active_nodes()
+    total_ms = sum(ms for ms, _ in prof.values())
+    dominant = max(prof, key=lambda k: prof[k][0])
+    dom_ms, dom_launches = prof[dominant]
+    dom_bytes = kernel_bytes(dominant, n, active)
+    peak, peak_kind = _peaks()
+    achieved = dom_bytes / (dom_ms / dom_launches * 1e-3) / 1e9
+    substep_bytes = n * 104.0 + float(sum(active)) * 64.0
+    substep_ms = total_ms / plan["stepCount"]
+    gpu_launches = 0
+    launches_per_substep = sum(l for _, l in prof.values()) / plan["stepCount"]
+    gpu_launches = int(round(launches_per_substep * substeps / world)) if substeps else 0
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": device_s * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene, no dataset)",
+        "config": dict(meta, p2g=args.p2g, parallelism=f"replicas x{world}", l2="flushed (512 MiB write) "
+                       "between timed steps", committed_substeps=substeps, retries=retries,
+                       substeps_per_step=substeps / args.steps / world),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d // args.steps,
+                "d2h_bytes_per_step": d2h // args.steps,
+                "path": "Python host mirror of MpmMlsGpuSolver.stepCflBatchAdaptive -> C ABI"},
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": dom_ms / dom_launches,
+                     "kernel_share": dom_ms / total_ms,
+                     "substep": {"algorithmic_bytes": substep_bytes, "ms": substep_ms,
+                                 "achieved_gbs": substep_bytes / (substep_ms * 1e-3) / 1e9,
+                                 "frac": substep_bytes / (substep_ms * 1e-3) / 1e9 / peak},
+                     "active_channel_nodes": list(active),
+                     "kernels_ms_per_substep": {k: v[0] / plan["stepCount"] for k, v in prof.items()}},
+        "clocks": clock_info,
+        "gpu_launches": gpu_launches,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(particles, config, gravity, float(np.float32(plan["microDt"])),
+                                            args.cpu_substeps)
+    solver.dispose()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", default="dam-break-1m", choices=["dam-break-1m", "si-tank"])
+    ap.add_argument("--p2g", choices=["gather", "fixed"], default="gather")
+    ap.add_argument("--fixed-shift", type=int, default=16)
+    ap.add_argument("--cpu-substeps", type=int, default=12)
+    ap.add_argument("--reference-substeps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be at least 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,185 @@
+/*
+ * mpm_b200.h -- C ABI of the B200-native MLS-MPM substep library
+ * (libmpm_b200.so).  Plain pointers and sizes only; no CUDA or framework
+ * types cross this boundary.
+ *
+ * Each entry point backs one device-touching member of the reference's GPU
+ * solver interface `MpmMlsGpuSolver` (7korobi/powder-play,
+ * src/lib/mpm/kernels/solver.ts:106-144).  Host-side policy that the
+ * reference keeps in TypeScript (input validation and packing,
+ * src/lib/mpm/kernels/layout.ts; CFL planning, cfl.ts / cfl-bounds.ts /
+ * step-scheduler.ts; the adaptive retry loop, solver.ts:1724-2021) stays in
+ * the host language above this ABI.
+ *
+ * Wire format: a particle is the reference's packed 20-word record
+ * (src/lib/mpm/kernels/layout.ts:385-437): words 0-1 position, 2-3 velocity,
+ * 4-7 C (m00,m01,m10,m11), 8-11 F, 12 plastic volume, 13 model code (u32),
+ * 14 lambda, 15 mu, 16 density, 17 volume, 18 material parameter (Tait
+ * exponent / powder friction / Neo-Hookean damage), 19 bonded-vertex marker
+ * (u32, 0 = none, 1..3 = vertex 0..2).
+ *
+ * Status: the 8-word numerical status of the reference
+ * (src/lib/mpm/kernels/shaders.ts:157-172, decoded by solver.ts:232-284):
+ * [0] flag bits, [1] particle index (0xffffffff = none), [2..5] f32
+ * diagnostics, [6] diagnostic claim (1 deformation, 2 projected F, 3 CFL),
+ * [7] surface flags.
+ *
+ * Threading: a handle is not thread-safe.  Calls are ordered on the handle's
+ * CUDA stream; only the read* and queue-completion calls block.
+ */
+#ifndef MPM_B200_H
+#define MPM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPM_OK 0
+#define MPM_ERR_INVALID_ARGUMENT (-1) /* reference RangeError / TypeError class */
+#define MPM_ERR_CUDA (-2)             /* device allocation, launch or copy failed */
+#define MPM_ERR_STATE (-3)            /* call not valid in the handle's state */
+
+#define MPM_P2G_GATHER 0u      /* createMpmMlsGpuSolver (solver.ts:390-397) */
+#define MPM_P2G_FIXED_POINT 1u /* createExperimentalMpmMlsAtomicGpuSolver (solver.ts:399-406) */
+
+#define MPM_PARTICLE_WORDS 20u
+#define MPM_STATUS_WORDS 8u
+#define MPM_FRACTURE_BOND_WORDS 6u
+
+typedef struct mpm_solver mpm_solver;
+
+/* The validated configuration (MpmMlsGpuConfig, layout.ts:17-19) as the
+ * float32 values that the reference packs into SimulationParams
+ * (layout.ts:950-996). */
+typedef struct mpm_config {
+    uint32_t cells_x;
+    uint32_t cells_y;
+    float cell_size;
+    float particle_mass;
+    float particle_volume;
+    float bond_rest_length;   /* 0 when absent */
+    float bond_stiffness;     /* default 0.35 */
+    float bond_reference_dt;  /* 0 when absent: each batch supplies it */
+    float wall_friction;
+    float lambda;             /* config material, as packed in SimulationParams */
+    float mu;
+    uint32_t capacity;        /* >= initial particle count */
+    uint32_t p2g_mode;        /* MPM_P2G_GATHER or MPM_P2G_FIXED_POINT */
+    uint32_t fixed_point_shift; /* fixed-point scale 2^shift; 24 = reference */
+    int32_t device;           /* CUDA device ordinal */
+} mpm_config;
+
+/* CFL guard of one batch: cflBounds.x/y of SimulationParams. */
+typedef struct mpm_cfl_guard {
+    float wave_speed_bound;
+    float velocity_limit;
+} mpm_cfl_guard;
+
+/* Interaction drag of finishGridVelocity (shaders.ts:1748-1777). */
+typedef struct mpm_drag {
+    float target_x, target_y, radius, stiffness, damping;
+} mpm_drag;
+
+/* Replaces createMpmMlsGpuSolver / createExperimentalMpmMlsAtomicGpuSolver
+ * (solver.ts:390-406 -> createGpuSolver :408-469, createRuntime :605-1230)
+ * minus the canvas: uploads validated, packed input.  `body_starts` are the
+ * bonded-triangle body starts (layout.ts:457-493); `fracture_bonds` are
+ * packed 6-word bonds (layout.ts:508-545) and `fracture_topology` the CSR
+ * incidence (layout.ts:546-564). */
+int mpm_create(const mpm_config *config, const float *packed_particles, const uint32_t *object_ids,
+               uint32_t particle_count, const uint32_t *body_starts, uint32_t body_count,
+               const uint32_t *fracture_bonds, uint32_t fracture_bond_count,
+               const uint32_t *fracture_topology, uint32_t fracture_topology_words, mpm_solver **out);
+
+/* Encodes `step_count` full substeps of `dt` in one graph launch:
+ * stepBatch (solver.ts:1407-1599).  `guard` non-NULL = CFL batch
+ * (stepCflBatch, solver.ts:1601-1722, after host-side plan certification):
+ * the committed-microstep counter is reset, per-particle CFL validation
+ * runs, and the batch ends with the maximum-speed reduction.
+ * `bond_reference_dt` <= 0 uses the configured value, else dt. */
+int mpm_step_batch(mpm_solver *solver, uint32_t step_count, float dt, float gravity_x, float gravity_y,
+                   const mpm_cfl_guard *guard, float bond_reference_dt);
+
+/* measureMaximumParticleSpeed (solver.ts:2388-2512): the 40-byte compact
+ * readback of maximum speed, committed microsteps and status.  Blocks. */
+int mpm_read_compact(mpm_solver *solver, float *maximum_speed, uint32_t *completed_microsteps,
+                     uint32_t status[8]);
+
+/* checkNumericalStatus (solver.ts:2514-2570).  Blocks. */
+int mpm_read_status(mpm_solver *solver, uint32_t status[8]);
+
+/* Clears the persistent status before an adaptive retry
+ * (solver.ts:1878-1882, :1933-1937). */
+int mpm_clear_status(mpm_solver *solver);
+
+/* readParticles (solver.ts:2594-): packed 20-word records and object ids of
+ * the requested particles (all when indices == NULL).  Blocks. */
+int mpm_read_particles(mpm_solver *solver, const uint32_t *indices, uint32_t count, float *packed_out,
+                       uint32_t *object_ids_out);
+
+/* Overwrites the particle state from packed records (the upload of
+ * createRuntime, solver.ts:724-): count must equal the particle count. */
+int mpm_write_particles(mpm_solver *solver, const float *packed_particles, uint32_t count);
+
+/* Interaction drag (beginDrag/updateDrag/endDrag, solver.ts:2700-2790);
+ * drag == NULL ends the drag. */
+int mpm_set_drag(mpm_solver *solver, const mpm_drag *drag);
+
+/* measureQueueCompletionMs (solver.ts:106-144): milliseconds until the
+ * handle's queued work completes.  Blocks. */
+int mpm_queue_completion_ms(mpm_solver *solver, double *milliseconds);
+
+/* particleCount / particleCapacity (solver.ts:108-110). */
+uint32_t mpm_particle_count(const mpm_solver *solver);
+uint32_t mpm_particle_capacity(const mpm_solver *solver);
+
+/* dispose (solver.ts:143). */
+void mpm_destroy(mpm_solver *solver);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *mpm_last_error(void);
+
+/* ---- parity probes (no reference counterpart; used by the parity tests) ---- */
+
+/* Runs the cell sort of the next substep on the current state and returns,
+ * per particle, its base-cell key, the sorted permutation (slot -> particle)
+ * and cell starts (node_count + 1 words).  Does not advance the state. */
+int mpm_probe_sort(mpm_solver *solver, float dt, uint32_t *keys_out, uint32_t *perm_out,
+                   uint32_t *cell_start_out);
+
+/* Runs the fixed-point scatter of the next substep on the current state and
+ * returns the 11 integer words per halo node and each particle's prepared
+ * affine momentum (4 floats).  Does not advance the state. */
+int mpm_probe_fixed_point(mpm_solver *solver, float dt, int32_t *words_out, float *affine_out);
+
+/* Halo node count ((cells_x + 3) * (cells_y + 3)). */
+uint32_t mpm_node_count(const mpm_solver *solver);
+
+/* ---- measurement (no reference counterpart; the reference times batches
+ * with WebGPU timestamp queries, src/lib/mpm/experiments/si-performance.ts:131-196) ---- */
+
+/* Device time of the last mpm_step_batch, from CUDA events recorded on the
+ * handle's stream around it.  Blocks until that batch completes. */
+int mpm_last_batch_device_ms(mpm_solver *solver, double *milliseconds);
+
+/* Runs `step_count` real substeps without a graph, with an event after every
+ * kernel, and returns per kernel slot the summed milliseconds and launch
+ * counts (arrays of mpm_profile_kernel_slots() entries). */
+int mpm_profile_substeps(mpm_solver *solver, uint32_t step_count, float dt, float gravity_x, float gravity_y,
+                         const mpm_cfl_guard *guard, double *kernel_ms, uint32_t *kernel_launches);
+const char *mpm_profile_kernel_name(uint32_t slot);
+uint32_t mpm_profile_kernel_slots(void);
+
+/* Nodes of the last substep with positive solid / water / oil mass. */
+int mpm_count_active_nodes(mpm_solver *solver, uint32_t counts[3]);
+
+/* The handle's CUDA stream (cudaStream_t), for callers that order their own
+ * work after the solver's. */
+void *mpm_stream(mpm_solver *solver);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

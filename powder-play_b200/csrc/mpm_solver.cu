@@ -1,0 +1,856 @@
+// mpm_solver.cu -- host side of the C ABI (include/mpm_b200.h): device
+// allocation, packing between the reference's 20-word particle record and the
+// SoA device layout, CUDA-graph capture of substep batches, and the compact
+// status/speed readback.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/mpm_b200.h"
+#include "mpm_kernels.cuh"
+
+using namespace mpm;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int set_error(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                                   \
+    do {                                                                                                 \
+        cudaError_t err__ = (expr);                                                                      \
+        if (err__ != cudaSuccess)                                                                        \
+            return set_error(MPM_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(err__));          \
+    } while (0)
+
+template <typename T>
+cudaError_t dalloc(T **ptr, size_t count)
+{
+    *ptr = nullptr;
+    if (count == 0) count = 1;
+    return cudaMalloc(reinterpret_cast<void **>(ptr), count * sizeof(T));
+}
+
+uint32_t f2u(float v)
+{
+    uint32_t u;
+    std::memcpy(&u, &v, 4);
+    return u;
+}
+
+float u2f(uint32_t u)
+{
+    float v;
+    std::memcpy(&v, &u, 4);
+    return v;
+}
+
+}  // namespace
+
+struct mpm_solver {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    mpm_config cfg{};
+    uint32_t n = 0, capacity = 0;
+    uint32_t node_w = 0, node_h = 0, node_count = 0, tiles_x = 0, tiles_y = 0;
+    uint32_t cell_pad = 0, n_chunks = 0;
+    uint32_t n_bodies = 0, n_bonds = 0;
+    int cur = 0;  // buffer holding the current particle state
+
+    StepParams *d_params = nullptr;
+    StepParams *h_params = nullptr;  // pinned staging
+    cudaEvent_t params_copied = nullptr;
+    uint32_t *d_status = nullptr;
+    uint32_t *d_counters = nullptr;
+    uint32_t *h_readback = nullptr;  // pinned: 2 counters + 8 status words
+
+    ParticleBuffers buf[2]{};
+    float *vol = nullptr;
+    uint32_t *mat = nullptr, *bonded = nullptr, *obj = nullptr;
+    Material *d_mats = nullptr;
+    std::vector<Material> mats;
+
+    uint32_t *keys = nullptr, *ranks = nullptr, *tmp = nullptr, *perm = nullptr;
+    uint32_t *cell_count = nullptr, *cell_start = nullptr, *block_sums = nullptr;
+    float4 *rec0 = nullptr, *rec1 = nullptr;
+    float2 *rec2 = nullptr;
+    float4 *p2g_solid = nullptr, *p2g_water = nullptr, *p2g_oil = nullptr;
+    float2 *g_solid = nullptr;
+    float4 *g_water = nullptr, *g_oil = nullptr;
+    int32_t *fixed = nullptr;
+    uint32_t *tile_stamp = nullptr;
+
+    mpm_drag drag{};
+    bool drag_active = false;
+
+    cudaEvent_t batch_start = nullptr, batch_stop = nullptr;
+    bool batch_timed = false;
+    uint32_t *d_active = nullptr;
+
+    // graphs of 2^k substeps starting from buffer parity p
+    std::map<std::tuple<int, int>, cudaGraphExec_t> graphs;
+};
+
+namespace {
+
+Ctx make_ctx(mpm_solver *s, int parity)
+{
+    Ctx c{};
+    c.P = s->d_params;
+    c.in = s->buf[parity];
+    c.out = s->buf[1 - parity];
+    c.vol = s->vol;
+    c.mat = s->mat;
+    c.mats = s->d_mats;
+    c.bonded = s->bonded;
+    c.obj = s->obj;
+    c.status = s->d_status;
+    c.counters = s->d_counters;
+    c.keys = s->keys;
+    c.ranks = s->ranks;
+    c.tmp = s->tmp;
+    c.perm = s->perm;
+    c.cell_count = s->cell_count;
+    c.cell_start = s->cell_start;
+    c.block_sums = s->block_sums;
+    c.cell_pad = s->cell_pad;
+    c.rec0 = s->rec0;
+    c.rec1 = s->rec1;
+    c.rec2 = s->rec2;
+    c.p2g_solid = s->p2g_solid;
+    c.p2g_water = s->p2g_water;
+    c.p2g_oil = s->p2g_oil;
+    c.g_solid = s->g_solid;
+    c.g_water = s->g_water;
+    c.g_oil = s->g_oil;
+    c.fixed = s->fixed;
+    c.tile_stamp = s->tile_stamp;
+    c.affine_out = nullptr;
+    return c;
+}
+
+inline unsigned blocks_for(uint32_t n, unsigned threads) { return std::max(1u, (n + threads - 1) / threads); }
+
+constexpr unsigned PARTICLE_THREADS = 256;
+
+// Kernel slots of the profiled substep (mpm_profile_substeps).
+enum KernelSlot {
+    K_COUNT, K_SCAN_REDUCE, K_SCAN_TOP, K_SCAN_APPLY, K_SCATTER, K_RANK_PREPARE, K_P2G_GATHER,
+    K_PREPARE_SCATTER, K_FIXED_DECODE, K_GRID_UPDATE, K_G2P, K_COMMIT, K_SPEED_MAX, K_SLOTS
+};
+const char *const KERNEL_NAMES[K_SLOTS] = {
+    "k_count", "k_scan_reduce", "k_scan_top", "k_scan_apply", "k_scatter", "k_rank_prepare", "k_p2g_gather",
+    "k_prepare_scatter", "k_fixed_decode", "k_grid_update", "k_g2p", "k_commit", "k_speed_max"};
+
+// When set, an event is recorded after every kernel launch so that the
+// kernels of a substep can be timed one by one (never during graph capture).
+struct Recorder {
+    cudaStream_t stream;
+    std::vector<cudaEvent_t> events;
+    std::vector<int> slots;
+    void mark(int slot)
+    {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, stream);
+        events.push_back(e);
+        slots.push_back(slot);
+    }
+};
+thread_local Recorder *g_recorder = nullptr;
+
+inline void mark(int slot)
+{
+    if (g_recorder) g_recorder->mark(slot);
+}
+
+// Enqueues the cell sort (count -> scan -> scatter -> stable rank + prepare).
+void enqueue_sort(mpm_solver *s, const Ctx &c)
+{
+    const unsigned pb = blocks_for(s->n, PARTICLE_THREADS);
+    k_count<<<pb, PARTICLE_THREADS, 0, s->stream>>>(c);
+    mark(K_COUNT);
+    k_scan_reduce<<<s->n_chunks, SCAN_THREADS, 0, s->stream>>>(c, s->n_chunks);
+    mark(K_SCAN_REDUCE);
+    k_scan_top<<<1, SCAN_TOP_THREADS, 0, s->stream>>>(c, s->n_chunks);
+    mark(K_SCAN_TOP);
+    k_scan_apply<<<s->n_chunks, SCAN_THREADS, 0, s->stream>>>(c, s->n_chunks);
+    mark(K_SCAN_APPLY);
+    k_scatter<<<pb, PARTICLE_THREADS, 0, s->stream>>>(c);
+    mark(K_SCATTER);
+    k_rank_prepare<<<pb, PARTICLE_THREADS, 0, s->stream>>>(c);
+    mark(K_RANK_PREPARE);
+}
+
+// One full substep from buffer `parity` into 1 - parity.
+void enqueue_substep(mpm_solver *s, int parity)
+{
+    const Ctx c = make_ctx(s, parity);
+    const unsigned pb = blocks_for(s->n, PARTICLE_THREADS);
+    const dim3 tiles(s->tiles_x, s->tiles_y);
+    if (s->cfg.p2g_mode == MPM_P2G_FIXED_POINT) {
+        k_prepare_scatter<<<pb, PARTICLE_THREADS, 0, s->stream>>>(c);
+        mark(K_PREPARE_SCATTER);
+        k_fixed_decode<<<tiles, TILE_NODES, 0, s->stream>>>(c);
+        mark(K_FIXED_DECODE);
+    } else {
+        enqueue_sort(s, c);
+        k_p2g_gather<<<tiles, TILE_NODES, 0, s->stream>>>(c);
+        mark(K_P2G_GATHER);
+    }
+    k_grid_update<<<tiles, TILE_NODES, 0, s->stream>>>(c);
+    mark(K_GRID_UPDATE);
+    k_g2p<<<pb, PARTICLE_THREADS, 0, s->stream>>>(c);
+    mark(K_G2P);
+    const unsigned cb = std::min(blocks_for(s->n, PARTICLE_THREADS), 592u);
+    k_commit<<<cb, PARTICLE_THREADS, 0, s->stream>>>(c);
+    mark(K_COMMIT);
+}
+
+int get_graph(mpm_solver *s, int log2_steps, int parity, cudaGraphExec_t *out)
+{
+    auto key = std::make_tuple(log2_steps, parity);
+    auto it = s->graphs.find(key);
+    if (it != s->graphs.end()) {
+        *out = it->second;
+        return MPM_OK;
+    }
+    cudaGraph_t graph = nullptr;
+    CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    int p = parity;
+    for (int k = 0; k < (1 << log2_steps); ++k) {
+        enqueue_substep(s, p);
+        p = 1 - p;
+    }
+    cudaError_t err = cudaStreamEndCapture(s->stream, &graph);
+    if (err != cudaSuccess) return set_error(MPM_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(err));
+    cudaGraphExec_t exec = nullptr;
+    err = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (err != cudaSuccess) return set_error(MPM_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(err));
+    s->graphs[key] = exec;
+    *out = exec;
+    return MPM_OK;
+}
+
+void fill_params(mpm_solver *s, StepParams &p, float dt, float gx, float gy, const mpm_cfl_guard *guard,
+                 float bond_reference_dt)
+{
+    std::memset(&p, 0, sizeof p);
+    const mpm_config &c = s->cfg;
+    p.cells_x = c.cells_x;
+    p.cells_y = c.cells_y;
+    p.node_w = s->node_w;
+    p.node_h = s->node_h;
+    p.n_particles = s->n;
+    p.n_nodes = s->node_count;
+    p.tiles_x = s->tiles_x;
+    p.tiles_y = s->tiles_y;
+    p.n_bodies = s->n_bodies;
+    p.cfl_enabled = guard ? 1u : 0u;
+    p.n_bonds = s->n_bonds;
+    p.fixed_shift = c.fixed_point_shift;
+    p.dx = c.cell_size;
+    p.particle_mass = c.particle_mass;
+    p.particle_volume = c.particle_volume;
+    p.dt = dt;
+    p.lambda = c.lambda;
+    p.mu = c.mu;
+    // stress scale and gradient scale as float32 (layout.ts:944-948, :235)
+    const double cs = (double)c.cell_size;
+    p.gradient_scale = (float)(4.0 / (cs * cs));
+    p.stress_scale = (float)(-(double)dt * (double)c.particle_volume * (4.0 / (cs * cs)));
+    p.gx = gx;
+    p.gy = gy;
+    p.domain_w = (float)((double)c.cells_x * (double)c.cell_size);
+    p.domain_h = (float)((double)c.cells_y * (double)c.cell_size);
+    p.bond_rest_length = c.bond_rest_length;
+    p.bond_stiffness = c.bond_stiffness;
+    p.band = c.cell_size * 2.0f;
+    p.contact_reach = (float)(std::sqrt((double)c.particle_volume / M_PI) + (double)c.cell_size * 0.75);
+    p.cfl_wave_bound = guard ? guard->wave_speed_bound : 0.0f;
+    p.cfl_velocity_limit = guard ? guard->velocity_limit : 0.0f;
+    p.bond_reference_dt = bond_reference_dt > 0.0f ? bond_reference_dt
+                                                   : (c.bond_reference_dt > 0.0f ? c.bond_reference_dt : dt);
+    p.wall_friction = c.wall_friction;
+    p.fixed_scale = std::ldexp(1.0f, (int)c.fixed_point_shift);
+    if (s->drag_active) {
+        p.drag_x = s->drag.target_x;
+        p.drag_y = s->drag.target_y;
+        p.drag_radius = s->drag.radius;
+        p.drag_stiffness = s->drag.stiffness;
+        p.drag_damping = s->drag.damping;
+    }
+}
+
+int upload_params(mpm_solver *s, float dt, float gx, float gy, const mpm_cfl_guard *guard, float bond_reference_dt)
+{
+    CUDA_TRY(cudaEventSynchronize(s->params_copied));
+    fill_params(s, *s->h_params, dt, gx, gy, guard, bond_reference_dt);
+    CUDA_TRY(cudaMemcpyAsync(s->d_params, s->h_params, sizeof(StepParams), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaEventRecord(s->params_copied, s->stream));
+    return MPM_OK;
+}
+
+// material table key: model + lambda + mu + density + parameter (the
+// parameter of a Neo-Hookean particle is its damage, kept per particle)
+uint32_t intern_material(std::vector<Material> &table, const float *w)
+{
+    Material m{};
+    m.model = f2u(w[13]);
+    m.lambda = w[14];
+    m.mu = w[15];
+    m.density = w[16];
+    m.param = m.model == MODEL_NEO_HOOKEAN ? 0.0f : w[18];
+    for (size_t k = 0; k < table.size(); ++k) {
+        const Material &t = table[k];
+        if (t.model == m.model && f2u(t.lambda) == f2u(m.lambda) && f2u(t.mu) == f2u(m.mu) &&
+            f2u(t.density) == f2u(m.density) && f2u(t.param) == f2u(m.param))
+            return (uint32_t)k;
+    }
+    table.push_back(m);
+    return (uint32_t)(table.size() - 1);
+}
+
+int unpack_and_upload(mpm_solver *s, const float *packed, uint32_t count, int target)
+{
+    std::vector<float2> pos(count), vel(count);
+    std::vector<float4> C(count), F(count);
+    std::vector<float> pvol(count), damage(count), vol(count);
+    std::vector<uint32_t> mat(count), bonded(count);
+    const size_t before = s->mats.size();
+    for (uint32_t i = 0; i < count; ++i) {
+        const float *w = packed + (size_t)i * MPM_PARTICLE_WORDS;
+        const uint32_t model = f2u(w[13]);
+        if (model > MODEL_FIXED_COROTATED)
+            return set_error(MPM_ERR_INVALID_ARGUMENT, "particle %u has an unsupported MPM material model %u", i, model);
+        pos[i] = make_float2(w[0], w[1]);
+        vel[i] = make_float2(w[2], w[3]);
+        C[i] = make_float4(w[4], w[5], w[6], w[7]);
+        F[i] = make_float4(w[8], w[9], w[10], w[11]);
+        pvol[i] = w[12];
+        damage[i] = model == MODEL_NEO_HOOKEAN ? w[18] : 0.0f;
+        vol[i] = w[17];
+        mat[i] = intern_material(s->mats, w);
+        bonded[i] = f2u(w[19]);
+        if (bonded[i] > 3u) return set_error(MPM_ERR_INVALID_ARGUMENT, "particle %u has an invalid bonded triangle marker", i);
+    }
+    if (s->mats.size() > 65536) return set_error(MPM_ERR_INVALID_ARGUMENT, "more than 65536 distinct materials");
+    if (s->mats.size() != before || s->d_mats == nullptr) {
+        if (s->d_mats) cudaFree(s->d_mats);
+        s->d_mats = nullptr;
+        CUDA_TRY(dalloc(&s->d_mats, s->mats.size()));
+        CUDA_TRY(cudaMemcpyAsync(s->d_mats, s->mats.data(), s->mats.size() * sizeof(Material), cudaMemcpyHostToDevice,
+                                 s->stream));
+    }
+    ParticleBuffers &b = s->buf[target];
+    CUDA_TRY(cudaMemcpyAsync(b.pos, pos.data(), count * sizeof(float2), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(b.vel, vel.data(), count * sizeof(float2), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(b.C, C.data(), count * sizeof(float4), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(b.F, F.data(), count * sizeof(float4), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(b.pvol, pvol.data(), count * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(b.damage, damage.data(), count * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->vol, vol.data(), count * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->mat, mat.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->bonded, bonded.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+    // the copies above read pageable host vectors; wait before they go away
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return MPM_OK;
+}
+
+void free_solver(mpm_solver *s)
+{
+    if (!s) return;
+    if (s->device >= 0) cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    s->graphs.clear();
+    void *ptrs[] = {s->d_params, s->d_status, s->d_counters, s->vol, s->mat, s->bonded, s->obj, s->d_mats, s->keys,
+                    s->ranks, s->tmp, s->perm, s->cell_count, s->cell_start, s->block_sums, s->rec0, s->rec1, s->rec2,
+                    s->p2g_solid, s->p2g_water, s->p2g_oil, s->g_solid, s->g_water, s->g_oil, s->fixed, s->tile_stamp,
+                    s->d_active};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    for (int b = 0; b < 2; ++b) {
+        void *bp[] = {s->buf[b].pos, s->buf[b].vel, s->buf[b].C, s->buf[b].F, s->buf[b].pvol, s->buf[b].damage};
+        for (void *p : bp)
+            if (p) cudaFree(p);
+    }
+    if (s->h_params) cudaFreeHost(s->h_params);
+    if (s->h_readback) cudaFreeHost(s->h_readback);
+    if (s->params_copied) cudaEventDestroy(s->params_copied);
+    if (s->batch_start) cudaEventDestroy(s->batch_start);
+    if (s->batch_stop) cudaEventDestroy(s->batch_stop);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+int create_impl(const mpm_config *config, const float *packed, const uint32_t *object_ids, uint32_t count,
+                const uint32_t *body_starts, uint32_t body_count, mpm_solver **out)
+{
+    if (!config || !out) return set_error(MPM_ERR_INVALID_ARGUMENT, "config and out must not be NULL");
+    *out = nullptr;
+    if (count > 0 && (!packed || !object_ids))
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "packed_particles and object_ids must not be NULL");
+    const mpm_config &c = *config;
+    if (c.cells_x < 1 || c.cells_y < 1 || (uint64_t)c.cells_x + 3 > 0xffffffffull || (uint64_t)c.cells_y + 3 > 0xffffffffull)
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "grid.cellsX must be a positive safe integer that fits the GPU layout");
+    if (!(c.cell_size > 0.0f) || !std::isfinite(c.cell_size))
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "grid.cellSize must be greater than zero");
+    if (!(c.particle_mass > 0.0f) || !(c.particle_volume > 0.0f))
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "particleMass and particleVolume must be greater than zero");
+    if (c.capacity < count) return set_error(MPM_ERR_INVALID_ARGUMENT, "capacity must be at least the initial particle count and fit the GPU layout");
+    if (c.p2g_mode > MPM_P2G_FIXED_POINT) return set_error(MPM_ERR_INVALID_ARGUMENT, "unknown p2g_mode %u", c.p2g_mode);
+    if (c.fixed_point_shift > 30) return set_error(MPM_ERR_INVALID_ARGUMENT, "fixed_point_shift must be at most 30");
+    const uint64_t nodes = ((uint64_t)c.cells_x + 3) * ((uint64_t)c.cells_y + 3);
+    if (nodes > 0x7fffffffull / FIXED_WORDS)
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "halo grid dimensions exceed the GPU index range");
+    if ((uint64_t)c.capacity * 9ull > 0x7fffffffull)
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "particle stencil entries exceed the index range");
+    if (body_count > 0 && !body_starts) return set_error(MPM_ERR_INVALID_ARGUMENT, "body_starts must not be NULL");
+
+    int device_count = 0;
+    CUDA_TRY(cudaGetDeviceCount(&device_count));
+    if (c.device < 0 || c.device >= device_count)
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "device %d is not available (%d devices)", c.device, device_count);
+    CUDA_TRY(cudaSetDevice(c.device));
+
+    mpm_solver *s = new mpm_solver();
+    s->device = c.device;
+    s->cfg = c;
+    s->n = count;
+    s->capacity = std::max<uint32_t>(c.capacity, 1u);
+    s->n_bodies = body_count;
+    s->node_w = c.cells_x + 3;
+    s->node_h = c.cells_y + 3;
+    s->node_count = (uint32_t)nodes;
+    s->tiles_x = (s->node_w + TILE_X - 1) / TILE_X;
+    s->tiles_y = (s->node_h + TILE_Y - 1) / TILE_Y;
+    s->cell_pad = ((s->node_count + SCAN_CHUNK - 1) / SCAN_CHUNK) * SCAN_CHUNK;
+    s->n_chunks = s->cell_pad / SCAN_CHUNK;
+
+    auto fail = [&](int code) {
+        free_solver(s);
+        return code;
+    };
+#define ALLOC(ptr, n)                                                                                          \
+    do {                                                                                                       \
+        cudaError_t e__ = dalloc(&(ptr), (n));                                                                 \
+        if (e__ != cudaSuccess) return fail(set_error(MPM_ERR_CUDA, "cudaMalloc(%s) failed: %s", #ptr, cudaGetErrorString(e__))); \
+    } while (0)
+
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(set_error(MPM_ERR_CUDA, "cudaStreamCreate failed"));
+    if (cudaEventCreateWithFlags(&s->params_copied, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreate(&s->batch_start) != cudaSuccess || cudaEventCreate(&s->batch_stop) != cudaSuccess)
+        return fail(set_error(MPM_ERR_CUDA, "cudaEventCreate failed"));
+    if (cudaMallocHost(reinterpret_cast<void **>(&s->h_params), sizeof(StepParams)) != cudaSuccess ||
+        cudaMallocHost(reinterpret_cast<void **>(&s->h_readback), 16 * sizeof(uint32_t)) != cudaSuccess)
+        return fail(set_error(MPM_ERR_CUDA, "cudaMallocHost failed"));
+    cudaEventRecord(s->params_copied, s->stream);
+
+    const size_t cap = s->capacity;
+    ALLOC(s->d_params, 1);
+    ALLOC(s->d_status, 32);
+    ALLOC(s->d_counters, 32);
+    for (int b = 0; b < 2; ++b) {
+        ALLOC(s->buf[b].pos, cap);
+        ALLOC(s->buf[b].vel, cap);
+        ALLOC(s->buf[b].C, cap);
+        ALLOC(s->buf[b].F, cap);
+        ALLOC(s->buf[b].pvol, cap);
+        ALLOC(s->buf[b].damage, cap);
+    }
+    ALLOC(s->vol, cap);
+    ALLOC(s->mat, cap);
+    ALLOC(s->bonded, cap);
+    ALLOC(s->obj, cap);
+    ALLOC(s->keys, cap);
+    ALLOC(s->ranks, cap);
+    ALLOC(s->tmp, cap);
+    ALLOC(s->perm, cap);
+    ALLOC(s->rec0, cap);
+    ALLOC(s->rec1, cap);
+    ALLOC(s->rec2, cap);
+    ALLOC(s->cell_count, s->cell_pad);
+    ALLOC(s->cell_start, (size_t)s->cell_pad + 1);
+    ALLOC(s->block_sums, (size_t)s->n_chunks + 1);
+    ALLOC(s->p2g_solid, s->node_count);
+    ALLOC(s->p2g_water, s->node_count);
+    ALLOC(s->p2g_oil, s->node_count);
+    ALLOC(s->g_solid, s->node_count);
+    ALLOC(s->g_water, s->node_count);
+    ALLOC(s->g_oil, s->node_count);
+    ALLOC(s->tile_stamp, (size_t)s->tiles_x * s->tiles_y);
+    ALLOC(s->d_active, 4);
+    if (c.p2g_mode == MPM_P2G_FIXED_POINT) {
+        ALLOC(s->fixed, (size_t)s->node_count * FIXED_WORDS);
+        if (cudaMemsetAsync(s->fixed, 0, (size_t)s->node_count * FIXED_WORDS * sizeof(int32_t), s->stream) != cudaSuccess)
+            return fail(set_error(MPM_ERR_CUDA, "cudaMemset failed"));
+    }
+#undef ALLOC
+    cudaMemsetAsync(s->cell_count, 0, (size_t)s->cell_pad * sizeof(uint32_t), s->stream);
+    cudaMemsetAsync(s->tile_stamp, 0, (size_t)s->tiles_x * s->tiles_y * sizeof(uint32_t), s->stream);
+    cudaMemsetAsync(s->d_counters, 0, 32 * sizeof(uint32_t), s->stream);
+    const uint32_t init_status[32] = {0, 0xffffffffu};
+    cudaMemcpyAsync(s->d_status, init_status, sizeof init_status, cudaMemcpyHostToDevice, s->stream);
+    const uint32_t one = 1;  // tile stamps start at 0, so the first substep stamp is 1
+    cudaMemcpyAsync(s->d_counters + COUNTER_STAMP, &one, sizeof one, cudaMemcpyHostToDevice, s->stream);
+    if (count > 0) {
+        int rc = unpack_and_upload(s, packed, count, 0);
+        if (rc != MPM_OK) return fail(rc);
+        if (cudaMemcpyAsync(s->obj, object_ids, count * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream) !=
+            cudaSuccess)
+            return fail(set_error(MPM_ERR_CUDA, "object id upload failed"));
+    } else {
+        Material dummy{};
+        s->mats.push_back(dummy);
+        if (dalloc(&s->d_mats, 1) != cudaSuccess) return fail(set_error(MPM_ERR_CUDA, "cudaMalloc failed"));
+        cudaMemcpyAsync(s->d_mats, &dummy, sizeof dummy, cudaMemcpyHostToDevice, s->stream);
+    }
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return fail(set_error(MPM_ERR_CUDA, "initial upload failed: %s", cudaGetErrorString(e)));
+    *out = s;
+    return MPM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mpm_create(const mpm_config *config, const float *packed_particles, const uint32_t *object_ids,
+               uint32_t particle_count, const uint32_t *body_starts, uint32_t body_count,
+               const uint32_t *fracture_bonds, uint32_t fracture_bond_count, const uint32_t *fracture_topology,
+               uint32_t fracture_topology_words, mpm_solver **out)
+{
+    g_last_error.clear();
+    if (body_count > 0 || fracture_bond_count > 0)
+        return set_error(MPM_ERR_INVALID_ARGUMENT,
+                         "bonded triangle bodies and fracture bonds are not supported by this build yet");
+    (void)fracture_bonds;
+    (void)fracture_topology;
+    (void)fracture_topology_words;
+    return create_impl(config, packed_particles, object_ids, particle_count, body_starts, body_count, out);
+}
+
+int mpm_step_batch(mpm_solver *s, uint32_t step_count, float dt, float gx, float gy, const mpm_cfl_guard *guard,
+                   float bond_reference_dt)
+{
+    g_last_error.clear();
+    if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
+    if (step_count < 1) return set_error(MPM_ERR_INVALID_ARGUMENT, "stepCount must be a positive safe integer.");
+    if (!(dt > 0.0f) || !std::isfinite(dt)) return set_error(MPM_ERR_INVALID_ARGUMENT, "dt must be greater than zero");
+    if (!std::isfinite(gx) || !std::isfinite(gy)) return set_error(MPM_ERR_INVALID_ARGUMENT, "gravity must be finite");
+    CUDA_TRY(cudaSetDevice(s->device));
+    int rc = upload_params(s, dt, gx, gy, guard, bond_reference_dt);
+    if (rc != MPM_OK) return rc;
+    const Ctx c0 = make_ctx(s, s->cur);
+    CUDA_TRY(cudaEventRecord(s->batch_start, s->stream));
+    k_begin_batch<<<1, 32, 0, s->stream>>>(c0, guard ? 1u : 0u);
+    CUDA_TRY(cudaGetLastError());
+    if (s->n > 0) {
+        uint32_t remaining = step_count;
+        for (int k = 30; k >= 0; --k) {
+            if (!(remaining & (1u << k))) continue;
+            cudaGraphExec_t exec;
+            rc = get_graph(s, k, s->cur, &exec);
+            if (rc != MPM_OK) return rc;
+            CUDA_TRY(cudaGraphLaunch(exec, s->stream));
+            if (k == 0) s->cur = 1 - s->cur;  // only an odd substep count flips the buffer
+        }
+    }
+    if (guard) {
+        const Ctx c1 = make_ctx(s, s->cur);
+        const unsigned blocks = std::min(blocks_for(s->n, PARTICLE_THREADS), 592u);
+        k_speed_max<<<blocks, PARTICLE_THREADS, 0, s->stream>>>(c1);
+        CUDA_TRY(cudaGetLastError());
+    }
+    CUDA_TRY(cudaEventRecord(s->batch_stop, s->stream));
+    s->batch_timed = true;
+    return MPM_OK;
+}
+
+int mpm_last_batch_device_ms(mpm_solver *s, double *milliseconds)
+{
+    g_last_error.clear();
+    if (!s || !milliseconds) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and milliseconds must not be NULL");
+    if (!s->batch_timed) return set_error(MPM_ERR_STATE, "no batch has been submitted");
+    CUDA_TRY(cudaSetDevice(s->device));
+    CUDA_TRY(cudaEventSynchronize(s->batch_stop));
+    float ms = 0.0f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, s->batch_start, s->batch_stop));
+    *milliseconds = ms;
+    return MPM_OK;
+}
+
+int mpm_profile_substeps(mpm_solver *s, uint32_t step_count, float dt, float gx, float gy,
+                         const mpm_cfl_guard *guard, double *kernel_ms, uint32_t *kernel_launches)
+{
+    g_last_error.clear();
+    if (!s || !kernel_ms || !kernel_launches)
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and outputs must not be NULL");
+    if (step_count < 1) return set_error(MPM_ERR_INVALID_ARGUMENT, "stepCount must be a positive safe integer.");
+    CUDA_TRY(cudaSetDevice(s->device));
+    int rc = upload_params(s, dt, gx, gy, guard, 0.0f);
+    if (rc != MPM_OK) return rc;
+    for (int k = 0; k < K_SLOTS; ++k) {
+        kernel_ms[k] = 0.0;
+        kernel_launches[k] = 0;
+    }
+    Recorder rec;
+    rec.stream = s->stream;
+    const Ctx c0 = make_ctx(s, s->cur);
+    k_begin_batch<<<1, 32, 0, s->stream>>>(c0, guard ? 1u : 0u);
+    rec.mark(-1);
+    g_recorder = &rec;
+    for (uint32_t k = 0; k < step_count; ++k) {
+        enqueue_substep(s, s->cur);
+        s->cur = 1 - s->cur;
+    }
+    if (guard) {
+        const Ctx c1 = make_ctx(s, s->cur);
+        k_speed_max<<<std::min(blocks_for(s->n, PARTICLE_THREADS), 592u), PARTICLE_THREADS, 0, s->stream>>>(c1);
+        mark(K_SPEED_MAX);
+    }
+    g_recorder = nullptr;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    for (size_t k = 1; e == cudaSuccess && k < rec.events.size(); ++k) {
+        float ms = 0.0f;
+        e = cudaEventElapsedTime(&ms, rec.events[k - 1], rec.events[k]);
+        if (rec.slots[k] >= 0) {
+            kernel_ms[rec.slots[k]] += ms;
+            kernel_launches[rec.slots[k]] += 1;
+        }
+    }
+    for (cudaEvent_t ev : rec.events) cudaEventDestroy(ev);
+    if (e != cudaSuccess) return set_error(MPM_ERR_CUDA, "profiled substeps failed: %s", cudaGetErrorString(e));
+    return MPM_OK;
+}
+
+const char *mpm_profile_kernel_name(uint32_t slot) { return slot < K_SLOTS ? KERNEL_NAMES[slot] : ""; }
+
+uint32_t mpm_profile_kernel_slots(void) { return K_SLOTS; }
+
+int mpm_count_active_nodes(mpm_solver *s, uint32_t counts[3])
+{
+    g_last_error.clear();
+    if (!s || !counts) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and counts must not be NULL");
+    CUDA_TRY(cudaSetDevice(s->device));
+    CUDA_TRY(cudaMemsetAsync(s->d_active, 0, 4 * sizeof(uint32_t), s->stream));
+    const Ctx c = make_ctx(s, s->cur);
+    k_count_active_nodes<<<dim3(s->tiles_x, s->tiles_y), TILE_NODES, 0, s->stream>>>(c, s->d_active);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(s->h_readback, s->d_active, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    std::memcpy(counts, s->h_readback, 3 * sizeof(uint32_t));
+    return MPM_OK;
+}
+
+void *mpm_stream(mpm_solver *s) { return s ? (void *)s->stream : nullptr; }
+
+int mpm_read_compact(mpm_solver *s, float *maximum_speed, uint32_t *completed, uint32_t status[8])
+{
+    g_last_error.clear();
+    if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
+    CUDA_TRY(cudaSetDevice(s->device));
+    CUDA_TRY(cudaMemcpyAsync(s->h_readback, s->d_counters + COUNTER_PROGRESS, 2 * sizeof(uint32_t),
+                             cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->h_readback + 2, s->d_status, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (completed) *completed = s->h_readback[0];
+    if (maximum_speed) *maximum_speed = u2f(s->h_readback[1]);
+    if (status) std::memcpy(status, s->h_readback + 2, 8 * sizeof(uint32_t));
+    return MPM_OK;
+}
+
+int mpm_read_status(mpm_solver *s, uint32_t status[8])
+{
+    return mpm_read_compact(s, nullptr, nullptr, status);
+}
+
+int mpm_clear_status(mpm_solver *s)
+{
+    g_last_error.clear();
+    if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
+    CUDA_TRY(cudaSetDevice(s->device));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    const uint32_t init_status[8] = {0, 0xffffffffu, 0, 0, 0, 0, 0, 0};
+    CUDA_TRY(cudaMemcpy(s->d_status, init_status, sizeof init_status, cudaMemcpyHostToDevice));
+    return MPM_OK;
+}
+
+int mpm_read_particles(mpm_solver *s, const uint32_t *indices, uint32_t count, float *packed_out,
+                       uint32_t *object_ids_out)
+{
+    g_last_error.clear();
+    if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
+    if (!packed_out) return set_error(MPM_ERR_INVALID_ARGUMENT, "packed_out must not be NULL");
+    if (!indices && count != s->n) return set_error(MPM_ERR_INVALID_ARGUMENT, "count must equal the particle count");
+    for (uint32_t k = 0; indices && k < count; ++k)
+        if (indices[k] >= s->n) return set_error(MPM_ERR_INVALID_ARGUMENT, "particleIndices must identify active GPU particles.");
+    CUDA_TRY(cudaSetDevice(s->device));
+    const uint32_t n = s->n;
+    std::vector<float2> pos(n), vel(n);
+    std::vector<float4> C(n), F(n);
+    std::vector<float> pvol(n), damage(n), vol(n);
+    std::vector<uint32_t> mat(n), bonded(n), obj(n);
+    const ParticleBuffers &b = s->buf[s->cur];
+    if (n > 0) {
+        CUDA_TRY(cudaMemcpyAsync(pos.data(), b.pos, n * sizeof(float2), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(vel.data(), b.vel, n * sizeof(float2), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(C.data(), b.C, n * sizeof(float4), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(F.data(), b.F, n * sizeof(float4), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(pvol.data(), b.pvol, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(damage.data(), b.damage, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(vol.data(), s->vol, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(mat.data(), s->mat, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(bonded.data(), s->bonded, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(obj.data(), s->obj, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    for (uint32_t k = 0; k < count; ++k) {
+        const uint32_t i = indices ? indices[k] : k;
+        float *w = packed_out + (size_t)k * MPM_PARTICLE_WORDS;
+        const Material &m = s->mats[mat[i]];
+        w[0] = pos[i].x;
+        w[1] = pos[i].y;
+        w[2] = vel[i].x;
+        w[3] = vel[i].y;
+        w[4] = C[i].x;
+        w[5] = C[i].y;
+        w[6] = C[i].z;
+        w[7] = C[i].w;
+        w[8] = F[i].x;
+        w[9] = F[i].y;
+        w[10] = F[i].z;
+        w[11] = F[i].w;
+        w[12] = pvol[i];
+        w[13] = u2f(m.model);
+        w[14] = m.lambda;
+        w[15] = m.mu;
+        w[16] = m.density;
+        w[17] = vol[i];
+        w[18] = m.model == MODEL_NEO_HOOKEAN ? damage[i] : m.param;
+        w[19] = u2f(bonded[i]);
+        if (object_ids_out) object_ids_out[k] = obj[i];
+    }
+    return MPM_OK;
+}
+
+int mpm_write_particles(mpm_solver *s, const float *packed, uint32_t count)
+{
+    g_last_error.clear();
+    if (!s || !packed) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and packed_particles must not be NULL");
+    if (count != s->n) return set_error(MPM_ERR_INVALID_ARGUMENT, "count must equal the particle count");
+    CUDA_TRY(cudaSetDevice(s->device));
+    return unpack_and_upload(s, packed, count, s->cur);
+}
+
+int mpm_set_drag(mpm_solver *s, const mpm_drag *drag)
+{
+    g_last_error.clear();
+    if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
+    if (drag) {
+        if (!(drag->radius > 0.0f) || !std::isfinite(drag->radius))
+            return set_error(MPM_ERR_INVALID_ARGUMENT, "drag radius must be greater than zero.");
+        s->drag = *drag;
+        s->drag_active = true;
+    } else {
+        s->drag_active = false;
+    }
+    return MPM_OK;
+}
+
+int mpm_queue_completion_ms(mpm_solver *s, double *ms)
+{
+    g_last_error.clear();
+    if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
+    CUDA_TRY(cudaSetDevice(s->device));
+    cudaEvent_t a, b;
+    CUDA_TRY(cudaEventCreate(&a));
+    CUDA_TRY(cudaEventCreate(&b));
+    cudaEventRecord(a, s->stream);
+    cudaEventRecord(b, s->stream);
+    cudaEventSynchronize(b);
+    float elapsed = 0.0f;
+    cudaEventElapsedTime(&elapsed, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (ms) *ms = elapsed;
+    return MPM_OK;
+}
+
+uint32_t mpm_particle_count(const mpm_solver *s) { return s ? s->n : 0u; }
+uint32_t mpm_particle_capacity(const mpm_solver *s) { return s ? s->capacity : 0u; }
+uint32_t mpm_node_count(const mpm_solver *s) { return s ? s->node_count : 0u; }
+
+void mpm_destroy(mpm_solver *s) { free_solver(s); }
+
+const char *mpm_last_error(void) { return g_last_error.c_str(); }
+
+int mpm_probe_sort(mpm_solver *s, float dt, uint32_t *keys_out, uint32_t *perm_out, uint32_t *cell_start_out)
+{
+    g_last_error.clear();
+    if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
+    if (s->cfg.p2g_mode != MPM_P2G_GATHER) return set_error(MPM_ERR_STATE, "the cell sort runs in gather mode only");
+    CUDA_TRY(cudaSetDevice(s->device));
+    int rc = upload_params(s, dt, 0.0f, 0.0f, nullptr, 0.0f);
+    if (rc != MPM_OK) return rc;
+    const Ctx c = make_ctx(s, s->cur);
+    enqueue_sort(s, c);
+    CUDA_TRY(cudaGetLastError());
+    if (keys_out) CUDA_TRY(cudaMemcpyAsync(keys_out, s->keys, s->n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    if (perm_out) CUDA_TRY(cudaMemcpyAsync(perm_out, s->perm, s->n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    if (cell_start_out)
+        CUDA_TRY(cudaMemcpyAsync(cell_start_out, s->cell_start, ((size_t)s->node_count + 1) * sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return MPM_OK;
+}
+
+int mpm_probe_fixed_point(mpm_solver *s, float dt, int32_t *words_out, float *affine_out)
+{
+    g_last_error.clear();
+    if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
+    if (s->cfg.p2g_mode != MPM_P2G_FIXED_POINT) return set_error(MPM_ERR_STATE, "the solver was not created in fixed-point mode");
+    CUDA_TRY(cudaSetDevice(s->device));
+    int rc = upload_params(s, dt, 0.0f, 0.0f, nullptr, 0.0f);
+    if (rc != MPM_OK) return rc;
+    float4 *aff = nullptr;
+    CUDA_TRY(dalloc(&aff, s->n));
+    Ctx c = make_ctx(s, s->cur);
+    c.affine_out = aff;
+    k_prepare_scatter<<<blocks_for(s->n, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c);
+    cudaError_t e = cudaGetLastError();
+    const size_t words = (size_t)s->node_count * FIXED_WORDS;
+    if (e == cudaSuccess && words_out)
+        e = cudaMemcpyAsync(words_out, s->fixed, words * sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess && affine_out)
+        e = cudaMemcpyAsync(affine_out, aff, (size_t)s->n * sizeof(float4), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->fixed, 0, words * sizeof(int32_t), s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    cudaFree(aff);
+    if (e != cudaSuccess) return set_error(MPM_ERR_CUDA, "fixed-point probe failed: %s", cudaGetErrorString(e));
+    return MPM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,298 @@
+"""Scenes of the reference and the seeded synthetic workloads built on them.
+
+* `create_si_fluid_scene` -- src/lib/mpm/scenes/si-fluid.ts:39-79 (the
+  reference SI Tait water tank, 1,600 particles on a 40x40 grid).
+* `create_si_tank_scene` -- the 1,600-particle SI tank on an 80x80 grid with
+  seeded jitter (40x40 lattice at 1.25 mm in a 50 mm block, Tait gamma 7,
+  c = 20 m/s, y-up gravity).
+* `create_mpm_gate4_scene` / `create_mpm_gate4_step_config` --
+  src/lib/mpm/scenes/gate4.ts:134-357 (LCG seeds, draw order, bonds).
+* `create_dam_break_scene` -- the 1,000,000-particle two-phase water/oil dam
+  break on a 1024x2048 grid (cellSize 10, gravity 90, Gate-4 liquids).
+
+All seeded randomness uses the reference's LCG (gate4.ts:134-144) so that a
+seed names the same scene in every language.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .layout import ParticleArrays
+from .materials import MPM_SI_BOX_DOMAIN
+
+UINT32_RANGE = 0x1_0000_0000
+
+
+class SeededRandom:
+    """createSeededRandom, gate4.ts:134-144 (Numerical Recipes LCG)."""
+
+    def __init__(self, seed: int):
+        if not isinstance(seed, int) or seed < 0 or seed >= UINT32_RANGE:
+            raise ValueError("The scene seed must be an unsigned 32-bit integer.")
+        self.state = seed
+
+    def __call__(self) -> float:
+        self.state = (self.state * 1_664_525 + 1_013_904_223) & 0xFFFFFFFF
+        return self.state / UINT32_RANGE
+
+    def many(self, count: int) -> np.ndarray:
+        return np.array([self() for _ in range(count)], dtype=np.float64)
+
+
+def lcg_sequence(seed: int, count: int) -> np.ndarray:
+    """`count` successive LCG draws, vectorised by jumping the recurrence a
+    block at a time (all products fit in uint64 before the mod 2^32)."""
+    a, c, m = 1_664_525, 1_013_904_223, 1 << 32
+    block = 1 << 12
+    mults = np.empty(block, dtype=np.uint64)
+    adds = np.empty(block, dtype=np.uint64)
+    am, ad = 1, 0
+    for k in range(block):
+        am, ad = (am * a) % m, (ad * a + c) % m
+        mults[k], adds[k] = am, ad
+    out = np.empty(count, dtype=np.float64)
+    state = np.uint64(seed)
+    for start in range(0, count, block):
+        n = min(block, count - start)
+        states = (mults[:n] * state + adds[:n]) % np.uint64(m)
+        out[start:start + n] = states.astype(np.float64) / UINT32_RANGE
+        state = states[n - 1]
+    return out
+
+
+# ------------------------------------------------------------------ tait --
+
+def derive_tait_pressure_coefficient_pa(reference_density, exponent, sound_speed):
+    """deriveTaitPressureCoefficientPa, src/lib/mpm/reference/tait-eos.ts:73-86."""
+    for name, v in (("referenceDensityKgPerM3", reference_density), ("exponent", exponent),
+                    ("soundSpeedMPerS", sound_speed)):
+        if not math.isfinite(v) or v <= 0:
+            raise ValueError(f"{name} must be a finite positive number.")
+    return (reference_density * sound_speed * sound_speed) / exponent
+
+
+def create_mpm_tait_liquid_material(parameters: dict, extrusion_depth_m: float, model: str = "water") -> dict:
+    """createMpmTaitLiquidMaterial, tait-eos.ts:26-44."""
+    density = parameters["referenceDensityKgPerM3"] * extrusion_depth_m
+    lam = parameters["pressureCoefficientPa"] * extrusion_depth_m
+    return {"model": model, "lambda": lam, "mu": 0.0, "density": density,
+            "equationOfState": {"model": "tait", "exponent": parameters["exponent"]}}
+
+
+SI_FLUID_GRID_CELLS = 40
+SI_FLUID_PARTICLE_SPACING_M = 0.0025
+SI_FLUID_FILL_HEIGHT_M = 0.05
+SI_FLUID_EFFECTIVE_SOUND_SPEED_M_PER_S = 20.0
+SI_FLUID_COURANT_LIMIT = 0.3
+SI_FLUID_FIXED_STEP_SECONDS = 1 / 120
+SI_FLUID_MAX_MICROSTEPS_PER_BATCH = 512
+SI_FLUID_WALL_FRICTION = 1.0
+SI_TAIT_WATER_PARAMETERS = {
+    "referenceDensityKgPerM3": 998.2,
+    "exponent": 7.15,
+    "pressureCoefficientPa": derive_tait_pressure_coefficient_pa(998.2, 7.15, SI_FLUID_EFFECTIVE_SOUND_SPEED_M_PER_S),
+    "ambientPressurePa": 101_325.0,
+}
+
+
+def create_si_fluid_scene():
+    """createSiFluidScene, si-fluid.ts:39-79 -> (ParticleArrays, config)."""
+    material = create_mpm_tait_liquid_material(SI_TAIT_WATER_PARAMETERS, MPM_SI_BOX_DOMAIN["extrusionDepthM"])
+    area = SI_FLUID_PARTICLE_SPACING_M ** 2
+    columns = math.floor(MPM_SI_BOX_DOMAIN["innerWidthM"] / SI_FLUID_PARTICLE_SPACING_M)
+    rows = math.floor(SI_FLUID_FILL_HEIGHT_M / SI_FLUID_PARTICLE_SPACING_M)
+    n = rows * columns
+    p = ParticleArrays.empty(n)
+    r, c = np.divmod(np.arange(n), columns)
+    p.px[:] = (c + 0.5) * SI_FLUID_PARTICLE_SPACING_M
+    p.py[:] = MPM_SI_BOX_DOMAIN["innerHeightM"] - SI_FLUID_FILL_HEIGHT_M + (r + 0.5) * SI_FLUID_PARTICLE_SPACING_M
+    p.volume[:] = area
+    grid = {"cellsX": SI_FLUID_GRID_CELLS, "cellsY": SI_FLUID_GRID_CELLS,
+            "cellSize": MPM_SI_BOX_DOMAIN["innerWidthM"] / SI_FLUID_GRID_CELLS}
+    config = {"grid": grid, "particleMass": material["density"] * area, "particleVolume": area,
+              "material": material, "wallFriction": SI_FLUID_WALL_FRICTION}
+    return p, config
+
+
+def create_si_tank_scene(seed: int = 1):
+    """The SI tank workload: 80x80 grid over 0.2 m (dx 2.5 mm), 40x40 lattice at
+    1.25 mm filling [0, 50 mm]^2, jitter U(+-0.1 dx), rho 1000 kg/m^3 with 0.02 m
+    extrusion, Tait gamma 7, c 20 m/s, gravity (0, -9.81), no-slip walls."""
+    depth = MPM_SI_BOX_DOMAIN["extrusionDepthM"]
+    tait = {"referenceDensityKgPerM3": 1000.0, "exponent": 7.0,
+            "pressureCoefficientPa": derive_tait_pressure_coefficient_pa(1000.0, 7.0, 20.0)}
+    material = create_mpm_tait_liquid_material(tait, depth)
+    dx = 0.2 / 80
+    spacing = 0.00125
+    side = 40
+    n = side * side
+    rnd = lcg_sequence(seed, 2 * n)
+    p = ParticleArrays.empty(n)
+    r, c = np.divmod(np.arange(n), side)
+    p.px[:] = (c + 0.5) * spacing + (rnd[0::2] * 2 - 1) * 0.1 * dx
+    p.py[:] = (r + 0.5) * spacing + (rnd[1::2] * 2 - 1) * 0.1 * dx
+    area = spacing * spacing
+    p.volume[:] = area
+    config = {"grid": {"cellsX": 80, "cellsY": 80, "cellSize": dx}, "particleMass": material["density"] * area,
+              "particleVolume": area, "material": material, "wallFriction": 1.0}
+    return p, config
+
+
+SI_TANK_GRAVITY = {"x": 0.0, "y": -9.81}
+SI_TANK_FIXED_STEP_SECONDS = 1 / 120
+
+# ----------------------------------------------------------------- gate 4 --
+
+GATE4_GRID = {"cellsX": 220, "cellsY": 150, "cellSize": 10}
+GATE4_SCENE_SEED = 0x4D504D34
+GATE4_FIXED_STEP_SECONDS = 1 / 240
+GATE4_DEFAULT_GRAVITY = {"x": 0.0, "y": 90.0}
+GATE4_LIQUID_PARTICLE_SPACING = 18
+GATE4_PARTICLE_AREA = 100
+GATE4_LIQUID_PARTICLE_DIAMETER = 20
+GATE4_SOLID_PARTICLE_MASS = 4
+GATE4_PEBBLE_COUNT = 50
+GATE4_PEBBLE_COLUMNS = 8
+GATE4_PEBBLE_ROWS = math.ceil(GATE4_PEBBLE_COUNT / GATE4_PEBBLE_COLUMNS)
+GATE4_PEBBLE_SPACING = 150
+GATE4_FRACTURE_COLUMNS, GATE4_FRACTURE_ROWS, GATE4_FRACTURE_SPACING = 6, 4, 20
+GATE4_FRACTURE_FAILURE_STRAIN = 0.12
+GATE4_PEBBLE_EDGE_LENGTH = GATE4_GRID["cellsX"] * GATE4_GRID["cellSize"] * 0.005 * 12
+GATE4_WATER_MATERIAL = {"lambda": 40_000 * 4, "mu": 0.0, "model": "water", "density": 0.02}
+GATE4_OIL_MATERIAL = {"lambda": 30_000 * 4, "mu": 0.0, "model": "oil", "density": 0.016}
+GATE4_PEBBLE_MATERIAL = {"lambda": 20.0, "mu": 10.0, "model": "neo-hookean"}
+
+
+def create_mpm_gate4_scene(seed: int = GATE4_SCENE_SEED, liquid_particle_diameter: float = 20,
+                           liquid_particle_area: float | None = None, y_shift: float = 0.0):
+    """createMpmGate4Scene, gate4.ts:191-339 -> (ParticleArrays, fractureBonds,
+    parityProbeIndices).  `liquid_particle_area` and `y_shift` give the
+    enlarged variant (220x600 grid, liquid area 1,600, +4,500 in y)."""
+    if not (10 <= liquid_particle_diameter <= 21):
+        raise ValueError("liquidParticleDiameter must be between 10 and 21.")
+    area = liquid_particle_area if liquid_particle_area is not None else liquid_particle_diameter ** 2
+    random = SeededRandom(seed)
+    rows_out = []
+    probes = []
+    objects = [
+        (1, 100, 640, 50, 40, 0, 25, GATE4_WATER_MATERIAL, 64),
+        (2, 100, 100, 50, 30, 29, 25, GATE4_OIL_MATERIAL, 64),
+    ]
+    mats = [GATE4_WATER_MATERIAL, GATE4_OIL_MATERIAL, GATE4_PEBBLE_MATERIAL]
+    for oid, sx, sy, cols, rows, prow, pcol, mat, vmax in objects:
+        start = len(rows_out)
+        for r in range(rows):
+            for c in range(cols):
+                vx = (random() * 2 - 1) * vmax
+                vy = (random() * 2 - 1) * vmax
+                rows_out.append((sx + c * GATE4_LIQUID_PARTICLE_SPACING, sy + r * GATE4_LIQUID_PARTICLE_SPACING + y_shift,
+                                 vx, vy, oid, -1, area, mats.index(mat)))
+        probes.append(start + prow * cols + pcol)
+    parity_pebble = (GATE4_PEBBLE_ROWS // 2) * GATE4_PEBBLE_COLUMNS + GATE4_PEBBLE_COLUMNS // 2
+    edge = GATE4_PEBBLE_EDGE_LENGTH
+    for k in range(GATE4_PEBBLE_COUNT):
+        row = k // GATE4_PEBBLE_COLUMNS
+        row_start = row * GATE4_PEBBLE_COLUMNS
+        in_row = min(GATE4_PEBBLE_COLUMNS, GATE4_PEBBLE_COUNT - row_start)
+        column = k - row_start + (GATE4_PEBBLE_COLUMNS - in_row) * 0.5
+        cx = 700 + (column - (GATE4_PEBBLE_COLUMNS - 1) / 2) * GATE4_PEBBLE_SPACING
+        cy = 569 + (row - (GATE4_PEBBLE_ROWS - 1) / 2) * GATE4_PEBBLE_SPACING + y_shift
+        verts = [(cx - edge * 0.5, cy - edge / (2 * math.sqrt(3))), (cx + edge * 0.5, cy - edge / (2 * math.sqrt(3))),
+                 (cx, cy + edge / math.sqrt(3))]
+        start = len(rows_out)
+        for v, (x, y) in enumerate(verts):
+            vx = (random() * 2 - 1) * 240
+            vy = (random() * 2 - 1) * 240
+            rows_out.append((x, y, vx, vy, 3 + k, v, GATE4_PARTICLE_AREA, 2))
+        if k == parity_pebble:
+            probes.append(start + 2)
+    fstart = len(rows_out)
+    fvx = (random() * 2 - 1) * 80
+    fvy = (random() * 2 - 1) * 80
+    for r in range(GATE4_FRACTURE_ROWS):
+        for c in range(GATE4_FRACTURE_COLUMNS):
+            x = 1520 + (c - (GATE4_FRACTURE_COLUMNS - 1) / 2) * GATE4_FRACTURE_SPACING
+            y = 1380 + (r - (GATE4_FRACTURE_ROWS - 1) / 2) * GATE4_FRACTURE_SPACING + y_shift
+            rows_out.append((x, y, fvx, fvy, 3 + GATE4_PEBBLE_COUNT, -1, GATE4_PARTICLE_AREA, 2))
+    bonds = []
+    idx = lambda r, c: fstart + r * GATE4_FRACTURE_COLUMNS + c  # noqa: E731
+    for r in range(GATE4_FRACTURE_ROWS):
+        for c in range(GATE4_FRACTURE_COLUMNS):
+            first = idx(r, c)
+            if c + 1 < GATE4_FRACTURE_COLUMNS:
+                bonds.append({"firstParticle": first, "secondParticle": first + 1,
+                              "restLength": GATE4_FRACTURE_SPACING, "failureStrain": GATE4_FRACTURE_FAILURE_STRAIN})
+            if r + 1 < GATE4_FRACTURE_ROWS:
+                bonds.append({"firstParticle": first, "secondParticle": first + GATE4_FRACTURE_COLUMNS,
+                              "restLength": GATE4_FRACTURE_SPACING, "failureStrain": GATE4_FRACTURE_FAILURE_STRAIN})
+            if r + 1 < GATE4_FRACTURE_ROWS and c + 1 < GATE4_FRACTURE_COLUMNS:
+                bonds.append({"firstParticle": first, "secondParticle": first + GATE4_FRACTURE_COLUMNS + 1,
+                              "restLength": GATE4_FRACTURE_SPACING * math.sqrt(2),
+                              "failureStrain": GATE4_FRACTURE_FAILURE_STRAIN})
+    n = len(rows_out)
+    arr = np.array(rows_out, dtype=np.float64)
+    p = ParticleArrays.empty(n)
+    p.px[:], p.py[:], p.vx[:], p.vy[:] = arr[:, 0], arr[:, 1], arr[:, 2], arr[:, 3]
+    p.object_id[:] = arr[:, 4].astype(np.int64)
+    p.bonded_vertex[:] = arr[:, 5].astype(np.int8)
+    p.volume[:] = arr[:, 6]
+    p.plastic_volume[:] = 1.0
+    p.material[:] = arr[:, 7].astype(np.int32)
+    p.materials = mats
+    return p, bonds, probes
+
+
+def create_mpm_gate4_step_config(gravity=None, dt=GATE4_FIXED_STEP_SECONDS, fracture_bonds=None, grid=None):
+    """createMpmGate4StepConfig, gate4.ts:341-357."""
+    cfg = {"dt": dt, "bondReferenceDt": GATE4_FIXED_STEP_SECONDS, "grid": dict(grid or GATE4_GRID),
+           "particleMass": GATE4_SOLID_PARTICLE_MASS, "particleVolume": GATE4_PARTICLE_AREA,
+           "bondRestLength": GATE4_PEBBLE_EDGE_LENGTH, "material": GATE4_PEBBLE_MATERIAL,
+           "gravity": dict(gravity or GATE4_DEFAULT_GRAVITY)}
+    if fracture_bonds is not None:
+        cfg["fractureBonds"] = fracture_bonds
+    return cfg
+
+
+# -------------------------------------------------------------- dam break --
+
+DAM_BREAK_GRID = {"cellsX": 1024, "cellsY": 2048, "cellSize": 10}
+DAM_BREAK_GRAVITY = {"x": 0.0, "y": 90.0}
+DAM_BREAK_FIXED_STEP_SECONDS = 1 / 240
+
+
+def create_dam_break_scene(particles_per_phase: int = 500_000, columns: int = 500, grid=None):
+    """Two stacked liquid blocks (y-down, gravity +y): water on the floor, oil
+    above it, both at the left wall; 2x2 particles per 10-unit cell (spacing 5,
+    area 25), zero velocity, Gate-4 liquid materials (legacy linear EOS,
+    lambda 160,000 / 120,000, density 0.02 / 0.016)."""
+    grid = dict(grid or DAM_BREAK_GRID)
+    spacing = grid["cellSize"] / 2
+    rows = particles_per_phase // columns
+    if rows * columns != particles_per_phase:
+        raise ValueError("particles_per_phase must be a multiple of columns")
+    height = grid["cellsY"] * grid["cellSize"]
+    margin = 2 * grid["cellSize"]
+    n = 2 * particles_per_phase
+    p = ParticleArrays.empty(n)
+    k = np.arange(particles_per_phase)
+    r, c = np.divmod(k, columns)
+    x = margin + (c + 0.5) * spacing
+    water_y = height - margin - (r + 0.5) * spacing
+    oil_y = height - margin - rows * spacing - (r + 0.5) * spacing
+    if oil_y.min() < 0 or x.max() > grid["cellsX"] * grid["cellSize"]:
+        raise ValueError("the dam-break blocks do not fit the grid")
+    p.px[:particles_per_phase], p.py[:particles_per_phase] = x, water_y
+    p.px[particles_per_phase:], p.py[particles_per_phase:] = x, oil_y
+    p.object_id[:particles_per_phase] = 1
+    p.object_id[particles_per_phase:] = 2
+    p.volume[:] = spacing * spacing
+    p.plastic_volume[:] = 1.0
+    p.materials = [GATE4_WATER_MATERIAL, GATE4_OIL_MATERIAL]
+    p.material[:particles_per_phase] = 0
+    p.material[particles_per_phase:] = 1
+    mass = GATE4_WATER_MATERIAL["density"] * spacing * spacing
+    config = {"grid": grid, "particleMass": mass, "particleVolume": spacing * spacing,
+              "material": GATE4_WATER_MATERIAL, "wallFriction": 0.0}
+    return p, config

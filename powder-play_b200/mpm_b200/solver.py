@@ -1,0 +1,559 @@
+"""The GPU solver host API: a drop-in for `MpmMlsGpuSolver`.
+
+Restates the host control flow of src/lib/mpm/kernels/solver.ts
+(7korobi/powder-play): the factories `createMpmMlsGpuSolver` /
+`createExperimentalMpmMlsAtomicGpuSolver` (:390-469), CFL-bound certification
+`validateCflBounds` (:471-528), `stepBatch` (:1407-1599), `stepCflBatch`
+(:1601-1722), the adaptive retry/rollback loop `stepCflBatchAdaptive`
+(:1724-2021), `measureMaximumParticleSpeed` (:2388-2512),
+`checkNumericalStatus` (:2514-2570) and `readParticles` (:2594-).  The device
+work runs in libmpm_b200.so through the C ABI of include/mpm_b200.h; the
+reference's Promises become blocking calls.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+
+import numpy as np
+
+from . import _lib
+from .cfl import calculate_mpm_cfl_microsteps, calculate_mpm_cfl_safe_dt, calculate_mpm_cfl_velocity_limit
+from .cfl_bounds import derive_mpm_mls_gpu_cfl_bounds
+from .errors import (MpmMlsGpuNumericalError, MpmNativeError, RangeError, decode_numerical_error,
+                     is_recoverable_cfl_error)
+from .layout import (PARTICLE_FLOATS, ValidatedInput, fround, pack_step_parameters, unpack_particles,
+                     validate_mpm_mls_gpu_input, _is_safe_integer)
+
+CFL_RECOVERY_BOUND_SAFETY_FACTOR = 1.25
+MPM_MLS_GPU_DRAG_STIFFNESS = 20.0
+MPM_MLS_GPU_DRAG_DAMPING = 8.0
+EPSILON = 2.220446049250313e-16
+MIN_VALUE = 5e-324
+DEFAULT_FIXED_POINT_SHIFT = 24
+
+
+def _is_capacity_error(error) -> bool:
+    import re
+    return isinstance(error, RangeError) and re.search(
+        r"exceeds maxMicrosteps|microDt is too small to represent", str(error)) is not None
+
+
+def _check(rc: int, what: str):
+    if rc == _lib.MPM_OK:
+        return
+    message = _lib.last_error()
+    if rc == _lib.MPM_ERR_INVALID_ARGUMENT:
+        raise RangeError(message or f"{what}: invalid argument")
+    raise MpmNativeError(f"{what}: {message}")
+
+
+def validate_cfl_bounds(bounds, state: ValidatedInput, derived):
+    """validateCflBounds, solver.ts:471-528."""
+    if bounds is None:
+        return derived
+    if not isinstance(bounds, dict):
+        raise RangeError("cflBounds must be an object of valid speed bounds.")
+    if derived is None:
+        raise RangeError("this solver configuration has no derived CFL bounds for its constitutive material.")
+    wave, vel = bounds.get("waveSpeedBound"), bounds.get("velocityBound")
+    if not isinstance(wave, (int, float)) or not math.isfinite(wave) or wave < 0:
+        raise RangeError("cflBounds.waveSpeedBound must be finite and non-negative.")
+    if not isinstance(vel, (int, float)) or not math.isfinite(vel) or vel < 0:
+        raise RangeError("cflBounds.velocityBound must be finite and non-negative.")
+    courant = bounds.get("courantLimit")
+    if courant is not None and (not math.isfinite(courant) or courant <= 0):
+        raise RangeError("cflBounds.courantLimit must be positive and finite.")
+    if wave < derived["waveSpeedBound"]:
+        raise RangeError("cflBounds.waveSpeedBound must not be lower than the material-derived initial bound.")
+    if vel < derived["velocityBound"]:
+        raise RangeError("cflBounds.velocityBound must not be lower than the configured initial-state bound.")
+    speeds = np.hypot(state.packed_particles[:, 2].astype(np.float64), state.packed_particles[:, 3].astype(np.float64))
+    over = np.flatnonzero(speeds > vel)
+    if over.size:
+        raise RangeError(f"initial velocity at particle {int(over[0])} exceeds cflBounds.velocityBound.")
+    out = {"waveSpeedBound": float(wave), "velocityBound": float(vel)}
+    if courant is not None:
+        out["courantLimit"] = float(courant)
+    return out
+
+
+class MpmMlsGpuSolver:
+    """MpmMlsGpuSolver, solver.ts:106-144, backed by libmpm_b200.so."""
+
+    def __init__(self, state: ValidatedInput, cfl_bounds, atomic_p2g: bool, device: int = 0,
+                 fixed_point_shift: int = DEFAULT_FIXED_POINT_SHIFT):
+        self._lib = _lib.load_library()
+        self._state = state
+        cfg = state.config
+        c = _lib.MpmConfig()
+        c.cells_x, c.cells_y = cfg["grid"]["cellsX"], cfg["grid"]["cellsY"]
+        c.cell_size = state.cell_size_f32
+        c.particle_mass = state.particle_mass_f32
+        c.particle_volume = state.particle_volume_f32
+        c.bond_rest_length = state.bond_rest_length_f32
+        c.bond_stiffness = state.bond_stiffness_f32
+        c.bond_reference_dt = state.bond_reference_dt_f32 or 0.0
+        c.wall_friction = state.wall_friction_f32
+        c.lambda_ = state.lambda_f32
+        c.mu = state.mu_f32
+        c.capacity = state.particle_capacity
+        c.p2g_mode = _lib.MPM_P2G_FIXED_POINT if atomic_p2g else _lib.MPM_P2G_GATHER
+        c.fixed_point_shift = fixed_point_shift
+        c.device = device
+        handle = ctypes.c_void_p()
+        packed = np.ascontiguousarray(state.packed_particles, dtype=np.float32)
+        ids = np.ascontiguousarray(state.packed_object_ids, dtype=np.uint32)
+        starts = np.ascontiguousarray(state.bonded_body_starts, dtype=np.uint32)
+        bonds = np.ascontiguousarray(state.packed_fracture_bonds, dtype=np.uint32)
+        topo = np.ascontiguousarray(state.packed_fracture_bond_topology, dtype=np.uint32)
+        rc = self._lib.mpm_create(ctypes.byref(c), _lib.ptr(packed), _lib.ptr(ids), state.particle_count,
+                                  _lib.ptr(starts), len(starts), _lib.ptr(bonds), state.fracture_bond_count,
+                                  _lib.ptr(topo), len(topo), ctypes.byref(handle))
+        if rc != _lib.MPM_OK:
+            message = _lib.last_error()
+            raise RuntimeError(f"Failed to initialize the GPU MLS-MPM solver: {message}")
+        self._handle = handle
+        self.cfl_bounds = cfl_bounds
+        self.atomic_p2g = atomic_p2g
+        self.fixed_point_shift = fixed_point_shift
+        self._disposed = False
+        self._slot_count = state.particle_count
+        self._cfl_speed_measurement_submitted = False
+        self._cfl_state_usable = cfl_bounds is not None
+        self._last_scheduled_velocity_bound = None if cfl_bounds is None else cfl_bounds["velocityBound"]
+        self._latest_cfl_batch_sequence = 0
+        self._latest_cfl_batch_microstep_count = 0
+        self._latest_completed_cfl_measurement_sequence = 0
+        self._active_drag = None
+        self.device_ms_total = 0.0
+        self.committed_microsteps_total = 0
+
+    # ---------------------------------------------------------------- props --
+    @property
+    def particle_count(self) -> int:
+        return self._slot_count
+
+    @property
+    def allocated_particle_count(self) -> int:
+        return self._slot_count
+
+    @property
+    def particle_capacity(self) -> int:
+        return self._state.particle_capacity
+
+    @property
+    def node_count(self) -> int:
+        return int(self._lib.mpm_node_count(self._handle))
+
+    def _assert_active(self):
+        if self._disposed:
+            raise RuntimeError("GPU MLS-MPM solver has been disposed.")
+
+    # ----------------------------------------------------------------- steps --
+    def step(self, dt: float, gravity: dict) -> None:
+        self.step_batch(1, dt, gravity)
+
+    def step_batch(self, step_count: int, dt: float, gravity: dict, cfl_velocity_bound=None,
+                   bond_reference_dt=None) -> None:
+        """stepBatch, solver.ts:1407-1599."""
+        self._assert_active()
+        if not _is_safe_integer(step_count) or step_count < 1:
+            raise RangeError("stepCount must be a positive safe integer.")
+        guard = None
+        if cfl_velocity_bound is not None:
+            if self.cfl_bounds is None:
+                raise RangeError("this solver configuration has no safely derived CFL bounds.")
+            if not math.isfinite(cfl_velocity_bound) or cfl_velocity_bound < 0:
+                raise RangeError("velocityBound must be finite and non-negative.")
+            guard = {"waveSpeedBound": self.cfl_bounds["waveSpeedBound"], "velocityBound": cfl_velocity_bound}
+        dt32, gx, gy, wave, vel, bref = pack_step_parameters(self._state, dt, gravity, guard, bond_reference_dt)
+        native_guard = None
+        if guard is not None:
+            native_guard = _lib.MpmCflGuard(wave, vel)
+        try:
+            rc = self._lib.mpm_step_batch(self._handle, int(step_count), dt32, gx, gy,
+                                          ctypes.byref(native_guard) if native_guard is not None else None, bref)
+            _check(rc, f"Failed to encode or submit an MLS-MPM batch of {step_count} step(s).")
+        except Exception:
+            self._cfl_state_usable = False
+            self._cfl_speed_measurement_submitted = False
+            raise
+        self._cfl_speed_measurement_submitted = guard is not None
+        if guard is None:
+            self._cfl_state_usable = False
+
+    def step_cfl_batch(self, macro_step_count, macro_dt, microstep_plan, velocity_bound, max_microsteps, gravity,
+                       bond_reference_dt=None) -> None:
+        """stepCflBatch, solver.ts:1601-1722."""
+        self._assert_active()
+        if self.cfl_bounds is None:
+            raise RangeError("CFL stepping requires a material-derived wave-speed bound; this solver configuration "
+                             "has no safely derived CFL bounds.")
+        if not self._cfl_state_usable:
+            raise RuntimeError("a direct non-CFL GPU step or a failed CFL measurement invalidated the tracked "
+                               "velocity bound; recreate the solver before CFL stepping.")
+        if self._cfl_speed_measurement_submitted:
+            raise RuntimeError("queue measureMaximumParticleSpeed() after the previous CFL batch before submitting "
+                               "another one.")
+        if self._last_scheduled_velocity_bound is not None and velocity_bound < self._last_scheduled_velocity_bound:
+            raise RangeError("velocityBound must cover the last submitted GPU maximum-particle envelope.")
+        if not _is_safe_integer(macro_step_count) or macro_step_count < 1:
+            raise RangeError("macroStepCount must be a positive safe integer.")
+        if not _is_safe_integer(max_microsteps) or max_microsteps < 1:
+            raise RangeError("maxMicrosteps must be a positive safe integer.")
+        cell = self._state.config["grid"]["cellSize"]
+        b = self.cfl_bounds
+        expected = calculate_mpm_cfl_microsteps(macro_dt, cell, b["waveSpeedBound"], velocity_bound, max_microsteps,
+                                                courantLimit=b.get("courantLimit"))
+        certified = None
+        if (isinstance(microstep_plan, dict) and _is_safe_integer(microstep_plan.get("stepCount"))
+                and microstep_plan["stepCount"] >= expected["stepCount"]):
+            certified = calculate_mpm_cfl_microsteps(macro_dt, cell, b["waveSpeedBound"], velocity_bound,
+                                                     max_microsteps, minimumStepCount=microstep_plan["stepCount"],
+                                                     courantLimit=b.get("courantLimit"))
+        if (certified is None or microstep_plan["stepCount"] != certified["stepCount"]
+                or microstep_plan["microDt"] != certified["microDt"] or microstep_plan["safeDt"] != certified["safeDt"]):
+            raise RangeError("microstepPlan does not match this solver configuration or is not a certified CFL "
+                             "refinement.")
+        micro_count = macro_step_count * certified["stepCount"]
+        if not _is_safe_integer(micro_count) or micro_count > max_microsteps:
+            raise RangeError(f"requested microstep count ({micro_count}) exceeds maxMicrosteps ({max_microsteps}).")
+        represented = certified["microDt"] * certified["stepCount"]
+        tolerance = max(macro_dt, MIN_VALUE) * EPSILON * 4
+        if abs(represented - macro_dt) > tolerance:
+            raise RangeError("microstepPlan does not preserve the requested macro dt.")
+        gpu_micro = fround(certified["microDt"])
+        if self._active_drag is not None and (not math.isfinite(gpu_micro) or gpu_micro <= 0
+                                              or gpu_micro * MPM_MLS_GPU_DRAG_DAMPING > 1):
+            raise RangeError("CFL microDt is too large for the explicit drag damping update to remain dissipative.")
+        limit = calculate_mpm_cfl_velocity_limit(cell, b["waveSpeedBound"], certified["microDt"], b.get("courantLimit"))
+        if limit < velocity_bound:
+            raise RangeError("float32 microDt does not preserve the planned CFL velocity bound; increase the "
+                             "microstep count.")
+        sb = self._state.bond_reference_dt_f32
+        self.step_batch(micro_count, certified["microDt"], gravity, limit,
+                        bond_reference_dt if bond_reference_dt is not None else (sb if sb is not None else macro_dt))
+        self._latest_cfl_batch_sequence += 1
+        self._latest_cfl_batch_microstep_count = micro_count
+        self._last_scheduled_velocity_bound = velocity_bound
+
+    def step_cfl_batch_adaptive(self, macro_step_count, macro_dt, microstep_plan, velocity_bound, max_microsteps,
+                                gravity, gravity_for_duration=None) -> dict:
+        """stepCflBatchAdaptive, solver.ts:1724-2021 (the retry/rollback loop)."""
+        if self.cfl_bounds is None:
+            raise RangeError("CFL stepping requires a material-derived wave-speed bound; this solver configuration "
+                             "has no safely derived CFL bounds.")
+        if not _is_safe_integer(macro_step_count) or macro_step_count < 1:
+            raise RangeError("macroStepCount must be a positive safe integer.")
+        if not math.isfinite(macro_dt) or macro_dt <= 0:
+            raise RangeError("macroDt must be positive and finite.")
+        total = macro_step_count * macro_dt
+        if not math.isfinite(total):
+            raise RangeError("CFL batch duration is outside the supported range.")
+        bref = self._state.bond_reference_dt_f32 if self._state.bond_reference_dt_f32 is not None else macro_dt
+        remaining = total
+        attempt_macro_count, attempt_macro_dt = macro_step_count, macro_dt
+        attempt_plan, attempt_velocity = microstep_plan, velocity_bound
+        consumed = retry_count = submissions = 0
+        retry_ms = readback_ms = 0.0
+        tolerance = max(total, MIN_VALUE) * EPSILON * 4
+        cell = self._state.config["grid"]["cellSize"]
+
+        def result(measurement, recommended=None):
+            return dict(measurement,
+                        recommendedVelocityBound=measurement["maximumSpeed"] if recommended is None else recommended,
+                        attemptedMicroStepCount=consumed, retryCount=retry_count,
+                        retrySubmissionMilliseconds=retry_ms, readbackMilliseconds=readback_ms,
+                        simulatedDuration=max(0.0, total - remaining), remainingDuration=remaining)
+
+        while True:
+            attempt_micro = attempt_macro_count * attempt_plan["stepCount"]
+            attempt_duration = attempt_macro_count * attempt_macro_dt
+            budget = max_microsteps - consumed
+            if (not _is_safe_integer(attempt_micro) or attempt_micro < 1 or not math.isfinite(attempt_duration)
+                    or attempt_duration <= 0 or attempt_micro > budget):
+                raise RangeError(f"adaptive CFL retry requires {attempt_micro} microsteps with {budget} remaining.")
+            started = time.perf_counter()
+            attempt_gravity = gravity if gravity_for_duration is None else gravity_for_duration(
+                total - remaining, attempt_duration)
+            self.step_cfl_batch(attempt_macro_count, attempt_macro_dt, attempt_plan, attempt_velocity, budget,
+                                attempt_gravity, bref)
+            if submissions > 0:
+                retry_ms += (time.perf_counter() - started) * 1e3
+            submissions += 1
+            read_started = time.perf_counter()
+            try:
+                measurement = self.measure_maximum_particle_speed()
+            except MpmMlsGpuNumericalError as error:
+                readback_ms += (time.perf_counter() - read_started) * 1e3
+                if not is_recoverable_cfl_error(error):
+                    raise
+                completed = error.completed_microsteps
+                if completed is None or completed < 0 or completed >= attempt_micro:
+                    raise RuntimeError(f"Adaptive CFL recovery could not determine completed microsteps: {error}") from error
+                completed_duration = completed * attempt_plan["microDt"]
+                if not math.isfinite(completed_duration) or completed_duration >= remaining:
+                    raise RuntimeError(f"Adaptive CFL recovery received invalid simulation progress: {error}") from error
+                remaining -= completed_duration
+                consumed += attempt_micro
+                self.committed_microsteps_total += completed
+                observed = max(error.measured_maximum_speed or 0.0,
+                               (error.cfl_details or {}).get("particleSpeed", 0.0))
+                retry_velocity = max(attempt_velocity, self._last_scheduled_velocity_bound or 0.0,
+                                     observed * CFL_RECOVERY_BOUND_SAFETY_FACTOR)
+                if not math.isfinite(retry_velocity):
+                    raise RuntimeError(f"Adaptive CFL recovery stopped after {retry_count} retry attempt(s) "
+                                       f"(non-finite velocity bound); last GPU error: {error}") from error
+                self._last_scheduled_velocity_bound = retry_velocity
+                if error.cfl_details is not None:
+                    retry_wave = error.cfl_details["waveSpeed"] * CFL_RECOVERY_BOUND_SAFETY_FACTOR
+                    if not math.isfinite(retry_wave):
+                        raise RuntimeError(f"Adaptive CFL recovery stopped after {retry_count} retry attempt(s) "
+                                           f"(non-finite wave-speed bound); last GPU error: {error}") from error
+                    self.cfl_bounds = dict(self.cfl_bounds,
+                                           waveSpeedBound=max(self.cfl_bounds["waveSpeedBound"], retry_wave))
+                retry_budget = max_microsteps - consumed
+                if retry_budget < 2:
+                    self._clear_status()
+                    self._cfl_state_usable = True
+                    return result({"maximumSpeed": observed, "sequence": self._latest_cfl_batch_sequence},
+                                  retry_velocity)
+                failed_interval = min(remaining, attempt_plan["microDt"])
+                try:
+                    attempt_plan = calculate_mpm_cfl_microsteps(
+                        failed_interval, cell, self.cfl_bounds["waveSpeedBound"], retry_velocity, retry_budget,
+                        minimumStepCount=2, courantLimit=self.cfl_bounds.get("courantLimit"))
+                except RangeError as cause:
+                    if not _is_capacity_error(cause):
+                        raise RuntimeError(f"Adaptive CFL recovery could not schedule a finer step ({cause}; "
+                                           f"retry={retry_count + 1}): {error}") from cause
+                    self._clear_status()
+                    self._cfl_state_usable = True
+                    return result({"maximumSpeed": observed, "sequence": self._latest_cfl_batch_sequence},
+                                  retry_velocity)
+                self._clear_status()
+                self._cfl_state_usable = True
+                attempt_macro_count, attempt_macro_dt = 1, failed_interval
+                attempt_velocity = retry_velocity
+                retry_count += 1
+                continue
+            readback_ms += (time.perf_counter() - read_started) * 1e3
+            consumed += attempt_micro
+            self.committed_microsteps_total += attempt_micro
+            remaining = max(0.0, remaining - attempt_duration)
+            if remaining <= tolerance:
+                remaining = 0.0
+                return result(measurement, max(attempt_velocity, measurement["maximumSpeed"]) if retry_count > 0
+                              else measurement["maximumSpeed"])
+            continuation_budget = max_microsteps - consumed
+            if continuation_budget < 2:
+                return result(measurement, max(attempt_velocity, measurement["maximumSpeed"]))
+            attempt_velocity = max(attempt_velocity, measurement["maximumSpeed"])
+            safe = calculate_mpm_cfl_safe_dt(cell, self.cfl_bounds["waveSpeedBound"], attempt_velocity,
+                                             self.cfl_bounds.get("courantLimit", 0.3))
+            max_step = min(attempt_plan["microDt"], safe)
+            if not math.isfinite(max_step) or max_step <= 0:
+                raise RangeError(f"Adaptive CFL recovery produced an invalid continuation timestep ({max_step}).")
+            required = math.ceil(remaining / max_step)
+            continuation = remaining
+            minimum = max(1, required)
+            if required >= continuation_budget:
+                continuation = min(remaining, max_step * (continuation_budget - 1) * (1 - EPSILON * 8))
+                minimum = max(1, math.ceil(continuation / max_step))
+            if not math.isfinite(continuation) or continuation <= 0:
+                return result(measurement, max(attempt_velocity, measurement["maximumSpeed"]))
+            attempt_plan = calculate_mpm_cfl_microsteps(continuation, cell, self.cfl_bounds["waveSpeedBound"],
+                                                        attempt_velocity, continuation_budget,
+                                                        minimumStepCount=minimum,
+                                                        courantLimit=self.cfl_bounds.get("courantLimit"))
+            attempt_macro_count, attempt_macro_dt = 1, continuation
+
+    # -------------------------------------------------------------- readback --
+    def _read_compact(self):
+        speed = ctypes.c_float()
+        done = ctypes.c_uint32()
+        status = np.zeros(8, dtype=np.uint32)
+        _check(self._lib.mpm_read_compact(self._handle, ctypes.byref(speed), ctypes.byref(done), _lib.ptr(status)),
+               "Failed to read the compact GPU CFL speed measurement.")
+        return float(speed.value), int(done.value), status
+
+    def _clear_status(self):
+        _check(self._lib.mpm_clear_status(self._handle), "Failed to clear the GPU numerical status.")
+
+    def measure_maximum_particle_speed(self) -> dict:
+        """measureMaximumParticleSpeed, solver.ts:2388-2512."""
+        self._assert_active()
+        if not self._cfl_speed_measurement_submitted:
+            raise RuntimeError("No completed CFL batch has a maximum-speed measurement to read.")
+        self._cfl_speed_measurement_submitted = False
+        sequence = self._latest_cfl_batch_sequence
+        try:
+            speed, completed, status = self._read_compact()
+            self.device_ms_total += self.last_batch_device_ms()
+            if completed > self._latest_cfl_batch_microstep_count:
+                raise RangeError(f"GPU reported {completed} completed microsteps for a batch of "
+                                 f"{self._latest_cfl_batch_microstep_count}.")
+            error = decode_numerical_error(status, completed, speed)
+            if error is not None:
+                raise error
+            if status[7] != 0:
+                raise RuntimeError(f"GPU free-surface occupancy generation failed (status 0x{int(status[7]):x}); "
+                                   "particle state was not modified.")
+            if not math.isfinite(speed) or speed < 0:
+                raise RangeError("GPU returned an invalid maximum-particle-speed scalar.")
+            if sequence >= self._latest_completed_cfl_measurement_sequence:
+                self._latest_completed_cfl_measurement_sequence = sequence
+                if sequence == self._latest_cfl_batch_sequence:
+                    self._last_scheduled_velocity_bound = speed
+            return {"maximumSpeed": speed, "sequence": sequence}
+        except Exception:
+            self._cfl_state_usable = False
+            raise
+
+    def last_batch_device_ms(self) -> float:
+        """Device time of the last submitted batch (CUDA events on the solver's stream)."""
+        out = ctypes.c_double()
+        _check(self._lib.mpm_last_batch_device_ms(self._handle, ctypes.byref(out)), "batch timing failed")
+        return float(out.value)
+
+    def profile_substeps(self, step_count: int, dt: float, gravity: dict, velocity_limit=None) -> dict:
+        """Runs real substeps kernel by kernel with CUDA events between them:
+        {kernel name: (milliseconds, launches)}."""
+        slots = int(self._lib.mpm_profile_kernel_slots())
+        ms = np.zeros(slots, dtype=np.float64)
+        launches = np.zeros(slots, dtype=np.uint32)
+        guard = None
+        if velocity_limit is not None:
+            guard = _lib.MpmCflGuard(fround(self.cfl_bounds["waveSpeedBound"]), fround(velocity_limit))
+        _check(self._lib.mpm_profile_substeps(self._handle, step_count, fround(dt), fround(gravity["x"]),
+                                              fround(gravity["y"]), ctypes.byref(guard) if guard else None,
+                                              _lib.ptr(ms), _lib.ptr(launches)), "profiled substeps failed")
+        out = {}
+        for k in range(slots):
+            if launches[k]:
+                out[self._lib.mpm_profile_kernel_name(k).decode()] = (float(ms[k]), int(launches[k]))
+        return out
+
+    def count_active_nodes(self):
+        counts = np.zeros(3, dtype=np.uint32)
+        _check(self._lib.mpm_count_active_nodes(self._handle, _lib.ptr(counts)), "active node count failed")
+        return tuple(int(c) for c in counts)
+
+    def check_numerical_status(self) -> None:
+        """checkNumericalStatus, solver.ts:2514-2570."""
+        self._assert_active()
+        _, _, status = self._read_compact()
+        error = decode_numerical_error(status)
+        if error is not None:
+            raise error
+
+    def read_status_words(self) -> np.ndarray:
+        self._assert_active()
+        return self._read_compact()[2]
+
+    def read_particles_packed(self, particle_indices=None):
+        """The packed 20-word records and object ids (readParticles without decoding)."""
+        self._assert_active()
+        if particle_indices is None:
+            count = self._slot_count
+            idx = None
+        else:
+            if not isinstance(particle_indices, (list, tuple, np.ndarray)):
+                raise TypeError("particleIndices must be an array of active particle indices.")
+            idx = np.ascontiguousarray(particle_indices, dtype=np.int64)
+            if idx.size and (idx.min() < 0 or idx.max() >= self._slot_count):
+                raise RangeError("particleIndices must identify active GPU particles.")
+            idx = idx.astype(np.uint32)
+            count = idx.size
+        packed = np.zeros((count, PARTICLE_FLOATS), dtype=np.float32)
+        ids = np.zeros(count, dtype=np.uint32)
+        _check(self._lib.mpm_read_particles(self._handle, _lib.ptr(idx), count, _lib.ptr(packed), _lib.ptr(ids)),
+               "Failed to read GPU MLS-MPM particles.")
+        status = self._read_compact()[2]
+        error = decode_numerical_error(status)
+        if error is not None:
+            raise error
+        return packed, ids
+
+    def read_particles(self, particle_indices=None) -> list:
+        """readParticles, solver.ts:2594- (decoded like unpackParticles :3148-3226)."""
+        packed, ids = self.read_particles_packed(particle_indices)
+        return unpack_particles(packed, ids)
+
+    def write_particles_packed(self, packed: np.ndarray) -> None:
+        self._assert_active()
+        packed = np.ascontiguousarray(packed, dtype=np.float32)
+        _check(self._lib.mpm_write_particles(self._handle, _lib.ptr(packed), packed.shape[0]),
+               "Failed to upload GPU MLS-MPM particles.")
+
+    def measure_queue_completion_ms(self) -> float:
+        self._assert_active()
+        out = ctypes.c_double()
+        _check(self._lib.mpm_queue_completion_ms(self._handle, ctypes.byref(out)), "Failed to measure the queue.")
+        return float(out.value)
+
+    def begin_drag(self, target: dict, radius: float) -> None:
+        """beginDrag/updateDrag (solver.ts:2700-2790): grid-node spring and damping."""
+        self._assert_active()
+        drag = _lib.MpmDrag(fround(target["x"]), fround(target["y"]), fround(radius), MPM_MLS_GPU_DRAG_STIFFNESS,
+                            MPM_MLS_GPU_DRAG_DAMPING)
+        _check(self._lib.mpm_set_drag(self._handle, ctypes.byref(drag)), "Failed to set the drag target.")
+        self._active_drag = {"radius": radius}
+
+    def end_drag(self) -> None:
+        self._assert_active()
+        _check(self._lib.mpm_set_drag(self._handle, None), "Failed to end the drag.")
+        self._active_drag = None
+
+    # ---------------------------------------------------------------- probes --
+    def probe_sort(self, dt: float):
+        n, nodes = self._slot_count, self.node_count
+        keys = np.zeros(n, dtype=np.uint32)
+        perm = np.zeros(n, dtype=np.uint32)
+        starts = np.zeros(nodes + 1, dtype=np.uint32)
+        _check(self._lib.mpm_probe_sort(self._handle, fround(dt), _lib.ptr(keys), _lib.ptr(perm), _lib.ptr(starts)),
+               "sort probe failed")
+        return keys, perm, starts
+
+    def probe_fixed_point(self, dt: float):
+        n, nodes = self._slot_count, self.node_count
+        words = np.zeros((nodes, 11), dtype=np.int32)
+        affine = np.zeros((n, 4), dtype=np.float32)
+        _check(self._lib.mpm_probe_fixed_point(self._handle, fround(dt), _lib.ptr(words), _lib.ptr(affine)),
+               "fixed-point probe failed")
+        return words, affine
+
+    def dispose(self) -> None:
+        if self._disposed:
+            return
+        self._disposed = True
+        self._lib.mpm_destroy(self._handle)
+        self._handle = None
+
+    def __del__(self):
+        try:
+            self.dispose()
+        except Exception:
+            pass
+
+
+def _create(particles, config, cfl_bounds, atomic, device, fixed_point_shift):
+    state = validate_mpm_mls_gpu_input(particles, config)
+    derived = derive_mpm_mls_gpu_cfl_bounds(particles, state.config)
+    certified = validate_cfl_bounds(cfl_bounds, state, derived)
+    return MpmMlsGpuSolver(state, certified, atomic, device, fixed_point_shift)
+
+
+def create_mpm_mls_gpu_solver(particles, config, cfl_bounds=None, device: int = 0) -> MpmMlsGpuSolver:
+    """createMpmMlsGpuSolver, solver.ts:390-397 (headless: a device ordinal
+    replaces the canvas)."""
+    return _create(particles, config, cfl_bounds, False, device, DEFAULT_FIXED_POINT_SHIFT)
+
+
+def create_experimental_mpm_mls_atomic_gpu_solver(particles, config, cfl_bounds=None, device: int = 0,
+                                                  fixed_point_shift: int = DEFAULT_FIXED_POINT_SHIFT):
+    """createExperimentalMpmMlsAtomicGpuSolver, solver.ts:399-406.  The
+    fixed-point scale 2^fixed_point_shift defaults to the reference's 2^24."""
+    return _create(particles, config, cfl_bounds, True, device, fixed_point_shift)
