@@ -17,6 +17,7 @@ import pytest
 from helpers import (max_abs_difference, oracle_columns, packed_columns, transfer_regression_fixture)
 from mpm_b200 import (MpmMlsGpuNumericalError, calculate_mpm_cfl_microsteps, create_experimental_mpm_mls_atomic_gpu_solver,
                       create_mpm_mls_gpu_solver, particles_from_dicts)
+from mpm_b200.cfl_bounds import calculate_mpm_cfl_velocity_bound
 from mpm_b200.layout import ParticleArrays, validate_mpm_mls_gpu_input
 from mpm_b200.scenes import (DAM_BREAK_GRAVITY, create_dam_break_scene, create_si_fluid_scene, create_si_tank_scene)
 from oracle import OracleState, emulate_fixed_point_scatter
@@ -209,11 +210,15 @@ def test_cfl_adaptive_batches_commit_every_microstep():
         bounds = solver.cfl_bounds
         velocity = bounds["velocityBound"]
         for _ in range(5):
+            # the scheduler's velocity envelope: current bound + |g| * duration
+            envelope = calculate_mpm_cfl_velocity_bound(velocity, 1 / 120, 9.81, 0, 0, 0, 0)
             plan = calculate_mpm_cfl_microsteps(1 / 120, config["grid"]["cellSize"], bounds["waveSpeedBound"],
-                                                max(velocity, 0.5), 512)
-            m = solver.step_cfl_batch_adaptive(1, 1 / 120, plan, max(velocity, 0.5), 512, gravity)
-            assert m["remainingDuration"] == 0 and m["retryCount"] == 0
-            assert m["attemptedMicroStepCount"] == plan["stepCount"]
+                                                envelope, 512)
+            before = solver.committed_microsteps_total
+            m = solver.step_cfl_batch_adaptive(1, 1 / 120, plan, envelope, 512, gravity)
+            assert m["remainingDuration"] == 0
+            assert m["attemptedMicroStepCount"] >= plan["stepCount"]
+            assert solver.committed_microsteps_total - before >= plan["stepCount"]
             velocity = m["recommendedVelocityBound"]
         assert 0 < velocity < 5
     finally:
