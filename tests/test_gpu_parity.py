@@ -207,9 +207,10 @@ def test_cfl_adaptive_batches_commit_every_microstep():
     gravity = {"x": 0.0, "y": 9.81}
     solver = create_mpm_mls_gpu_solver(p, config)
     try:
-        bounds = solver.cfl_bounds
-        velocity = bounds["velocityBound"]
+        velocity = solver.cfl_bounds["velocityBound"]
         for _ in range(5):
+            # a recovered retry may raise the wave-speed bound: plan with the current one
+            bounds = solver.cfl_bounds
             # the scheduler's velocity envelope: current bound + |g| * duration
             envelope = calculate_mpm_cfl_velocity_bound(velocity, 1 / 120, 9.81, 0, 0, 0, 0)
             plan = calculate_mpm_cfl_microsteps(1 / 120, config["grid"]["cellSize"], bounds["waveSpeedBound"],
