@@ -179,6 +179,26 @@ int mpm_count_active_nodes(mpm_solver *solver, uint32_t counts[3]);
  * work after the solver's. */
 void *mpm_stream(mpm_solver *solver);
 
+/* ---- allocation-free cell sort ---- */
+
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (a host whose GPU memory belongs to an embedding application with a fixed
+ * budget, a frame loop that must not take an allocation's implicit device
+ * synchronisation, a foreign-function host with no allocator of its own):
+ * the stable counting sort of particles by base cell that the gather path
+ * runs (same keys, permutation and cell starts as mpm_probe_sort), with all
+ * device scratch in one static array built into the library (about 3.5 MiB
+ * held by every GPU that loads it, until exit).  `positions` are `count`
+ * (x, y) float pairs in host memory; outputs are host arrays of `count`,
+ * `count` and (cells_x+3)*(cells_y+3)+1 words.  Limits: count <= 65536 and
+ * (cells_x+3)*(cells_y+3) <= 262144, else MPM_ERR_INVALID_ARGUMENT with the
+ * reason written to `error_out` (may be NULL).  The first call on a device
+ * resolves the array's address (make it before any stream capture); calls
+ * share the array, so calls that overlap on one GPU race.  Blocks until done. */
+int mpm_cell_sort_static(int32_t device, uint32_t cells_x, uint32_t cells_y, float cell_size,
+                         const float *positions, uint32_t count, uint32_t *keys_out, uint32_t *perm_out,
+                         uint32_t *cell_start_out, char *error_out, uint32_t error_capacity);
+
 #ifdef __cplusplus
 }
 #endif
