@@ -159,14 +159,22 @@ def kernel_bytes(name: str, n: int, active: tuple) -> float:
     split of 104 B per particle + 64 B per active channel-node)."""
     channel_nodes = float(sum(active))
     table = {
-        "k_g2p": n * 104.0 + channel_nodes * 16.0,
-        "k_p2g_gather": n * 40.0 + channel_nodes * 16.0,
+        # G2P: reads x, F, volume, material (32 B), writes x, v, C, F (48 B),
+        # reads one 16 B grid record per active channel-node
+        "k_g2p": n * 80.0 + channel_nodes * 16.0,
+        # P2G: the particle state it depends on, x, v, C, F, volume, material
+        # (56 B; G2P hands it over as a prepared record), writes one 16 B sum
+        # record per active channel-node
+        "k_p2g_gather": n * 56.0 + channel_nodes * 16.0,
+        # grid update: reads the sums, writes one 16 B velocity record
+        "k_grid_from_parts": channel_nodes * 32.0,
         "k_grid_update": channel_nodes * 32.0,
-        "k_rank_prepare": n * (56.0 + 40.0 + 12.0),
         "k_prepare_scatter": n * 56.0 + channel_nodes * 16.0,
         "k_fixed_decode": channel_nodes * 16.0,
-        "k_count": n * 16.0,
-        "k_scatter": n * 16.0,
+        # tile bucketing: reads x (8 B), writes key + rank (8 B); then reads
+        # key + rank and writes the permutation (12 B)
+        "k_tile_count": n * 16.0,
+        "k_tile_scatter": n * 12.0,
     }
     return table.get(name, 0.0)
 

@@ -1,8 +1,12 @@
 // mpm_kernels.cu -- sm_100a kernels of one MLS-MPM substep.
 //
-// Substep, gather P2G (the reference default path, src/lib/mpm/kernels/solver.ts:1465-1570):
-//   k_count -> k_scan_reduce -> k_scan_top -> k_scan_apply -> k_scatter
-//   -> k_rank_prepare -> k_p2g_gather -> k_grid_update -> k_g2p -> k_commit
+// Substep, default P2G (the role of the reference's gather path,
+// src/lib/mpm/kernels/solver.ts:1465-1570):
+//   k_tile_scan -> k_tile_scatter -> k_p2g_gather -> k_grid_from_parts
+//   -> k_g2p (+ next substep's tile counts) -> k_commit
+//   (k_tile_count runs once at the start of a batch)
+// The cell sort (k_count, k_scan_*, k_scatter, k_stable_rank) backs the sort
+// probe and the allocation-free cell sort.
 // Substep, fixed-point atomic P2G (createExperimentalMpmMlsAtomicGpuSolver):
 //   k_prepare_scatter -> k_fixed_decode -> k_grid_update -> k_g2p -> k_commit
 // After a CFL-guarded batch: k_speed_max.
@@ -60,28 +64,23 @@ __device__ __forceinline__ bool make_stencil(const StepParams &P, float2 pos, St
 
 // prepareParticle: shaders.ts:808-963.  Computes the per-particle stress
 // cache (affine momentum A = m C + (-dt V 4/dx^2) P F^T), mass and current
-// liquid area.  Returns false after raising the reference's status flags.
-__device__ bool prepare_particle(const Ctx &c, uint32_t i, float4 &affine, float &mass, float &vliq,
-                                 uint32_t &model)
+// liquid area from the particle's state.  Returns 0, or the reference's
+// status flags for the failure with `indexed` telling whether the reference
+// also reports the particle index.
+__device__ __forceinline__ uint32_t prepare_core(const StepParams &P, const Material &m, float4 F, float volume,
+                                                 float damage, float pvol, float4 C, float4 &affine, float &mass,
+                                                 float &vliq, bool &indexed, float tait_pow = -1.0f)
 {
-    const StepParams &P = *c.P;
-    const float4 F = c.in.F[i];
-    const float volume = c.vol[i];
-    const Material m = c.mats[c.mat[i]];
-    model = m.model;
+    indexed = true;
     const float det = det2(F);
     if (!finite_f(det) || det <= 0.0f || !finite_f(volume) || volume <= 0.0f) {
-        fail(c.status, ERROR_DEFORMATION);
-        return false;
+        indexed = false;
+        return ERROR_DEFORMATION;
     }
     float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
     const uint32_t bad = ERROR_P2G | ERROR_P2G_INVALID_MATERIAL;
     if (m.model == MODEL_NEO_HOOKEAN) {
-        const float damage = c.in.damage[i];
-        if (!finite_f(damage) || damage < 0.0f || damage > 1.0f) {
-            fail_at(c.status, i, bad);
-            return false;
-        }
+        if (!finite_f(damage) || damage < 0.0f || damage > 1.0f) return bad;
         const float4 it = make_float4(F.w / det, -F.z / det, -F.y / det, F.x / det);
         const float pressure = m.lambda * logf(det);
         const float4 pk = make_float4(m.mu * (F.x - it.x) + pressure * it.x, m.mu * (F.y - it.y) + pressure * it.y,
@@ -92,20 +91,13 @@ __device__ bool prepare_particle(const Ctx &c, uint32_t i, float4 &affine, float
     } else if (m.model == MODEL_SNOW || m.model == MODEL_FIXED_COROTATED) {
         float hardening = 1.0f;
         if (m.model == MODEL_SNOW) {
-            const float pv = c.in.pvol[i];
-            if (!finite_f(pv) || pv < SNOW_MIN_PLASTIC_VOLUME || pv > SNOW_MAX_PLASTIC_VOLUME) {
-                fail_at(c.status, i, bad);
-                return false;
-            }
-            const float e = fminf(fmaxf(SNOW_HARDENING * (1.0f - pv), -SNOW_MAX_HARDENING_EXPONENT),
+            if (!finite_f(pvol) || pvol < SNOW_MIN_PLASTIC_VOLUME || pvol > SNOW_MAX_PLASTIC_VOLUME) return bad;
+            const float e = fminf(fmaxf(SNOW_HARDENING * (1.0f - pvol), -SNOW_MAX_HARDENING_EXPONENT),
                                   SNOW_MAX_HARDENING_EXPONENT);
             hardening = expf(e);
         }
         const Decomp d = decompose(F);
-        if (!finite_f(d.s0) || !finite_f(d.s1) || d.s0 <= 0.0f || d.s1 <= 0.0f) {
-            fail_at(c.status, i, bad);
-            return false;
-        }
+        if (!finite_f(d.s0) || !finite_f(d.s1) || d.s0 <= 0.0f || d.s1 <= 0.0f) return bad;
         const float4 R = polar_rotation(d);
         const float mu = m.mu * hardening, lambda = m.lambda * hardening;
         const float4 diff = make_float4(F.x - R.x, F.y - R.y, F.z - R.z, F.w - R.w);
@@ -115,12 +107,11 @@ __device__ bool prepare_particle(const Ctx &c, uint32_t i, float4 &affine, float
                         shear * (diff.z * F.x + diff.w * F.y), shear * (diff.z * F.z + diff.w * F.w) + volumetric);
     } else if (m.model == MODEL_WATER || m.model == MODEL_OIL) {
         if (!finite_f(m.density) || m.density <= 0.0f || !finite_f(m.lambda) || m.lambda <= 0.0f ||
-            !finite_f(m.param) || m.param < 0.0f) {
-            fail_at(c.status, i, bad);
-            return false;
-        }
+            !finite_f(m.param) || m.param < 0.0f)
+            return bad;
         if (m.param > 0.0f) {
-            const float pressure = m.lambda * (powf(__fdiv_rn(1.0f, det), m.param) - 1.0f);
+            const float pw = tait_pow >= 0.0f ? tait_pow : powf(__fdiv_rn(1.0f, det), m.param);
+            const float pressure = m.lambda * (pw - 1.0f);
             const float stress = -det * pressure;
             s = make_float4(stress, 0.f, 0.f, stress);
         } else {
@@ -128,10 +119,8 @@ __device__ bool prepare_particle(const Ctx &c, uint32_t i, float4 &affine, float
             s = make_float4(pressure, 0.f, 0.f, pressure);
         }
     } else if (m.model == MODEL_POWDER) {
-        if (!finite_f(m.lambda) || !finite_f(m.mu) || m.mu <= 0.0f || !finite_f(m.param) || m.param < 0.0f) {
-            fail_at(c.status, i, bad);
-            return false;
-        }
+        if (!finite_f(m.lambda) || !finite_f(m.mu) || m.mu <= 0.0f || !finite_f(m.param) || m.param < 0.0f)
+            return bad;
         // granularStressTimesFt: shaders.ts:408-441
         const Decomp d = decompose(F);
         const float l0 = logf(d.s0), l1 = logf(d.s1);
@@ -147,22 +136,74 @@ __device__ bool prepare_particle(const Ctx &c, uint32_t i, float4 &affine, float
         s = make_float4(p0 * d.u0.x * d.u0.x + p1 * d.u1.x * d.u1.x, p0 * d.u0.x * d.u0.y + p1 * d.u1.x * d.u1.y,
                         p0 * d.u0.y * d.u0.x + p1 * d.u1.y * d.u1.x, p0 * d.u0.y * d.u0.y + p1 * d.u1.y * d.u1.y);
     } else {
-        fail_at(c.status, i, bad);
-        return false;
+        return bad;
     }
     const bool liquid = m.model == MODEL_WATER || m.model == MODEL_OIL;
     mass = liquid ? __fmul_rn(m.density, volume) : P.particle_mass;
     vliq = liquid ? __fmul_rn(volume, det) : 0.0f;
     const float scale = -P.dt * volume * P.gradient_scale;
-    const float4 C = c.in.C[i];
     affine = make_float4(mass * C.x + scale * s.x, mass * C.y + scale * s.y, mass * C.z + scale * s.z,
                          mass * C.w + scale * s.w);
-    if (!finite4(s) || !finite4(affine)) {
-        fail_at(c.status, i, ERROR_P2G | ERROR_P2G_NONFINITE_PARTICLE);
-        return false;
-    }
-    return true;
+    if (!finite4(s) || !finite4(affine)) return ERROR_P2G | ERROR_P2G_NONFINITE_PARTICLE;
+    return 0u;
 }
+
+// prepareParticle for the particle in slot i, raising its status on failure.
+__device__ bool prepare_particle(const Ctx &c, uint32_t i, float4 &affine, float &mass, float &vliq,
+                                 uint32_t &model)
+{
+    const Material m = c.mats[c.in.mat[i]];
+    model = m.model;
+    const float damage = m.model == MODEL_NEO_HOOKEAN ? c.in.damage[i] : 0.0f;
+    const float pvol = m.model == MODEL_SNOW ? c.in.pvol[i] : 1.0f;
+    bool indexed;
+    const uint32_t flags =
+        prepare_core(*c.P, m, c.in.F[i], c.in.vol[i], damage, pvol, c.in.C[i], affine, mass, vliq, indexed);
+    if (flags == 0u) return true;
+    if (indexed)
+        fail_at(c.status, c.in.orig[i], flags);
+    else
+        fail(c.status, flags);
+    return false;
+}
+
+// Writes the P2G record of slot d for a particle with the given state and
+// base stencil (the next substep's prepareParticle, evaluated early).  A
+// failure is kept in the record and raised by the P2G that reads it, so the
+// status appears in the same substep as in the reference.
+__device__ __forceinline__ void write_record(const Ctx &c, uint32_t d, const Material &m, const Stencil &st,
+                                             float2 vel, float4 F, float volume, float damage, float pvol, float4 C,
+                                             float tait_pow = -1.0f)
+{
+    float4 A;
+    float mass, vliq;
+    bool indexed;
+    const uint32_t flags = prepare_core(*c.P, m, F, volume, damage, pvol, C, A, mass, vliq, indexed, tait_pow);
+    const uint32_t lx = (uint32_t)(st.bx + 1) % TILE_X, ly = (uint32_t)(st.by + 1) % TILE_Y;
+    const uint32_t ch = m.model == MODEL_WATER ? 1u : (m.model == MODEL_OIL ? 2u : 0u);
+    uint32_t cell = (ly * TILE_X + lx) | (ch << 8);
+    if (flags != 0u) {
+        c.rec_state[d] = make_float4(__uint_as_float(flags), __uint_as_float(indexed ? 1u : 0u), 0.f, 0.f);
+        cell |= REC_FAILED;
+    } else {
+        c.rec_state[d] = make_float4(st.fx, st.fy, mass, vliq);
+        c.rec_affine[d] = A;
+        c.rec_mom[d] = make_float2(mass * vel.x, mass * vel.y);
+    }
+    c.rec_cell[d] = cell;
+}
+
+template <int N>
+__device__ __forceinline__ void cp_async(void *dst, const void *src)
+{
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    if (N == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"(N) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 __device__ __forceinline__ uint32_t warp_sum(uint32_t v)
 {
@@ -176,6 +217,7 @@ template <int THREADS>
 __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t &total)
 {
     __shared__ uint32_t warp_totals[THREADS / 32];
+    __shared__ uint32_t s_total;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t inc = v;
 #pragma unroll
@@ -194,16 +236,27 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t &t
             if (lane >= o) wi += n;
         }
         if (lane < THREADS / 32) warp_totals[lane] = wi - w;
-        if (lane == THREADS / 32 - 1) warp_totals[THREADS / 32 - 1] += 0u;
     }
     __syncthreads();
     const uint32_t warp_offset = warp_totals[warp];
-    // total = last warp offset + last warp inclusive total
-    __shared__ uint32_t s_total;
     if (threadIdx.x == THREADS - 1) s_total = warp_offset + inc;
     __syncthreads();
     total = s_total;
     return warp_offset + inc - v;
+}
+
+// Adds one to the cell count of `key` for every active lane, one atomic per
+// distinct key in the warp; returns this lane's rank among the cell's
+// particles counted so far (ranks are made stable later).
+__device__ __forceinline__ uint32_t warp_count(uint32_t *cell_count, uint32_t key, unsigned active)
+{
+    const unsigned peers = __match_any_sync(active, key);
+    const int leader = __ffs(peers) - 1;
+    const unsigned lane = threadIdx.x & 31u;
+    uint32_t base = 0;
+    if ((int)lane == leader) base = atomicAdd(&cell_count[key], (uint32_t)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    return base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
 }
 
 }  // namespace
@@ -217,27 +270,35 @@ __global__ void k_begin_batch(Ctx c, uint32_t reset_progress)
     if (threadIdx.x == 0) {
         if (reset_progress) c.counters[COUNTER_PROGRESS] = 0u;
         c.counters[COUNTER_MAX_SPEED] = 0u;
+        for (int k = 0; k < 4; ++k) c.counters[COUNTER_ACTIVE + k] = 0u;
     }
 }
 
 // ----------------------------------------------------------- cell sort --
 
-// Base-cell key and rank within the cell for each particle; replaces the
-// per-node linked lists of insertParticleBucket (shaders.ts:657-693).
+// Base-cell key and rank within the cell of the particle in each slot;
+// replaces the per-node linked lists of insertParticleBucket
+// (shaders.ts:657-693).  Runs at the start of a batch; later substeps get
+// their counts from the previous G2P.
 __global__ void k_count(Ctx c)
 {
     const StepParams &P = *c.P;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n_particles) return;
-    if (*(volatile uint32_t *)c.status != 0u) return;
-    Stencil s;
-    if (!make_stencil(P, c.in.pos[i], s) || !stencil_fits(P, s.bx, s.by)) {
-        fail(c.status, ERROR_STENCIL);
-        return;
+    bool valid = i < P.n_particles && *(volatile uint32_t *)c.status == 0u;
+    uint32_t key = 0;
+    if (valid) {
+        Stencil s;
+        if (!make_stencil(P, c.in.pos[i], s) || !stencil_fits(P, s.bx, s.by)) {
+            fail(c.status, ERROR_STENCIL);
+            valid = false;
+        } else {
+            key = node_index(P, s.bx, s.by);
+        }
     }
-    const uint32_t key = node_index(P, s.bx, s.by);
+    const unsigned active = __ballot_sync(0xffffffffu, valid);
+    if (!valid) return;
+    c.ranks[i] = warp_count(c.cell_count, key, active);
     c.keys[i] = key;
-    c.ranks[i] = atomicAdd(&c.cell_count[key], 1u);
 }
 
 // Exclusive scan of the dense cell counts in three launches; the counts are
@@ -315,119 +376,637 @@ __global__ void k_scatter(Ctx c)
     c.tmp[c.cell_start[c.keys[i]] + c.ranks[i]] = i;
 }
 
-// Stable in-cell order (ascending particle index, i.e. a stable counting sort)
-// fused with the stress-cache preparation; writes the P2G record of each
-// particle at its sorted slot.
-__global__ void k_rank_prepare(Ctx c)
+// Stable order within each cell: ascending original particle index, so the
+// sorted order is a pure function of (cell key, original index) -- a stable
+// counting sort of the particles in their original order.
+__global__ void k_stable_rank(Ctx c)
 {
     const StepParams &P = *c.P;
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= P.n_particles) return;
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= P.n_particles) return;
     if (*(volatile uint32_t *)c.status != 0u) return;
-    const uint32_t i = c.tmp[s];
-    const uint32_t key = c.keys[i];
+    const uint32_t s = c.tmp[j];
+    const uint32_t key = c.keys[s];
+    const uint32_t id = c.in.orig[s];
     const uint32_t lo = c.cell_start[key], hi = c.cell_start[key + 1];
     uint32_t rank = 0;
-    for (uint32_t j = lo; j < hi; ++j) rank += c.tmp[j] < i ? 1u : 0u;
-    const uint32_t d = lo + rank;
-    c.perm[d] = i;
-    float4 A;
-    float mass, vliq;
-    uint32_t model;
-    if (!prepare_particle(c, i, A, mass, vliq, model)) return;
-    Stencil st;
-    make_stencil(P, c.in.pos[i], st);
-    const float2 v = c.in.vel[i];
-    const float sv = model == MODEL_WATER ? vliq : (model == MODEL_OIL ? -vliq : 0.0f);
-    c.rec0[d] = make_float4(st.fx, st.fy, mass, sv);
-    c.rec1[d] = make_float4(mass * v.x, mass * v.y, A.x, A.y);
-    c.rec2[d] = make_float2(A.z, A.w);
-    if (c.affine_out) c.affine_out[i] = A;
+    for (uint32_t t = lo; t < hi; ++t) rank += c.in.orig[c.tmp[t]] < id ? 1u : 0u;
+    c.perm[lo + rank] = s;
 }
 
-// ---------------------------------------------------------- gather P2G --
+// ----------------------------------------------- fused gather P2G + grid --
 
-// One CTA per 16x8 node tile.  Each node sums, in a fixed order (base-cell
-// rows, then cells, then ascending particle index), the contributions of the
-// particles whose 3x3 stencil covers it: the gather of shaders.ts:1072-1211
-// without linked lists and therefore deterministic.
-__global__ void __launch_bounds__(TILE_NODES) k_p2g_gather(Ctx c)
+namespace {
+
+__device__ __forceinline__ float2 finish_velocity(const StepParams &P, float mass, float px, float py, int x, int y)
+{
+    // finishGridVelocity: shaders.ts:1748-1777
+    if (mass <= 0.0f) return make_float2(0.f, 0.f);
+    float2 vel = make_float2(px / mass + P.dt * P.gx, py / mass + P.dt * P.gy);
+    if (P.drag_radius > 0.0f && x >= 0 && y >= 0 && x <= (int)P.cells_x && y <= (int)P.cells_y) {
+        const float nx = (float)x * P.dx, ny = (float)y * P.dx;
+        const float ddx = P.drag_x - nx, ddy = P.drag_y - ny;
+        const float dist = sqrtf(ddx * ddx + ddy * ddy);
+        if (dist < P.drag_radius) {
+            const float falloff = 1.0f - dist / P.drag_radius;
+            const float ax = ddx * P.drag_stiffness - vel.x * P.drag_damping;
+            const float ay = ddy * P.drag_stiffness - vel.y * P.drag_damping;
+            vel.x += P.dt * falloff * ax;
+            vel.y += P.dt * falloff * ay;
+        }
+    }
+    return vel;
+}
+
+// The node update of updateGrid (shaders.ts:1485-1746) for one node given its
+// P2G sums and the water/oil volumes of its four neighbours (xp, xm, yp, ym;
+// zero outside the halo or where no particle deposited).  Writes the
+// per-channel velocities G2P reads.  Returns false after raising a status.
+__device__ bool update_node(const Ctx &c, uint32_t n, int x, int y, float4 S, float4 W, float4 O, float2 xp,
+                            float2 xm, float2 yp, float2 ym)
 {
     const StepParams &P = *c.P;
-    const int tx = blockIdx.x, ty = blockIdx.y;
-    __shared__ uint32_t s_count;
-    if (threadIdx.x < 32) {
-        uint32_t cnt = 0;
-        const int kx0 = max(tx * TILE_X - 2, 0), kx1 = min(tx * TILE_X + TILE_X - 1, (int)P.cells_x);
-        for (int r = threadIdx.x; r < TILE_Y + 2; r += 32) {
-            const int ky = ty * TILE_Y - 2 + r;
-            if (ky >= 0 && ky <= (int)P.cells_y && kx0 <= kx1) {
-                const uint32_t row = (uint32_t)ky * P.node_w;
-                cnt += c.cell_start[row + kx1 + 1] - c.cell_start[row + kx0];
+    if (!finite_f(S.x) || S.x < 0.f || !finite_f(S.y) || !finite_f(S.z) || !finite_f(W.x) || W.x < 0.f ||
+        !finite_f(W.y) || !finite_f(W.z) || !finite_f(W.w) || W.w < 0.f || !finite_f(O.x) || O.x < 0.f ||
+        !finite_f(O.y) || !finite_f(O.z) || !finite_f(O.w) || O.w < 0.f) {
+        fail(c.status, ERROR_GRID);
+        return false;
+    }
+    float2 vs = finish_velocity(P, S.x, S.y, S.z, x, y);
+    float2 vw = finish_velocity(P, W.x, W.y, W.z, x, y);
+    float2 vo = finish_velocity(P, O.x, O.y, O.z, x, y);
+    if (x >= 0 && y >= 0 && x <= (int)P.cells_x && y <= (int)P.cells_y && W.x > 0.f && O.x > 0.f && W.w > 0.f &&
+        O.w > 0.f) {
+        // phaseVolumeGradient (shaders.ts:1779-1799): unscaled central differences
+        const float2 wgrad = make_float2(xp.x - xm.x, yp.x - ym.x);
+        const float2 ograd = make_float2(xp.y - xm.y, yp.y - ym.y);
+        const float2 sep = make_float2(ograd.x - wgrad.x, ograd.y - wgrad.y);
+        const float sl = sqrtf(sep.x * sep.x + sep.y * sep.y);
+        if (finite_f(sl) && sl > 1e-8f) {
+            float2 nrm = make_float2(sep.x / sl, sep.y / sl);
+            const float wd = W.x / W.w, od = O.x / O.w;
+            const float ds = fmaxf(wd, od);
+            const float contrast = (od - wd) / ds;
+            const float gm = sqrtf(P.gx * P.gx + P.gy * P.gy);
+            float align = 0.f;
+            if (!finite_f(wd) || wd <= 0.f || !finite_f(od) || od <= 0.f || !finite_f(contrast) || !finite_f(gm)) {
+                fail(c.status, ERROR_GRID);
+                return false;
+            }
+            if (gm > 0.f) align = (nrm.x * P.gx + nrm.y * P.gy) / gm;
+            if (!finite_f(align)) {
+                fail(c.status, ERROR_GRID);
+                return false;
+            }
+            if (contrast * align < -LIQUID_STABLE_ORDER_EPSILON) nrm = make_float2(-nrm.x, -nrm.y);
+            const float rel = (vo.x - vw.x) * nrm.x + (vo.y - vw.y) * nrm.y;
+            const float overlap = fminf(fmaxf(2.0f * fminf(W.w, O.w) / (W.w + O.w), 0.f), 1.f);
+            const float minsep = fmaxf(LIQUID_CONTACT_SEPARATION_FRACTION * overlap * P.dx / LIQUID_CONTACT_RELAXATION_SECONDS,
+                                       fmaxf(-rel, 0.f) * LIQUID_CONTACT_APPROACH_SPEED_MULTIPLIER);
+            if (rel < minsep) {
+                const float mag = (minsep - rel) / (1.0f / W.x + 1.0f / O.x);
+                const float ix = mag * nrm.x, iy = mag * nrm.y;
+                vw = make_float2(vw.x - ix / W.x, vw.y - iy / W.x);
+                vo = make_float2(vo.x + ix / O.x, vo.y + iy / O.x);
             }
         }
-        cnt = warp_sum(cnt);
-        if (threadIdx.x == 0) s_count = cnt;
+    }
+    if (!finite2(vs) || !finite2(vw) || !finite2(vo)) {
+        fail(c.status, ERROR_GRID | ERROR_TRIANGLE_CONTACT);
+        return false;
+    }
+    const int cx = (int)P.cells_x, cy = (int)P.cells_y;
+    const float fr = P.wall_friction;
+    vs.x = wall_cushion(vs.x, x, cx);
+    vs.y = wall_cushion(vs.y, y, cy);
+    vw.x = wall_cushion(vw.x, x, cx);
+    vw.y = wall_cushion(vw.y, y, cy);
+    vo.x = wall_cushion(vo.x, x, cx);
+    vo.y = wall_cushion(vo.y, y, cy);
+    vs.x = wall_friction(vs.x, y, cy, fr);
+    vs.y = wall_friction(vs.y, x, cx, fr);
+    vw.x = wall_friction(vw.x, y, cy, fr);
+    vw.y = wall_friction(vw.y, x, cx, fr);
+    vo.x = wall_friction(vo.x, y, cy, fr);
+    vo.y = wall_friction(vo.y, x, cx, fr);
+    const float lm = W.x + O.x, lv = W.w + O.w;
+    c.g_solid[n] = vs;
+    c.g_water[n] = make_float4(vw.x, vw.y, lm, lv);
+    c.g_oil[n] = make_float4(vo.x, vo.y, lm, lv);
+    return true;
+}
+
+}  // namespace
+
+// ---------------------------------------------------- tile buckets + P2G --
+
+// The tile (16x8 nodes) that holds a particle's base node; its 3x3 stencil
+// then lies in the tile's 18x10-node ring (tile plus two columns and rows).
+__device__ __forceinline__ uint32_t particle_tile(const StepParams &P, int bx, int by)
+{
+    return tile_of_node(P, (uint32_t)(bx + 1), (uint32_t)(by + 1));
+}
+
+// Batch prologue of the default path: tile key, rank within the tile and
+// P2G record of the particle in each slot (later substeps get them from G2P).
+__global__ void k_tile_count(Ctx c)
+{
+    const StepParams &P = *c.P;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool valid = i < P.n_particles && *(volatile uint32_t *)c.status == 0u;
+    uint32_t key = 0;
+    if (valid) {
+        Stencil s;
+        if (!make_stencil(P, c.in.pos[i], s) || !stencil_fits(P, s.bx, s.by)) {
+            fail(c.status, ERROR_STENCIL);
+            valid = false;
+        } else {
+            key = particle_tile(P, s.bx, s.by);
+            const Material m = c.mats[c.in.mat[i]];
+            const float damage = m.model == MODEL_NEO_HOOKEAN ? c.in.damage[i] : 0.0f;
+            const float pvol = m.model == MODEL_SNOW ? c.in.pvol[i] : 1.0f;
+            write_record(c, i, m, s, c.in.vel[i], c.in.F[i], c.in.vol[i], damage, pvol, c.in.C[i]);
+        }
+    }
+    const unsigned active = __ballot_sync(0xffffffffu, valid);
+    if (!valid) return;
+    c.ranks[i] = warp_count(c.tile_count, key, active);
+    c.keys[i] = key;
+}
+
+// Exclusive scan of the tile counts in one CTA, 8 consecutive tiles per
+// thread and pass (vector loads and stores), plus the ascending list of
+// tiles holding particles; zeroes the counts for the next substep.  Ignores
+// the status word so counts never leak into a later batch.
+__global__ void __launch_bounds__(SCAN_TOP_THREADS) k_tile_scan(Ctx c)
+{
+    constexpr int ITEMS = 8;
+    constexpr uint32_t PASS = SCAN_TOP_THREADS * ITEMS;
+    const uint32_t n_tiles = c.n_tiles;
+    uint32_t running = 0, running_active = 0;
+    for (uint32_t base = 0; base < n_tiles; base += PASS) {
+        const uint32_t first = base + threadIdx.x * ITEMS;
+        const bool whole = first + ITEMS <= n_tiles;
+        uint32_t v[ITEMS];
+        if (whole) {
+            const uint4 a = *reinterpret_cast<const uint4 *>(c.tile_count + first);
+            const uint4 b = *reinterpret_cast<const uint4 *>(c.tile_count + first + 4);
+            v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+        } else {
+#pragma unroll
+            for (int k = 0; k < ITEMS; ++k) v[k] = first + k < n_tiles ? c.tile_count[first + k] : 0u;
+        }
+        uint32_t sum = 0, nonempty = 0;
+#pragma unroll
+        for (int k = 0; k < ITEMS; ++k) {
+            sum += v[k];
+            nonempty += v[k] != 0u;
+        }
+        uint32_t total, total_active;
+        const uint32_t offset = running + block_exclusive_scan<SCAN_TOP_THREADS>(sum, total);
+        uint32_t slot = running_active + block_exclusive_scan<SCAN_TOP_THREADS>(nonempty, total_active);
+        uint32_t st[ITEMS];
+        uint32_t acc = offset;
+#pragma unroll
+        for (int k = 0; k < ITEMS; ++k) {
+            st[k] = acc;
+            acc += v[k];
+        }
+        if (whole) {
+            *reinterpret_cast<uint4 *>(c.tile_start + first) = make_uint4(st[0], st[1], st[2], st[3]);
+            *reinterpret_cast<uint4 *>(c.tile_start + first + 4) = make_uint4(st[4], st[5], st[6], st[7]);
+            *reinterpret_cast<uint4 *>(c.tile_count + first) = make_uint4(0u, 0u, 0u, 0u);
+            *reinterpret_cast<uint4 *>(c.tile_count + first + 4) = make_uint4(0u, 0u, 0u, 0u);
+        } else {
+#pragma unroll
+            for (int k = 0; k < ITEMS; ++k) {
+                if (first + k < n_tiles) {
+                    c.tile_start[first + k] = st[k];
+                    c.tile_count[first + k] = 0u;
+                }
+            }
+        }
+        if (nonempty) {
+#pragma unroll
+            for (int k = 0; k < ITEMS; ++k)
+                if (v[k] != 0u) c.active_tiles[slot++] = first + k;
+        }
+        running += total;
+        running_active += total_active;
+    }
+    if (threadIdx.x == 0) {
+        c.tile_start[n_tiles] = running;
+        c.counters[COUNTER_ACTIVE_TILES] = running_active;
+    }
+}
+
+// Bucket the slots by tile: perm[tile start + rank] = slot, four slots per
+// thread.  The status word is read along with the keys (no launch in this
+// kernel writes it): keys and ranks of a failed substep may be stale.
+__global__ void k_tile_scatter(Ctx c)
+{
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) * 4u;
+    if (i >= c.n) return;
+    const uint32_t status = __ldcg(c.status);
+    if (i + 4u <= c.n) {
+        const uint4 key = __ldcs(reinterpret_cast<const uint4 *>(c.keys + i));
+        const uint4 rank = __ldcs(reinterpret_cast<const uint4 *>(c.ranks + i));
+        if (status != 0u) return;
+        const uint32_t s0 = c.tile_start[key.x], s1 = c.tile_start[key.y], s2 = c.tile_start[key.z],
+                       s3 = c.tile_start[key.w];
+        c.perm[s0 + rank.x] = i;
+        c.perm[s1 + rank.y] = i + 1u;
+        c.perm[s2 + rank.z] = i + 2u;
+        c.perm[s3 + rank.w] = i + 3u;
+    } else {
+        if (status != 0u) return;
+        for (uint32_t j = i; j < c.n; ++j) c.perm[c.tile_start[c.keys[j]] + c.ranks[j]] = j;
+    }
+}
+
+namespace {
+
+// Shared-memory staging of the particles of one tile (or of one chunk of a
+// crowded tile): their P2G records, their grouping by base cell (in the
+// order channel, original index within a cell) and the ring accumulator.
+struct Stage {
+    float4 state[STAGE_CAP];     // fx, fy, mass, liquid volume
+    float4 affine[STAGE_CAP];    // A = m C + (-dt V 4/dx^2) P F^T
+    float2 momentum[STAGE_CAP];  // m v
+    uint32_t orig[STAGE_CAP];
+    uint32_t cell[STAGE_CAP];    // local cell | channel << 8 | REC_FAILED
+    uint16_t order[STAGE_CAP];   // arrival rank within the cell
+    uint16_t sorted[STAGE_CAP];  // staged indices grouped by cell
+    uint32_t count[TILE_CELLS];
+    uint32_t start[TILE_CELLS + 1];
+    float acc[ACC_WORDS][RING_NODES];
+    uint32_t rows[TILE_Y];
+    uint32_t staged;
+    uint32_t mask;
+    int failed;
+};
+
+__device__ __forceinline__ uint32_t sort_key(const Stage &sm, uint32_t k)
+{
+    return (((sm.cell[k] >> 8) & 3u) << 30) | sm.orig[k];
+}
+
+// Stages the records of bucket entries [i0, i1) whose local cell row lies in
+// [r0, r1) (all of them when `filtered` is false) with asynchronous copies,
+// raises the status of failed records and groups the entries by cell.  Then
+// the thread of each cell sums the P2G contributions of its particles of
+// one channel, in original-index order, over the 3x3 stencil nodes in
+// registers, and the cells add those sums into the ring accumulator in nine
+// phases, one stencil offset per phase (no two cells of a phase share a
+// node), so every sum has a fixed order.  Returns false once a record had
+// failed.
+__device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, uint32_t begin, uint32_t i0, uint32_t i1,
+                                          uint32_t r0, uint32_t r1, bool filtered)
+{
+    const StepParams &P = *c.P;
+    const uint32_t me = threadIdx.x;  // this thread's cell
+    sm.count[me] = 0u;
+    if (me == 0) sm.staged = 0u;
+    __syncthreads();
+    for (uint32_t i = i0 + me; i < i1; i += TILE_CELLS) {
+        const uint32_t s = c.perm[begin + i];
+        uint32_t k = i - i0;
+        if (filtered) {
+            const uint32_t row = (c.rec_cell[s] & 0xffu) / TILE_X;
+            if (row < r0 || row >= r1) continue;
+            k = atomicAdd(&sm.staged, 1u);
+        }
+        cp_async<16>(&sm.state[k], &c.rec_state[s]);
+        cp_async<16>(&sm.affine[k], &c.rec_affine[s]);
+        cp_async<8>(&sm.momentum[k], &c.rec_mom[s]);
+        cp_async<4>(&sm.orig[k], &c.in.orig[s]);
+        cp_async<4>(&sm.cell[k], &c.rec_cell[s]);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const uint32_t n = filtered ? sm.staged : i1 - i0;
+    uint32_t mask = 0;
+    for (uint32_t k = me; k < n; k += TILE_CELLS) {
+        const uint32_t cell = sm.cell[k];
+        if (cell & REC_FAILED) {
+            const float4 f = sm.state[k];
+            if (__float_as_uint(f.y) != 0u)
+                fail_at(c.status, sm.orig[k], __float_as_uint(f.x));
+            else
+                fail(c.status, __float_as_uint(f.x));
+            sm.failed = 1;
+            continue;
+        }
+        sm.order[k] = (uint16_t)atomicAdd(&sm.count[cell & 0xffu], 1u);
+        mask |= 1u << ((cell >> 8) & 3u);
+    }
+    if (mask) atomicOr(&sm.mask, mask);
+    __syncthreads();
+    if (sm.failed) return false;
+    // exclusive scan of the 128 cell counts (one warp, 4 cells per lane)
+    if (me < 32) {
+        const uint32_t a = sm.count[4 * me], b = sm.count[4 * me + 1], d = sm.count[4 * me + 2],
+                       e = sm.count[4 * me + 3];
+        const uint32_t t = a + b + d + e;
+        uint32_t inc = t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t up = __shfl_up_sync(0xffffffffu, inc, o);
+            if (me >= (uint32_t)o) inc += up;
+        }
+        const uint32_t ex = inc - t;
+        sm.start[4 * me] = ex;
+        sm.start[4 * me + 1] = ex + a;
+        sm.start[4 * me + 2] = ex + a + b;
+        sm.start[4 * me + 3] = ex + a + b + d;
+        if (me == 31) sm.start[TILE_CELLS] = inc;
     }
     __syncthreads();
-    if (s_count == 0u) return;
-    if (*(volatile uint32_t *)c.status != 0u) return;
-    if (threadIdx.x == 0) c.tile_stamp[ty * P.tiles_x + tx] = c.counters[COUNTER_STAMP];
-    const int hx = tx * TILE_X + (threadIdx.x % TILE_X), hy = ty * TILE_Y + (threadIdx.x / TILE_X);
-    if (hx >= (int)P.node_w || hy >= (int)P.node_h) return;
-
-    float sm = 0.f, spx = 0.f, spy = 0.f;
-    float wm = 0.f, wpx = 0.f, wpy = 0.f, wv = 0.f;
-    float om = 0.f, opx = 0.f, opy = 0.f, ov = 0.f;
+    for (uint32_t k = me; k < n; k += TILE_CELLS) sm.sorted[sm.start[sm.cell[k] & 0xffu] + sm.order[k]] = (uint16_t)k;
+    __syncthreads();
+    // each cell orders its own entries by (channel, original index)
+    const uint32_t lo = sm.start[me], hi = sm.start[me + 1];
+    for (uint32_t j = lo + 1; j < hi; ++j) {
+        const uint16_t v = sm.sorted[j];
+        const uint32_t key = sort_key(sm, v);
+        uint32_t q = j;
+        while (q > lo && sort_key(sm, sm.sorted[q - 1]) > key) {
+            sm.sorted[q] = sm.sorted[q - 1];
+            --q;
+        }
+        sm.sorted[q] = v;
+    }
+    const int cx = (int)(me % TILE_X), cy = (int)(me / TILE_X);
     const float dx = P.dx;
-    for (int oy = 0; oy < 3; ++oy) {
-        const int ky = hy - oy;
-        if (ky < 0 || ky > (int)P.cells_y) continue;
-        for (int ox = 0; ox < 3; ++ox) {
-            const int kx = hx - ox;
-            if (kx < 0 || kx > (int)P.cells_x) continue;
-            const uint32_t key = (uint32_t)ky * P.node_w + (uint32_t)kx;
-            const uint32_t lo = c.cell_start[key], hi = c.cell_start[key + 1];
-            for (uint32_t j = lo; j < hi; ++j) {
-                const float4 r0 = c.rec0[j];
-                const float4 r1 = c.rec1[j];
-                const float2 r2 = c.rec2[j];
-                const float w = quad_weight(r0.x, ox) * quad_weight(r0.y, oy);
-                const float dpx = ((float)ox - r0.x) * dx, dpy = ((float)oy - r0.y) * dx;
-                const float mx = r1.x + r1.z * dpx + r1.w * dpy;
-                const float my = r1.y + r2.x * dpx + r2.y * dpy;
-                if (!finite_f(w) || w < 0.0f || !finite_f(mx) || !finite_f(my)) {
-                    fail_at(c.status, c.perm[j], ERROR_P2G | ERROR_P2G_NONFINITE_PARTICLE);
-                    return;
-                }
-                const float wmass = w * r0.z;
-                if (r0.w > 0.0f) {
-                    wm += wmass;
-                    wpx += w * mx;
-                    wpy += w * my;
-                    wv += w * r0.w;
-                } else if (r0.w < 0.0f) {
-                    om += wmass;
-                    opx += w * mx;
-                    opy += w * my;
-                    ov += w * -r0.w;
-                } else {
-                    sm += wmass;
-                    spx += w * mx;
-                    spy += w * my;
+    const uint32_t tile_mask = sm.mask;
+    uint32_t j = lo;
+#pragma unroll 1
+    for (uint32_t ch = 0; ch < 3u; ++ch) {
+        if (!(tile_mask & (1u << ch))) continue;
+        float m[9], px[9], py[9], vl[9];
+#pragma unroll
+        for (int o = 0; o < 9; ++o) m[o] = px[o] = py[o] = vl[o] = 0.f;
+        for (; j < hi; ++j) {
+            const uint32_t k = sm.sorted[j];
+            if (((sm.cell[k] >> 8) & 3u) != ch) break;
+            const float4 q = sm.state[k];
+            const float4 A = sm.affine[k];
+            const float2 mv = sm.momentum[k];
+            float wx[3], wy[3], dpx[3], dpy[3];
+#pragma unroll
+            for (int t = 0; t < 3; ++t) {
+                wx[t] = quad_weight(q.x, t);
+                wy[t] = quad_weight(q.y, t);
+                dpx[t] = ((float)t - q.x) * dx;
+                dpy[t] = ((float)t - q.y) * dx;
+            }
+#pragma unroll
+            for (int oy = 0; oy < 3; ++oy) {
+#pragma unroll
+                for (int ox = 0; ox < 3; ++ox) {
+                    const int o = oy * 3 + ox;
+                    const float w = wx[ox] * wy[oy];
+                    const float mx = mv.x + A.x * dpx[ox] + A.y * dpy[oy];
+                    const float my = mv.y + A.z * dpx[ox] + A.w * dpy[oy];
+                    m[o] += w * q.z;
+                    px[o] += w * mx;
+                    py[o] += w * my;
+                    vl[o] += w * q.w;
                 }
             }
         }
+        const int word = ch == 0u ? 0 : (ch == 1u ? 3 : 7);
+#pragma unroll
+        for (int oy = 0; oy < 3; ++oy) {
+#pragma unroll
+            for (int ox = 0; ox < 3; ++ox) {
+                const int o = oy * 3 + ox;
+                __syncthreads();  // the previous phase's adds are done
+                const int r = (cy + oy) * RING_X + cx + ox;
+                sm.acc[word][r] += m[o];
+                sm.acc[word + 1][r] += px[o];
+                sm.acc[word + 2][r] += py[o];
+                if (ch != 0u) sm.acc[word + 3][r] += vl[o];
+            }
+        }
     }
-    if (!finite_f(sm) || !finite_f(spx) || !finite_f(spy) || !finite_f(wm) || !finite_f(wpx) || !finite_f(wpy) ||
-        !finite_f(wv) || !finite_f(om) || !finite_f(opx) || !finite_f(opy) || !finite_f(ov)) {
-        fail(c.status, ERROR_P2G | ERROR_P2G_NONFINITE_ACCUMULATION);
-        return;
+    __syncthreads();
+    return true;
+}
+
+}  // namespace
+
+// P2G (prepareParticle + the p2g of shaders.ts:808-963, :1072-1211; the
+// records carry prepareParticle's result from the previous G2P) for the
+// tiles holding particles, one tile per CTA iteration, one thread per cell.
+// The sums of a tile's particles over its 18x10-node ring have a fixed
+// order (cell-major phases, original particle index within a cell), so
+// they do not depend on the order of the tile buckets and every run is
+// bit-identical.  A tile with more than STAGE_CAP particles is taken in
+// chunks of whole cell rows (rows holding more than STAGE_CAP particles in
+// chunks of the bucket, whose order then decides the rounding of their
+// sums).  The sums go to the tile's own ring record; k_grid_from_parts adds
+// the up to four records that cover a node.
+__global__ void __launch_bounds__(TILE_CELLS) k_p2g_gather(Ctx c)
+{
+    __shared__ Stage sm;
+    const uint32_t n_active = c.counters[COUNTER_ACTIVE_TILES];
+    const uint32_t stamp = c.counters[COUNTER_STAMP];
+    for (uint32_t item = blockIdx.x; item < n_active; item += gridDim.x) {
+        if (*(volatile uint32_t *)c.status != 0u) return;
+        const uint32_t tile = c.active_tiles[item];
+        const uint32_t begin = c.tile_start[tile], n_tile = c.tile_start[tile + 1] - begin;
+        __syncthreads();  // the previous tile's readers of sm are done
+        for (int k = threadIdx.x; k < ACC_WORDS * RING_NODES; k += TILE_CELLS) (&sm.acc[0][0])[k] = 0.f;
+        if (threadIdx.x == 0) {
+            sm.failed = 0;
+            sm.mask = 0u;
+        }
+        if (n_tile > (uint32_t)STAGE_CAP) {
+            if (threadIdx.x < TILE_Y) sm.rows[threadIdx.x] = 0u;
+            __syncthreads();
+            for (uint32_t i = threadIdx.x; i < n_tile; i += TILE_CELLS)
+                atomicAdd(&sm.rows[(c.rec_cell[c.perm[begin + i]] & 0xffu) / TILE_X], 1u);
+            __syncthreads();
+        }
+        // chunks: the whole tile; or runs of whole cell rows holding at most
+        // STAGE_CAP particles, a row holding more taken in bucket chunks
+        bool ok = true;
+        uint32_t r = 0, i0 = 0;
+        while (ok && r < (uint32_t)TILE_Y) {
+            uint32_t r1 = TILE_Y, i1 = n_tile;
+            bool filtered = false;
+            if (n_tile > (uint32_t)STAGE_CAP) {
+                filtered = true;
+                if (sm.rows[r] > (uint32_t)STAGE_CAP) {
+                    r1 = r + 1;
+                    i1 = min(i0 + (uint32_t)STAGE_CAP, n_tile);
+                } else {
+                    uint32_t held = 0;
+                    r1 = r;
+                    while (r1 < (uint32_t)TILE_Y && sm.rows[r1] <= (uint32_t)STAGE_CAP &&
+                           held + sm.rows[r1] <= (uint32_t)STAGE_CAP)
+                        held += sm.rows[r1++];
+                    i0 = 0;
+                }
+            }
+            ok = p2g_chunk(c, sm, begin, i0, i1, r, r1, filtered);
+            if (filtered && r1 == r + 1 && i1 < n_tile && sm.rows[r] > (uint32_t)STAGE_CAP) {
+                i0 = i1;  // next bucket chunk of the same crowded row
+            } else {
+                r = r1;
+                i0 = 0;
+            }
+        }
+        if (!ok) return;
+        const uint32_t mask = sm.mask;
+        if (threadIdx.x == 0) c.tile_info[tile] = make_uint2(stamp, mask);
+        float *out = c.part + (size_t)tile * (ACC_WORDS * RING_NODES);
+        for (int k = threadIdx.x; k < ACC_WORDS * RING_NODES; k += TILE_CELLS) {
+            const int word = k / RING_NODES;
+            const uint32_t bit = word < 3 ? 1u : (word < 7 ? 2u : 4u);
+            if (mask & bit) out[k] = (&sm.acc[0][0])[k];
+        }
     }
-    const uint32_t n = (uint32_t)hy * P.node_w + (uint32_t)hx;
-    c.p2g_solid[n] = make_float4(sm, spx, spy, 0.f);
-    c.p2g_water[n] = make_float4(wm, wpx, wpy, wv);
-    c.p2g_oil[n] = make_float4(om, opx, opy, ov);
+}
+
+namespace {
+
+// The (up to four) tile ring records that hold sums for one halo node, in
+// the fixed order own tile, left, below, below-left: `base` is the record
+// offset of the node's first word, `mask` the record's channels (0: none).
+struct NodeSources {
+    uint32_t base[4];
+    uint32_t mask[4];
+};
+
+// Sources of halo node (hx, hy), which lies in the 3x3 tiles around tile
+// (tx, ty); info[] holds those tiles' (stamp, mask), row-major from (-1, -1).
+__device__ __forceinline__ NodeSources node_sources(const StepParams &P, const uint2 *info, int tx, int ty, int hx,
+                                                    int hy, uint32_t stamp)
+{
+    NodeSources ns;
+    const int ntx = hx / TILE_X, nty = hy / TILE_Y, lx = hx % TILE_X, ly = hy % TILE_Y;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int sx = (k & 1) ? ntx - 1 : ntx, sy = (k & 2) ? nty - 1 : nty;
+        const int rx = (k & 1) ? lx + TILE_X : lx, ry = (k & 2) ? ly + TILE_Y : ly;
+        const int ox = sx - tx, oy = sy - ty;
+        ns.base[k] = 0u;
+        ns.mask[k] = 0u;
+        if (rx >= RING_X || ry >= RING_Y || ox < -1 || ox > 1 || oy < -1 || oy > 1) continue;
+        const uint2 in = info[(oy + 1) * 3 + (ox + 1)];
+        if (in.x != stamp) continue;
+        ns.base[k] = ((uint32_t)sy * P.tiles_x + (uint32_t)sx) * (uint32_t)(ACC_WORDS * RING_NODES) +
+                     (uint32_t)(ry * RING_X + rx);
+        ns.mask[k] = in.y;
+    }
+    return ns;
+}
+
+__device__ __forceinline__ float node_word(const Ctx &c, const NodeSources &ns, int word, uint32_t channel)
+{
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (ns.mask[k] & channel) s += c.part[ns.base[k] + (uint32_t)(word * RING_NODES)];
+    return s;
+}
+
+}  // namespace
+
+// updateGrid (shaders.ts:1485-1746) over the tiles a particle reaches this
+// substep: each active tile A covers itself and, where no tile before it in
+// the order (tile, left, below, below-left) is active, its right, upper and
+// upper-right neighbours, so every reached tile is updated exactly once.
+// Node sums add the ring records in the fixed order of node_sources.  The
+// water / oil volumes of the tile's nodes and of the ring of nodes around it
+// (the neighbours phaseVolumeGradient reads) are gathered into shared memory
+// once per tile.
+__global__ void __launch_bounds__(TILE_NODES) k_grid_from_parts(Ctx c)
+{
+    const StepParams &P = *c.P;
+    __shared__ uint2 s_info[9];
+    __shared__ float2 s_vol[RING_NODES];  // nodes (x0 - 1 .. x0 + 16, y0 - 1 .. y0 + 8)
+    const uint32_t n_active = c.counters[COUNTER_ACTIVE_TILES];
+    const uint32_t stamp = c.counters[COUNTER_STAMP];
+    if (*(volatile uint32_t *)c.status != 0u) return;
+    const int tiles_x = (int)P.tiles_x, tiles_y = (int)P.tiles_y;
+    const int node_w = (int)P.node_w, node_h = (int)P.node_h;
+    const int lx = (int)(threadIdx.x % TILE_X), ly = (int)(threadIdx.x / TILE_X);
+    uint32_t ws = 0, ww = 0, wo = 0;
+    for (uint32_t item = blockIdx.x; item < 4u * n_active; item += gridDim.x) {
+        const uint32_t a = c.active_tiles[item >> 2], k = item & 3u;
+        const int tx = (int)(a % P.tiles_x) + (int)(k & 1u), ty = (int)(a / P.tiles_x) + (int)(k >> 1);
+        if (tx >= tiles_x || ty >= tiles_y) continue;
+        __syncthreads();  // readers of the previous item's shared data are done
+        if (threadIdx.x < 9) {
+            const int sx = tx + (int)(threadIdx.x % 3) - 1, sy = ty + (int)(threadIdx.x / 3) - 1;
+            s_info[threadIdx.x] = (sx >= 0 && sy >= 0 && sx < tiles_x && sy < tiles_y)
+                                      ? c.tile_info[sy * tiles_x + sx]
+                                      : make_uint2(0xffffffffu, 0u);
+        }
+        __syncthreads();
+        const bool self = s_info[4].x == stamp, left = s_info[3].x == stamp, below = s_info[1].x == stamp;
+        bool owner = true;
+        if (k == 1u) owner = !self;
+        if (k == 2u) owner = !self && !left;
+        if (k == 3u) owner = !self && !left && !below;
+        if (!owner) continue;
+        const int x0 = tx * TILE_X, y0 = ty * TILE_Y;
+        const int hx = x0 + lx, hy = y0 + ly;
+        const bool inside = hx < node_w && hy < node_h;
+        float4 S = make_float4(0.f, 0.f, 0.f, 0.f), W = S, O = S;
+        if (inside) {
+            const NodeSources ns = node_sources(P, s_info, tx, ty, hx, hy, stamp);
+            S = make_float4(node_word(c, ns, 0, 1u), node_word(c, ns, 1, 1u), node_word(c, ns, 2, 1u), 0.f);
+            W = make_float4(node_word(c, ns, 3, 2u), node_word(c, ns, 4, 2u), node_word(c, ns, 5, 2u),
+                            node_word(c, ns, 6, 2u));
+            O = make_float4(node_word(c, ns, 7, 4u), node_word(c, ns, 8, 4u), node_word(c, ns, 9, 4u),
+                            node_word(c, ns, 10, 4u));
+        }
+        s_vol[(ly + 1) * RING_X + lx + 1] = make_float2(W.w, O.w);
+        // the 52 border nodes of the 18 x 10 region
+        if (threadIdx.x < 2 * RING_X + 2 * TILE_Y) {
+            int rx, ry;
+            const int t = (int)threadIdx.x;
+            if (t < RING_X) {
+                rx = t, ry = 0;
+            } else if (t < 2 * RING_X) {
+                rx = t - RING_X, ry = RING_Y - 1;
+            } else if (t < 2 * RING_X + TILE_Y) {
+                rx = 0, ry = t - 2 * RING_X + 1;
+            } else {
+                rx = RING_X - 1, ry = t - 2 * RING_X - TILE_Y + 1;
+            }
+            const int bx = x0 - 1 + rx, by = y0 - 1 + ry;
+            float2 v = make_float2(0.f, 0.f);
+            if (bx >= 0 && by >= 0 && bx < node_w && by < node_h) {
+                const NodeSources ns = node_sources(P, s_info, tx, ty, bx, by, stamp);
+                v = make_float2(node_word(c, ns, 6, 2u), node_word(c, ns, 10, 4u));
+            }
+            s_vol[ry * RING_X + rx] = v;
+        }
+        __syncthreads();
+        if (inside) {
+            const int r = (ly + 1) * RING_X + lx + 1;
+            const uint32_t n = (uint32_t)hy * P.node_w + (uint32_t)hx;
+            if (update_node(c, n, hx - 1, hy - 1, S, W, O, s_vol[r + 1], s_vol[r - 1], s_vol[r + RING_X],
+                            s_vol[r - RING_X])) {
+                ws += S.x > 0.f;
+                ww += W.x > 0.f;
+                wo += O.x > 0.f;
+            }
+        }
+    }
+    ws = warp_sum(ws);
+    ww = warp_sum(ww);
+    wo = warp_sum(wo);
+    if ((threadIdx.x & 31u) == 0u) {
+        if (ws) atomicAdd(c.counters + COUNTER_ACTIVE, ws);
+        if (ww) atomicAdd(c.counters + COUNTER_ACTIVE + 1, ww);
+        if (wo) atomicAdd(c.counters + COUNTER_ACTIVE + 2, wo);
+    }
 }
 
 // ----------------------------------------------------- fixed-point P2G --
@@ -490,7 +1069,7 @@ __global__ void k_prepare_scatter(Ctx c)
             const float mx = __fadd_rn(__fadd_rn(__fmul_rn(mass, v.x), __fmul_rn(A.x, dpx)), __fmul_rn(A.y, dpy));
             const float my = __fadd_rn(__fadd_rn(__fmul_rn(mass, v.y), __fmul_rn(A.z, dpx)), __fmul_rn(A.w, dpy));
             if (!finite_f(w) || w < 0.0f || !finite_f(mx) || !finite_f(my)) {
-                fail_at(c.status, i, ERROR_P2G | ERROR_P2G_NONFINITE_PARTICLE);
+                fail_at(c.status, c.in.orig[i], ERROR_P2G | ERROR_P2G_NONFINITE_PARTICLE);
                 return;
             }
             const uint32_t field = node_index(P, s.bx + ox, s.by + oy) * FIXED_WORDS + channel;
@@ -528,29 +1107,7 @@ __global__ void __launch_bounds__(TILE_NODES) k_fixed_decode(Ctx c)
     c.p2g_oil[n] = make_float4(v[7] * pm, v[8] * pm, v[9] * pm, v[10] * pv);
 }
 
-// ---------------------------------------------------------- grid update --
-
 namespace {
-
-__device__ __forceinline__ float2 finish_velocity(const StepParams &P, float mass, float px, float py, int x, int y)
-{
-    // finishGridVelocity: shaders.ts:1748-1777
-    if (mass <= 0.0f) return make_float2(0.f, 0.f);
-    float2 vel = make_float2(px / mass + P.dt * P.gx, py / mass + P.dt * P.gy);
-    if (P.drag_radius > 0.0f && x >= 0 && y >= 0 && x <= (int)P.cells_x && y <= (int)P.cells_y) {
-        const float nx = (float)x * P.dx, ny = (float)y * P.dx;
-        const float ddx = P.drag_x - nx, ddy = P.drag_y - ny;
-        const float dist = sqrtf(ddx * ddx + ddy * ddy);
-        if (dist < P.drag_radius) {
-            const float falloff = 1.0f - dist / P.drag_radius;
-            const float ax = ddx * P.drag_stiffness - vel.x * P.drag_damping;
-            const float ay = ddy * P.drag_stiffness - vel.y * P.drag_damping;
-            vel.x += P.dt * falloff * ax;
-            vel.y += P.dt * falloff * ay;
-        }
-    }
-    return vel;
-}
 
 // volumeAtNode: shaders.ts:1779-1790, reading zero for tiles that no particle
 // touched this substep (their storage is stale, not cleared).
@@ -565,10 +1122,8 @@ __device__ __forceinline__ float2 phase_volume(const Ctx &c, int hx, int hy, uin
 
 }  // namespace
 
-// updateGrid: shaders.ts:1485-1746 (mass normalise, gravity, drag, water/oil
-// normal contact from phase-volume gradients, walls).  Writes the per-channel
-// velocities G2P reads, with the liquid mass/area sums packed beside the
-// water and oil velocities.
+// updateGrid of the fixed-point path: the same node update over the decoded
+// sums of touched tiles.
 __global__ void __launch_bounds__(TILE_NODES) k_grid_update(Ctx c)
 {
     const StepParams &P = *c.P;
@@ -579,76 +1134,9 @@ __global__ void __launch_bounds__(TILE_NODES) k_grid_update(Ctx c)
     const int hx = tx * TILE_X + (threadIdx.x % TILE_X), hy = ty * TILE_Y + (threadIdx.x / TILE_X);
     if (hx >= (int)P.node_w || hy >= (int)P.node_h) return;
     const uint32_t n = (uint32_t)hy * P.node_w + (uint32_t)hx;
-    const int x = hx - 1, y = hy - 1;
-    const float4 S = c.p2g_solid[n], W = c.p2g_water[n], O = c.p2g_oil[n];
-    if (!finite_f(S.x) || S.x < 0.f || !finite_f(S.y) || !finite_f(S.z) || !finite_f(W.x) || W.x < 0.f ||
-        !finite_f(W.y) || !finite_f(W.z) || !finite_f(W.w) || W.w < 0.f || !finite_f(O.x) || O.x < 0.f ||
-        !finite_f(O.y) || !finite_f(O.z) || !finite_f(O.w) || O.w < 0.f) {
-        fail(c.status, ERROR_GRID);
-        return;
-    }
-    float2 vs = finish_velocity(P, S.x, S.y, S.z, x, y);
-    float2 vw = finish_velocity(P, W.x, W.y, W.z, x, y);
-    float2 vo = finish_velocity(P, O.x, O.y, O.z, x, y);
-    if (x >= 0 && y >= 0 && x <= (int)P.cells_x && y <= (int)P.cells_y && W.x > 0.f && O.x > 0.f && W.w > 0.f &&
-        O.w > 0.f) {
-        const float2 xp = phase_volume(c, hx + 1, hy, stamp), xm = phase_volume(c, hx - 1, hy, stamp);
-        const float2 yp = phase_volume(c, hx, hy + 1, stamp), ym = phase_volume(c, hx, hy - 1, stamp);
-        const float2 wgrad = make_float2(xp.x - xm.x, yp.x - ym.x);
-        const float2 ograd = make_float2(xp.y - xm.y, yp.y - ym.y);
-        const float2 sep = make_float2(ograd.x - wgrad.x, ograd.y - wgrad.y);
-        const float sl = sqrtf(sep.x * sep.x + sep.y * sep.y);
-        if (finite_f(sl) && sl > 1e-8f) {
-            float2 nrm = make_float2(sep.x / sl, sep.y / sl);
-            const float wd = W.x / W.w, od = O.x / O.w;
-            const float ds = fmaxf(wd, od);
-            const float contrast = (od - wd) / ds;
-            const float gm = sqrtf(P.gx * P.gx + P.gy * P.gy);
-            float align = 0.f;
-            if (!finite_f(wd) || wd <= 0.f || !finite_f(od) || od <= 0.f || !finite_f(contrast) || !finite_f(gm)) {
-                fail(c.status, ERROR_GRID);
-                return;
-            }
-            if (gm > 0.f) align = (nrm.x * P.gx + nrm.y * P.gy) / gm;
-            if (!finite_f(align)) {
-                fail(c.status, ERROR_GRID);
-                return;
-            }
-            if (contrast * align < -LIQUID_STABLE_ORDER_EPSILON) nrm = make_float2(-nrm.x, -nrm.y);
-            const float rel = (vo.x - vw.x) * nrm.x + (vo.y - vw.y) * nrm.y;
-            const float overlap = fminf(fmaxf(2.0f * fminf(W.w, O.w) / (W.w + O.w), 0.f), 1.f);
-            const float minsep = fmaxf(LIQUID_CONTACT_SEPARATION_FRACTION * overlap * P.dx / LIQUID_CONTACT_RELAXATION_SECONDS,
-                                       fmaxf(-rel, 0.f) * LIQUID_CONTACT_APPROACH_SPEED_MULTIPLIER);
-            if (rel < minsep) {
-                const float mag = (minsep - rel) / (1.0f / W.x + 1.0f / O.x);
-                const float ix = mag * nrm.x, iy = mag * nrm.y;
-                vw = make_float2(vw.x - ix / W.x, vw.y - iy / W.x);
-                vo = make_float2(vo.x + ix / O.x, vo.y + iy / O.x);
-            }
-        }
-    }
-    if (!finite2(vs) || !finite2(vw) || !finite2(vo)) {
-        fail(c.status, ERROR_GRID | ERROR_TRIANGLE_CONTACT);
-        return;
-    }
-    const int cx = (int)P.cells_x, cy = (int)P.cells_y;
-    const float fr = P.wall_friction;
-    vs.x = wall_cushion(vs.x, x, cx);
-    vs.y = wall_cushion(vs.y, y, cy);
-    vw.x = wall_cushion(vw.x, x, cx);
-    vw.y = wall_cushion(vw.y, y, cy);
-    vo.x = wall_cushion(vo.x, x, cx);
-    vo.y = wall_cushion(vo.y, y, cy);
-    vs.x = wall_friction(vs.x, y, cy, fr);
-    vs.y = wall_friction(vs.y, x, cx, fr);
-    vw.x = wall_friction(vw.x, y, cy, fr);
-    vw.y = wall_friction(vw.y, x, cx, fr);
-    vo.x = wall_friction(vo.x, y, cy, fr);
-    vo.y = wall_friction(vo.y, x, cx, fr);
-    const float lm = W.x + O.x, lv = W.w + O.w;
-    c.g_solid[n] = vs;
-    c.g_water[n] = make_float4(vw.x, vw.y, lm, lv);
-    c.g_oil[n] = make_float4(vo.x, vo.y, lm, lv);
+    update_node(c, n, hx - 1, hy - 1, c.p2g_solid[n], c.p2g_water[n], c.p2g_oil[n],
+                phase_volume(c, hx + 1, hy, stamp), phase_volume(c, hx - 1, hy, stamp),
+                phase_volume(c, hx, hy + 1, stamp), phase_volume(c, hx, hy - 1, stamp));
 }
 
 // ------------------------------------------------------------------ G2P --
@@ -656,7 +1144,10 @@ __global__ void __launch_bounds__(TILE_NODES) k_grid_update(Ctx c)
 namespace {
 
 // particleWaveSpeedBound: shaders.ts:268-353
-__device__ float wave_speed_bound(const Ctx &c, const Material &m, float4 F, float damage, float volume)
+// `tait_pow` is (1 / det F)^gamma of a Tait liquid when the caller has it
+// (negative: not computed); (1 / det)^(gamma - 1) is then tait_pow * det.
+__device__ float wave_speed_bound(const Ctx &c, const Material &m, float4 F, float damage, float volume,
+                                  float tait_pow)
 {
     if (m.model == MODEL_WATER || m.model == MODEL_OIL) {
         if (!finite_f(m.lambda) || !finite_f(m.density) || m.lambda <= 0.f || m.density <= 0.f) return FLOAT_MAX;
@@ -664,7 +1155,8 @@ __device__ float wave_speed_bound(const Ctx &c, const Material &m, float4 F, flo
         if (m.param > 0.0f) {
             const float det = det2(F);
             if (!finite_f(m.param) || m.param <= 0.f || !finite_f(det) || det <= 0.f) return FLOAT_MAX;
-            c2 = m.param * c2 * powf(1.0f / det, m.param - 1.0f);
+            const float scale = tait_pow >= 0.0f ? tait_pow * det : powf(1.0f / det, m.param - 1.0f);
+            c2 = m.param * c2 * scale;
         }
         if (!finite_f(c2) || c2 < 0.f) return FLOAT_MAX;
         return sqrtf(c2);
@@ -687,30 +1179,33 @@ __device__ float wave_speed_bound(const Ctx &c, const Material &m, float4 F, flo
     return sqrtf(c2);
 }
 
-__device__ __forceinline__ void copy_particle(const Ctx &c, uint32_t i)
+__device__ __forceinline__ void copy_particle(const Ctx &c, uint32_t from, uint32_t to)
 {
-    c.out.pos[i] = c.in.pos[i];
-    c.out.vel[i] = c.in.vel[i];
-    c.out.C[i] = c.in.C[i];
-    c.out.F[i] = c.in.F[i];
-    c.out.pvol[i] = c.in.pvol[i];
-    c.out.damage[i] = c.in.damage[i];
+    c.out.pos[to] = c.in.pos[from];
+    c.out.vel[to] = c.in.vel[from];
+    c.out.C[to] = c.in.C[from];
+    c.out.F[to] = c.in.F[from];
+    c.out.pvol[to] = c.in.pvol[from];
+    c.out.damage[to] = c.in.damage[from];
+    c.out.vol[to] = c.in.vol[from];
+    c.out.mat[to] = c.in.mat[from];
+    c.out.orig[to] = c.in.orig[from];
 }
 
 // validateCflParticle: shaders.ts:2423-2454
-__device__ void validate_cfl(const Ctx &c, uint32_t i, const Material &m, float2 vel, float4 F, float damage,
-                             float volume)
+__device__ void validate_cfl(const Ctx &c, uint32_t id, const Material &m, float2 vel, float4 F, float damage,
+                             float volume, float tait_pow)
 {
     const StepParams &P = *c.P;
     if (!P.cfl_enabled) return;
     if (*(volatile uint32_t *)c.status != 0u) return;
     const float speed = length2(vel);
-    const float wave = wave_speed_bound(c, m, F, damage, volume);
+    const float wave = wave_speed_bound(c, m, F, damage, volume, tait_pow);
     if (!finite2(vel) || !finite_f(speed) || !finite_f(wave) || speed > P.cfl_velocity_limit ||
         wave > P.cfl_wave_bound) {
         const uint32_t prev = atomicOr(c.status + 6, 3u);
         if (prev == 0u) {
-            atomicExch(c.status + 1, i);
+            atomicExch(c.status + 1, id);
             atomicExch(c.status + 2, __float_as_uint(speed));
             atomicExch(c.status + 3, __float_as_uint(wave));
             atomicExch(c.status + 4, __float_as_uint(P.cfl_velocity_limit));
@@ -720,59 +1215,61 @@ __device__ void validate_cfl(const Ctx &c, uint32_t i, const Material &m, float2
     }
 }
 
-}  // namespace
-
-// g2p: shaders.ts:2114-2421 (APIC velocity and affine C, liquid
-// density-contrast acceleration, adaptive fused F update with retries,
-// per-model projection, wall confinement, fused CFL validation).
-__global__ void k_g2p(Ctx c)
+// The G2P of one particle: reads slot s, writes slot d.  Returns false when
+// the particle raised a status (its output slot is then restored by commit).
+// When the next substep's tiles are counted, `next` receives the stencil of
+// the new position and the slot's P2G record is written.
+__device__ bool g2p_particle(const Ctx &c, uint32_t s, uint32_t d, Stencil &next)
 {
     const StepParams &P = *c.P;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n_particles) return;
-    if (*(volatile uint32_t *)c.status != 0u) {
-        copy_particle(c, i);
-        return;
-    }
-    const float2 pos = c.in.pos[i];
-    Stencil s;
-    if (!make_stencil(P, pos, s) || !stencil_fits(P, s.bx, s.by)) {
+    const float2 pos = c.in.pos[s];
+    Stencil st;
+    if (!make_stencil(P, pos, st) || !stencil_fits(P, st.bx, st.by)) {
         fail(c.status, ERROR_STENCIL);
-        return;
+        return false;
     }
-    const Material m = c.mats[c.mat[i]];
+    const uint32_t id = c.in.orig[s];
+    const Material m = c.mats[c.in.mat[s]];
     const bool water = m.model == MODEL_WATER, oil = m.model == MODEL_OIL, liquid = water || oil;
+    float wx[3], wy[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        wx[k] = quad_weight(st.fx, k);
+        wy[k] = quad_weight(st.fy, k);
+    }
     float2 vel = make_float2(0.f, 0.f);
     float4 aff = make_float4(0.f, 0.f, 0.f, 0.f);
     float pmass = 0.f, pvolume = 0.f;
+    const float4 *gliq = water ? c.g_water : c.g_oil;
+#pragma unroll
     for (int oy = 0; oy < 3; ++oy) {
-        const float wy = quad_weight(s.fy, oy);
-        const float dpy = ((float)oy - s.fy) * P.dx;
+        const float dpy = ((float)oy - st.fy) * P.dx;
+        const uint32_t row = node_index(P, st.bx, st.by + oy);
+#pragma unroll
         for (int ox = 0; ox < 3; ++ox) {
-            const uint32_t n = node_index(P, s.bx + ox, s.by + oy);
-            const float w = quad_weight(s.fx, ox) * wy;
-            const float dpx = ((float)ox - s.fx) * P.dx;
+            const uint32_t n = row + ox;
+            const float w = wx[ox] * wy[oy];
+            const float dpx = ((float)ox - st.fx) * P.dx;
+            // The reference also checks w, dp, the node velocity and the
+            // node's liquid mass and volume for finiteness and sign here.
+            // None of those checks can fire on this path: w and dp are
+            // finite and w >= 0 for a finite fraction in [0.5, 1.5), and every
+            // node G2P reads was written by this substep's grid update,
+            // which raises a status (and so stops this kernel) instead of
+            // writing a non-finite velocity or a negative or non-finite sum.
             float2 gv;
             float nm = 0.f, nv = 0.f;
             if (liquid) {
-                const float4 g = water ? c.g_water[n] : c.g_oil[n];
+                const float4 g = gliq[n];
                 gv = make_float2(g.x, g.y);
                 nm = g.z;
                 nv = g.w;
             } else {
                 gv = c.g_solid[n];
             }
-            if (!finite_f(w) || w < 0.f || !finite_f(dpx) || !finite_f(dpy) || !finite2(gv)) {
-                fail(c.status, ERROR_G2P);
-                return;
-            }
             vel.x += w * gv.x;
             vel.y += w * gv.y;
             if (liquid) {
-                if (!finite_f(nm) || nm < 0.f || !finite_f(nv) || nv < 0.f) {
-                    fail_at(c.status, i, ERROR_G2P);
-                    return;
-                }
                 pmass += w * nm;
                 pvolume += w * nv;
             }
@@ -782,13 +1279,13 @@ __global__ void k_g2p(Ctx c)
             aff.w += w * gv.y * dpy;
         }
     }
-    const float4 F0 = c.in.F[i];
+    const float4 F0 = c.in.F[s];
     if (liquid) {
         const float pdet = det2(F0);
         if (!finite_f(pmass) || pmass <= 0.f || !finite_f(pvolume) || pvolume <= 0.f || !finite_f(pdet) ||
             pdet <= 0.f) {
-            fail_at(c.status, i, ERROR_G2P);
-            return;
+            fail_at(c.status, id, ERROR_G2P);
+            return false;
         }
         const float pd = m.density / pdet;
         const float ld = pmass / pvolume;
@@ -796,8 +1293,8 @@ __global__ void k_g2p(Ctx c)
         vel.x += P.dt * (rd * P.gx);
         vel.y += P.dt * (rd * P.gy);
         if (!finite_f(pd) || pd <= 0.f || !finite_f(ld) || ld <= 0.f || !finite_f(rd) || !finite2(vel)) {
-            fail_at(c.status, i, ERROR_G2P);
-            return;
+            fail_at(c.status, id, ERROR_G2P);
+            return false;
         }
     }
     const float gs = P.gradient_scale, dt = P.dt;
@@ -805,20 +1302,20 @@ __global__ void k_g2p(Ctx c)
     const float2 npos = make_float2(pos.x + dt * vel.x, pos.y + dt * vel.y);
     if (!finite2(vel) || !finite4(Cn) || !finite2(npos)) {
         fail(c.status, ERROR_G2P);
-        return;
+        return false;
     }
     const float row = fmaxf(fabsf(Cn.x) + fabsf(Cn.y), fabsf(Cn.z) + fabsf(Cn.w));
     const float inc = dt * row;
     const float req = ceilf(inc / MAX_DEFORMATION_INCREMENT);
     if (!finite_f(req) || req > MAX_DEFORMATION_SUBSTEPS) {
-        fail_at(c.status, i, ERROR_DEFORMATION_SUBSTEP_LIMIT);
-        return;
+        fail_at(c.status, id, ERROR_DEFORMATION_SUBSTEP_LIMIT);
+        return false;
     }
     uint32_t sub = max(1u, (uint32_t)req);
     float4 trial = integrate_deformation(F0, Cn, dt, sub);
     if (!finite4(trial)) {
         fail(c.status, ERROR_G2P);
-        return;
+        return false;
     }
     float tdet = det2(trial);
     while (finite_f(tdet) && tdet <= 0.f && sub < 64u) {
@@ -826,42 +1323,42 @@ __global__ void k_g2p(Ctx c)
         trial = integrate_deformation(F0, Cn, dt, sub);
         if (!finite4(trial)) {
             fail(c.status, ERROR_G2P);
-            return;
+            return false;
         }
         tdet = det2(trial);
     }
     float4 Fn = trial;
-    float pv = c.in.pvol[i];
+    float pv = c.in.pvol[s];
     if (!finite_f(tdet) || tdet <= 0.f) {
         // recordDeformationFailure: shaders.ts:224-237
         const uint32_t prev = atomicOr(c.status + 6, 1u);
         if (prev == 0u) {
-            atomicExch(c.status + 1, i);
+            atomicExch(c.status + 1, id);
             atomicExch(c.status + 2, __float_as_uint(tdet));
             atomicExch(c.status + 3, __float_as_uint(inc));
             atomicExch(c.status + 4, __float_as_uint(det2(F0)));
         }
         fail(c.status, ERROR_DEFORMATION);
-        return;
+        return false;
     }
     if (m.model == MODEL_SNOW) {
-        const Decomp d = decompose(trial);
-        if (!finite_f(d.s0) || !finite_f(d.s1) || d.s0 <= 0.f || d.s1 <= 0.f) {
+        const Decomp dd = decompose(trial);
+        if (!finite_f(dd.s0) || !finite_f(dd.s1) || dd.s0 <= 0.f || dd.s1 <= 0.f) {
             fail(c.status, ERROR_G2P);
-            return;
+            return false;
         }
         const float lo = 1.0f - SNOW_COMPRESSION_YIELD, hi = 1.0f + SNOW_STRETCH_YIELD;
-        const float a = fminf(fmaxf(d.s0, lo), hi), b = fminf(fmaxf(d.s1, lo), hi);
+        const float a = fminf(fmaxf(dd.s0, lo), hi), b = fminf(fmaxf(dd.s1, lo), hi);
         pv = fminf(fmaxf(pv * tdet / (a * b), SNOW_MIN_PLASTIC_VOLUME), SNOW_MAX_PLASTIC_VOLUME);
-        Fn = reconstruct(d, a, b);
+        Fn = reconstruct(dd, a, b);
     } else if (m.model == MODEL_POWDER) {
         if (!finite_f(m.lambda) || !finite_f(m.mu) || m.mu <= 0.f || !finite_f(m.param) || m.param < 0.f) {
             fail(c.status, ERROR_G2P);
-            return;
+            return false;
         }
         // projectGranularDeformation: shaders.ts:443-472
-        const Decomp d = decompose(trial);
-        const float l0 = logf(d.s0), l1 = logf(d.s1);
+        const Decomp dd = decompose(trial);
+        const float l0 = logf(dd.s0), l1 = logf(dd.s1);
         const float lv = l0 + l1;
         const float minlv = logf(MIN_POWDER_DETERMINANT);
         const float blv = fmaxf(minlv, lv);
@@ -871,7 +1368,7 @@ __global__ void k_g2p(Ctx c)
         if (!(dev <= maxdev && lv >= minlv)) {
             const float pdev = fminf(dev, maxdev);
             const float mean = 0.5f * blv;
-            Fn = reconstruct(d, expf(mean + pdev), expf(mean - pdev));
+            Fn = reconstruct(dd, expf(mean + pdev), expf(mean - pdev));
         }
     } else if (liquid) {
         // projectLiquidDeformation: shaders.ts:474-488
@@ -888,60 +1385,111 @@ __global__ void k_g2p(Ctx c)
         const float tr = trial.x * trial.x + trial.y * trial.y + trial.z * trial.z + trial.w * trial.w;
         if (!finite_f(tr)) {
             fail(c.status, ERROR_G2P);
-            return;
+            return false;
         }
         if (tdet < MIN_NEO_HOOKEAN_STRETCH * sqrtf(tr) || tr > MAX_NEO_HOOKEAN_STRETCH * MAX_NEO_HOOKEAN_STRETCH) {
-            const Decomp d = decompose(trial);
-            Fn = reconstruct(d, fminf(fmaxf(d.s0, MIN_NEO_HOOKEAN_STRETCH), MAX_NEO_HOOKEAN_STRETCH),
-                             fminf(fmaxf(d.s1, MIN_NEO_HOOKEAN_STRETCH), MAX_NEO_HOOKEAN_STRETCH));
+            const Decomp dd = decompose(trial);
+            Fn = reconstruct(dd, fminf(fmaxf(dd.s0, MIN_NEO_HOOKEAN_STRETCH), MAX_NEO_HOOKEAN_STRETCH),
+                             fminf(fmaxf(dd.s1, MIN_NEO_HOOKEAN_STRETCH), MAX_NEO_HOOKEAN_STRETCH));
         }
     } else if (m.model != MODEL_FIXED_COROTATED) {
         fail(c.status, ERROR_G2P);
-        return;
+        return false;
     }
     const float udet = det2(Fn);
     if (!finite4(Fn) || !finite_f(pv) || pv < SNOW_MIN_PLASTIC_VOLUME || pv > SNOW_MAX_PLASTIC_VOLUME) {
         fail(c.status, ERROR_G2P);
-        return;
+        return false;
     }
     if (!finite_f(udet) || udet <= 0.f) {
         // recordProjectedDeformationFailure: shaders.ts:239-248
         const uint32_t prev = atomicOr(c.status + 6, 2u);
         if (prev == 0u) {
-            atomicExch(c.status + 1, i);
+            atomicExch(c.status + 1, id);
             atomicExch(c.status + 2, __float_as_uint(Fn.x));
             atomicExch(c.status + 3, __float_as_uint(Fn.y));
             atomicExch(c.status + 4, __float_as_uint(Fn.z));
             atomicExch(c.status + 5, __float_as_uint(Fn.w));
         }
         fail(c.status, ERROR_PROJECTED_DEFORMATION);
-        return;
+        return false;
     }
     const float2 bx = confine_axis(npos.x, vel.x, P.domain_w);
     const float2 by = confine_axis(npos.y, vel.y, P.domain_h);
     const float2 fx = confine_axis(bx.x, bx.y, P.domain_w);
     const float2 fy = confine_axis(by.x, by.y, P.domain_h);
     const float2 outv = make_float2(fx.y, fy.y);
-    const float damage = c.in.damage[i];
-    c.out.pos[i] = make_float2(fx.x, fy.x);
-    c.out.vel[i] = outv;
-    c.out.C[i] = Cn;
-    c.out.F[i] = Fn;
-    c.out.pvol[i] = pv;
-    c.out.damage[i] = damage;
-    if (P.n_bodies == 0u) validate_cfl(c, i, m, outv, Fn, damage, c.vol[i]);
+    const float damage = c.in.damage[s];
+    const float volume = c.in.vol[s];
+    const float2 out_pos = make_float2(fx.x, fy.x);
+    c.out.pos[d] = out_pos;
+    c.out.vel[d] = outv;
+    c.out.C[d] = Cn;
+    c.out.F[d] = Fn;
+    c.out.pvol[d] = pv;
+    c.out.damage[d] = damage;
+    c.out.vol[d] = volume;
+    c.out.mat[d] = c.in.mat[s];
+    c.out.orig[d] = id;
+    // (1 / det F)^gamma of a Tait liquid, shared by the CFL wave speed and the
+    // next substep's pressure (both evaluate it at the new F)
+    float tait_pow = -1.0f;
+    if (liquid && m.param > 0.0f && finite_f(m.param)) tait_pow = powf(__fdiv_rn(1.0f, udet), m.param);
+    if (P.n_bodies == 0u) validate_cfl(c, id, m, outv, Fn, damage, volume, tait_pow);
+    if (c.count_next) {
+        if (!make_stencil(P, out_pos, next) || !stencil_fits(P, next.bx, next.by)) {
+            fail(c.status, ERROR_STENCIL);
+            return false;
+        }
+        write_record(c, d, m, next, outv, Fn, volume, damage, pv, Cn, tait_pow);
+    }
+    return true;
 }
 
-// commitParticles: shaders.ts:3067-3080.  On a failed substep every particle
-// is restored from the substep's input (whole-substep rollback); otherwise the
-// committed CFL microstep counter advances.  The substep stamp advances
-// unconditionally.
+}  // namespace
+
+// g2p: shaders.ts:2114-2421 (APIC velocity and affine C, liquid
+// density-contrast acceleration, adaptive fused F update with retries,
+// per-model projection, wall confinement, fused CFL validation).  Thread d
+// takes the particle at sorted position d (slot perm[d]) and writes slot d,
+// so the output is sorted by cell; in the gather path it also counts the
+// particle's new base cell for the next substep's sort.
+__global__ void k_g2p(Ctx c)
+{
+    const StepParams &P = *c.P;
+    const uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in_range = d < P.n_particles;
+    const uint32_t s = in_range ? (c.perm ? c.perm[d] : d) : 0u;
+    bool counted = false;
+    uint32_t key = 0;
+    if (in_range) {
+        if (*(volatile uint32_t *)c.status != 0u) {
+            copy_particle(c, d, d);  // identity: perm may be stale once a status is set
+        } else {
+            Stencil st;
+            if (g2p_particle(c, s, d, st) && c.count_next) {
+                key = particle_tile(P, st.bx, st.by);
+                counted = true;
+            }
+        }
+    }
+    if (!c.count_next) return;
+    const unsigned active = __ballot_sync(0xffffffffu, counted);
+    if (!counted) return;
+    c.ranks[d] = warp_count(c.tile_count, key, active);
+    c.keys[d] = key;
+}
+
+// commitParticles: shaders.ts:3067-3080.  On a failed substep every slot is
+// restored from the substep's input (whole-substep rollback, keeping the
+// input's slot order); otherwise the committed CFL microstep counter
+// advances.  The substep stamp advances unconditionally.
 __global__ void k_commit(Ctx c)
 {
     const StepParams &P = *c.P;
     if (*(volatile uint32_t *)c.status != 0u) {
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n_particles; i += gridDim.x * blockDim.x)
-            copy_particle(c, i);
+            copy_particle(c, i, i);
     } else if (blockIdx.x == 0 && threadIdx.x == 0 && P.cfl_enabled) {
         c.counters[COUNTER_PROGRESS] += 1u;
     }
@@ -964,8 +1512,9 @@ __global__ void k_speed_max(Ctx c)
     if ((threadIdx.x & 31) == 0) atomicMax(c.counters + COUNTER_MAX_SPEED, __float_as_uint(best));
 }
 
-// Counts the nodes of the last substep whose solid / water / oil mass is
-// positive (the N_act of the algorithmic-byte model), over stamped tiles.
+// Counts the nodes of the last fixed-point substep whose solid / water / oil
+// mass is positive (the N_ch of the algorithmic-byte model), over stamped
+// tiles.  The default path counts them inside k_grid_from_acc instead.
 __global__ void __launch_bounds__(TILE_NODES) k_count_active_nodes(Ctx c, uint32_t *counts)
 {
     const StepParams &P = *c.P;

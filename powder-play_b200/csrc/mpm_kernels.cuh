@@ -1,19 +1,25 @@
 // mpm_kernels.cuh -- kernel entry points of one MLS-MPM substep on B200.
 //
 // Data layout in HBM (all per-particle arrays are SoA, 16-byte aligned):
-//   particle state (ping-pong A/B): pos float2, vel float2, C float4, F float4,
-//     plastic volume float, damage float           -> 56 B read + 56 B write
-//   particle constants: volume float, material index u32, object id u32,
-//     bonded-vertex marker u32 (1-based like the reference record word 19)
-//   cell sort (gather P2G): key u32, rank u32, scratch index u32, permutation
-//     u32, P2G record 40 B (float4 fx,fy,m,V | float4 m*vx,m*vy,A00,A01 |
-//     float2 A10,A11) stored in sorted order
-//   halo grid, (cellsX+3) x (cellsY+3) nodes, row-major by (y+1)*W + (x+1):
-//     per-cell count/start u32; P2G sums 3 x float4 (solid m,px,py,- |
-//     water m,px,py,V | oil m,px,py,V); updated velocities solid float2,
-//     water float4 (vx,vy,mass_l,vol_l), oil float4; fixed-point words
-//     11 x i32; one stamp u32 per 16x8 node tile marks tiles touched this
-//     substep so that untouched tiles are never cleared nor read.
+//   particle state, ping-pong A/B, indexed by slot: pos float2, vel float2,
+//     C float4, F float4, plastic volume float, damage float, volume float,
+//     material index u32, original index u32.  In the gather path the slots
+//     are kept sorted by base cell: G2P of substep k reads slot perm[d] and
+//     writes slot d, so every particle kernel reads and writes coalesced.
+//   per original particle (constant): object id u32, bonded-vertex marker u32
+//   P2G records per slot (default path): float4 (fx, fy, mass, liquid
+//     volume), float4 affine momentum, float2 m v, u32 local cell | channel
+//   tile buckets: tile key u32 and rank u32 per slot, permutation u32
+//     (bucketed position -> slot), per-tile count/start u32; the cell sort of
+//     the probes adds per-cell count/start u32 and a bucket scratch u32
+//   halo grid, (cellsX+3) x (cellsY+3) nodes, row-major by (y+1)*W + (x+1),
+//     cut into 16x8-node tiles: per tile the f32 P2G sums of its particles
+//     over its 18x10-node ring (11 words, word-major) with a (stamp, channel
+//     mask) pair, and the list of tiles holding particles; updated velocities solid
+//     float2, water float4 (vx,vy,mass_l,vol_l), oil float4 -- exactly what
+//     G2P reads per channel.  The reference-exact fixed-point path adds 11
+//     i32 words per node, its decoded sums 3 x float4, and one stamp u32 per
+//     tile (tiles touched this substep).
 #pragma once
 
 #include "mpm_device.cuh"
@@ -27,31 +33,44 @@ struct ParticleBuffers {
     float4 *F;
     float *pvol;
     float *damage;
+    float *vol;
+    uint32_t *mat;
+    uint32_t *orig;
 };
 
 struct Ctx {
     const StepParams *P;
+    uint32_t n;        // particle count (fixed for a solver; kernels read it from the parameter bank)
+    uint32_t n_tiles;  // 16x8-node tiles of the halo grid
     ParticleBuffers in;
     ParticleBuffers out;
-    const float *vol;
-    const uint32_t *mat;
     const Material *mats;
-    const uint32_t *bonded;
-    const uint32_t *obj;
+    const uint32_t *bonded;  // by original index
+    const uint32_t *obj;     // by original index
     uint32_t *status;
     uint32_t *counters;
     // cell sort
     uint32_t *keys;
     uint32_t *ranks;
     uint32_t *tmp;
-    uint32_t *perm;
+    uint32_t *perm;  // sorted position -> slot (NULL: identity, fixed-point path)
     uint32_t *cell_count;
     uint32_t *cell_start;
     uint32_t *block_sums;
     uint32_t cell_pad;  // padded length of cell_count (multiple of SCAN_CHUNK)
-    float4 *rec0;
-    float4 *rec1;
-    float2 *rec2;
+    uint32_t count_next;  // G2P also counts the next substep's tiles
+    // tile buckets and the per-tile partial node sums of the default P2G
+    uint32_t *tile_count;
+    uint32_t *tile_start;    // n_tiles + 1
+    uint32_t *active_tiles;  // tiles holding particles this substep, ascending
+    float *part;             // per tile: ACC_WORDS x RING_NODES sums, word-major
+    uint2 *tile_info;        // per tile: (substep stamp of the sums, channel mask)
+    // P2G records of the particles in the input slots, written by the batch
+    // prologue and by each G2P for the next substep (default path only)
+    float4 *rec_state;   // fx, fy, mass, liquid volume (failed: flags, indexed)
+    float4 *rec_affine;  // A = m C + (-dt V 4/dx^2) P F^T
+    float2 *rec_mom;     // m v
+    uint32_t *rec_cell;  // local cell in its tile | channel << 8 | REC_FAILED
     // grid
     float4 *p2g_solid;
     float4 *p2g_water;
@@ -61,7 +80,7 @@ struct Ctx {
     float4 *g_oil;
     int32_t *fixed;
     uint32_t *tile_stamp;
-    float4 *affine_out;  // optional: prepared affine per particle (parity checks)
+    float4 *affine_out;  // optional: prepared affine per slot (parity checks)
 };
 
 constexpr int SCAN_THREADS = 512;
@@ -69,13 +88,31 @@ constexpr int SCAN_ITEMS = 8;
 constexpr int SCAN_CHUNK = SCAN_THREADS * SCAN_ITEMS;
 constexpr int SCAN_TOP_THREADS = 1024;
 
+// default P2G: the particles whose base node lies in one 16x8-node tile reach
+// the 18x10 nodes of its ring (the tile plus two columns and two rows)
+constexpr int RING_X = TILE_X + 2;
+constexpr int RING_Y = TILE_Y + 2;
+constexpr int RING_NODES = RING_X * RING_Y;
+constexpr int TILE_CELLS = TILE_X * TILE_Y;
+constexpr int STAGE_CAP = 640;  // particles staged in shared memory at once
+constexpr int ACC_WORDS = 11;   // solid m,px,py | water m,px,py,V | oil m,px,py,V
+constexpr uint32_t REC_FAILED = 1u << 16;  // the record's prepareParticle failed
+
+// device counters beyond the three of mpm_device.cuh
+constexpr int COUNTER_ACTIVE = 4;        // [4..6] active solid/water/oil nodes
+constexpr int COUNTER_ACTIVE_TILES = 7;  // tiles holding particles this substep
+
 __global__ void k_count(Ctx c);
 __global__ void k_scan_reduce(Ctx c, uint32_t n_chunks);
 __global__ void k_scan_top(Ctx c, uint32_t n_chunks);
 __global__ void k_scan_apply(Ctx c, uint32_t n_chunks);
 __global__ void k_scatter(Ctx c);
-__global__ void k_rank_prepare(Ctx c);
+__global__ void k_stable_rank(Ctx c);
+__global__ void k_tile_count(Ctx c);
+__global__ void k_tile_scan(Ctx c);
+__global__ void k_tile_scatter(Ctx c);
 __global__ void k_p2g_gather(Ctx c);
+__global__ void k_grid_from_parts(Ctx c);
 __global__ void k_prepare_scatter(Ctx c);
 __global__ void k_fixed_decode(Ctx c);
 __global__ void k_grid_update(Ctx c);

@@ -2,6 +2,10 @@
 // allocation, packing between the reference's 20-word particle record and the
 // SoA device layout, CUDA-graph capture of substep batches, and the compact
 // status/speed readback.
+//
+// In the gather path the particle slots are re-sorted by cell every substep;
+// each slot carries its original index, and every transfer at this boundary
+// (upload, readback, probes, status particle indices) speaks original indices.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -74,29 +78,34 @@ struct mpm_solver {
     uint32_t cell_pad = 0, n_chunks = 0;
     uint32_t n_bodies = 0, n_bonds = 0;
     int cur = 0;  // buffer holding the current particle state
+    uint32_t substeps_since_begin = 0;
 
     StepParams *d_params = nullptr;
     StepParams *h_params = nullptr;  // pinned staging
     cudaEvent_t params_copied = nullptr;
     uint32_t *d_status = nullptr;
     uint32_t *d_counters = nullptr;
-    uint32_t *h_readback = nullptr;  // pinned: 2 counters + 8 status words
+    uint32_t *h_readback = nullptr;  // pinned: 2 counters + 8 status words (+ spare)
 
     ParticleBuffers buf[2]{};
-    float *vol = nullptr;
-    uint32_t *mat = nullptr, *bonded = nullptr, *obj = nullptr;
+    uint32_t *bonded = nullptr, *obj = nullptr;  // by original index
     Material *d_mats = nullptr;
     std::vector<Material> mats;
 
     uint32_t *keys = nullptr, *ranks = nullptr, *tmp = nullptr, *perm = nullptr;
     uint32_t *cell_count = nullptr, *cell_start = nullptr, *block_sums = nullptr;
-    float4 *rec0 = nullptr, *rec1 = nullptr;
-    float2 *rec2 = nullptr;
     float4 *p2g_solid = nullptr, *p2g_water = nullptr, *p2g_oil = nullptr;
     float2 *g_solid = nullptr;
     float4 *g_water = nullptr, *g_oil = nullptr;
     int32_t *fixed = nullptr;
     uint32_t *tile_stamp = nullptr;
+    uint32_t *tile_count = nullptr, *tile_start = nullptr, *active_tiles = nullptr;
+    float *part = nullptr;
+    uint2 *tile_info = nullptr;
+    float4 *rec_state = nullptr, *rec_affine = nullptr;
+    float2 *rec_mom = nullptr;
+    uint32_t *rec_cell = nullptr;
+    unsigned p2g_ctas = 1, grid_ctas = 1;  // persistent grids of the default path
 
     mpm_drag drag{};
     bool drag_active = false;
@@ -107,6 +116,8 @@ struct mpm_solver {
 
     // graphs of 2^k substeps starting from buffer parity p
     std::map<std::tuple<int, int>, cudaGraphExec_t> graphs;
+
+    bool gather() const { return cfg.p2g_mode == MPM_P2G_GATHER; }
 };
 
 namespace {
@@ -115,10 +126,10 @@ Ctx make_ctx(mpm_solver *s, int parity)
 {
     Ctx c{};
     c.P = s->d_params;
+    c.n = s->n;
+    c.n_tiles = s->tiles_x * s->tiles_y;
     c.in = s->buf[parity];
     c.out = s->buf[1 - parity];
-    c.vol = s->vol;
-    c.mat = s->mat;
     c.mats = s->d_mats;
     c.bonded = s->bonded;
     c.obj = s->obj;
@@ -127,14 +138,12 @@ Ctx make_ctx(mpm_solver *s, int parity)
     c.keys = s->keys;
     c.ranks = s->ranks;
     c.tmp = s->tmp;
-    c.perm = s->perm;
+    c.perm = s->gather() ? s->perm : nullptr;
     c.cell_count = s->cell_count;
     c.cell_start = s->cell_start;
     c.block_sums = s->block_sums;
     c.cell_pad = s->cell_pad;
-    c.rec0 = s->rec0;
-    c.rec1 = s->rec1;
-    c.rec2 = s->rec2;
+    c.count_next = s->gather() ? 1u : 0u;
     c.p2g_solid = s->p2g_solid;
     c.p2g_water = s->p2g_water;
     c.p2g_oil = s->p2g_oil;
@@ -143,6 +152,15 @@ Ctx make_ctx(mpm_solver *s, int parity)
     c.g_oil = s->g_oil;
     c.fixed = s->fixed;
     c.tile_stamp = s->tile_stamp;
+    c.tile_count = s->tile_count;
+    c.tile_start = s->tile_start;
+    c.active_tiles = s->active_tiles;
+    c.part = s->part;
+    c.tile_info = s->tile_info;
+    c.rec_state = s->rec_state;
+    c.rec_affine = s->rec_affine;
+    c.rec_mom = s->rec_mom;
+    c.rec_cell = s->rec_cell;
     c.affine_out = nullptr;
     return c;
 }
@@ -153,24 +171,31 @@ constexpr unsigned PARTICLE_THREADS = 256;
 
 // Kernel slots of the profiled substep (mpm_profile_substeps).
 enum KernelSlot {
-    K_COUNT, K_SCAN_REDUCE, K_SCAN_TOP, K_SCAN_APPLY, K_SCATTER, K_RANK_PREPARE, K_P2G_GATHER,
-    K_PREPARE_SCATTER, K_FIXED_DECODE, K_GRID_UPDATE, K_G2P, K_COMMIT, K_SPEED_MAX, K_SLOTS
+    K_TILE_COUNT, K_TILE_SCAN, K_TILE_SCATTER, K_P2G_GATHER, K_GRID_FROM_PARTS, K_PREPARE_SCATTER,
+    K_FIXED_DECODE, K_GRID_UPDATE, K_G2P, K_COMMIT, K_SPEED_MAX, K_SLOTS
 };
 const char *const KERNEL_NAMES[K_SLOTS] = {
-    "k_count", "k_scan_reduce", "k_scan_top", "k_scan_apply", "k_scatter", "k_rank_prepare", "k_p2g_gather",
-    "k_prepare_scatter", "k_fixed_decode", "k_grid_update", "k_g2p", "k_commit", "k_speed_max"};
+    "k_tile_count", "k_tile_scan", "k_tile_scatter", "k_p2g_gather", "k_grid_from_parts", "k_prepare_scatter",
+    "k_fixed_decode", "k_grid_update", "k_g2p", "k_commit", "k_speed_max"};
 
 // When set, an event is recorded after every kernel launch so that the
-// kernels of a substep can be timed one by one (never during graph capture).
+// kernels of a substep can be timed one by one.  The profiled substeps are
+// captured into a graph with external event-record nodes between the
+// kernels, so host launch gaps do not enter the timings.
 struct Recorder {
     cudaStream_t stream;
     std::vector<cudaEvent_t> events;
     std::vector<int> slots;
+    cudaError_t error = cudaSuccess;
     void mark(int slot)
     {
         cudaEvent_t e;
-        cudaEventCreate(&e);
-        cudaEventRecord(e, stream);
+        cudaError_t err = cudaEventCreate(&e);
+        if (err == cudaSuccess) err = cudaEventRecordWithFlags(e, stream, cudaEventRecordExternal);
+        if (err != cudaSuccess) {
+            if (error == cudaSuccess) error = err;
+            return;
+        }
         events.push_back(e);
         slots.push_back(slot);
     }
@@ -182,22 +207,25 @@ inline void mark(int slot)
     if (g_recorder) g_recorder->mark(slot);
 }
 
-// Enqueues the cell sort (count -> scan -> scatter -> stable rank + prepare).
-void enqueue_sort(mpm_solver *s, const Ctx &c)
+// The first tile count of a batch (later substeps are counted by G2P).
+void enqueue_tile_count(mpm_solver *s, const Ctx &c)
+{
+    cudaMemsetAsync(s->tile_count, 0, (size_t)s->tiles_x * s->tiles_y * sizeof(uint32_t), s->stream);
+    k_tile_count<<<blocks_for(s->n, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c);
+    mark(K_TILE_COUNT);
+}
+
+// The cell sort of the probes: count -> scan -> scatter -> stable rank.
+void enqueue_cell_sort(mpm_solver *s, const Ctx &c)
 {
     const unsigned pb = blocks_for(s->n, PARTICLE_THREADS);
+    cudaMemsetAsync(s->cell_count, 0, (size_t)s->cell_pad * sizeof(uint32_t), s->stream);
     k_count<<<pb, PARTICLE_THREADS, 0, s->stream>>>(c);
-    mark(K_COUNT);
     k_scan_reduce<<<s->n_chunks, SCAN_THREADS, 0, s->stream>>>(c, s->n_chunks);
-    mark(K_SCAN_REDUCE);
     k_scan_top<<<1, SCAN_TOP_THREADS, 0, s->stream>>>(c, s->n_chunks);
-    mark(K_SCAN_TOP);
     k_scan_apply<<<s->n_chunks, SCAN_THREADS, 0, s->stream>>>(c, s->n_chunks);
-    mark(K_SCAN_APPLY);
     k_scatter<<<pb, PARTICLE_THREADS, 0, s->stream>>>(c);
-    mark(K_SCATTER);
-    k_rank_prepare<<<pb, PARTICLE_THREADS, 0, s->stream>>>(c);
-    mark(K_RANK_PREPARE);
+    k_stable_rank<<<pb, PARTICLE_THREADS, 0, s->stream>>>(c);
 }
 
 // One full substep from buffer `parity` into 1 - parity.
@@ -206,18 +234,23 @@ void enqueue_substep(mpm_solver *s, int parity)
     const Ctx c = make_ctx(s, parity);
     const unsigned pb = blocks_for(s->n, PARTICLE_THREADS);
     const dim3 tiles(s->tiles_x, s->tiles_y);
-    if (s->cfg.p2g_mode == MPM_P2G_FIXED_POINT) {
+    if (s->gather()) {
+        k_tile_scan<<<1, SCAN_TOP_THREADS, 0, s->stream>>>(c);
+        mark(K_TILE_SCAN);
+        k_tile_scatter<<<blocks_for((s->n + 3) / 4, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c);
+        mark(K_TILE_SCATTER);
+        k_p2g_gather<<<s->p2g_ctas, TILE_CELLS, 0, s->stream>>>(c);
+        mark(K_P2G_GATHER);
+        k_grid_from_parts<<<s->grid_ctas, TILE_NODES, 0, s->stream>>>(c);
+        mark(K_GRID_FROM_PARTS);
+    } else {
         k_prepare_scatter<<<pb, PARTICLE_THREADS, 0, s->stream>>>(c);
         mark(K_PREPARE_SCATTER);
         k_fixed_decode<<<tiles, TILE_NODES, 0, s->stream>>>(c);
         mark(K_FIXED_DECODE);
-    } else {
-        enqueue_sort(s, c);
-        k_p2g_gather<<<tiles, TILE_NODES, 0, s->stream>>>(c);
-        mark(K_P2G_GATHER);
+        k_grid_update<<<tiles, TILE_NODES, 0, s->stream>>>(c);
+        mark(K_GRID_UPDATE);
     }
-    k_grid_update<<<tiles, TILE_NODES, 0, s->stream>>>(c);
-    mark(K_GRID_UPDATE);
     k_g2p<<<pb, PARTICLE_THREADS, 0, s->stream>>>(c);
     mark(K_G2P);
     const unsigned cb = std::min(blocks_for(s->n, PARTICLE_THREADS), 592u);
@@ -330,12 +363,13 @@ uint32_t intern_material(std::vector<Material> &table, const float *w)
     return (uint32_t)(table.size() - 1);
 }
 
+// Uploads packed records in original order: slot i holds particle i.
 int unpack_and_upload(mpm_solver *s, const float *packed, uint32_t count, int target)
 {
     std::vector<float2> pos(count), vel(count);
     std::vector<float4> C(count), F(count);
     std::vector<float> pvol(count), damage(count), vol(count);
-    std::vector<uint32_t> mat(count), bonded(count);
+    std::vector<uint32_t> mat(count), bonded(count), orig(count);
     const size_t before = s->mats.size();
     for (uint32_t i = 0; i < count; ++i) {
         const float *w = packed + (size_t)i * MPM_PARTICLE_WORDS;
@@ -351,15 +385,20 @@ int unpack_and_upload(mpm_solver *s, const float *packed, uint32_t count, int ta
         vol[i] = w[17];
         mat[i] = intern_material(s->mats, w);
         bonded[i] = f2u(w[19]);
+        orig[i] = i;
         if (bonded[i] > 3u) return set_error(MPM_ERR_INVALID_ARGUMENT, "particle %u has an invalid bonded triangle marker", i);
     }
     if (s->mats.size() > 65536) return set_error(MPM_ERR_INVALID_ARGUMENT, "more than 65536 distinct materials");
     if (s->mats.size() != before || s->d_mats == nullptr) {
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
         if (s->d_mats) cudaFree(s->d_mats);
         s->d_mats = nullptr;
         CUDA_TRY(dalloc(&s->d_mats, s->mats.size()));
         CUDA_TRY(cudaMemcpyAsync(s->d_mats, s->mats.data(), s->mats.size() * sizeof(Material), cudaMemcpyHostToDevice,
                                  s->stream));
+        // captured graphs hold the old table pointer
+        for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
+        s->graphs.clear();
     }
     ParticleBuffers &b = s->buf[target];
     CUDA_TRY(cudaMemcpyAsync(b.pos, pos.data(), count * sizeof(float2), cudaMemcpyHostToDevice, s->stream));
@@ -368,10 +407,47 @@ int unpack_and_upload(mpm_solver *s, const float *packed, uint32_t count, int ta
     CUDA_TRY(cudaMemcpyAsync(b.F, F.data(), count * sizeof(float4), cudaMemcpyHostToDevice, s->stream));
     CUDA_TRY(cudaMemcpyAsync(b.pvol, pvol.data(), count * sizeof(float), cudaMemcpyHostToDevice, s->stream));
     CUDA_TRY(cudaMemcpyAsync(b.damage, damage.data(), count * sizeof(float), cudaMemcpyHostToDevice, s->stream));
-    CUDA_TRY(cudaMemcpyAsync(s->vol, vol.data(), count * sizeof(float), cudaMemcpyHostToDevice, s->stream));
-    CUDA_TRY(cudaMemcpyAsync(s->mat, mat.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(b.vol, vol.data(), count * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(b.mat, mat.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(b.orig, orig.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
     CUDA_TRY(cudaMemcpyAsync(s->bonded, bonded.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
     // the copies above read pageable host vectors; wait before they go away
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return MPM_OK;
+}
+
+// Copies the slot arrays of the current buffer to the host.
+struct HostState {
+    std::vector<float2> pos, vel;
+    std::vector<float4> C, F;
+    std::vector<float> pvol, damage, vol;
+    std::vector<uint32_t> mat, orig;
+};
+
+int download_state(mpm_solver *s, HostState &h)
+{
+    const uint32_t n = s->n;
+    h.pos.resize(n);
+    h.vel.resize(n);
+    h.C.resize(n);
+    h.F.resize(n);
+    h.pvol.resize(n);
+    h.damage.resize(n);
+    h.vol.resize(n);
+    h.mat.resize(n);
+    h.orig.resize(n);
+    const ParticleBuffers &b = s->buf[s->cur];
+    if (n > 0) {
+        CUDA_TRY(cudaMemcpyAsync(h.pos.data(), b.pos, n * sizeof(float2), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(h.vel.data(), b.vel, n * sizeof(float2), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(h.C.data(), b.C, n * sizeof(float4), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(h.F.data(), b.F, n * sizeof(float4), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(h.pvol.data(), b.pvol, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(h.damage.data(), b.damage, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(h.vol.data(), b.vol, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(h.mat.data(), b.mat, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(h.orig.data(), b.orig, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    }
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     return MPM_OK;
 }
@@ -383,14 +459,16 @@ void free_solver(mpm_solver *s)
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
     s->graphs.clear();
-    void *ptrs[] = {s->d_params, s->d_status, s->d_counters, s->vol, s->mat, s->bonded, s->obj, s->d_mats, s->keys,
-                    s->ranks, s->tmp, s->perm, s->cell_count, s->cell_start, s->block_sums, s->rec0, s->rec1, s->rec2,
-                    s->p2g_solid, s->p2g_water, s->p2g_oil, s->g_solid, s->g_water, s->g_oil, s->fixed, s->tile_stamp,
-                    s->d_active};
+    void *ptrs[] = {s->d_params, s->d_status, s->d_counters, s->bonded, s->obj, s->d_mats, s->keys, s->ranks,
+                    s->tmp, s->perm, s->cell_count, s->cell_start, s->block_sums, s->p2g_solid, s->p2g_water,
+                    s->p2g_oil, s->g_solid, s->g_water, s->g_oil, s->fixed, s->tile_stamp, s->d_active,
+                    s->tile_count, s->tile_start, s->active_tiles, s->part, s->tile_info,
+                    s->rec_state, s->rec_affine, s->rec_mom, s->rec_cell};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (int b = 0; b < 2; ++b) {
-        void *bp[] = {s->buf[b].pos, s->buf[b].vel, s->buf[b].C, s->buf[b].F, s->buf[b].pvol, s->buf[b].damage};
+        void *bp[] = {s->buf[b].pos, s->buf[b].vel, s->buf[b].C, s->buf[b].F, s->buf[b].pvol,
+                      s->buf[b].damage, s->buf[b].vol, s->buf[b].mat, s->buf[b].orig};
         for (void *p : bp)
             if (p) cudaFree(p);
     }
@@ -422,6 +500,10 @@ int create_impl(const mpm_config *config, const float *packed, const uint32_t *o
     if (c.fixed_point_shift > 30) return set_error(MPM_ERR_INVALID_ARGUMENT, "fixed_point_shift must be at most 30");
     const uint64_t nodes = ((uint64_t)c.cells_x + 3) * ((uint64_t)c.cells_y + 3);
     if (nodes > 0x7fffffffull / FIXED_WORDS)
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "halo grid dimensions exceed the GPU index range");
+    const uint64_t tile_records = (((uint64_t)c.cells_x + 3 + TILE_X - 1) / TILE_X) *
+                                  (((uint64_t)c.cells_y + 3 + TILE_Y - 1) / TILE_Y) * (ACC_WORDS * RING_NODES);
+    if (tile_records > 0xffffffffull)
         return set_error(MPM_ERR_INVALID_ARGUMENT, "halo grid dimensions exceed the GPU index range");
     if ((uint64_t)c.capacity * 9ull > 0x7fffffffull)
         return set_error(MPM_ERR_INVALID_ARGUMENT, "particle stencil entries exceed the index range");
@@ -478,30 +560,58 @@ int create_impl(const mpm_config *config, const float *packed, const uint32_t *o
         ALLOC(s->buf[b].F, cap);
         ALLOC(s->buf[b].pvol, cap);
         ALLOC(s->buf[b].damage, cap);
+        ALLOC(s->buf[b].vol, cap);
+        ALLOC(s->buf[b].mat, cap);
+        ALLOC(s->buf[b].orig, cap);
     }
-    ALLOC(s->vol, cap);
-    ALLOC(s->mat, cap);
     ALLOC(s->bonded, cap);
     ALLOC(s->obj, cap);
     ALLOC(s->keys, cap);
     ALLOC(s->ranks, cap);
     ALLOC(s->tmp, cap);
     ALLOC(s->perm, cap);
-    ALLOC(s->rec0, cap);
-    ALLOC(s->rec1, cap);
-    ALLOC(s->rec2, cap);
     ALLOC(s->cell_count, s->cell_pad);
     ALLOC(s->cell_start, (size_t)s->cell_pad + 1);
     ALLOC(s->block_sums, (size_t)s->n_chunks + 1);
-    ALLOC(s->p2g_solid, s->node_count);
-    ALLOC(s->p2g_water, s->node_count);
-    ALLOC(s->p2g_oil, s->node_count);
     ALLOC(s->g_solid, s->node_count);
     ALLOC(s->g_water, s->node_count);
     ALLOC(s->g_oil, s->node_count);
+    cudaMemsetAsync(s->g_solid, 0, (size_t)s->node_count * sizeof(float2), s->stream);
+    cudaMemsetAsync(s->g_water, 0, (size_t)s->node_count * sizeof(float4), s->stream);
+    cudaMemsetAsync(s->g_oil, 0, (size_t)s->node_count * sizeof(float4), s->stream);
     ALLOC(s->tile_stamp, (size_t)s->tiles_x * s->tiles_y);
     ALLOC(s->d_active, 4);
+    const size_t n_tiles = (size_t)s->tiles_x * s->tiles_y;
+    ALLOC(s->tile_count, n_tiles);
+    ALLOC(s->tile_start, n_tiles + 1);
+    if (c.p2g_mode == MPM_P2G_GATHER) {
+        ALLOC(s->active_tiles, n_tiles);
+        ALLOC(s->part, n_tiles * ACC_WORDS * RING_NODES);
+        ALLOC(s->tile_info, n_tiles);
+        ALLOC(s->rec_state, cap);
+        ALLOC(s->rec_affine, cap);
+        ALLOC(s->rec_mom, cap);
+        ALLOC(s->rec_cell, cap);
+        if (cudaMemsetAsync(s->tile_info, 0xff, n_tiles * sizeof(uint2), s->stream) != cudaSuccess ||
+            cudaMemsetAsync(s->tile_count, 0, n_tiles * sizeof(uint32_t), s->stream) != cudaSuccess)
+            return fail(set_error(MPM_ERR_CUDA, "cudaMemset failed"));
+        int sms = 0, per_sm_p2g = 0, per_sm_grid = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device) != cudaSuccess ||
+            cudaFuncSetAttribute(k_p2g_gather, cudaFuncAttributePreferredSharedMemoryCarveout, 100) !=
+                cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_p2g, k_p2g_gather, TILE_CELLS, 0) !=
+                cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_grid, k_grid_from_parts, TILE_NODES, 0) !=
+                cudaSuccess)
+            return fail(set_error(MPM_ERR_CUDA, "occupancy query failed"));
+        s->p2g_ctas = (unsigned)std::max<size_t>(1, std::min<size_t>(n_tiles, (size_t)sms * std::max(1, per_sm_p2g)));
+        s->grid_ctas =
+            (unsigned)std::max<size_t>(1, std::min<size_t>(4 * n_tiles, (size_t)sms * std::max(1, per_sm_grid)));
+    }
     if (c.p2g_mode == MPM_P2G_FIXED_POINT) {
+        ALLOC(s->p2g_solid, s->node_count);
+        ALLOC(s->p2g_water, s->node_count);
+        ALLOC(s->p2g_oil, s->node_count);
         ALLOC(s->fixed, (size_t)s->node_count * FIXED_WORDS);
         if (cudaMemsetAsync(s->fixed, 0, (size_t)s->node_count * FIXED_WORDS * sizeof(int32_t), s->stream) != cudaSuccess)
             return fail(set_error(MPM_ERR_CUDA, "cudaMemset failed"));
@@ -565,6 +675,8 @@ int mpm_step_batch(mpm_solver *s, uint32_t step_count, float dt, float gx, float
     const Ctx c0 = make_ctx(s, s->cur);
     CUDA_TRY(cudaEventRecord(s->batch_start, s->stream));
     k_begin_batch<<<1, 32, 0, s->stream>>>(c0, guard ? 1u : 0u);
+    s->substeps_since_begin = 0;
+    if (s->gather() && s->n > 0) enqueue_tile_count(s, c0);
     CUDA_TRY(cudaGetLastError());
     if (s->n > 0) {
         uint32_t remaining = step_count;
@@ -576,6 +688,7 @@ int mpm_step_batch(mpm_solver *s, uint32_t step_count, float dt, float gx, float
             CUDA_TRY(cudaGraphLaunch(exec, s->stream));
             if (k == 0) s->cur = 1 - s->cur;  // only an odd substep count flips the buffer
         }
+        s->substeps_since_begin = step_count;
     }
     if (guard) {
         const Ctx c1 = make_ctx(s, s->cur);
@@ -618,21 +731,34 @@ int mpm_profile_substeps(mpm_solver *s, uint32_t step_count, float dt, float gx,
     Recorder rec;
     rec.stream = s->stream;
     const Ctx c0 = make_ctx(s, s->cur);
+    const int start_parity = s->cur;
+    CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
     k_begin_batch<<<1, 32, 0, s->stream>>>(c0, guard ? 1u : 0u);
     rec.mark(-1);
     g_recorder = &rec;
+    if (s->gather() && s->n > 0) enqueue_tile_count(s, c0);
+    int parity = start_parity;
     for (uint32_t k = 0; k < step_count; ++k) {
-        enqueue_substep(s, s->cur);
-        s->cur = 1 - s->cur;
+        enqueue_substep(s, parity);
+        parity = 1 - parity;
     }
     if (guard) {
-        const Ctx c1 = make_ctx(s, s->cur);
+        const Ctx c1 = make_ctx(s, parity);
         k_speed_max<<<std::min(blocks_for(s->n, PARTICLE_THREADS), 592u), PARTICLE_THREADS, 0, s->stream>>>(c1);
         mark(K_SPEED_MAX);
     }
     g_recorder = nullptr;
-    cudaError_t e = cudaGetLastError();
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+    if (e == cudaSuccess) e = rec.error;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e == cudaSuccess) {
+        s->cur = parity;
+        s->substeps_since_begin = step_count;
+    }
     for (size_t k = 1; e == cudaSuccess && k < rec.events.size(); ++k) {
         float ms = 0.0f;
         e = cudaEventElapsedTime(&ms, rec.events[k - 1], rec.events[k]);
@@ -641,6 +767,8 @@ int mpm_profile_substeps(mpm_solver *s, uint32_t step_count, float dt, float gx,
             kernel_launches[rec.slots[k]] += 1;
         }
     }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
     for (cudaEvent_t ev : rec.events) cudaEventDestroy(ev);
     if (e != cudaSuccess) return set_error(MPM_ERR_CUDA, "profiled substeps failed: %s", cudaGetErrorString(e));
     return MPM_OK;
@@ -655,6 +783,15 @@ int mpm_count_active_nodes(mpm_solver *s, uint32_t counts[3])
     g_last_error.clear();
     if (!s || !counts) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and counts must not be NULL");
     CUDA_TRY(cudaSetDevice(s->device));
+    if (s->gather()) {
+        // accumulated by k_p2g_grid since the last batch began: average per substep
+        CUDA_TRY(cudaMemcpyAsync(s->h_readback, s->d_counters + COUNTER_ACTIVE, 3 * sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
+        const uint32_t steps = std::max(1u, s->substeps_since_begin);
+        for (int k = 0; k < 3; ++k) counts[k] = s->h_readback[k] / steps;
+        return MPM_OK;
+    }
     CUDA_TRY(cudaMemsetAsync(s->d_active, 0, 4 * sizeof(uint32_t), s->stream));
     const Ctx c = make_ctx(s, s->cur);
     k_count_active_nodes<<<dim3(s->tiles_x, s->tiles_y), TILE_NODES, 0, s->stream>>>(c, s->d_active);
@@ -709,47 +846,43 @@ int mpm_read_particles(mpm_solver *s, const uint32_t *indices, uint32_t count, f
         if (indices[k] >= s->n) return set_error(MPM_ERR_INVALID_ARGUMENT, "particleIndices must identify active GPU particles.");
     CUDA_TRY(cudaSetDevice(s->device));
     const uint32_t n = s->n;
-    std::vector<float2> pos(n), vel(n);
-    std::vector<float4> C(n), F(n);
-    std::vector<float> pvol(n), damage(n), vol(n);
-    std::vector<uint32_t> mat(n), bonded(n), obj(n);
-    const ParticleBuffers &b = s->buf[s->cur];
+    HostState h;
+    int rc = download_state(s, h);
+    if (rc != MPM_OK) return rc;
+    std::vector<uint32_t> bonded(n), obj(n), slot_of(n);
     if (n > 0) {
-        CUDA_TRY(cudaMemcpyAsync(pos.data(), b.pos, n * sizeof(float2), cudaMemcpyDeviceToHost, s->stream));
-        CUDA_TRY(cudaMemcpyAsync(vel.data(), b.vel, n * sizeof(float2), cudaMemcpyDeviceToHost, s->stream));
-        CUDA_TRY(cudaMemcpyAsync(C.data(), b.C, n * sizeof(float4), cudaMemcpyDeviceToHost, s->stream));
-        CUDA_TRY(cudaMemcpyAsync(F.data(), b.F, n * sizeof(float4), cudaMemcpyDeviceToHost, s->stream));
-        CUDA_TRY(cudaMemcpyAsync(pvol.data(), b.pvol, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
-        CUDA_TRY(cudaMemcpyAsync(damage.data(), b.damage, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
-        CUDA_TRY(cudaMemcpyAsync(vol.data(), s->vol, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
-        CUDA_TRY(cudaMemcpyAsync(mat.data(), s->mat, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
         CUDA_TRY(cudaMemcpyAsync(bonded.data(), s->bonded, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
         CUDA_TRY(cudaMemcpyAsync(obj.data(), s->obj, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
     }
-    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    for (uint32_t d = 0; d < n; ++d) {
+        if (h.orig[d] >= n) return set_error(MPM_ERR_CUDA, "corrupt particle slot map");
+        slot_of[h.orig[d]] = d;
+    }
     for (uint32_t k = 0; k < count; ++k) {
         const uint32_t i = indices ? indices[k] : k;
+        const uint32_t d = slot_of[i];
         float *w = packed_out + (size_t)k * MPM_PARTICLE_WORDS;
-        const Material &m = s->mats[mat[i]];
-        w[0] = pos[i].x;
-        w[1] = pos[i].y;
-        w[2] = vel[i].x;
-        w[3] = vel[i].y;
-        w[4] = C[i].x;
-        w[5] = C[i].y;
-        w[6] = C[i].z;
-        w[7] = C[i].w;
-        w[8] = F[i].x;
-        w[9] = F[i].y;
-        w[10] = F[i].z;
-        w[11] = F[i].w;
-        w[12] = pvol[i];
+        const Material &m = s->mats[h.mat[d]];
+        w[0] = h.pos[d].x;
+        w[1] = h.pos[d].y;
+        w[2] = h.vel[d].x;
+        w[3] = h.vel[d].y;
+        w[4] = h.C[d].x;
+        w[5] = h.C[d].y;
+        w[6] = h.C[d].z;
+        w[7] = h.C[d].w;
+        w[8] = h.F[d].x;
+        w[9] = h.F[d].y;
+        w[10] = h.F[d].z;
+        w[11] = h.F[d].w;
+        w[12] = h.pvol[d];
         w[13] = u2f(m.model);
         w[14] = m.lambda;
         w[15] = m.mu;
         w[16] = m.density;
-        w[17] = vol[i];
-        w[18] = m.model == MODEL_NEO_HOOKEAN ? damage[i] : m.param;
+        w[17] = h.vol[d];
+        w[18] = m.model == MODEL_NEO_HOOKEAN ? h.damage[d] : m.param;
         w[19] = u2f(bonded[i]);
         if (object_ids_out) object_ids_out[k] = obj[i];
     }
@@ -811,19 +944,30 @@ int mpm_probe_sort(mpm_solver *s, float dt, uint32_t *keys_out, uint32_t *perm_o
 {
     g_last_error.clear();
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
-    if (s->cfg.p2g_mode != MPM_P2G_GATHER) return set_error(MPM_ERR_STATE, "the cell sort runs in gather mode only");
+    if (!s->gather()) return set_error(MPM_ERR_STATE, "the cell sort runs in gather mode only");
     CUDA_TRY(cudaSetDevice(s->device));
     int rc = upload_params(s, dt, 0.0f, 0.0f, nullptr, 0.0f);
     if (rc != MPM_OK) return rc;
     const Ctx c = make_ctx(s, s->cur);
-    enqueue_sort(s, c);
+    enqueue_cell_sort(s, c);
     CUDA_TRY(cudaGetLastError());
-    if (keys_out) CUDA_TRY(cudaMemcpyAsync(keys_out, s->keys, s->n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
-    if (perm_out) CUDA_TRY(cudaMemcpyAsync(perm_out, s->perm, s->n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    const uint32_t n = s->n;
+    std::vector<uint32_t> keys(n), perm(n), orig(n);
+    if (n > 0) {
+        CUDA_TRY(cudaMemcpyAsync(keys.data(), s->keys, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(perm.data(), s->perm, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(orig.data(), s->buf[s->cur].orig, n * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                 s->stream));
+    }
     if (cell_start_out)
         CUDA_TRY(cudaMemcpyAsync(cell_start_out, s->cell_start, ((size_t)s->node_count + 1) * sizeof(uint32_t),
                                  cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
+    // report by original particle index
+    for (uint32_t slot = 0; slot < n; ++slot)
+        if (keys_out) keys_out[orig[slot]] = keys[slot];
+    for (uint32_t d = 0; d < n; ++d)
+        if (perm_out) perm_out[d] = orig[perm[d]];
     return MPM_OK;
 }
 

@@ -74,6 +74,25 @@ def test_cell_sort_is_a_bit_exact_stable_counting_sort():
     assert np.array_equal(starts.astype(np.int64), np.concatenate(([0], np.cumsum(counts))))
 
 
+def test_cell_sort_stays_canonical_after_steps():
+    # after the slots have been re-sorted by several substeps, the sort is still
+    # the stable counting sort of the particles in their original order
+    p, config = create_si_tank_scene(seed=9)
+    solver = create_mpm_mls_gpu_solver(p, config)
+    try:
+        solver.step_batch(7, 2e-4, {"x": 0.0, "y": -9.81})
+        packed, _ = solver.read_particles_packed()
+        keys, perm, starts = solver.probe_sort(2e-4)
+    finally:
+        solver.dispose()
+    dx = np.float32(config["grid"]["cellSize"])
+    g = (packed[:, 0:2] / dx).astype(np.float32)
+    base = np.floor((g - np.float32(0.5)).astype(np.float32)).astype(np.int64)
+    expected_keys = (base[:, 1] + 1) * (config["grid"]["cellsX"] + 3) + (base[:, 0] + 1)
+    assert np.array_equal(keys.astype(np.int64), expected_keys)
+    assert np.array_equal(perm.astype(np.int64), np.argsort(expected_keys, kind="stable"))
+
+
 def _mixed_liquid_scene(seed=3, n_side=48):
     rng = np.random.default_rng(seed)
     n = n_side * n_side
@@ -175,6 +194,46 @@ def test_si_tank_scene_matches_the_oracle_and_is_deterministic():
     again, _ = _run_parity(p, config, gravity, plan["microDt"], 60, create_mpm_mls_gpu_solver)
     for key in gpu:
         assert np.array_equal(gpu[key], again[key])
+
+
+def _crowded_scene(per_side, seed=5):
+    # a 16 x 8-cell block at per_side^2 particles per cell: more particles in
+    # one tile than the P2G stages at once (640), and at per_side 8 more than
+    # that in a single cell row
+    rng = np.random.default_rng(seed)
+    dx = 10.0
+    spacing = dx / per_side
+    nx, ny = 16 * per_side, 8 * per_side
+    r, c = np.divmod(np.arange(nx * ny), nx)
+    p = ParticleArrays.empty(nx * ny)
+    p.px[:] = 60 + (c + 0.5) * spacing + rng.uniform(-0.1, 0.1, nx * ny) * spacing
+    p.py[:] = 60 + (r + 0.5) * spacing + rng.uniform(-0.1, 0.1, nx * ny) * spacing
+    p.vx[:] = rng.uniform(-2, 2, nx * ny)
+    p.vy[:] = rng.uniform(-2, 2, nx * ny)
+    water = {"lambda": 40_000, "mu": 0, "model": "water", "density": 0.02}
+    oil = {"lambda": 30_000, "mu": 0, "model": "oil", "density": 0.016}
+    p.materials = [water, oil]
+    p.material[:] = (c >= nx // 2).astype(np.int32)
+    p.volume[:] = spacing * spacing
+    config = {"grid": {"cellsX": 40, "cellsY": 40, "cellSize": dx}, "particleMass": 0.02 * spacing * spacing,
+              "particleVolume": spacing * spacing, "material": water}
+    return p, config
+
+
+@pytest.mark.parametrize("per_side", [5, 8])
+def test_crowded_tiles_match_the_oracle(per_side):
+    p, config = _crowded_scene(per_side)
+    gravity = {"x": 0.0, "y": -9.81}
+    gpu, ref = _run_parity(p, config, gravity, 2e-4, 12, create_mpm_mls_gpu_solver)
+    dx = config["grid"]["cellSize"]
+    assert np.max(np.abs(gpu["position"] - ref["position"])) <= 1e-3 * dx
+    vel_err = np.max(np.abs(gpu["velocity"] - ref["velocity"]) / (1 + np.abs(ref["velocity"])))
+    assert vel_err <= 1e-3, vel_err
+    if per_side == 5:
+        # tiles taken in chunks of whole cell rows keep a fixed summation order
+        again, _ = _run_parity(p, config, gravity, 2e-4, 12, create_mpm_mls_gpu_solver)
+        for key in gpu:
+            assert np.array_equal(gpu[key], again[key])
 
 
 def test_multi_material_models_match_the_oracle():
