@@ -94,7 +94,7 @@ struct alignas(16) StepParams {
     float bond_rest_length, bond_stiffness, band, contact_reach;
     float cfl_wave_bound, cfl_velocity_limit, bond_reference_dt, wall_friction;
     float fixed_scale, drag_x, drag_y, drag_radius;
-    float drag_stiffness, drag_damping, pad1, pad2;
+    float drag_stiffness, drag_damping, inv_dx, pad1;
 };
 
 // Device counters (one 32-word line): stamp of the current substep, committed
@@ -179,7 +179,7 @@ __device__ __forceinline__ float4 reconstruct(const Decomp &d, float a, float b)
 // rounded separately and every row-column product keeps one fused term.
 __device__ __forceinline__ float4 integrate_deformation(float4 f, float4 c, float dt, uint32_t substeps)
 {
-    float h = __fdiv_rn(dt, (float)substeps);
+    float h = substeps == 1u ? dt : __fdiv_rn(dt, (float)substeps);
     float4 u = make_float4(__fadd_rn(1.0f, __fmul_rn(h, c.x)), __fmul_rn(h, c.y), __fmul_rn(h, c.z),
                            __fadd_rn(1.0f, __fmul_rn(h, c.w)));
     float4 r = f;
@@ -199,10 +199,13 @@ __device__ __forceinline__ float2 confine_axis(float next, float vel, float maxi
 }
 
 // applyWallCushion / applyWallTangentialFriction: shaders.ts:1438-1457
+// (dist / cushion clamped to [0, 1] is exactly 1 once dist >= cushion, so
+// nodes away from the walls skip the division.)
 __device__ __forceinline__ float wall_cushion(float vel, int coord, int extent)
 {
     float cushion = fminf(WALL_CUSHION_CELLS, (float)extent / 4.0f);
     float dist = vel < 0.0f ? (float)coord : (float)(extent - coord);
+    if (dist >= cushion) return vel;
     return vel * fminf(fmaxf(dist / cushion, 0.0f), 1.0f);
 }
 
@@ -211,6 +214,7 @@ __device__ __forceinline__ float wall_friction(float vel, int coord, int extent,
     if (friction <= 0.0f) return vel;
     float dist = fmaxf(0.0f, fminf((float)coord, (float)(extent - coord)));
     float cushion = fminf(WALL_CUSHION_CELLS, (float)extent / 4.0f);
+    if (dist >= cushion) return vel;
     float influence = 1.0f - fminf(fmaxf(dist / cushion, 0.0f), 1.0f);
     return vel * (1.0f - friction * influence);
 }

@@ -2,8 +2,8 @@
 //
 // Substep, default P2G (the role of the reference's gather path,
 // src/lib/mpm/kernels/solver.ts:1465-1570):
-//   k_tile_scan -> k_tile_scatter -> k_p2g_gather -> k_grid_from_parts
-//   -> k_g2p (+ next substep's tile counts) -> k_commit
+//   k_tile_scan -> k_tile_scatter -> k_p2g_gather
+//   -> k_g2p_tile (grid update + G2P + next substep's tile counts) -> k_commit
 //   (k_tile_count runs once at the start of a batch)
 // The cell sort (k_count, k_scan_*, k_scatter, k_stable_rank) backs the sort
 // probe and the allocation-free cell sort.
@@ -50,9 +50,8 @@ struct Stencil {
     float fx, fy;
 };
 
-__device__ __forceinline__ bool make_stencil(const StepParams &P, float2 pos, Stencil &s)
+__device__ __forceinline__ bool stencil_from_grid(float gx, float gy, Stencil &s)
 {
-    float gx = __fdiv_rn(pos.x, P.dx), gy = __fdiv_rn(pos.y, P.dx);
     if (!finite_f(gx) || !finite_f(gy)) return false;
     float fbx = floorf(__fsub_rn(gx, 0.5f)), fby = floorf(__fsub_rn(gy, 0.5f));
     s.bx = (int)fbx;
@@ -61,6 +60,26 @@ __device__ __forceinline__ bool make_stencil(const StepParams &P, float2 pos, St
     s.fy = __fsub_rn(gy, (float)s.by);
     return true;
 }
+
+// Grid coordinates by a correctly rounded division (the cell sort probes and
+// the fixed-point path, whose CPU emulation divides the same way).
+__device__ __forceinline__ bool make_stencil(const StepParams &P, float2 pos, Stencil &s)
+{
+    return stencil_from_grid(__fdiv_rn(pos.x, P.dx), __fdiv_rn(pos.y, P.dx), s);
+}
+
+// Grid coordinates as position * (1 / cellSize), within an ulp of the
+// quotient (WGSL's f32 division itself is only specified to 2.5 ulp).  Every
+// stencil of the default path -- bucketing, P2G records, G2P -- comes from
+// this one formula, so they agree for every particle.
+__device__ __forceinline__ bool make_stencil_fast(const StepParams &P, float2 pos, Stencil &s)
+{
+    return stencil_from_grid(__fmul_rn(pos.x, P.inv_dx), __fmul_rn(pos.y, P.inv_dx), s);
+}
+
+// pow as WGSL specifies it: its accuracy is inherited from
+// exp2(y * log2(x)), so the reference's Tait terms are that expression.
+__device__ __forceinline__ float pow_wgsl(float x, float y) { return exp2f(y * log2f(x)); }
 
 // prepareParticle: shaders.ts:808-963.  Computes the per-particle stress
 // cache (affine momentum A = m C + (-dt V 4/dx^2) P F^T), mass and current
@@ -110,7 +129,7 @@ __device__ __forceinline__ uint32_t prepare_core(const StepParams &P, const Mate
             !finite_f(m.param) || m.param < 0.0f)
             return bad;
         if (m.param > 0.0f) {
-            const float pw = tait_pow >= 0.0f ? tait_pow : powf(__fdiv_rn(1.0f, det), m.param);
+            const float pw = tait_pow >= 0.0f ? tait_pow : pow_wgsl(__fdiv_rn(1.0f, det), m.param);
             const float pressure = m.lambda * (pw - 1.0f);
             const float stress = -det * pressure;
             s = make_float4(stress, 0.f, 0.f, stress);
@@ -402,7 +421,8 @@ __device__ __forceinline__ float2 finish_velocity(const StepParams &P, float mas
 {
     // finishGridVelocity: shaders.ts:1748-1777
     if (mass <= 0.0f) return make_float2(0.f, 0.f);
-    float2 vel = make_float2(px / mass + P.dt * P.gx, py / mass + P.dt * P.gy);
+    const float inv = __frcp_rn(mass);
+    float2 vel = make_float2(px * inv + P.dt * P.gx, py * inv + P.dt * P.gy);
     if (P.drag_radius > 0.0f && x >= 0 && y >= 0 && x <= (int)P.cells_x && y <= (int)P.cells_y) {
         const float nx = (float)x * P.dx, ny = (float)y * P.dx;
         const float ddx = P.drag_x - nx, ddy = P.drag_y - ny;
@@ -418,12 +438,19 @@ __device__ __forceinline__ float2 finish_velocity(const StepParams &P, float mas
     return vel;
 }
 
+// Per-channel node velocities G2P reads: solid (vx, vy); water and oil
+// (vx, vy, liquid mass, liquid volume).
+struct NodeVel {
+    float2 vs;
+    float4 vw, vo;
+};
+
 // The node update of updateGrid (shaders.ts:1485-1746) for one node given its
 // P2G sums and the water/oil volumes of its four neighbours (xp, xm, yp, ym;
-// zero outside the halo or where no particle deposited).  Writes the
-// per-channel velocities G2P reads.  Returns false after raising a status.
-__device__ bool update_node(const Ctx &c, uint32_t n, int x, int y, float4 S, float4 W, float4 O, float2 xp,
-                            float2 xm, float2 yp, float2 ym)
+// zero outside the halo or where no particle deposited).  Returns false
+// after raising a status.
+__device__ __forceinline__ bool node_velocity(const Ctx &c, int x, int y, float4 S, float4 W, float4 O, float2 xp,
+                                              float2 xm, float2 yp, float2 ym, NodeVel &out)
 {
     const StepParams &P = *c.P;
     if (!finite_f(S.x) || S.x < 0.f || !finite_f(S.y) || !finite_f(S.z) || !finite_f(W.x) || W.x < 0.f ||
@@ -443,31 +470,33 @@ __device__ bool update_node(const Ctx &c, uint32_t n, int x, int y, float4 S, fl
         const float2 sep = make_float2(ograd.x - wgrad.x, ograd.y - wgrad.y);
         const float sl = sqrtf(sep.x * sep.x + sep.y * sep.y);
         if (finite_f(sl) && sl > 1e-8f) {
-            float2 nrm = make_float2(sep.x / sl, sep.y / sl);
-            const float wd = W.x / W.w, od = O.x / O.w;
+            const float isl = __frcp_rn(sl);
+            float2 nrm = make_float2(sep.x * isl, sep.y * isl);
+            const float wd = __fdividef(W.x, W.w), od = __fdividef(O.x, O.w);
             const float ds = fmaxf(wd, od);
-            const float contrast = (od - wd) / ds;
+            const float contrast = __fdividef(od - wd, ds);
             const float gm = sqrtf(P.gx * P.gx + P.gy * P.gy);
             float align = 0.f;
             if (!finite_f(wd) || wd <= 0.f || !finite_f(od) || od <= 0.f || !finite_f(contrast) || !finite_f(gm)) {
                 fail(c.status, ERROR_GRID);
                 return false;
             }
-            if (gm > 0.f) align = (nrm.x * P.gx + nrm.y * P.gy) / gm;
+            if (gm > 0.f) align = __fdividef(nrm.x * P.gx + nrm.y * P.gy, gm);
             if (!finite_f(align)) {
                 fail(c.status, ERROR_GRID);
                 return false;
             }
             if (contrast * align < -LIQUID_STABLE_ORDER_EPSILON) nrm = make_float2(-nrm.x, -nrm.y);
             const float rel = (vo.x - vw.x) * nrm.x + (vo.y - vw.y) * nrm.y;
-            const float overlap = fminf(fmaxf(2.0f * fminf(W.w, O.w) / (W.w + O.w), 0.f), 1.f);
+            const float overlap = fminf(fmaxf(__fdividef(2.0f * fminf(W.w, O.w), W.w + O.w), 0.f), 1.f);
             const float minsep = fmaxf(LIQUID_CONTACT_SEPARATION_FRACTION * overlap * P.dx / LIQUID_CONTACT_RELAXATION_SECONDS,
                                        fmaxf(-rel, 0.f) * LIQUID_CONTACT_APPROACH_SPEED_MULTIPLIER);
             if (rel < minsep) {
-                const float mag = (minsep - rel) / (1.0f / W.x + 1.0f / O.x);
+                const float iwm = __frcp_rn(W.x), iom = __frcp_rn(O.x);
+                const float mag = __fdividef(minsep - rel, iwm + iom);
                 const float ix = mag * nrm.x, iy = mag * nrm.y;
-                vw = make_float2(vw.x - ix / W.x, vw.y - iy / W.x);
-                vo = make_float2(vo.x + ix / O.x, vo.y + iy / O.x);
+                vw = make_float2(vw.x - ix * iwm, vw.y - iy * iwm);
+                vo = make_float2(vo.x + ix * iom, vo.y + iy * iom);
             }
         }
     }
@@ -490,9 +519,21 @@ __device__ bool update_node(const Ctx &c, uint32_t n, int x, int y, float4 S, fl
     vo.x = wall_friction(vo.x, y, cy, fr);
     vo.y = wall_friction(vo.y, x, cx, fr);
     const float lm = W.x + O.x, lv = W.w + O.w;
-    c.g_solid[n] = vs;
-    c.g_water[n] = make_float4(vw.x, vw.y, lm, lv);
-    c.g_oil[n] = make_float4(vo.x, vo.y, lm, lv);
+    out.vs = vs;
+    out.vw = make_float4(vw.x, vw.y, lm, lv);
+    out.vo = make_float4(vo.x, vo.y, lm, lv);
+    return true;
+}
+
+// node_velocity stored to the global velocity grid (fixed-point path).
+__device__ bool update_node(const Ctx &c, uint32_t n, int x, int y, float4 S, float4 W, float4 O, float2 xp,
+                            float2 xm, float2 yp, float2 ym)
+{
+    NodeVel v;
+    if (!node_velocity(c, x, y, S, W, O, xp, xm, yp, ym, v)) return false;
+    c.g_solid[n] = v.vs;
+    c.g_water[n] = v.vw;
+    c.g_oil[n] = v.vo;
     return true;
 }
 
@@ -517,7 +558,7 @@ __global__ void k_tile_count(Ctx c)
     uint32_t key = 0;
     if (valid) {
         Stencil s;
-        if (!make_stencil(P, c.in.pos[i], s) || !stencil_fits(P, s.bx, s.by)) {
+        if (!make_stencil_fast(P, c.in.pos[i], s) || !stencil_fits(P, s.bx, s.by)) {
             fail(c.status, ERROR_STENCIL);
             valid = false;
         } else {
@@ -805,7 +846,7 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, uint32_t begi
 // bit-identical.  A tile with more than STAGE_CAP particles is taken in
 // chunks of whole cell rows (rows holding more than STAGE_CAP particles in
 // chunks of the bucket, whose order then decides the rounding of their
-// sums).  The sums go to the tile's own ring record; k_grid_from_parts adds
+// sums).  The sums go to the tile's own ring record; k_g2p_tile adds
 // the up to four records that cover a node.
 __global__ void __launch_bounds__(TILE_CELLS) k_p2g_gather(Ctx c)
 {
@@ -813,15 +854,16 @@ __global__ void __launch_bounds__(TILE_CELLS) k_p2g_gather(Ctx c)
     const uint32_t n_active = c.counters[COUNTER_ACTIVE_TILES];
     const uint32_t stamp = c.counters[COUNTER_STAMP];
     for (uint32_t item = blockIdx.x; item < n_active; item += gridDim.x) {
-        if (*(volatile uint32_t *)c.status != 0u) return;
         const uint32_t tile = c.active_tiles[item];
         const uint32_t begin = c.tile_start[tile], n_tile = c.tile_start[tile + 1] - begin;
         __syncthreads();  // the previous tile's readers of sm are done
         for (int k = threadIdx.x; k < ACC_WORDS * RING_NODES; k += TILE_CELLS) (&sm.acc[0][0])[k] = 0.f;
         if (threadIdx.x == 0) {
-            sm.failed = 0;
+            sm.failed = *(volatile uint32_t *)c.status != 0u ? 1 : 0;  // one read for the whole CTA
             sm.mask = 0u;
         }
+        __syncthreads();
+        if (sm.failed) return;
         if (n_tile > (uint32_t)STAGE_CAP) {
             if (threadIdx.x < TILE_Y) sm.rows[threadIdx.x] = 0u;
             __syncthreads();
@@ -904,110 +946,39 @@ __device__ __forceinline__ NodeSources node_sources(const StepParams &P, const u
     return ns;
 }
 
-__device__ __forceinline__ float node_word(const Ctx &c, const NodeSources &ns, int word, uint32_t channel)
+// Adds the ring records of a node into sum[] in source order: every word
+// when `all`, else only the water and oil volumes (words 6 and 10).
+__device__ __forceinline__ void add_sources(const Ctx &c, const NodeSources &ns, bool all, float (&sum)[ACC_WORDS])
 {
-    float s = 0.f;
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
-        if (ns.mask[k] & channel) s += c.part[ns.base[k] + (uint32_t)(word * RING_NODES)];
-    return s;
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t mask = ns.mask[k];
+        if (!mask) continue;
+        const float *src = c.part + ns.base[k];
+        if (all) {
+            if (mask & 1u) {
+                sum[0] += src[0];
+                sum[1] += src[RING_NODES];
+                sum[2] += src[2 * RING_NODES];
+            }
+            if (mask & 2u) {
+                sum[3] += src[3 * RING_NODES];
+                sum[4] += src[4 * RING_NODES];
+                sum[5] += src[5 * RING_NODES];
+            }
+            if (mask & 4u) {
+                sum[7] += src[7 * RING_NODES];
+                sum[8] += src[8 * RING_NODES];
+                sum[9] += src[9 * RING_NODES];
+            }
+        }
+        if (mask & 2u) sum[6] += src[6 * RING_NODES];
+        if (mask & 4u) sum[10] += src[10 * RING_NODES];
+    }
 }
 
 }  // namespace
 
-// updateGrid (shaders.ts:1485-1746) over the tiles a particle reaches this
-// substep: each active tile A covers itself and, where no tile before it in
-// the order (tile, left, below, below-left) is active, its right, upper and
-// upper-right neighbours, so every reached tile is updated exactly once.
-// Node sums add the ring records in the fixed order of node_sources.  The
-// water / oil volumes of the tile's nodes and of the ring of nodes around it
-// (the neighbours phaseVolumeGradient reads) are gathered into shared memory
-// once per tile.
-__global__ void __launch_bounds__(TILE_NODES) k_grid_from_parts(Ctx c)
-{
-    const StepParams &P = *c.P;
-    __shared__ uint2 s_info[9];
-    __shared__ float2 s_vol[RING_NODES];  // nodes (x0 - 1 .. x0 + 16, y0 - 1 .. y0 + 8)
-    const uint32_t n_active = c.counters[COUNTER_ACTIVE_TILES];
-    const uint32_t stamp = c.counters[COUNTER_STAMP];
-    if (*(volatile uint32_t *)c.status != 0u) return;
-    const int tiles_x = (int)P.tiles_x, tiles_y = (int)P.tiles_y;
-    const int node_w = (int)P.node_w, node_h = (int)P.node_h;
-    const int lx = (int)(threadIdx.x % TILE_X), ly = (int)(threadIdx.x / TILE_X);
-    uint32_t ws = 0, ww = 0, wo = 0;
-    for (uint32_t item = blockIdx.x; item < 4u * n_active; item += gridDim.x) {
-        const uint32_t a = c.active_tiles[item >> 2], k = item & 3u;
-        const int tx = (int)(a % P.tiles_x) + (int)(k & 1u), ty = (int)(a / P.tiles_x) + (int)(k >> 1);
-        if (tx >= tiles_x || ty >= tiles_y) continue;
-        __syncthreads();  // readers of the previous item's shared data are done
-        if (threadIdx.x < 9) {
-            const int sx = tx + (int)(threadIdx.x % 3) - 1, sy = ty + (int)(threadIdx.x / 3) - 1;
-            s_info[threadIdx.x] = (sx >= 0 && sy >= 0 && sx < tiles_x && sy < tiles_y)
-                                      ? c.tile_info[sy * tiles_x + sx]
-                                      : make_uint2(0xffffffffu, 0u);
-        }
-        __syncthreads();
-        const bool self = s_info[4].x == stamp, left = s_info[3].x == stamp, below = s_info[1].x == stamp;
-        bool owner = true;
-        if (k == 1u) owner = !self;
-        if (k == 2u) owner = !self && !left;
-        if (k == 3u) owner = !self && !left && !below;
-        if (!owner) continue;
-        const int x0 = tx * TILE_X, y0 = ty * TILE_Y;
-        const int hx = x0 + lx, hy = y0 + ly;
-        const bool inside = hx < node_w && hy < node_h;
-        float4 S = make_float4(0.f, 0.f, 0.f, 0.f), W = S, O = S;
-        if (inside) {
-            const NodeSources ns = node_sources(P, s_info, tx, ty, hx, hy, stamp);
-            S = make_float4(node_word(c, ns, 0, 1u), node_word(c, ns, 1, 1u), node_word(c, ns, 2, 1u), 0.f);
-            W = make_float4(node_word(c, ns, 3, 2u), node_word(c, ns, 4, 2u), node_word(c, ns, 5, 2u),
-                            node_word(c, ns, 6, 2u));
-            O = make_float4(node_word(c, ns, 7, 4u), node_word(c, ns, 8, 4u), node_word(c, ns, 9, 4u),
-                            node_word(c, ns, 10, 4u));
-        }
-        s_vol[(ly + 1) * RING_X + lx + 1] = make_float2(W.w, O.w);
-        // the 52 border nodes of the 18 x 10 region
-        if (threadIdx.x < 2 * RING_X + 2 * TILE_Y) {
-            int rx, ry;
-            const int t = (int)threadIdx.x;
-            if (t < RING_X) {
-                rx = t, ry = 0;
-            } else if (t < 2 * RING_X) {
-                rx = t - RING_X, ry = RING_Y - 1;
-            } else if (t < 2 * RING_X + TILE_Y) {
-                rx = 0, ry = t - 2 * RING_X + 1;
-            } else {
-                rx = RING_X - 1, ry = t - 2 * RING_X - TILE_Y + 1;
-            }
-            const int bx = x0 - 1 + rx, by = y0 - 1 + ry;
-            float2 v = make_float2(0.f, 0.f);
-            if (bx >= 0 && by >= 0 && bx < node_w && by < node_h) {
-                const NodeSources ns = node_sources(P, s_info, tx, ty, bx, by, stamp);
-                v = make_float2(node_word(c, ns, 6, 2u), node_word(c, ns, 10, 4u));
-            }
-            s_vol[ry * RING_X + rx] = v;
-        }
-        __syncthreads();
-        if (inside) {
-            const int r = (ly + 1) * RING_X + lx + 1;
-            const uint32_t n = (uint32_t)hy * P.node_w + (uint32_t)hx;
-            if (update_node(c, n, hx - 1, hy - 1, S, W, O, s_vol[r + 1], s_vol[r - 1], s_vol[r + RING_X],
-                            s_vol[r - RING_X])) {
-                ws += S.x > 0.f;
-                ww += W.x > 0.f;
-                wo += O.x > 0.f;
-            }
-        }
-    }
-    ws = warp_sum(ws);
-    ww = warp_sum(ww);
-    wo = warp_sum(wo);
-    if ((threadIdx.x & 31u) == 0u) {
-        if (ws) atomicAdd(c.counters + COUNTER_ACTIVE, ws);
-        if (ww) atomicAdd(c.counters + COUNTER_ACTIVE + 1, ww);
-        if (wo) atomicAdd(c.counters + COUNTER_ACTIVE + 2, wo);
-    }
-}
 
 // ----------------------------------------------------- fixed-point P2G --
 
@@ -1155,7 +1126,7 @@ __device__ float wave_speed_bound(const Ctx &c, const Material &m, float4 F, flo
         if (m.param > 0.0f) {
             const float det = det2(F);
             if (!finite_f(m.param) || m.param <= 0.f || !finite_f(det) || det <= 0.f) return FLOAT_MAX;
-            const float scale = tait_pow >= 0.0f ? tait_pow * det : powf(1.0f / det, m.param - 1.0f);
+            const float scale = tait_pow >= 0.0f ? tait_pow * det : pow_wgsl(1.0f / det, m.param - 1.0f);
             c2 = m.param * c2 * scale;
         }
         if (!finite_f(c2) || c2 < 0.f) return FLOAT_MAX;
@@ -1215,21 +1186,56 @@ __device__ void validate_cfl(const Ctx &c, uint32_t id, const Material &m, float
     }
 }
 
-// The G2P of one particle: reads slot s, writes slot d.  Returns false when
-// the particle raised a status (its output slot is then restored by commit).
-// When the next substep's tiles are counted, `next` receives the stencil of
-// the new position and the slot's P2G record is written.
-__device__ bool g2p_particle(const Ctx &c, uint32_t s, uint32_t d, Stencil &next)
+// Node velocities of the global grid, around base node n00.
+struct GlobalGrid {
+    const float2 *solid;
+    const float4 *water, *oil;
+    uint32_t n00, row;
+    __device__ __forceinline__ uint32_t at(int ox, int oy) const { return n00 + (uint32_t)oy * row + (uint32_t)ox; }
+};
+
+// Node velocities of a tile's ring in shared memory, around ring node r00.
+struct RingGrid {
+    const float2 *solid;
+    const float4 *water, *oil;
+    uint32_t n00, row;
+    __device__ __forceinline__ uint32_t at(int ox, int oy) const { return n00 + (uint32_t)oy * row + (uint32_t)ox; }
+};
+
+// The input state G2P reads for one particle.
+struct ParticleIn {
+    float2 pos;
+    float4 F;
+    float vol, pvol, damage;
+    uint32_t mat, orig;
+};
+
+__device__ __forceinline__ ParticleIn load_particle(const Ctx &c, uint32_t s)
+{
+    ParticleIn in;
+    in.pos = c.in.pos[s];
+    in.F = c.in.F[s];
+    in.vol = c.in.vol[s];
+    in.pvol = c.in.pvol[s];
+    in.damage = c.in.damage[s];
+    in.mat = c.in.mat[s];
+    in.orig = c.in.orig[s];
+    return in;
+}
+
+// The G2P of one particle with base stencil st: reads `in`, writes slot d.
+// Returns false when the particle raised a status (its output slot is then
+// restored by commit).  When the next substep's tiles are counted, `next`
+// receives the stencil of the new position and the slot's P2G record is
+// written.
+template <class Grid>
+__device__ __forceinline__ bool g2p_particle(const Ctx &c, const ParticleIn &in, uint32_t d, const Stencil &st,
+                                             const Grid &grid, Stencil &next)
 {
     const StepParams &P = *c.P;
-    const float2 pos = c.in.pos[s];
-    Stencil st;
-    if (!make_stencil(P, pos, st) || !stencil_fits(P, st.bx, st.by)) {
-        fail(c.status, ERROR_STENCIL);
-        return false;
-    }
-    const uint32_t id = c.in.orig[s];
-    const Material m = c.mats[c.in.mat[s]];
+    const float2 pos = in.pos;
+    const uint32_t id = in.orig;
+    const Material m = c.mats[in.mat];
     const bool water = m.model == MODEL_WATER, oil = m.model == MODEL_OIL, liquid = water || oil;
     float wx[3], wy[3];
 #pragma unroll
@@ -1240,14 +1246,13 @@ __device__ bool g2p_particle(const Ctx &c, uint32_t s, uint32_t d, Stencil &next
     float2 vel = make_float2(0.f, 0.f);
     float4 aff = make_float4(0.f, 0.f, 0.f, 0.f);
     float pmass = 0.f, pvolume = 0.f;
-    const float4 *gliq = water ? c.g_water : c.g_oil;
+    const float4 *gliq = water ? grid.water : grid.oil;
 #pragma unroll
     for (int oy = 0; oy < 3; ++oy) {
         const float dpy = ((float)oy - st.fy) * P.dx;
-        const uint32_t row = node_index(P, st.bx, st.by + oy);
 #pragma unroll
         for (int ox = 0; ox < 3; ++ox) {
-            const uint32_t n = row + ox;
+            const uint32_t n = grid.at(ox, oy);
             const float w = wx[ox] * wy[oy];
             const float dpx = ((float)ox - st.fx) * P.dx;
             // The reference also checks w, dp, the node velocity and the
@@ -1265,7 +1270,7 @@ __device__ bool g2p_particle(const Ctx &c, uint32_t s, uint32_t d, Stencil &next
                 nm = g.z;
                 nv = g.w;
             } else {
-                gv = c.g_solid[n];
+                gv = grid.solid[n];
             }
             vel.x += w * gv.x;
             vel.y += w * gv.y;
@@ -1279,7 +1284,7 @@ __device__ bool g2p_particle(const Ctx &c, uint32_t s, uint32_t d, Stencil &next
             aff.w += w * gv.y * dpy;
         }
     }
-    const float4 F0 = c.in.F[s];
+    const float4 F0 = in.F;
     if (liquid) {
         const float pdet = det2(F0);
         if (!finite_f(pmass) || pmass <= 0.f || !finite_f(pvolume) || pvolume <= 0.f || !finite_f(pdet) ||
@@ -1287,9 +1292,9 @@ __device__ bool g2p_particle(const Ctx &c, uint32_t s, uint32_t d, Stencil &next
             fail_at(c.status, id, ERROR_G2P);
             return false;
         }
-        const float pd = m.density / pdet;
-        const float ld = pmass / pvolume;
-        const float rd = (pd - ld) / pd;
+        const float pd = __fdividef(m.density, pdet);
+        const float ld = __fdividef(pmass, pvolume);
+        const float rd = __fdividef(pd - ld, pd);
         vel.x += P.dt * (rd * P.gx);
         vel.y += P.dt * (rd * P.gy);
         if (!finite_f(pd) || pd <= 0.f || !finite_f(ld) || ld <= 0.f || !finite_f(rd) || !finite2(vel)) {
@@ -1306,7 +1311,7 @@ __device__ bool g2p_particle(const Ctx &c, uint32_t s, uint32_t d, Stencil &next
     }
     const float row = fmaxf(fabsf(Cn.x) + fabsf(Cn.y), fabsf(Cn.z) + fabsf(Cn.w));
     const float inc = dt * row;
-    const float req = ceilf(inc / MAX_DEFORMATION_INCREMENT);
+    const float req = ceilf(inc * (1.0f / MAX_DEFORMATION_INCREMENT));  // exact: the increment is 2^-2
     if (!finite_f(req) || req > MAX_DEFORMATION_SUBSTEPS) {
         fail_at(c.status, id, ERROR_DEFORMATION_SUBSTEP_LIMIT);
         return false;
@@ -1328,7 +1333,7 @@ __device__ bool g2p_particle(const Ctx &c, uint32_t s, uint32_t d, Stencil &next
         tdet = det2(trial);
     }
     float4 Fn = trial;
-    float pv = c.in.pvol[s];
+    float pv = in.pvol;
     if (!finite_f(tdet) || tdet <= 0.f) {
         // recordDeformationFailure: shaders.ts:224-237
         const uint32_t prev = atomicOr(c.status + 6, 1u);
@@ -1374,9 +1379,10 @@ __device__ bool g2p_particle(const Ctx &c, uint32_t s, uint32_t d, Stencil &next
         // projectLiquidDeformation: shaders.ts:474-488
         const float2 rn = make_float2(trial.x + trial.w, trial.z - trial.y);
         const float rs = fmaxf(fabsf(rn.x), fabsf(rn.y));
-        const float2 nr = make_float2(rn.x / rs, rn.y / rs);
-        const float rl = sqrtf(nr.x * nr.x + nr.y * nr.y);
-        const float2 rot = make_float2(nr.x / rl, nr.y / rl);
+        const float irs = __frcp_rn(rs);
+        const float2 nr = make_float2(rn.x * irs, rn.y * irs);
+        const float irl = rsqrtf(nr.x * nr.x + nr.y * nr.y);
+        const float2 rot = make_float2(nr.x * irl, nr.y * irl);
         const float vol = det2(trial);
         const float bv = fminf(fmaxf(vol, MIN_LIQUID_DETERMINANT), MAX_LIQUID_DETERMINANT);
         const float sc = sqrtf(bv);
@@ -1419,8 +1425,8 @@ __device__ bool g2p_particle(const Ctx &c, uint32_t s, uint32_t d, Stencil &next
     const float2 fx = confine_axis(bx.x, bx.y, P.domain_w);
     const float2 fy = confine_axis(by.x, by.y, P.domain_h);
     const float2 outv = make_float2(fx.y, fy.y);
-    const float damage = c.in.damage[s];
-    const float volume = c.in.vol[s];
+    const float damage = in.damage;
+    const float volume = in.vol;
     const float2 out_pos = make_float2(fx.x, fy.x);
     c.out.pos[d] = out_pos;
     c.out.vel[d] = outv;
@@ -1429,15 +1435,15 @@ __device__ bool g2p_particle(const Ctx &c, uint32_t s, uint32_t d, Stencil &next
     c.out.pvol[d] = pv;
     c.out.damage[d] = damage;
     c.out.vol[d] = volume;
-    c.out.mat[d] = c.in.mat[s];
+    c.out.mat[d] = in.mat;
     c.out.orig[d] = id;
     // (1 / det F)^gamma of a Tait liquid, shared by the CFL wave speed and the
     // next substep's pressure (both evaluate it at the new F)
     float tait_pow = -1.0f;
-    if (liquid && m.param > 0.0f && finite_f(m.param)) tait_pow = powf(__fdiv_rn(1.0f, udet), m.param);
+    if (liquid && m.param > 0.0f && finite_f(m.param)) tait_pow = pow_wgsl(__fdiv_rn(1.0f, udet), m.param);
     if (P.n_bodies == 0u) validate_cfl(c, id, m, outv, Fn, damage, volume, tait_pow);
     if (c.count_next) {
-        if (!make_stencil(P, out_pos, next) || !stencil_fits(P, next.bx, next.by)) {
+        if (!make_stencil_fast(P, out_pos, next) || !stencil_fits(P, next.bx, next.by)) {
             fail(c.status, ERROR_STENCIL);
             return false;
         }
@@ -1466,10 +1472,16 @@ __global__ void k_g2p(Ctx c)
         if (*(volatile uint32_t *)c.status != 0u) {
             copy_particle(c, d, d);  // identity: perm may be stale once a status is set
         } else {
-            Stencil st;
-            if (g2p_particle(c, s, d, st) && c.count_next) {
-                key = particle_tile(P, st.bx, st.by);
-                counted = true;
+            const ParticleIn in = load_particle(c, s);
+            Stencil st, next;
+            if (!make_stencil(P, in.pos, st) || !stencil_fits(P, st.bx, st.by)) {
+                fail(c.status, ERROR_STENCIL);
+            } else {
+                const GlobalGrid grid{c.g_solid, c.g_water, c.g_oil, node_index(P, st.bx, st.by), P.node_w};
+                if (g2p_particle(c, in, d, st, grid, next) && c.count_next) {
+                    key = particle_tile(P, next.bx, next.by);
+                    counted = true;
+                }
             }
         }
     }
@@ -1478,6 +1490,198 @@ __global__ void k_g2p(Ctx c)
     if (!counted) return;
     c.ranks[d] = warp_count(c.tile_count, key, active);
     c.keys[d] = key;
+}
+
+namespace {
+
+// Copies the G2P input of slot s to shared-memory index i (asynchronously).
+__device__ __forceinline__ void stage_particle(const Ctx &c, uint32_t s, uint32_t i, float2 *pos, float4 *F,
+                                               float *vol, float *pvol, float *damage, uint32_t *mat, uint32_t *orig)
+{
+    cp_async<8>(&pos[i], &c.in.pos[s]);
+    cp_async<16>(&F[i], &c.in.F[s]);
+    cp_async<4>(&vol[i], &c.in.vol[s]);
+    cp_async<4>(&pvol[i], &c.in.pvol[s]);
+    cp_async<4>(&damage[i], &c.in.damage[s]);
+    cp_async<4>(&mat[i], &c.in.mat[s]);
+    cp_async<4>(&orig[i], &c.in.orig[s]);
+}
+
+// Copies the G2P inputs of bucket entries [base, base + count) to shared
+// indices 0..count-1; count <= G2P_STAGE = 2 * G2P_THREADS, and both bucket
+// entries of a thread are read before either copy is issued.
+__device__ __forceinline__ void stage_chunk(const Ctx &c, uint32_t base, uint32_t count, float2 *pos, float4 *F,
+                                            float *vol, float *pvol, float *damage, uint32_t *mat, uint32_t *orig)
+{
+    const uint32_t i0 = threadIdx.x, i1 = threadIdx.x + G2P_THREADS;
+    const uint32_t s0 = i0 < count ? c.perm[base + i0] : 0u;
+    const uint32_t s1 = i1 < count ? c.perm[base + i1] : 0u;
+    if (i0 < count) stage_particle(c, s0, i0, pos, F, vol, pvol, damage, mat, orig);
+    if (i1 < count) stage_particle(c, s1, i1, pos, F, vol, pvol, damage, mat, orig);
+}
+
+}  // namespace
+
+// The grid update and G2P of one tile holding particles (updateGrid,
+// shaders.ts:1485-1746, then g2p as in k_g2p), one tile per CTA iteration.
+// The CTA first evaluates the node update of the tile's 18x10-node ring --
+// every node its particles' stencils reach -- from the P2G ring records
+// (sums added in the fixed order of node_sources, neighbour volumes from the
+// 20x12 nodes around the ring) into shared memory, then moves its particles with
+// those velocities.  Ring nodes shared by neighbouring tiles are evaluated
+// by each of them from the same sums, so they agree bit for bit.  A tile
+// whose ring holds a failing node raises the grid status and moves none of
+// its particles (the substep is rolled back); tiles elsewhere still move
+// theirs, so their G2P flags can join the status of that substep.
+__global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c)
+{
+    const StepParams &P = *c.P;
+    __shared__ uint2 s_info[9];
+    __shared__ float2 s_vol[VOL_X * VOL_Y];
+    __shared__ float2 s_vs[RING_NODES];
+    __shared__ float4 s_vw[RING_NODES];
+    __shared__ float4 s_vo[RING_NODES];
+    __shared__ int s_fail;
+    // the particles of the tile (or of one chunk of a crowded tile), copied
+    // in while the node phase runs
+    __shared__ float4 p_F[G2P_STAGE];
+    __shared__ float2 p_pos[G2P_STAGE];
+    __shared__ float p_vol[G2P_STAGE], p_pvol[G2P_STAGE], p_damage[G2P_STAGE];
+    __shared__ uint32_t p_mat[G2P_STAGE], p_orig[G2P_STAGE];
+    const uint32_t n_active = c.counters[COUNTER_ACTIVE_TILES];
+    const uint32_t stamp = c.counters[COUNTER_STAMP];
+    const int tiles_x = (int)P.tiles_x, tiles_y = (int)P.tiles_y;
+    const int node_w = (int)P.node_w, node_h = (int)P.node_h;
+    uint32_t ws = 0, ww = 0, wo = 0;
+    for (uint32_t item = blockIdx.x; item < n_active; item += gridDim.x) {
+        const uint32_t tile = c.active_tiles[item];
+        const int tx = (int)(tile % P.tiles_x), ty = (int)(tile / P.tiles_x);
+        const int x0 = tx * TILE_X, y0 = ty * TILE_Y;
+        const uint32_t begin = c.tile_start[tile], end = c.tile_start[tile + 1];
+        __syncthreads();  // readers of the previous tile's shared data are done
+        if (threadIdx.x < 9) {
+            const int sx = tx + (int)(threadIdx.x % 3) - 1, sy = ty + (int)(threadIdx.x / 3) - 1;
+            s_info[threadIdx.x] = (sx >= 0 && sy >= 0 && sx < tiles_x && sy < tiles_y)
+                                      ? c.tile_info[sy * tiles_x + sx]
+                                      : make_uint2(0xffffffffu, 0u);
+        }
+        if (threadIdx.x == 0) s_fail = *(volatile uint32_t *)c.status != 0u ? 2 : 0;
+        // the first chunk of particles, copied in while the node phase runs
+        stage_chunk(c, begin, min(end - begin, (uint32_t)G2P_STAGE), p_pos, p_F, p_vol, p_pvol, p_damage, p_mat,
+                    p_orig);
+        __syncthreads();
+        if (s_fail) {
+            cp_async_wait_all();  // no copy may land after the CTA has left
+            break;
+        }
+        // node phase: thread t takes node (x0 - 1 + t % VOL_X, y0 - 1 + t / VOL_X)
+        // of the region around the ring; ring nodes load their full sums,
+        // the border only its water / oil volumes
+        const int t = (int)threadIdx.x;
+        const int vx = t % VOL_X, vy = t / VOL_X;
+        const int hx = x0 - 1 + vx, hy = y0 - 1 + vy;
+        const bool in_region = t < VOL_X * VOL_Y;
+        const bool ring_node = in_region && vx >= 1 && vx <= RING_X && vy >= 1 && vy <= RING_Y;
+        const bool in_grid = in_region && hx >= 0 && hy >= 0 && hx < node_w && hy < node_h;
+        float sum[ACC_WORDS];
+#pragma unroll
+        for (int k = 0; k < ACC_WORDS; ++k) sum[k] = 0.f;
+        if (in_grid) {
+            const NodeSources ns = node_sources(P, s_info, tx, ty, hx, hy, stamp);
+            add_sources(c, ns, ring_node, sum);
+        }
+        if (in_region) s_vol[t] = make_float2(sum[6], sum[10]);
+        __syncthreads();
+        if (ring_node) {
+            const int rx = vx - 1, ry = vy - 1, r = ry * RING_X + rx;
+            NodeVel v;
+            v.vs = make_float2(0.f, 0.f);
+            v.vw = v.vo = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (in_grid) {
+                const float4 S = make_float4(sum[0], sum[1], sum[2], 0.f);
+                const float4 W = make_float4(sum[3], sum[4], sum[5], sum[6]);
+                const float4 O = make_float4(sum[7], sum[8], sum[9], sum[10]);
+                if (!node_velocity(c, hx - 1, hy - 1, S, W, O, s_vol[t + 1], s_vol[t - 1], s_vol[t + VOL_X],
+                                   s_vol[t - VOL_X], v)) {
+                    s_fail = 1;
+                } else {
+                    // count the node once: in the first active tile of (its
+                    // tile, left, below, below-left)
+                    const int dx = rx >= TILE_X ? 1 : 0, dy = ry >= TILE_Y ? 1 : 0;
+                    int ox = dx, oy = dy;
+                    if (s_info[(dy + 1) * 3 + dx + 1].x != stamp) {
+                        if (s_info[(dy + 1) * 3 + dx].x == stamp)
+                            ox = dx - 1;
+                        else if (s_info[dy * 3 + dx + 1].x == stamp)
+                            oy = dy - 1;
+                        else
+                            ox = dx - 1, oy = dy - 1;
+                    }
+                    if (ox == 0 && oy == 0) {
+                        ws += S.x > 0.f;
+                        ww += W.x > 0.f;
+                        wo += O.x > 0.f;
+                    }
+                }
+            }
+            s_vs[r] = v.vs;
+            s_vw[r] = v.vw;
+            s_vo[r] = v.vo;
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        if (s_fail) continue;
+        for (uint32_t base = begin; base < end; base += G2P_THREADS) {
+            const uint32_t p = base + threadIdx.x;
+            const uint32_t chunk = (base - begin) % G2P_STAGE;
+            if (base != begin && chunk == 0u) {
+                // next chunk of a crowded tile
+                __syncthreads();
+                stage_chunk(c, base, min(end - base, (uint32_t)G2P_STAGE), p_pos, p_F, p_vol, p_pvol, p_damage,
+                            p_mat, p_orig);
+                cp_async_wait_all();
+                __syncthreads();
+            }
+            bool counted = false;
+            uint32_t key = 0;
+            if (p < end) {
+                const uint32_t k = chunk + threadIdx.x;
+                ParticleIn in;
+                in.pos = p_pos[k];
+                in.F = p_F[k];
+                in.vol = p_vol[k];
+                in.pvol = p_pvol[k];
+                in.damage = p_damage[k];
+                in.mat = p_mat[k];
+                in.orig = p_orig[k];
+                Stencil st, next;
+                const bool ok = make_stencil_fast(P, in.pos, st) && stencil_fits(P, st.bx, st.by);
+                const int lx = st.bx + 1 - x0, ly = st.by + 1 - y0;  // base node in the tile
+                if (!ok || lx < 0 || lx >= TILE_X || ly < 0 || ly >= TILE_Y) {
+                    fail(c.status, ERROR_STENCIL);
+                } else {
+                    const RingGrid grid{s_vs, s_vw, s_vo, (uint32_t)(ly * RING_X + lx), RING_X};
+                    if (g2p_particle(c, in, p, st, grid, next)) {
+                        key = particle_tile(P, next.bx, next.by);
+                        counted = true;
+                    }
+                }
+            }
+            const unsigned active = __ballot_sync(0xffffffffu, counted);
+            if (counted) {
+                c.ranks[p] = warp_count(c.tile_count, key, active);
+                c.keys[p] = key;
+            }
+        }
+    }
+    ws = warp_sum(ws);
+    ww = warp_sum(ww);
+    wo = warp_sum(wo);
+    if ((threadIdx.x & 31u) == 0u) {
+        if (ws) atomicAdd(c.counters + COUNTER_ACTIVE, ws);
+        if (ww) atomicAdd(c.counters + COUNTER_ACTIVE + 1, ww);
+        if (wo) atomicAdd(c.counters + COUNTER_ACTIVE + 2, wo);
+    }
 }
 
 // commitParticles: shaders.ts:3067-3080.  On a failed substep every slot is

@@ -97,6 +97,11 @@ constexpr int TILE_CELLS = TILE_X * TILE_Y;
 constexpr int STAGE_CAP = 640;  // particles staged in shared memory at once
 constexpr int ACC_WORDS = 11;   // solid m,px,py | water m,px,py,V | oil m,px,py,V
 constexpr uint32_t REC_FAILED = 1u << 16;  // the record's prepareParticle failed
+constexpr int VOL_X = RING_X + 2;          // ring nodes and their neighbours
+constexpr int VOL_Y = RING_Y + 2;
+constexpr int G2P_THREADS = 256;
+constexpr int G2P_STAGE = 2 * G2P_THREADS;  // particles of a tile staged at once
+static_assert(VOL_X * VOL_Y <= G2P_THREADS && RING_NODES <= G2P_THREADS, "one node per thread");
 
 // device counters beyond the three of mpm_device.cuh
 constexpr int COUNTER_ACTIVE = 4;        // [4..6] active solid/water/oil nodes
@@ -112,7 +117,7 @@ __global__ void k_tile_count(Ctx c);
 __global__ void k_tile_scan(Ctx c);
 __global__ void k_tile_scatter(Ctx c);
 __global__ void k_p2g_gather(Ctx c);
-__global__ void k_grid_from_parts(Ctx c);
+__global__ void k_g2p_tile(Ctx c);
 __global__ void k_prepare_scatter(Ctx c);
 __global__ void k_fixed_decode(Ctx c);
 __global__ void k_grid_update(Ctx c);

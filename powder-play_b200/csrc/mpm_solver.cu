@@ -105,7 +105,7 @@ struct mpm_solver {
     float4 *rec_state = nullptr, *rec_affine = nullptr;
     float2 *rec_mom = nullptr;
     uint32_t *rec_cell = nullptr;
-    unsigned p2g_ctas = 1, grid_ctas = 1;  // persistent grids of the default path
+    unsigned p2g_ctas = 1, g2p_ctas = 1;  // persistent grids of the default path
 
     mpm_drag drag{};
     bool drag_active = false;
@@ -171,11 +171,11 @@ constexpr unsigned PARTICLE_THREADS = 256;
 
 // Kernel slots of the profiled substep (mpm_profile_substeps).
 enum KernelSlot {
-    K_TILE_COUNT, K_TILE_SCAN, K_TILE_SCATTER, K_P2G_GATHER, K_GRID_FROM_PARTS, K_PREPARE_SCATTER,
+    K_TILE_COUNT, K_TILE_SCAN, K_TILE_SCATTER, K_P2G_GATHER, K_G2P_TILE, K_PREPARE_SCATTER,
     K_FIXED_DECODE, K_GRID_UPDATE, K_G2P, K_COMMIT, K_SPEED_MAX, K_SLOTS
 };
 const char *const KERNEL_NAMES[K_SLOTS] = {
-    "k_tile_count", "k_tile_scan", "k_tile_scatter", "k_p2g_gather", "k_grid_from_parts", "k_prepare_scatter",
+    "k_tile_count", "k_tile_scan", "k_tile_scatter", "k_p2g_gather", "k_g2p_tile", "k_prepare_scatter",
     "k_fixed_decode", "k_grid_update", "k_g2p", "k_commit", "k_speed_max"};
 
 // When set, an event is recorded after every kernel launch so that the
@@ -241,8 +241,8 @@ void enqueue_substep(mpm_solver *s, int parity)
         mark(K_TILE_SCATTER);
         k_p2g_gather<<<s->p2g_ctas, TILE_CELLS, 0, s->stream>>>(c);
         mark(K_P2G_GATHER);
-        k_grid_from_parts<<<s->grid_ctas, TILE_NODES, 0, s->stream>>>(c);
-        mark(K_GRID_FROM_PARTS);
+        k_g2p_tile<<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
+        mark(K_G2P_TILE);
     } else {
         k_prepare_scatter<<<pb, PARTICLE_THREADS, 0, s->stream>>>(c);
         mark(K_PREPARE_SCATTER);
@@ -250,9 +250,9 @@ void enqueue_substep(mpm_solver *s, int parity)
         mark(K_FIXED_DECODE);
         k_grid_update<<<tiles, TILE_NODES, 0, s->stream>>>(c);
         mark(K_GRID_UPDATE);
+        k_g2p<<<pb, PARTICLE_THREADS, 0, s->stream>>>(c);
+        mark(K_G2P);
     }
-    k_g2p<<<pb, PARTICLE_THREADS, 0, s->stream>>>(c);
-    mark(K_G2P);
     const unsigned cb = std::min(blocks_for(s->n, PARTICLE_THREADS), 592u);
     k_commit<<<cb, PARTICLE_THREADS, 0, s->stream>>>(c);
     mark(K_COMMIT);
@@ -302,6 +302,7 @@ void fill_params(mpm_solver *s, StepParams &p, float dt, float gx, float gy, con
     p.n_bonds = s->n_bonds;
     p.fixed_shift = c.fixed_point_shift;
     p.dx = c.cell_size;
+    p.inv_dx = 1.0f / c.cell_size;
     p.particle_mass = c.particle_mass;
     p.particle_volume = c.particle_volume;
     p.dt = dt;
@@ -595,18 +596,16 @@ int create_impl(const mpm_config *config, const float *packed, const uint32_t *o
         if (cudaMemsetAsync(s->tile_info, 0xff, n_tiles * sizeof(uint2), s->stream) != cudaSuccess ||
             cudaMemsetAsync(s->tile_count, 0, n_tiles * sizeof(uint32_t), s->stream) != cudaSuccess)
             return fail(set_error(MPM_ERR_CUDA, "cudaMemset failed"));
-        int sms = 0, per_sm_p2g = 0, per_sm_grid = 0;
+        int sms = 0, per_sm_p2g = 0, per_sm_g2p = 0;
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device) != cudaSuccess ||
             cudaFuncSetAttribute(k_p2g_gather, cudaFuncAttributePreferredSharedMemoryCarveout, 100) !=
                 cudaSuccess ||
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_p2g, k_p2g_gather, TILE_CELLS, 0) !=
                 cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_grid, k_grid_from_parts, TILE_NODES, 0) !=
-                cudaSuccess)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_g2p, k_g2p_tile, G2P_THREADS, 0) != cudaSuccess)
             return fail(set_error(MPM_ERR_CUDA, "occupancy query failed"));
         s->p2g_ctas = (unsigned)std::max<size_t>(1, std::min<size_t>(n_tiles, (size_t)sms * std::max(1, per_sm_p2g)));
-        s->grid_ctas =
-            (unsigned)std::max<size_t>(1, std::min<size_t>(4 * n_tiles, (size_t)sms * std::max(1, per_sm_grid)));
+        s->g2p_ctas = (unsigned)std::max<size_t>(1, std::min<size_t>(n_tiles, (size_t)sms * std::max(1, per_sm_g2p)));
     }
     if (c.p2g_mode == MPM_P2G_FIXED_POINT) {
         ALLOC(s->p2g_solid, s->node_count);
