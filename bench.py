@@ -162,6 +162,9 @@ def kernel_bytes(name: str, n: int, active: tuple) -> float:
         # G2P: reads x, F, volume, material (32 B), writes x, v, C, F (48 B),
         # reads one 16 B grid record per active channel-node
         "k_g2p": n * 80.0 + channel_nodes * 16.0,
+        # grid update + G2P: writes x, v, C, F (48 B); reads the sums, writes and
+        # reads one velocity record per active channel-node (3 x 16 B)
+        "k_g2p_tile": n * 48.0 + channel_nodes * 48.0,
         # P2G: the particle state it depends on, x, v, C, F, volume, material
         # (56 B; G2P hands it over as a prepared record), writes one 16 B sum
         # record per active channel-node
@@ -177,6 +180,21 @@ def kernel_bytes(name: str, n: int, active: tuple) -> float:
         "k_tile_scatter": n * 12.0,
     }
     return table.get(name, 0.0)
+
+
+def dram_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu capture
+    (profiles/dram_traffic.txt), or None when it has not been captured."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "dram_traffic.txt")
+    try:
+        with open(path) as fh:
+            for line in fh:
+                parts = line.split()
+                if len(parts) == 2 and not line.startswith("#") and parts[0] == kernel:
+                    return float(parts[1])
+    except OSError:
+        pass
+    return None
 
 
 def run_reference(args):
@@ -298,7 +316,7 @@ def run_b200(args):
                 "d2h_bytes_per_step": d2h // args.steps,
                 "path": "Python host mirror of MpmMlsGpuSolver.stepCflBatchAdaptive -> C ABI"},
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": dram_traffic(dominant),
                      "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": dom_ms / dom_launches,
                      "kernel_share": dom_ms / total_ms,
                      "substep": {"algorithmic_bytes": substep_bytes, "ms": substep_ms,
