@@ -154,6 +154,15 @@ int mpm_probe_sort(mpm_solver *solver, float dt, uint32_t *keys_out, uint32_t *p
  * affine momentum (4 floats).  Does not advance the state. */
 int mpm_probe_fixed_point(mpm_solver *solver, float dt, int32_t *words_out, float *affine_out);
 
+/* Builds the bonded-triangle field of the current particles
+ * (buildTriangleField, src/lib/mpm/kernels/shaders.ts:1299-1436) and copies
+ * it out: 8 words per halo node, row-major (cellsX+3) x (cellsY+3): signed
+ * distance f32, first-vertex index + 1 u32 (0: none), normal 2 x f32,
+ * barycentric weights of the second and third vertex 2 x f32, impulse 2 x f32
+ * (zero).  MPM_ERR_STATE when the scene has no bodies.  No reference
+ * counterpart: the reference keeps this buffer internal. */
+int mpm_probe_triangle_field(mpm_solver *solver, float dt, float *field_out);
+
 /* Halo node count ((cells_x + 3) * (cells_y + 3)). */
 uint32_t mpm_node_count(const mpm_solver *solver);
 

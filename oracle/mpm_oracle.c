@@ -1512,6 +1512,48 @@ int32_t orc_run(const orc_material *mats, int32_t n_mats, const orc_config *cfg,
     return done;
 }
 
+/* The bonded-triangle field of the given particles (buildTriangleField,
+ * src/lib/mpm/reference/solver.ts:1064-1165), dense over the halo nodes:
+ * per node the signed distance (the band where no body is near), the body's
+ * first-vertex index (-1: none), the normal and the three barycentric
+ * weights.  Returns 0, or 1 with the reference's message in err. */
+int orc_triangle_field(const orc_material *mats, int32_t n_mats, const orc_config *cfg,
+                       const orc_particle *particles, int32_t n, double *sd, int32_t *body, double *normal,
+                       double *bary, char *err, int32_t err_len)
+{
+    work_t w;
+    ctx_t ctx;
+    ctx.err = err;
+    ctx.err_len = err_len;
+    if (err && err_len > 0) err[0] = 0;
+    if (!work_prepare(&w, cfg, n)) {
+        work_free(&w);
+        if (err && err_len > 0) snprintf(err, (size_t)err_len, "grid dimensions exceed the oracle's dense grid");
+        return 1;
+    }
+    if (setjmp(ctx.jump)) {
+        work_free(&w);
+        return 1;
+    }
+    vcfg_t v;
+    validate_config(&ctx, mats, n_mats, cfg, &v);
+    validate_particles(&ctx, mats, n_mats, particles, n, &v);
+    int32_t nb = collect_body_starts(&ctx, mats, n_mats, particles, n, &v, w.starts);
+    grid_begin(&w.grid);
+    build_triangle_field(&ctx, &w.grid, w.starts, nb, particles, &v);
+    double band = v.cell_size * TRIANGLE_FIELD_BAND_CELLS;
+    for (int64_t k = 0; k < v.node_count; ++k) {
+        field_t *f = field_get(&w.grid, k);
+        sd[k] = f ? f->signed_distance : band;
+        body[k] = f ? f->body_start : -1;
+        normal[2 * k] = f ? f->nx : 0;
+        normal[2 * k + 1] = f ? f->ny : 0;
+        for (int j = 0; j < 3; ++j) bary[3 * k + j] = f ? f->bary[j] : 0;
+    }
+    work_free(&w);
+    return 0;
+}
+
 int32_t orc_sizeof_particle(void) { return (int32_t)sizeof(orc_particle); }
 int32_t orc_sizeof_material(void) { return (int32_t)sizeof(orc_material); }
 int32_t orc_sizeof_bond(void) { return (int32_t)sizeof(orc_bond); }

@@ -110,6 +110,14 @@ int32_t orc_run(const orc_material *mats, int32_t n_mats, const orc_config *cfg,
                 orc_particle *particles, int32_t n, orc_bond *bonds,
                 int32_t steps, char *err, int32_t err_len);
 
+/* The bonded-triangle field of `particles`, dense over the halo nodes
+ * ((cellsX+3) x (cellsY+3), row-major): signed distance, first-vertex index of
+ * the nearest body (-1: none), normal (2 per node), barycentric weights (3 per
+ * node).  Returns 0, or 1 with the reference's message in err. */
+int orc_triangle_field(const orc_material *mats, int32_t n_mats, const orc_config *cfg,
+                       const orc_particle *particles, int32_t n, double *sd, int32_t *body, double *normal,
+                       double *bary, char *err, int32_t err_len);
+
 /* Sizes of the structs, so a binding can check its layout. */
 int32_t orc_sizeof_particle(void);
 int32_t orc_sizeof_material(void);

@@ -79,6 +79,9 @@ def load() -> ctypes.CDLL:
     lib.orc_run.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(OrcConfig), vp, ctypes.c_int32, vp, ctypes.c_int32,
                             ctypes.c_char_p, ctypes.c_int32]
     lib.orc_run.restype = ctypes.c_int32
+    lib.orc_triangle_field.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(OrcConfig), vp, ctypes.c_int32, vp, vp, vp,
+                                       vp, ctypes.c_char_p, ctypes.c_int32]
+    lib.orc_triangle_field.restype = ctypes.c_int
     lib.emu_fixed_point_scatter.argtypes = [ctypes.c_int32] + [vp] * 7 + [ctypes.c_float] * 3 + [ctypes.c_int32] * 3 + [vp]
     lib.emu_fixed_point_scatter.restype = ctypes.c_uint32
     for name in ("orc_sizeof_particle", "orc_sizeof_material", "orc_sizeof_bond", "orc_sizeof_config"):
@@ -182,6 +185,25 @@ class OracleState:
         if done != steps:
             raise OracleError(err.value.decode())
         return done
+
+    def triangle_field(self, config: dict) -> dict:
+        """The bonded-triangle field of the current particles, dense over the
+        halo nodes: sd, body (first-vertex index, -1: none), normal, bary."""
+        lib = load()
+        c = self.config_struct(config)
+        h, w = int(config["grid"]["cellsY"]) + 3, int(config["grid"]["cellsX"]) + 3
+        sd = np.zeros(h * w)
+        body = np.zeros(h * w, dtype=np.int32)
+        normal = np.zeros((h * w, 2))
+        bary = np.zeros((h * w, 3))
+        err = ctypes.create_string_buffer(512)
+        rc = lib.orc_triangle_field(self.mats.ctypes.data, len(self.mats), ctypes.byref(c),
+                                    self.particles.ctypes.data, len(self.particles), sd.ctypes.data,
+                                    body.ctypes.data, normal.ctypes.data, bary.ctypes.data, err, 512)
+        if rc != 0:
+            raise OracleError(err.value.decode())
+        return {"sd": sd.reshape(h, w), "body": body.reshape(h, w), "normal": normal.reshape(h, w, 2),
+                "bary": bary.reshape(h, w, 3)}
 
     def positions(self) -> np.ndarray:
         return np.stack([self.particles["px"], self.particles["py"]], axis=1)

@@ -13,6 +13,8 @@
 //
 // Every kernel returns early once the persistent status word is non-zero, as
 // every WGSL entry point does (shaders.ts: `atomicLoad(&stateError[0]) != 0u`).
+#include <math_constants.h>
+
 #include "mpm_kernels.cuh"
 
 namespace mpm {
@@ -184,6 +186,13 @@ __device__ bool prepare_particle(const Ctx &c, uint32_t i, float4 &affine, float
     else
         fail(c.status, flags);
     return false;
+}
+
+// Whether the slot of original particle `orig` is tracked (a bonded-triangle
+// vertex or a fracture-bond endpoint).
+__device__ __forceinline__ bool is_tracked(const Ctx &c, uint32_t orig)
+{
+    return c.track_flag != nullptr && c.track_flag[orig] != 0u;
 }
 
 // Writes the P2G record of slot d for a particle with the given state and
@@ -443,14 +452,15 @@ __device__ __forceinline__ float2 finish_velocity(const StepParams &P, float mas
 struct NodeVel {
     float2 vs;
     float4 vw, vo;
+    float2 impulse;  // the fluid's impulse on a nearby body (zero without one)
 };
 
 // The node update of updateGrid (shaders.ts:1485-1746) for one node given its
 // P2G sums and the water/oil volumes of its four neighbours (xp, xm, yp, ym;
 // zero outside the halo or where no particle deposited).  Returns false
 // after raising a status.
-__device__ __forceinline__ bool node_velocity(const Ctx &c, int x, int y, float4 S, float4 W, float4 O, float2 xp,
-                                              float2 xm, float2 yp, float2 ym, NodeVel &out)
+__device__ __forceinline__ bool node_velocity(const Ctx &c, uint32_t n, int x, int y, float4 S, float4 W, float4 O,
+                                              float2 xp, float2 xm, float2 yp, float2 ym, NodeVel &out)
 {
     const StepParams &P = *c.P;
     if (!finite_f(S.x) || S.x < 0.f || !finite_f(S.y) || !finite_f(S.z) || !finite_f(W.x) || W.x < 0.f ||
@@ -500,7 +510,54 @@ __device__ __forceinline__ bool node_velocity(const Ctx &c, int x, int y, float4
             }
         }
     }
-    if (!finite2(vs) || !finite2(vw) || !finite2(vo)) {
+    float2 impulse = make_float2(0.f, 0.f);
+    if (c.field) {
+        // fluid-pebble contact: updateGrid, shaders.ts:1596-1665
+        const TriField f = c.field[n];
+        if (f.body1 != 0u && f.sd <= P.contact_reach) {
+            const uint32_t start = f.body1 - 1u;
+            if (start + 2u >= P.n_particles) {
+                fail(c.status, ERROR_TRIANGLE_CONTACT);
+                return false;
+            }
+            const float3 bary = make_float3(1.0f - f.b1 - f.b2, f.b1, f.b2);
+            const float2 v0 = c.in.vel[c.slot_in[start]], v1 = c.in.vel[c.slot_in[start + 1u]],
+                         v2 = c.in.vel[c.slot_in[start + 2u]];
+            const float2 sv = make_float2(bary.x * v0.x + bary.y * v1.x + bary.z * v2.x,
+                                          bary.x * v0.y + bary.y * v1.y + bary.z * v2.y);
+            const float inv_body = (bary.x * bary.x + bary.y * bary.y + bary.z * bary.z) / P.particle_mass;
+            const float nl = sqrtf(f.nx * f.nx + f.ny * f.ny);
+            if (!finite2(sv) || !finite_f(inv_body) || inv_body <= 0.f || !finite_f(nl) || nl <= 1e-8f) {
+                fail(c.status, ERROR_TRIANGLE_CONTACT);
+                return false;
+            }
+            const float2 nrm = make_float2(f.nx / nl, f.ny / nl);
+            const float damping = 1.0f - expf(-TRIANGLE_FLUID_TANGENTIAL_DRAG_RATE * P.dt);
+            if (W.x > 0.f && W.w > 0.f) {
+                const float2 rel = make_float2(vw.x - sv.x, vw.y - sv.y);
+                const float rn = rel.x * nrm.x + rel.y * nrm.y;
+                const float iem = 1.0f / W.x + inv_body;
+                float2 imp = make_float2(0.f, 0.f);
+                if (rn < 0.f) imp = make_float2((-rn / iem) * nrm.x, (-rn / iem) * nrm.y);
+                const float2 tv = make_float2(rel.x - rn * nrm.x, rel.y - rn * nrm.y);
+                imp = make_float2(imp.x - (damping / iem) * tv.x, imp.y - (damping / iem) * tv.y);
+                vw = make_float2(vw.x + imp.x / W.x, vw.y + imp.y / W.x);
+                impulse = make_float2(impulse.x - imp.x, impulse.y - imp.y);
+            }
+            if (O.x > 0.f && O.w > 0.f) {
+                const float2 rel = make_float2(vo.x - sv.x, vo.y - sv.y);
+                const float rn = rel.x * nrm.x + rel.y * nrm.y;
+                const float iem = 1.0f / O.x + inv_body;
+                float2 imp = make_float2(0.f, 0.f);
+                if (rn < 0.f) imp = make_float2((-rn / iem) * nrm.x, (-rn / iem) * nrm.y);
+                const float2 tv = make_float2(rel.x - rn * nrm.x, rel.y - rn * nrm.y);
+                imp = make_float2(imp.x - (damping / iem) * tv.x, imp.y - (damping / iem) * tv.y);
+                vo = make_float2(vo.x + imp.x / O.x, vo.y + imp.y / O.x);
+                impulse = make_float2(impulse.x - imp.x, impulse.y - imp.y);
+            }
+        }
+    }
+    if (!finite2(vs) || !finite2(vw) || !finite2(vo) || !finite2(impulse)) {
         fail(c.status, ERROR_GRID | ERROR_TRIANGLE_CONTACT);
         return false;
     }
@@ -522,6 +579,7 @@ __device__ __forceinline__ bool node_velocity(const Ctx &c, int x, int y, float4
     out.vs = vs;
     out.vw = make_float4(vw.x, vw.y, lm, lv);
     out.vo = make_float4(vo.x, vo.y, lm, lv);
+    out.impulse = impulse;
     return true;
 }
 
@@ -530,10 +588,14 @@ __device__ bool update_node(const Ctx &c, uint32_t n, int x, int y, float4 S, fl
                             float2 xm, float2 yp, float2 ym)
 {
     NodeVel v;
-    if (!node_velocity(c, x, y, S, W, O, xp, xm, yp, ym, v)) return false;
+    if (!node_velocity(c, n, x, y, S, W, O, xp, xm, yp, ym, v)) return false;
     c.g_solid[n] = v.vs;
     c.g_water[n] = v.vw;
     c.g_oil[n] = v.vo;
+    if (c.field) {
+        c.field[n].ix = v.impulse.x;
+        c.field[n].iy = v.impulse.y;
+    }
     return true;
 }
 
@@ -563,6 +625,8 @@ __global__ void k_tile_count(Ctx c)
             valid = false;
         } else {
             key = particle_tile(P, s.bx, s.by);
+            const uint32_t orig = c.in.orig[i];
+            if (is_tracked(c, orig)) c.slot_in[orig] = i;
             const Material m = c.mats[c.in.mat[i]];
             const float damage = m.model == MODEL_NEO_HOOKEAN ? c.in.damage[i] : 0.0f;
             const float pvol = m.model == MODEL_SNOW ? c.in.pvol[i] : 1.0f;
@@ -1202,6 +1266,55 @@ struct RingGrid {
     __device__ __forceinline__ uint32_t at(int ox, int oy) const { return n00 + (uint32_t)oy * row + (uint32_t)ox; }
 };
 
+// projectLiquidFromTriangles (shaders.ts:1801-1854): pushes a liquid
+// particle of the given radius out of the nearest pebble of its stencil.
+__device__ float2 project_from_triangles(const Ctx &c, float2 pos, float radius)
+{
+    const StepParams &P = *c.P;
+    Stencil st;
+    if (!make_stencil(P, pos, st)) return pos;
+    float wx[3], wy[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        wx[k] = quad_weight(st.fx, k);
+        wy[k] = quad_weight(st.fy, k);
+    }
+    float sd = 0.f, closest = FLOAT_MAX;
+    uint32_t body1 = 0u;
+    float2 selected = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+        for (int ox = 0; ox < 3; ++ox) {
+            const TriField f = c.field[node_index(P, st.bx + ox, st.by + oy)];
+            sd += wx[ox] * wy[oy] * f.sd;
+            if (f.body1 != 0u && f.sd < closest) {
+                closest = f.sd;
+                body1 = f.body1;
+                selected = make_float2(f.nx, f.ny);
+            }
+        }
+    if (body1 == 0u) return pos;
+    float2 nrm = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+        for (int ox = 0; ox < 3; ++ox) {
+            const TriField f = c.field[node_index(P, st.bx + ox, st.by + oy)];
+            if (f.body1 == body1) {
+                nrm.x += wx[ox] * wy[oy] * f.nx;
+                nrm.y += wx[ox] * wy[oy] * f.ny;
+            }
+        }
+    const float nl = sqrtf(nrm.x * nrm.x + nrm.y * nrm.y);
+    if (!finite_f(nl) || nl <= 1e-8f)
+        nrm = selected;
+    else
+        nrm = make_float2(nrm.x / nl, nrm.y / nl);
+    if (!finite_f(sd) || sd >= radius || !finite2(nrm)) return pos;
+    return make_float2(pos.x + (radius - sd) * nrm.x, pos.y + (radius - sd) * nrm.y);
+}
+
 // The input state G2P reads for one particle.
 struct ParticleIn {
     float2 pos;
@@ -1230,8 +1343,9 @@ __device__ __forceinline__ ParticleIn load_particle(const Ctx &c, uint32_t s)
 // written.
 template <class Grid>
 __device__ __forceinline__ bool g2p_particle(const Ctx &c, const ParticleIn &in, uint32_t d, const Stencil &st,
-                                             const Grid &grid, Stencil &next)
+                                             const Grid &grid, Stencil &next, bool &count_next)
 {
+    count_next = false;
     const StepParams &P = *c.P;
     const float2 pos = in.pos;
     const uint32_t id = in.orig;
@@ -1422,8 +1536,17 @@ __device__ __forceinline__ bool g2p_particle(const Ctx &c, const ParticleIn &in,
     }
     const float2 bx = confine_axis(npos.x, vel.x, P.domain_w);
     const float2 by = confine_axis(npos.y, vel.y, P.domain_h);
-    const float2 fx = confine_axis(bx.x, bx.y, P.domain_w);
-    const float2 fy = confine_axis(by.x, by.y, P.domain_h);
+    float2 projected = make_float2(bx.x, by.x);
+    if (liquid && c.field) {
+        const float radius = sqrtf(in.vol * udet / 3.14159265359f);
+        if (!finite_f(radius)) {
+            fail_at(c.status, id, ERROR_G2P);
+            return false;
+        }
+        projected = project_from_triangles(c, projected, radius);
+    }
+    const float2 fx = confine_axis(projected.x, bx.y, P.domain_w);
+    const float2 fy = confine_axis(projected.y, by.y, P.domain_h);
     const float2 outv = make_float2(fx.y, fy.y);
     const float damage = in.damage;
     const float volume = in.vol;
@@ -1442,12 +1565,17 @@ __device__ __forceinline__ bool g2p_particle(const Ctx &c, const ParticleIn &in,
     float tait_pow = -1.0f;
     if (liquid && m.param > 0.0f && finite_f(m.param)) tait_pow = pow_wgsl(__fdiv_rn(1.0f, udet), m.param);
     if (P.n_bodies == 0u) validate_cfl(c, id, m, outv, Fn, damage, volume, tait_pow);
-    if (c.count_next) {
+    if (is_tracked(c, id)) {
+        // a body vertex or fracture particle: its final state comes after the
+        // body kernels, which then count its tile and write its record
+        c.slot_out[id] = d;
+    } else if (c.count_next) {
         if (!make_stencil_fast(P, out_pos, next) || !stencil_fits(P, next.bx, next.by)) {
             fail(c.status, ERROR_STENCIL);
             return false;
         }
         write_record(c, d, m, next, outv, Fn, volume, damage, pv, Cn, tait_pow);
+        count_next = true;
     }
     return true;
 }
@@ -1478,7 +1606,8 @@ __global__ void k_g2p(Ctx c)
                 fail(c.status, ERROR_STENCIL);
             } else {
                 const GlobalGrid grid{c.g_solid, c.g_water, c.g_oil, node_index(P, st.bx, st.by), P.node_w};
-                if (g2p_particle(c, in, d, st, grid, next) && c.count_next) {
+                bool count_it;
+                if (g2p_particle(c, in, d, st, grid, next, count_it) && count_it) {
                     key = particle_tile(P, next.bx, next.by);
                     counted = true;
                 }
@@ -1601,7 +1730,8 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c)
                 const float4 S = make_float4(sum[0], sum[1], sum[2], 0.f);
                 const float4 W = make_float4(sum[3], sum[4], sum[5], sum[6]);
                 const float4 O = make_float4(sum[7], sum[8], sum[9], sum[10]);
-                if (!node_velocity(c, hx - 1, hy - 1, S, W, O, s_vol[t + 1], s_vol[t - 1], s_vol[t + VOL_X],
+                const uint32_t n = (uint32_t)hy * (uint32_t)node_w + (uint32_t)hx;
+                if (!node_velocity(c, n, hx - 1, hy - 1, S, W, O, s_vol[t + 1], s_vol[t - 1], s_vol[t + VOL_X],
                                    s_vol[t - VOL_X], v)) {
                     s_fail = 1;
                 } else {
@@ -1621,6 +1751,10 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c)
                         ws += S.x > 0.f;
                         ww += W.x > 0.f;
                         wo += O.x > 0.f;
+                        if (c.field) {  // the body impulse of a node is stored once
+                            c.field[n].ix = v.impulse.x;
+                            c.field[n].iy = v.impulse.y;
+                        }
                     }
                 }
             }
@@ -1661,7 +1795,8 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c)
                     fail(c.status, ERROR_STENCIL);
                 } else {
                     const RingGrid grid{s_vs, s_vw, s_vo, (uint32_t)(ly * RING_X + lx), RING_X};
-                    if (g2p_particle(c, in, p, st, grid, next)) {
+                    bool count_it;
+                    if (g2p_particle(c, in, p, st, grid, next, count_it) && count_it) {
                         key = particle_tile(P, next.bx, next.by);
                         counted = true;
                     }
@@ -1694,6 +1829,9 @@ __global__ void k_commit(Ctx c)
     if (*(volatile uint32_t *)c.status != 0u) {
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n_particles; i += gridDim.x * blockDim.x)
             copy_particle(c, i, i);
+        // the restored output keeps the input's slots
+        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < c.n_tracked; k += gridDim.x * blockDim.x)
+            c.slot_out[c.tracked[k]] = c.slot_in[c.tracked[k]];
     } else if (blockIdx.x == 0 && threadIdx.x == 0 && P.cfl_enabled) {
         c.counters[COUNTER_PROGRESS] += 1u;
     }
@@ -1741,6 +1879,622 @@ __global__ void __launch_bounds__(TILE_NODES) k_count_active_nodes(Ctx c, uint32
         atomicAdd(counts + 1, w);
         atomicAdd(counts + 2, o);
     }
+}
+
+
+// ------------------------------------------------------ bodies, fracture --
+// Bonded-triangle bodies ("pebbles") and fracture bonds of the multi-material
+// scenes.  Body vertices and fracture endpoints are particles whose slots
+// move every substep; their current slots are tracked per original index
+// (slot_in for the substep's input buffer, slot_out for its output).
+
+namespace {
+
+// triangleDistanceSample of the CPU reference (src/lib/mpm/reference/solver.ts:
+// 1190-1291) in float64 with its operations in order and no contraction.  The
+// field uses this form: next to an edge the float32 offset to the closest
+// point is rounding noise, and its direction is the node's normal, which the
+// liquid projection and the contact impulses follow.  Returns false for a
+// degenerate triangle.
+__device__ bool triangle_sample_f64(double px, double py, double ax, double ay, double bx, double by, double cx,
+                                    double cy, double &sd, double &nx, double &ny, double (&bary)[3])
+{
+    const double abx = __dsub_rn(bx, ax), aby = __dsub_rn(by, ay), acx = __dsub_rn(cx, ax), acy = __dsub_rn(cy, ay);
+    const double area = __dsub_rn(__dmul_rn(abx, acy), __dmul_rn(aby, acx));
+    if (!isfinite(area) || fabs(area) <= 1e-10) return false;
+    const double bcx = __dsub_rn(cx, bx), bcy = __dsub_rn(cy, by), cax = __dsub_rn(ax, cx), cay = __dsub_rn(ay, cy);
+    const double apx = __dsub_rn(px, ax), apy = __dsub_rn(py, ay), bpx = __dsub_rn(px, bx), bpy = __dsub_rn(py, by),
+                 cpx = __dsub_rn(px, cx), cpy = __dsub_rn(py, cy);
+    const double cab = __dsub_rn(__dmul_rn(abx, apy), __dmul_rn(aby, apx));
+    const double cbc = __dsub_rn(__dmul_rn(bcx, bpy), __dmul_rn(bcy, bpx));
+    const double cca = __dsub_rn(__dmul_rn(cax, cpy), __dmul_rn(cay, cpx));
+    const bool inside = area > 0 ? (cab >= -1e-10 && cbc >= -1e-10 && cca >= -1e-10)
+                                 : (cab <= 1e-10 && cbc <= 1e-10 && cca <= 1e-10);
+    double best = CUDART_INF, bnx = 0, bny = 0;
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+        const double sx = e == 0 ? ax : (e == 1 ? bx : cx), sy = e == 0 ? ay : (e == 1 ? by : cy);
+        const double ex = e == 0 ? bx : (e == 1 ? cx : ax), ey = e == 0 ? by : (e == 1 ? cy : ay);
+        const double dx = __dsub_rn(ex, sx), dy = __dsub_rn(ey, sy);
+        const double l2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+        const double ox = __dsub_rn(px, sx), oy = __dsub_rn(py, sy);
+        const double t = fmax(0.0, fmin(1.0, __ddiv_rn(__dadd_rn(__dmul_rn(ox, dx), __dmul_rn(oy, dy)), l2)));
+        const double qx = __dadd_rn(sx, __dmul_rn(dx, t)), qy = __dadd_rn(sy, __dmul_rn(dy, t));
+        const double ddx = __dsub_rn(px, qx), ddy = __dsub_rn(py, qy);
+        const double d2 = __dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy));
+        if (d2 >= best) continue;
+        best = d2;
+        if (e == 0) {
+            bary[0] = __dsub_rn(1.0, t), bary[1] = t, bary[2] = 0;
+        } else if (e == 1) {
+            bary[0] = 0, bary[1] = __dsub_rn(1.0, t), bary[2] = t;
+        } else {
+            bary[0] = t, bary[1] = 0, bary[2] = __dsub_rn(1.0, t);
+        }
+        if (d2 > 1e-20 && !inside) {
+            const double inv = __ddiv_rn(1.0, __dsqrt_rn(d2));
+            bnx = __dmul_rn(ddx, inv);
+            bny = __dmul_rn(ddy, inv);
+        } else {
+            const double orient = area > 0 ? 1.0 : -1.0;
+            const double inv = __ddiv_rn(1.0, __dsqrt_rn(l2));
+            bnx = __dmul_rn(__dmul_rn(orient, dy), inv);
+            bny = __dmul_rn(-__dmul_rn(orient, dx), inv);
+        }
+    }
+    const double d = __dsqrt_rn(best);
+    if (!isfinite(d) || !isfinite(bnx) || !isfinite(bny)) return false;
+    sd = inside ? -d : d;
+    nx = bnx;
+    ny = bny;
+    return true;
+}
+
+__device__ __forceinline__ bool body_markers_valid(const Ctx &c, uint32_t start)
+{
+    return start + 2u < c.n && c.bonded[start] == 1u && c.bonded[start + 1u] == 2u && c.bonded[start + 2u] == 3u;
+}
+
+__device__ __forceinline__ float2 in_position(const Ctx &c, uint32_t orig) { return c.in.pos[c.slot_in[orig]]; }
+
+// trianglePairContact: shaders.ts:1873-1953 (SAT over the six edge normals);
+// (normal, penetration), zero when apart beyond the skin or degenerate.
+__device__ float3 triangle_pair_contact(const float2 (&A)[3], const float2 (&B)[3], float skin)
+{
+    float2 axes[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const float2 *T = k < 3 ? A : B;
+        const int e = k % 3;
+        const float2 edge = make_float2(T[(e + 1) % 3].x - T[e].x, T[(e + 1) % 3].y - T[e].y);
+        const float el = sqrtf(edge.x * edge.x + edge.y * edge.y);
+        if (!finite_f(el) || el <= 1e-10f) return make_float3(0.f, 0.f, 0.f);
+        axes[k] = make_float2(edge.y / el, -edge.x / el);
+    }
+    bool separated = false;
+    float largest = -FLOAT_MAX, smallest = FLOAT_MAX;
+    float2 axis = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const float2 u = axes[k];
+        const float a0 = A[0].x * u.x + A[0].y * u.y, a1 = A[1].x * u.x + A[1].y * u.y, a2 = A[2].x * u.x + A[2].y * u.y;
+        const float b0 = B[0].x * u.x + B[0].y * u.y, b1 = B[1].x * u.x + B[1].y * u.y, b2 = B[2].x * u.x + B[2].y * u.y;
+        const float min_a = fminf(a0, fminf(a1, a2)), max_a = fmaxf(a0, fmaxf(a1, a2));
+        const float min_b = fminf(b0, fminf(b1, b2)), max_b = fmaxf(b0, fmaxf(b1, b2));
+        const float gap = fmaxf(min_b - max_a, min_a - max_b);
+        if (gap > 0.f) {
+            separated = true;
+            if (gap > largest) {
+                largest = gap;
+                axis = u;
+            }
+        } else if (!separated && -gap < smallest) {
+            smallest = -gap;
+            axis = u;
+        }
+    }
+    if (separated && largest > skin) return make_float3(0.f, 0.f, 0.f);
+    const float2 delta = make_float2((A[0].x + A[1].x + A[2].x - B[0].x - B[1].x - B[2].x) / 3.0f,
+                                     (A[0].y + A[1].y + A[2].y - B[0].y - B[1].y - B[2].y) / 3.0f);
+    if (delta.x * axis.x + delta.y * axis.y < 0.f) axis = make_float2(-axis.x, -axis.y);
+    const float pen = separated ? skin - largest : skin + smallest;
+    if (!finite_f(pen) || pen <= 0.f) return make_float3(0.f, 0.f, 0.f);
+    return make_float3(axis.x, axis.y, pen);
+}
+
+// triangleBodyContact: shaders.ts:1955-1992, on the substep's input
+// positions; the normal points from `other` towards `body`.
+__device__ float3 body_contact(const Ctx &c, uint32_t body, uint32_t other)
+{
+    const bool first_is_body = body < other;
+    const uint32_t fs = c.body_starts[first_is_body ? body : other];
+    const uint32_t ss = c.body_starts[first_is_body ? other : body];
+    float2 A[3], B[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        A[k] = in_position(c, fs + (uint32_t)k);
+        B[k] = in_position(c, ss + (uint32_t)k);
+    }
+    const float2 amin = make_float2(fminf(A[0].x, fminf(A[1].x, A[2].x)), fminf(A[0].y, fminf(A[1].y, A[2].y)));
+    const float2 amax = make_float2(fmaxf(A[0].x, fmaxf(A[1].x, A[2].x)), fmaxf(A[0].y, fmaxf(A[1].y, A[2].y)));
+    const float2 bmin = make_float2(fminf(B[0].x, fminf(B[1].x, B[2].x)), fminf(B[0].y, fminf(B[1].y, B[2].y)));
+    const float2 bmax = make_float2(fmaxf(B[0].x, fmaxf(B[1].x, B[2].x)), fmaxf(B[0].y, fmaxf(B[1].y, B[2].y)));
+    const float2 gap = make_float2(fmaxf(bmin.x - amax.x, amin.x - bmax.x), fmaxf(bmin.y - amax.y, amin.y - bmax.y));
+    const float skin = c.P->dx * TRIANGLE_CONTACT_SKIN_CELLS;
+    if (fmaxf(gap.x, gap.y) > skin) return make_float3(0.f, 0.f, 0.f);
+    const float3 contact = triangle_pair_contact(A, B, skin);
+    return first_is_body ? contact : make_float3(-contact.x, -contact.y, contact.z);
+}
+
+// bondEdgeCorrection: shaders.ts:1856-1871
+__device__ __forceinline__ bool edge_correction(float2 first, float2 second, float rest, float stiffness,
+                                                float2 &corr)
+{
+    const float2 d = make_float2(second.x - first.x, second.y - first.y);
+    const float dist = sqrtf(d.x * d.x + d.y * d.y);
+    if (!finite_f(dist) || dist <= 1e-10f) return false;
+    const float k = (dist - rest) * stiffness * 0.5f / dist;
+    corr = make_float2(d.x * k, d.y * k);
+    return true;
+}
+
+__device__ __forceinline__ bool move_vertex(const Ctx &c, uint32_t slot, float2 pos, float2 vel)
+{
+    const StepParams &P = *c.P;
+    const float2 bx = confine_axis(pos.x, vel.x, P.domain_w);
+    const float2 by = confine_axis(pos.y, vel.y, P.domain_h);
+    const float2 p = make_float2(bx.x, by.x), v = make_float2(bx.y, by.y);
+    if (!finite2(p) || !finite2(v)) return false;
+    c.out.pos[slot] = p;
+    c.out.vel[slot] = v;
+    return true;
+}
+
+}  // namespace
+
+// buildTriangleField (shaders.ts:1299-1436): for every halo node, the nearest
+// body within the band (ties keep the lower body), its normal and barycentric
+// weights, with bodies staged in shared memory in ascending order; samples in
+// float64 (triangle_sample_f64).
+__global__ void __launch_bounds__(TILE_NODES) k_triangle_field(Ctx c)
+{
+    const StepParams &P = *c.P;
+    __shared__ float2 s_v0[FIELD_BODY_CHUNK], s_v1[FIELD_BODY_CHUNK], s_v2[FIELD_BODY_CHUNK];
+    __shared__ float2 s_min[FIELD_BODY_CHUNK], s_max[FIELD_BODY_CHUNK];
+    __shared__ uint32_t s_start[FIELD_BODY_CHUNK], s_valid[FIELD_BODY_CHUNK];
+    const int hx = blockIdx.x * TILE_X + (int)(threadIdx.x % TILE_X);
+    const int hy = blockIdx.y * TILE_Y + (int)(threadIdx.x / TILE_X);
+    const bool active = hx < (int)P.node_w && hy < (int)P.node_h && *(volatile uint32_t *)c.status == 0u;
+    const double px = (double)(hx - 1) * (double)P.dx, py = (double)(hy - 1) * (double)P.dx;
+    const double band = (double)P.band;
+    double best = band, best_nx = 0, best_ny = 0, best_bary[3] = {0, 0, 0};
+    uint32_t body1 = 0u;
+    bool failed = false;
+    for (uint32_t chunk = 0; chunk < P.n_bodies; chunk += FIELD_BODY_CHUNK) {
+        __syncthreads();
+        const uint32_t b = chunk + threadIdx.x;
+        if (b < P.n_bodies) {
+            const uint32_t start = c.body_starts[b];
+            s_start[threadIdx.x] = start;
+            if (start + 2u >= c.n) {
+                s_valid[threadIdx.x] = 0u;
+            } else {
+                const float2 p0 = in_position(c, start), p1 = in_position(c, start + 1u),
+                             p2 = in_position(c, start + 2u);
+                s_v0[threadIdx.x] = p0;
+                s_v1[threadIdx.x] = p1;
+                s_v2[threadIdx.x] = p2;
+                s_min[threadIdx.x] = make_float2(fminf(p0.x, fminf(p1.x, p2.x)), fminf(p0.y, fminf(p1.y, p2.y)));
+                s_max[threadIdx.x] = make_float2(fmaxf(p0.x, fmaxf(p1.x, p2.x)), fmaxf(p0.y, fmaxf(p1.y, p2.y)));
+                s_valid[threadIdx.x] = 1u;
+            }
+        }
+        __syncthreads();
+        if (!active || failed) continue;
+        const uint32_t count = min((uint32_t)FIELD_BODY_CHUNK, P.n_bodies - chunk);
+        for (uint32_t k = 0; k < count; ++k) {
+            if (!s_valid[k]) {
+                fail(c.status, ERROR_TRIANGLE_BOND);
+                failed = true;
+                break;
+            }
+            const double ox = fmax(fmax((double)s_min[k].x - px, 0.0), px - (double)s_max[k].x);
+            const double oy = fmax(fmax((double)s_min[k].y - py, 0.0), py - (double)s_max[k].y);
+            if (ox * ox + oy * oy > band * band) continue;
+            double sd, nx, ny, bary[3];
+            if (!triangle_sample_f64(px, py, s_v0[k].x, s_v0[k].y, s_v1[k].x, s_v1[k].y, s_v2[k].x, s_v2[k].y, sd, nx,
+                                     ny, bary)) {
+                fail_at(c.status, s_start[k], ERROR_TRIANGLE_CONTACT);
+                failed = true;
+                break;
+            }
+            // a node joins the field within the band; a later body takes it
+            // only when strictly nearer (buildTriangleField, solver.ts:1064-1165)
+            if (body1 == 0u ? sd <= band : sd < best) {
+                best = sd;
+                body1 = s_start[k] + 1u;
+                best_nx = nx;
+                best_ny = ny;
+                best_bary[0] = bary[0];
+                best_bary[1] = bary[1];
+                best_bary[2] = bary[2];
+            }
+        }
+    }
+    if (active && !failed) {
+        TriField f;
+        f.sd = (float)best;
+        f.body1 = body1;
+        f.nx = (float)best_nx;
+        f.ny = (float)best_ny;
+        f.b1 = (float)best_bary[1];
+        f.b2 = (float)best_bary[2];
+        f.ix = 0.f;
+        f.iy = 0.f;
+        c.field[(uint32_t)hy * P.node_w + (uint32_t)hx] = f;
+    }
+}
+
+// applyTriangleContactImpulses (shaders.ts:2535-2670): one CTA per body sums
+// the barycentric shares of the fluid impulses stored at the field nodes it
+// owns (strided partial sums, then a halving reduction) and adds them to the
+// vertex velocities.
+__global__ void __launch_bounds__(BODY_THREADS) k_body_impulses(Ctx c)
+{
+    const StepParams &P = *c.P;
+    __shared__ int s_valid;
+    __shared__ int s_box[4];
+    __shared__ uint32_t s_start;
+    __shared__ float2 s_i[3][BODY_THREADS];
+    for (uint32_t b = blockIdx.x; b < P.n_bodies; b += gridDim.x) {
+        if (threadIdx.x == 0) {
+            s_valid = 0;
+            if (*(volatile uint32_t *)c.status == 0u) {
+                const uint32_t start = c.body_starts[b];
+                if (!body_markers_valid(c, start)) {
+                    fail_at(c.status, start, ERROR_TRIANGLE_BOND);
+                } else {
+                    const float2 p0 = in_position(c, start), p1 = in_position(c, start + 1u),
+                                 p2 = in_position(c, start + 2u);
+                    const float r = P.contact_reach;
+                    const float mnx = fminf(p0.x, fminf(p1.x, p2.x)) - r, mny = fminf(p0.y, fminf(p1.y, p2.y)) - r;
+                    const float mxx = fmaxf(p0.x, fmaxf(p1.x, p2.x)) + r, mxy = fmaxf(p0.y, fmaxf(p1.y, p2.y)) + r;
+                    const int hi_x = (int)P.cells_x + 1, hi_y = (int)P.cells_y + 1;
+                    s_box[0] = min(max((int)floorf(mnx / P.dx), -1), hi_x);
+                    s_box[1] = min(max((int)floorf(mny / P.dx), -1), hi_y);
+                    s_box[2] = min(max((int)ceilf(mxx / P.dx), -1), hi_x);
+                    s_box[3] = min(max((int)ceilf(mxy / P.dx), -1), hi_y);
+                    s_start = start;
+                    s_valid = 1;
+                }
+            }
+        }
+        __syncthreads();
+        float2 i0 = make_float2(0.f, 0.f), i1 = i0, i2 = i0;
+        if (s_valid) {
+            const int w = s_box[2] - s_box[0] + 1, h = s_box[3] - s_box[1] + 1;
+            const uint32_t body1 = s_start + 1u;
+            for (int k = threadIdx.x; k < w * h; k += BODY_THREADS) {
+                const TriField f = c.field[node_index(P, s_box[0] + k % w, s_box[1] + k / w)];
+                if (f.body1 != body1) continue;
+                const float w0 = 1.0f - f.b1 - f.b2;
+                i0 = make_float2(i0.x + w0 * f.ix, i0.y + w0 * f.iy);
+                i1 = make_float2(i1.x + f.b1 * f.ix, i1.y + f.b1 * f.iy);
+                i2 = make_float2(i2.x + f.b2 * f.ix, i2.y + f.b2 * f.iy);
+            }
+        }
+        s_i[0][threadIdx.x] = i0;
+        s_i[1][threadIdx.x] = i1;
+        s_i[2][threadIdx.x] = i2;
+        __syncthreads();
+        for (int stride = BODY_THREADS / 2; stride > 0; stride /= 2) {
+            if ((int)threadIdx.x < stride) {
+#pragma unroll
+                for (int v = 0; v < 3; ++v)
+                    s_i[v][threadIdx.x] = make_float2(s_i[v][threadIdx.x].x + s_i[v][threadIdx.x + stride].x,
+                                                      s_i[v][threadIdx.x].y + s_i[v][threadIdx.x + stride].y);
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0 && s_valid && *(volatile uint32_t *)c.status == 0u) {
+            const float inv_m = 1.0f / P.particle_mass;
+            float2 v[3];
+            bool ok = true;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float2 old = c.out.vel[c.slot_out[s_start + (uint32_t)k]];
+                v[k] = make_float2(old.x + inv_m * s_i[k][0].x, old.y + inv_m * s_i[k][0].y);
+                ok = ok && finite2(v[k]);
+            }
+            if (!ok) {
+                fail_at(c.status, s_start, ERROR_TRIANGLE_CONTACT);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) c.out.vel[c.slot_out[s_start + (uint32_t)k]] = v[k];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// solveBondedTriangles (shaders.ts:2672-2797): two Gauss-Seidel passes over
+// the three edges in offsets from the first vertex, stiffness
+// min(k (dt / dtRef)^2, 1); the displacement also enters the velocity.
+__global__ void k_body_bonded(Ctx c)
+{
+    const StepParams &P = *c.P;
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= P.n_bodies || *(volatile uint32_t *)c.status != 0u) return;
+    const uint32_t start = c.body_starts[b];
+    if (!body_markers_valid(c, start)) {
+        fail_at(c.status, start, ERROR_TRIANGLE_BOND);
+        return;
+    }
+    uint32_t slot[3];
+    float2 pos[3], vel[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        slot[k] = c.slot_out[start + (uint32_t)k];
+        pos[k] = c.out.pos[slot[k]];
+        vel[k] = c.out.vel[slot[k]];
+    }
+    const float2 orig[3] = {make_float2(0.f, 0.f), make_float2(pos[1].x - pos[0].x, pos[1].y - pos[0].y),
+                            make_float2(pos[2].x - pos[0].x, pos[2].y - pos[0].y)};
+    float2 off[3] = {orig[0], orig[1], orig[2]};
+    const float dt = P.dt, inv_dt = 1.0f / dt;
+    const float ratio = dt / P.bond_reference_dt;
+    const float stiffness = fminf(P.bond_stiffness * ratio * ratio, 1.0f);
+    for (int it = 0; it < BONDED_TRIANGLE_SOLVER_ITERATIONS; ++it) {
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+            const int a0 = e, a1 = (e + 1) % 3;
+            float2 corr;
+            if (!edge_correction(off[a0], off[a1], P.bond_rest_length, stiffness, corr)) {
+                fail_at(c.status, start, ERROR_TRIANGLE_BOND);
+                return;
+            }
+            off[a0] = make_float2(off[a0].x + corr.x, off[a0].y + corr.y);
+            off[a1] = make_float2(off[a1].x - corr.x, off[a1].y - corr.y);
+        }
+    }
+    float2 np[3], nv[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float2 disp = make_float2(off[k].x - orig[k].x, off[k].y - orig[k].y);
+        np[k] = make_float2(pos[k].x + disp.x, pos[k].y + disp.y);
+        nv[k] = make_float2(vel[k].x + disp.x * inv_dt, vel[k].y + disp.y * inv_dt);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float2 bx = confine_axis(np[k].x, nv[k].x, P.domain_w);
+        const float2 by = confine_axis(np[k].y, nv[k].y, P.domain_h);
+        np[k] = make_float2(bx.x, by.x);
+        nv[k] = make_float2(bx.y, by.y);
+        if (!finite2(np[k]) || !finite2(nv[k])) {
+            fail_at(c.status, start, ERROR_TRIANGLE_CONTACT);
+            return;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        c.out.pos[slot[k]] = np[k];
+        c.out.vel[slot[k]] = nv[k];
+    }
+}
+
+// gatherTriangleContactStates (shaders.ts:2044-2112): mean vertex velocity;
+// the contact degree comes from k_body_pairs when pair contacts are cached,
+// else from a scan of the other bodies here.
+__global__ void k_body_states(Ctx c)
+{
+    const StepParams &P = *c.P;
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= P.n_bodies || *(volatile uint32_t *)c.status != 0u) return;
+    const uint32_t start = c.body_starts[b];
+    if (!body_markers_valid(c, start)) {
+        fail_at(c.status, start, ERROR_TRIANGLE_BOND);
+        return;
+    }
+    uint32_t count = 0;
+    if (!c.pair_cache) {
+        const uint32_t obj = c.obj[start];
+        for (uint32_t o = 0; o < P.n_bodies; ++o) {
+            if (o == b) continue;
+            const uint32_t os = c.body_starts[o];
+            if (!body_markers_valid(c, os)) {
+                fail_at(c.status, os, ERROR_TRIANGLE_BOND);
+                return;
+            }
+            if (c.obj[os] == obj) continue;
+            if (body_contact(c, b, o).z > 0.f) ++count;
+        }
+    }
+    float2 v = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float2 vk = c.out.vel[c.slot_out[start + (uint32_t)k]];
+        v = make_float2(v.x + vk.x, v.y + vk.y);
+    }
+    c.body_vel[b] = make_float2(v.x / 3.0f, v.y / 3.0f);
+    c.contact_count[b] = count;
+}
+
+// gatherTrianglePairContacts (shaders.ts:1994-2042): the contact of every
+// unordered body pair of different objects, and the contact degrees.
+__global__ void k_body_pairs(Ctx c)
+{
+    const StepParams &P = *c.P;
+    const uint32_t nb = P.n_bodies;
+    const uint32_t pair = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pair >= nb * nb) return;
+    const uint32_t b = pair / nb, o = pair % nb;
+    if (b >= o || *(volatile uint32_t *)c.status != 0u) return;
+    const uint32_t bs = c.body_starts[b], os = c.body_starts[o];
+    if (c.obj[os] == c.obj[bs]) return;
+    const float3 contact = body_contact(c, b, o);
+    c.pair_cache[pair] = make_float4(contact.x, contact.y, contact.z, 0.f);
+    if (contact.z > 0.f) {
+        atomicAdd(&c.contact_count[b], 1u);
+        atomicAdd(&c.contact_count[o], 1u);
+    }
+}
+
+// applyTrianglePairContacts (shaders.ts:2799-2955): Jacobi normal impulses
+// against every contacting body in ascending order, relaxed by 0.25 over the
+// larger contact degree, added to the three vertex velocities.
+__global__ void k_body_apply(Ctx c)
+{
+    const StepParams &P = *c.P;
+    const uint32_t nb = P.n_bodies;
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb || *(volatile uint32_t *)c.status != 0u) return;
+    const uint32_t start = c.body_starts[b];
+    if (!body_markers_valid(c, start)) {
+        fail_at(c.status, start, ERROR_TRIANGLE_BOND);
+        return;
+    }
+    const float2 vb = c.body_vel[b];
+    const uint32_t count = c.contact_count[b];
+    const uint32_t obj = c.obj[start];
+    const float body_mass = 3.0f * P.particle_mass;
+    float2 delta = make_float2(0.f, 0.f);
+    for (uint32_t o = 0; count != 0u && o < nb; ++o) {
+        if (o == b) continue;
+        float3 contact = make_float3(0.f, 0.f, 0.f);
+        if (c.pair_cache) {
+            const float4 cached = c.pair_cache[min(b, o) * nb + max(b, o)];
+            if (c.obj[c.body_starts[o]] == obj || cached.z <= 0.f) continue;
+            contact = b < o ? make_float3(cached.x, cached.y, cached.z) : make_float3(-cached.x, -cached.y, cached.z);
+        }
+        const uint32_t os = c.body_starts[o];
+        if (!body_markers_valid(c, os)) {
+            fail_at(c.status, os, ERROR_TRIANGLE_BOND);
+            return;
+        }
+        if (c.obj[os] == obj) continue;
+        if (!c.pair_cache) {
+            contact = body_contact(c, b, o);
+            if (contact.z <= 0.f) continue;
+        }
+        const float2 vo = c.body_vel[o];
+        const uint32_t degree = max(count, c.contact_count[o]);
+        if (degree == 0u) {
+            fail_at(c.status, start, ERROR_TRIANGLE_CONTACT);
+            return;
+        }
+        const float weight = 1.0f / (float)degree;
+        const float rn = (vb.x - vo.x) * contact.x + (vb.y - vo.y) * contact.y;
+        if (rn < 0.f) {
+            const float magnitude = -rn / (2.0f / body_mass);
+            const float iw = TRIANGLE_CONTACT_IMPULSE_RELAXATION * weight;
+            delta = make_float2(delta.x + iw * magnitude * contact.x / body_mass,
+                                delta.y + iw * magnitude * contact.y / body_mass);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const uint32_t slot = c.slot_out[start + (uint32_t)k];
+        const float2 v = c.out.vel[slot];
+        if (!move_vertex(c, slot, c.out.pos[slot], make_float2(v.x + delta.x, v.y + delta.y))) {
+            fail_at(c.status, start, ERROR_TRIANGLE_CONTACT);
+            return;
+        }
+    }
+}
+
+// validateCflParticles (shaders.ts:2456-2461): the CFL check of every particle
+// after the body passes (G2P checks them itself when there are no bodies).
+__global__ void k_validate_cfl(Ctx c)
+{
+    const uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= c.n) return;
+    const Material m = c.mats[c.out.mat[d]];
+    validate_cfl(c, c.out.orig[d], m, c.out.vel[d], c.out.F[d], c.out.damage[d], c.out.vol[d], -1.0f);
+}
+
+// updateFractureBonds (shaders.ts:2957-3003): tensile strain of each bond
+// from the committed positions -> damage, broken latch.
+__global__ void k_fracture_bonds(Ctx c)
+{
+    const StepParams &P = *c.P;
+    const uint32_t bi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (bi >= P.n_bonds || *(volatile uint32_t *)c.status != 0u) return;
+    uint32_t *w = c.bonds + 6u * bi;
+    const uint32_t first = w[0], second = w[1];
+    const float rest = __uint_as_float(w[2]), failure = __uint_as_float(w[3]);
+    float damage = __uint_as_float(w[4]);
+    if (first >= P.fracture_particles || second >= P.fracture_particles || first >= c.n || second >= c.n ||
+        !finite_f(rest) || rest <= 0.f || !finite_f(failure) || failure <= 0.f) {
+        fail_at(c.status, min(first, second), ERROR_FRACTURE_BOND);
+        return;
+    }
+    if (w[5] != 0u) {
+        w[4] = __float_as_uint(1.0f);
+        return;
+    }
+    const float2 a = c.out.pos[c.slot_out[first]], b = c.out.pos[c.slot_out[second]];
+    const float sx = b.x - a.x, sy = b.y - a.y;
+    const float dist = sqrtf(sx * sx + sy * sy);
+    if (!finite_f(dist)) {
+        fail_at(c.status, first, ERROR_FRACTURE_BOND);
+        return;
+    }
+    const float strain = fmaxf(0.f, (dist - rest) / rest);
+    damage = fmaxf(damage, fminf(1.0f, strain / failure));
+    if (strain >= failure) {
+        damage = 1.0f;
+        w[5] = 1u;
+    }
+    w[4] = __float_as_uint(damage);
+}
+
+// applyFractureParticleDamage (shaders.ts:3005-3039): a Neo-Hookean endpoint
+// takes the largest damage of its bonds (CSR incidence).
+__global__ void k_fracture_damage(Ctx c)
+{
+    const StepParams &P = *c.P;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= c.n_endpoints || *(volatile uint32_t *)c.status != 0u) return;
+    const uint32_t i = c.endpoints[k];
+    const uint32_t first = c.topology[i], next = c.topology[i + 1u];
+    if (next < first || next > P.fracture_incidence) {
+        fail_at(c.status, i, ERROR_FRACTURE_BOND);
+        return;
+    }
+    const uint32_t slot = c.slot_out[i];
+    if (c.mats[c.out.mat[slot]].model != MODEL_NEO_HOOKEAN) return;
+    float damage = fminf(fmaxf(c.out.damage[slot], 0.f), 1.0f);
+    const uint32_t base = P.fracture_particles + 1u;
+    for (uint32_t inc = first; inc < next; ++inc) {
+        const uint32_t bond = c.topology[base + inc];
+        if (bond >= P.n_bonds) {
+            fail_at(c.status, i, ERROR_FRACTURE_BOND);
+            return;
+        }
+        damage = fmaxf(damage, __uint_as_float(c.bonds[6u * bond + 4u]));
+    }
+    c.out.damage[slot] = damage;
+}
+
+// The tile count and P2G record of each tracked particle, from its state
+// after the body and fracture passes (G2P left them out).
+__global__ void k_body_finish(Ctx c)
+{
+    const StepParams &P = *c.P;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= c.n_tracked || *(volatile uint32_t *)c.status != 0u) return;
+    const uint32_t orig = c.tracked[k];
+    const uint32_t d = c.slot_out[orig];
+    Stencil st;
+    if (!make_stencil_fast(P, c.out.pos[d], st) || !stencil_fits(P, st.bx, st.by)) {
+        fail(c.status, ERROR_STENCIL);
+        return;
+    }
+    const uint32_t key = particle_tile(P, st.bx, st.by);
+    c.ranks[d] = atomicAdd(&c.tile_count[key], 1u);
+    c.keys[d] = key;
+    const Material m = c.mats[c.out.mat[d]];
+    write_record(c, d, m, st, c.out.vel[d], c.out.F[d], c.out.vol[d], c.out.damage[d], c.out.pvol[d], c.out.C[d]);
 }
 
 }  // namespace mpm

@@ -38,6 +38,16 @@ struct ParticleBuffers {
     uint32_t *orig;
 };
 
+// Nearest bonded-triangle (pebble) sample of one halo node
+// (TriangleFieldNode, src/lib/mpm/kernels/shaders.ts; 32 B).
+struct TriField {
+    float sd;        // signed distance, the band when no body is near
+    uint32_t body1;  // original index of the body's first vertex + 1 (0: none)
+    float nx, ny;    // outward normal
+    float b1, b2;    // barycentric weights of the second and third vertex
+    float ix, iy;    // impulse the fluid put on the body at this node
+};
+
 struct Ctx {
     const StepParams *P;
     uint32_t n;        // particle count (fixed for a solver; kernels read it from the parameter bank)
@@ -81,6 +91,20 @@ struct Ctx {
     int32_t *fixed;
     uint32_t *tile_stamp;
     float4 *affine_out;  // optional: prepared affine per slot (parity checks)
+    // bonded-triangle bodies and fracture bonds (NULL / 0 when the scene has none)
+    TriField *field;              // per halo node
+    const uint32_t *body_starts;  // per body: original index of its first vertex
+    uint32_t *slot_in, *slot_out; // current slot of each tracked original index (input / output buffer)
+    const uint32_t *track_flag;   // per original index: 1 when its slot is tracked
+    const uint32_t *tracked;      // tracked original indices
+    uint32_t n_tracked;
+    float4 *pair_cache;           // per ordered body pair (a < b): contact normal, penetration
+    uint32_t *contact_count;      // per body
+    float2 *body_vel;             // per body: mean vertex velocity
+    uint32_t *bonds;              // 6 words per fracture bond
+    const uint32_t *topology;     // fracture CSR: offsets[n + 1], then bond indices
+    const uint32_t *endpoints;    // original indices with at least one fracture bond
+    uint32_t n_endpoints;
 };
 
 constexpr int SCAN_THREADS = 512;
@@ -100,6 +124,10 @@ constexpr uint32_t REC_FAILED = 1u << 16;  // the record's prepareParticle faile
 constexpr int VOL_X = RING_X + 2;          // ring nodes and their neighbours
 constexpr int VOL_Y = RING_Y + 2;
 constexpr int G2P_THREADS = 256;
+constexpr int FIELD_BODY_CHUNK = TILE_NODES;  // bodies staged per pass of k_triangle_field
+constexpr int BODY_THREADS = 64;              // k_body_impulses: one CTA per body
+constexpr uint32_t PAIR_CACHE_BODIES = 2048;  // bodies up to which pair contacts are cached
+constexpr int BONDED_TRIANGLE_SOLVER_ITERATIONS = 2;
 constexpr int G2P_STAGE = 2 * G2P_THREADS;  // particles of a tile staged at once
 static_assert(VOL_X * VOL_Y <= G2P_THREADS && RING_NODES <= G2P_THREADS, "one node per thread");
 
@@ -125,6 +153,17 @@ __global__ void k_g2p(Ctx c);
 __global__ void k_commit(Ctx c);
 __global__ void k_speed_max(Ctx c);
 __global__ void k_begin_batch(Ctx c, uint32_t reset_progress);
+// bodies and fracture
+__global__ void k_triangle_field(Ctx c);
+__global__ void k_body_impulses(Ctx c);
+__global__ void k_body_bonded(Ctx c);
+__global__ void k_body_states(Ctx c);
+__global__ void k_body_pairs(Ctx c);
+__global__ void k_body_apply(Ctx c);
+__global__ void k_validate_cfl(Ctx c);
+__global__ void k_fracture_bonds(Ctx c);
+__global__ void k_fracture_damage(Ctx c);
+__global__ void k_body_finish(Ctx c);
 __global__ void k_count_active_nodes(Ctx c, uint32_t *counts);
 
 }  // namespace mpm

@@ -105,6 +105,15 @@ struct mpm_solver {
     float4 *rec_state = nullptr, *rec_affine = nullptr;
     float2 *rec_mom = nullptr;
     uint32_t *rec_cell = nullptr;
+    // bonded-triangle bodies and fracture bonds
+    TriField *field = nullptr;
+    uint32_t *body_starts = nullptr, *slot_of[2] = {nullptr, nullptr}, *track_flag = nullptr, *tracked = nullptr;
+    uint32_t n_tracked = 0;
+    float4 *pair_cache = nullptr;
+    uint32_t *contact_count = nullptr;
+    float2 *body_vel = nullptr;
+    uint32_t *bonds = nullptr, *topology = nullptr, *endpoints = nullptr;
+    uint32_t n_endpoints = 0, fracture_particles = 0, fracture_incidence = 0;
     unsigned p2g_ctas = 1, g2p_ctas = 1;  // persistent grids of the default path
 
     mpm_drag drag{};
@@ -162,6 +171,20 @@ Ctx make_ctx(mpm_solver *s, int parity)
     c.rec_mom = s->rec_mom;
     c.rec_cell = s->rec_cell;
     c.affine_out = nullptr;
+    c.field = s->field;
+    c.body_starts = s->body_starts;
+    c.slot_in = s->slot_of[parity];
+    c.slot_out = s->slot_of[1 - parity];
+    c.track_flag = s->track_flag;
+    c.tracked = s->tracked;
+    c.n_tracked = s->n_tracked;
+    c.pair_cache = s->pair_cache;
+    c.contact_count = s->contact_count;
+    c.body_vel = s->body_vel;
+    c.bonds = s->bonds;
+    c.topology = s->topology;
+    c.endpoints = s->endpoints;
+    c.n_endpoints = s->n_endpoints;
     return c;
 }
 
@@ -228,6 +251,31 @@ void enqueue_cell_sort(mpm_solver *s, const Ctx &c)
     k_stable_rank<<<pb, PARTICLE_THREADS, 0, s->stream>>>(c);
 }
 
+// The passes after G2P for bonded-triangle bodies and fracture bonds, in the
+// reference's order (solver.ts:1505-1562): contact impulses, bonded edges,
+// contact states, pair contacts, the CFL check, fracture; then the tile
+// counts and P2G records of the particles those passes moved.
+void enqueue_bodies(mpm_solver *s, const Ctx &c)
+{
+    const uint32_t nb = s->n_bodies;
+    if (nb) {
+        const unsigned bb = blocks_for(nb, 64);
+        k_body_impulses<<<std::min(nb, 1024u), BODY_THREADS, 0, s->stream>>>(c);
+        k_body_bonded<<<bb, 64, 0, s->stream>>>(c);
+        k_body_states<<<bb, 64, 0, s->stream>>>(c);
+        if (s->pair_cache) k_body_pairs<<<blocks_for(nb * nb, 256), 256, 0, s->stream>>>(c);
+        k_body_apply<<<bb, 64, 0, s->stream>>>(c);
+        // captured graphs serve batches with and without a CFL guard: the
+        // kernel reads the batch's flag from the device parameters
+        k_validate_cfl<<<blocks_for(s->n, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c);
+    }
+    if (s->n_bonds) {
+        k_fracture_bonds<<<blocks_for(s->n_bonds, 64), 64, 0, s->stream>>>(c);
+        if (s->n_endpoints) k_fracture_damage<<<blocks_for(s->n_endpoints, 64), 64, 0, s->stream>>>(c);
+    }
+    if (s->gather() && s->n_tracked) k_body_finish<<<blocks_for(s->n_tracked, 64), 64, 0, s->stream>>>(c);
+}
+
 // One full substep from buffer `parity` into 1 - parity.
 void enqueue_substep(mpm_solver *s, int parity)
 {
@@ -241,6 +289,7 @@ void enqueue_substep(mpm_solver *s, int parity)
         mark(K_TILE_SCATTER);
         k_p2g_gather<<<s->p2g_ctas, TILE_CELLS, 0, s->stream>>>(c);
         mark(K_P2G_GATHER);
+        if (s->n_bodies) k_triangle_field<<<tiles, TILE_NODES, 0, s->stream>>>(c);
         k_g2p_tile<<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
         mark(K_G2P_TILE);
     } else {
@@ -248,11 +297,13 @@ void enqueue_substep(mpm_solver *s, int parity)
         mark(K_PREPARE_SCATTER);
         k_fixed_decode<<<tiles, TILE_NODES, 0, s->stream>>>(c);
         mark(K_FIXED_DECODE);
+        if (s->n_bodies) k_triangle_field<<<tiles, TILE_NODES, 0, s->stream>>>(c);
         k_grid_update<<<tiles, TILE_NODES, 0, s->stream>>>(c);
         mark(K_GRID_UPDATE);
         k_g2p<<<pb, PARTICLE_THREADS, 0, s->stream>>>(c);
         mark(K_G2P);
     }
+    enqueue_bodies(s, c);
     const unsigned cb = std::min(blocks_for(s->n, PARTICLE_THREADS), 592u);
     k_commit<<<cb, PARTICLE_THREADS, 0, s->stream>>>(c);
     mark(K_COMMIT);
@@ -300,6 +351,9 @@ void fill_params(mpm_solver *s, StepParams &p, float dt, float gx, float gy, con
     p.n_bodies = s->n_bodies;
     p.cfl_enabled = guard ? 1u : 0u;
     p.n_bonds = s->n_bonds;
+    p.fracture_particles = s->fracture_particles;
+    p.fracture_incidence = s->fracture_incidence;
+    p.pair_cache_enabled = s->pair_cache ? 1u : 0u;
     p.fixed_shift = c.fixed_point_shift;
     p.dx = c.cell_size;
     p.inv_dx = 1.0f / c.cell_size;
@@ -412,6 +466,11 @@ int unpack_and_upload(mpm_solver *s, const float *packed, uint32_t count, int ta
     CUDA_TRY(cudaMemcpyAsync(b.mat, mat.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
     CUDA_TRY(cudaMemcpyAsync(b.orig, orig.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
     CUDA_TRY(cudaMemcpyAsync(s->bonded, bonded.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+    if (s->slot_of[target]) {
+        // the uploaded slots are in original order
+        CUDA_TRY(cudaMemcpyAsync(s->slot_of[target], orig.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                 s->stream));
+    }
     // the copies above read pageable host vectors; wait before they go away
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     return MPM_OK;
@@ -464,7 +523,9 @@ void free_solver(mpm_solver *s)
                     s->tmp, s->perm, s->cell_count, s->cell_start, s->block_sums, s->p2g_solid, s->p2g_water,
                     s->p2g_oil, s->g_solid, s->g_water, s->g_oil, s->fixed, s->tile_stamp, s->d_active,
                     s->tile_count, s->tile_start, s->active_tiles, s->part, s->tile_info,
-                    s->rec_state, s->rec_affine, s->rec_mom, s->rec_cell};
+                    s->rec_state, s->rec_affine, s->rec_mom, s->rec_cell, s->field, s->body_starts,
+                    s->slot_of[0], s->slot_of[1], s->track_flag, s->tracked, s->pair_cache, s->contact_count,
+                    s->body_vel, s->bonds, s->topology, s->endpoints};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (int b = 0; b < 2; ++b) {
@@ -483,7 +544,8 @@ void free_solver(mpm_solver *s)
 }
 
 int create_impl(const mpm_config *config, const float *packed, const uint32_t *object_ids, uint32_t count,
-                const uint32_t *body_starts, uint32_t body_count, mpm_solver **out)
+                const uint32_t *body_starts, uint32_t body_count, const uint32_t *bonds, uint32_t bond_count,
+                const uint32_t *topology, uint32_t topology_words, mpm_solver **out)
 {
     if (!config || !out) return set_error(MPM_ERR_INVALID_ARGUMENT, "config and out must not be NULL");
     *out = nullptr;
@@ -509,6 +571,23 @@ int create_impl(const mpm_config *config, const float *packed, const uint32_t *o
     if ((uint64_t)c.capacity * 9ull > 0x7fffffffull)
         return set_error(MPM_ERR_INVALID_ARGUMENT, "particle stencil entries exceed the index range");
     if (body_count > 0 && !body_starts) return set_error(MPM_ERR_INVALID_ARGUMENT, "body_starts must not be NULL");
+    for (uint32_t b = 0; b < body_count; ++b)
+        if ((uint64_t)body_starts[b] + 2u >= count)
+            return set_error(MPM_ERR_INVALID_ARGUMENT, "bonded triangle body %u starts outside the particles", b);
+    if (bond_count > 0) {
+        // packed 6-word bonds and CSR incidence (layout.ts:498-564)
+        if (!bonds || !topology) return set_error(MPM_ERR_INVALID_ARGUMENT, "fracture bonds and topology must not be NULL");
+        if ((uint64_t)topology_words != (uint64_t)count + 1u + 2ull * bond_count)
+            return set_error(MPM_ERR_INVALID_ARGUMENT, "fracture topology must hold %u offsets and %u incidences",
+                             count + 1u, 2u * bond_count);
+        for (uint32_t i = 0; i < count; ++i)
+            if (topology[i + 1] < topology[i]) return set_error(MPM_ERR_INVALID_ARGUMENT, "fracture topology offsets must not decrease");
+        if (topology[0] != 0u || topology[count] != 2u * bond_count)
+            return set_error(MPM_ERR_INVALID_ARGUMENT, "fracture topology offsets must span every incidence");
+        for (uint32_t b = 0; b < bond_count; ++b)
+            if (bonds[6 * b] >= count || bonds[6 * b + 1] >= count)
+                return set_error(MPM_ERR_INVALID_ARGUMENT, "fracture bond %u connects a missing particle", b);
+    }
 
     int device_count = 0;
     CUDA_TRY(cudaGetDeviceCount(&device_count));
@@ -522,6 +601,11 @@ int create_impl(const mpm_config *config, const float *packed, const uint32_t *o
     s->n = count;
     s->capacity = std::max<uint32_t>(c.capacity, 1u);
     s->n_bodies = body_count;
+    s->n_bonds = bond_count;
+    if (bond_count > 0) {
+        s->fracture_particles = count;
+        s->fracture_incidence = 2u * bond_count;
+    }
     s->node_w = c.cells_x + 3;
     s->node_h = c.cells_y + 3;
     s->node_count = (uint32_t)nodes;
@@ -615,6 +699,55 @@ int create_impl(const mpm_config *config, const float *packed, const uint32_t *o
         if (cudaMemsetAsync(s->fixed, 0, (size_t)s->node_count * FIXED_WORDS * sizeof(int32_t), s->stream) != cudaSuccess)
             return fail(set_error(MPM_ERR_CUDA, "cudaMemset failed"));
     }
+    if (body_count > 0 || bond_count > 0) {
+        // tracked particles: bonded-triangle vertices and fracture endpoints
+        std::vector<uint32_t> flag(count, 0u), tracked, endpoints, identity(count);
+        for (uint32_t i = 0; i < count; ++i) {
+            identity[i] = i;
+            const uint32_t marker = f2u(packed[(size_t)i * MPM_PARTICLE_WORDS + 19]);
+            const bool endpoint = bond_count > 0 && topology[i + 1] > topology[i];
+            if (endpoint) endpoints.push_back(i);
+            if (marker != 0u || endpoint) {
+                flag[i] = 1u;
+                tracked.push_back(i);
+            }
+        }
+        s->n_tracked = (uint32_t)tracked.size();
+        s->n_endpoints = (uint32_t)endpoints.size();
+        ALLOC(s->track_flag, count);
+        ALLOC(s->tracked, tracked.size());
+        ALLOC(s->endpoints, endpoints.size());
+        for (int b = 0; b < 2; ++b) ALLOC(s->slot_of[b], count);
+        if (body_count > 0) {
+            ALLOC(s->field, s->node_count);
+            ALLOC(s->body_starts, body_count);
+            ALLOC(s->contact_count, body_count);
+            ALLOC(s->body_vel, body_count);
+            if (body_count <= PAIR_CACHE_BODIES) {
+                ALLOC(s->pair_cache, (size_t)body_count * body_count);
+                cudaMemsetAsync(s->pair_cache, 0, (size_t)body_count * body_count * sizeof(float4), s->stream);
+            }
+            cudaMemsetAsync(s->field, 0, (size_t)s->node_count * sizeof(TriField), s->stream);
+        }
+        if (bond_count > 0) {
+            ALLOC(s->bonds, 6u * (size_t)bond_count);
+            ALLOC(s->topology, topology_words);
+        }
+        bool ok = cudaMemcpy(s->track_flag, flag.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice) == cudaSuccess;
+        if (!tracked.empty())
+            ok = ok && cudaMemcpy(s->tracked, tracked.data(), tracked.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) == cudaSuccess;
+        if (!endpoints.empty())
+            ok = ok && cudaMemcpy(s->endpoints, endpoints.data(), endpoints.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) == cudaSuccess;
+        for (int b = 0; b < 2; ++b)
+            ok = ok && cudaMemcpy(s->slot_of[b], identity.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice) == cudaSuccess;
+        if (body_count > 0)
+            ok = ok && cudaMemcpy(s->body_starts, body_starts, body_count * sizeof(uint32_t), cudaMemcpyHostToDevice) == cudaSuccess;
+        if (bond_count > 0) {
+            ok = ok && cudaMemcpy(s->bonds, bonds, 6u * (size_t)bond_count * sizeof(uint32_t), cudaMemcpyHostToDevice) == cudaSuccess;
+            ok = ok && cudaMemcpy(s->topology, topology, (size_t)topology_words * sizeof(uint32_t), cudaMemcpyHostToDevice) == cudaSuccess;
+        }
+        if (!ok) return fail(set_error(MPM_ERR_CUDA, "body and fracture upload failed"));
+    }
 #undef ALLOC
     cudaMemsetAsync(s->cell_count, 0, (size_t)s->cell_pad * sizeof(uint32_t), s->stream);
     cudaMemsetAsync(s->tile_stamp, 0, (size_t)s->tiles_x * s->tiles_y * sizeof(uint32_t), s->stream);
@@ -651,13 +784,8 @@ int mpm_create(const mpm_config *config, const float *packed_particles, const ui
                uint32_t fracture_topology_words, mpm_solver **out)
 {
     g_last_error.clear();
-    if (body_count > 0 || fracture_bond_count > 0)
-        return set_error(MPM_ERR_INVALID_ARGUMENT,
-                         "bonded triangle bodies and fracture bonds are not supported by this build yet");
-    (void)fracture_bonds;
-    (void)fracture_topology;
-    (void)fracture_topology_words;
-    return create_impl(config, packed_particles, object_ids, particle_count, body_starts, body_count, out);
+    return create_impl(config, packed_particles, object_ids, particle_count, body_starts, body_count, fracture_bonds,
+                       fracture_bond_count, fracture_topology, fracture_topology_words, out);
 }
 
 int mpm_step_batch(mpm_solver *s, uint32_t step_count, float dt, float gx, float gy, const mpm_cfl_guard *guard,
@@ -967,6 +1095,24 @@ int mpm_probe_sort(mpm_solver *s, float dt, uint32_t *keys_out, uint32_t *perm_o
         if (keys_out) keys_out[orig[slot]] = keys[slot];
     for (uint32_t d = 0; d < n; ++d)
         if (perm_out) perm_out[d] = orig[perm[d]];
+    return MPM_OK;
+}
+
+int mpm_probe_triangle_field(mpm_solver *s, float dt, float *field_out)
+{
+    g_last_error.clear();
+    if (!s || !field_out) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and field_out must not be NULL");
+    if (!s->field) return set_error(MPM_ERR_STATE, "the scene has no bonded triangle bodies");
+    CUDA_TRY(cudaSetDevice(s->device));
+    int rc = upload_params(s, dt, 0.0f, 0.0f, nullptr, 0.0f);
+    if (rc != MPM_OK) return rc;
+    const Ctx c = make_ctx(s, s->cur);
+    if (s->gather()) enqueue_tile_count(s, c);  // the tracked slots of the current buffer
+    k_triangle_field<<<dim3(s->tiles_x, s->tiles_y), TILE_NODES, 0, s->stream>>>(c);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(field_out, s->field, (size_t)s->node_count * sizeof(TriField), cudaMemcpyDeviceToHost,
+                             s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
     return MPM_OK;
 }
 

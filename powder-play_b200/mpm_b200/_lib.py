@@ -22,7 +22,7 @@ EXPORTED_SYMBOLS = (
     "mpm_create", "mpm_step_batch", "mpm_read_compact", "mpm_read_status", "mpm_clear_status",
     "mpm_read_particles", "mpm_write_particles", "mpm_set_drag", "mpm_queue_completion_ms",
     "mpm_particle_count", "mpm_particle_capacity", "mpm_destroy", "mpm_last_error", "mpm_probe_sort",
-    "mpm_probe_fixed_point", "mpm_node_count", "mpm_last_batch_device_ms", "mpm_profile_substeps",
+    "mpm_probe_fixed_point", "mpm_probe_triangle_field", "mpm_node_count", "mpm_last_batch_device_ms", "mpm_profile_substeps",
     "mpm_profile_kernel_name", "mpm_profile_kernel_slots", "mpm_count_active_nodes", "mpm_stream",
 )
 
@@ -91,6 +91,8 @@ def load_library(path: str = LIBRARY_PATH) -> ctypes.CDLL:
     lib.mpm_last_error.restype = ctypes.c_char_p
     lib.mpm_probe_sort.argtypes = [vp, f32, vp, vp, vp]
     lib.mpm_probe_sort.restype = i32
+    lib.mpm_probe_triangle_field.argtypes = [vp, f32, vp]
+    lib.mpm_probe_triangle_field.restype = i32
     lib.mpm_probe_fixed_point.argtypes = [vp, f32, vp, vp]
     lib.mpm_probe_fixed_point.restype = i32
     lib.mpm_last_batch_device_ms.argtypes = [vp, P(ctypes.c_double)]

@@ -525,6 +525,22 @@ class MpmMlsGpuSolver:
                "fixed-point probe failed")
         return words, affine
 
+    def probe_triangle_field(self, dt: float) -> dict:
+        """The bonded-triangle field of the current particles (measurement /
+        parity probe): sd, body (first-vertex index, -1: none), normal, bary
+        (three weights), as (cellsY+3, cellsX+3) arrays."""
+        nodes = self.node_count
+        raw = np.zeros((nodes, 8), dtype=np.float32)
+        _check(self._lib.mpm_probe_triangle_field(self._handle, fround(dt), _lib.ptr(raw)),
+               "triangle field probe failed")
+        grid = self._state.config["grid"]
+        h, w = int(grid["cellsY"]) + 3, int(grid["cellsX"]) + 3
+        words = raw.view(np.uint32)
+        b1, b2 = raw[:, 4].astype(np.float64), raw[:, 5].astype(np.float64)
+        return {"sd": raw[:, 0].reshape(h, w), "body": (words[:, 1].astype(np.int64) - 1).reshape(h, w),
+                "normal": raw[:, 2:4].reshape(h, w, 2),
+                "bary": np.stack([1.0 - b1 - b2, b1, b2], axis=1).reshape(h, w, 3)}
+
     def dispose(self) -> None:
         if self._disposed:
             return

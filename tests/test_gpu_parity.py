@@ -19,7 +19,9 @@ from mpm_b200 import (MpmMlsGpuNumericalError, calculate_mpm_cfl_microsteps, cre
                       create_mpm_mls_gpu_solver, particles_from_dicts)
 from mpm_b200.cfl_bounds import calculate_mpm_cfl_velocity_bound
 from mpm_b200.layout import ParticleArrays, validate_mpm_mls_gpu_input
-from mpm_b200.scenes import (DAM_BREAK_GRAVITY, create_dam_break_scene, create_si_fluid_scene, create_si_tank_scene)
+from mpm_b200.scenes import (DAM_BREAK_GRAVITY, GATE4_FIXED_STEP_SECONDS, create_dam_break_scene,
+                              create_mpm_gate4_scene, create_mpm_gate4_step_config, create_si_fluid_scene,
+                              create_si_tank_scene)
 from oracle import OracleState, emulate_fixed_point_scatter
 
 pytestmark = pytest.mark.gpu
@@ -234,6 +236,118 @@ def test_crowded_tiles_match_the_oracle(per_side):
         again, _ = _run_parity(p, config, gravity, 2e-4, 12, create_mpm_mls_gpu_solver)
         for key in gpu:
             assert np.array_equal(gpu[key], again[key])
+
+
+def _gate4_float32():
+    # the Gate 4 scene with positions and velocities already float32, so the
+    # oracle and the device start from the same values
+    p, bonds, probes = create_mpm_gate4_scene()
+    for a in (p.px, p.py, p.vx, p.vy):
+        a[:] = a.astype(np.float32)
+    return p, bonds, probes
+
+
+def test_triangle_field_matches_the_oracle():
+    # buildTriangleField of the 50 pebbles at the start of the scene; the
+    # device samples in float64 with the CPU reference's operations
+    p, bonds, _ = _gate4_float32()
+    config = create_mpm_gate4_step_config(fracture_bonds=bonds)
+    solver = create_mpm_mls_gpu_solver(p, config)
+    try:
+        gpu = solver.probe_triangle_field(GATE4_FIXED_STEP_SECONDS / 16)
+    finally:
+        solver.dispose()
+    ref = OracleState(p, config).triangle_field(config)
+    near = ref["body"] >= 0
+    assert near.sum() > 0
+    assert np.array_equal(gpu["body"], ref["body"])  # ties included (the pebbles sit on a lattice)
+    # float32 storage of the float64 samples
+    assert np.max(np.abs(gpu["sd"] - ref["sd"]) / (1 + np.abs(ref["sd"]))) <= 1e-6
+    assert np.max(np.abs(gpu["normal"][near] - ref["normal"][near])) <= 1e-6
+    assert np.max(np.abs(gpu["bary"][near] - ref["bary"][near])) <= 1e-6
+
+
+@pytest.mark.parametrize("variant", ["gather", "atomic"])
+def test_gate4_pebbles_and_fracture_match_the_oracle(variant):
+    # the reference's multi-material scene: 2,000 water, 1,500 oil, 50 bonded
+    # triangle pebbles (fluid contact, bonded edges, pair contacts) and a
+    # fractured Neo-Hookean block (53 bonds); fixed microsteps of 1/3840 s
+    p, bonds, probes = _gate4_float32()
+    config = create_mpm_gate4_step_config(fracture_bonds=bonds)
+    # the scene's CFL microstep (about five per 1/240 s macrostep): the bonded
+    # edges turn position rounding into velocity by 1/dt, and pebble contacts
+    # switch on thresholds, so float32 and float64 runs part after a few
+    # microsteps; compare over 4 with the reference's own CPU-vs-GPU bounds
+    dt = GATE4_FIXED_STEP_SECONDS / 5
+    steps = 4
+    gravity = config["gravity"]
+    # the reference's 2^24 fixed-point scale overflows at these velocities
+    solver = (create_mpm_mls_gpu_solver(p, config) if variant == "gather"
+              else create_experimental_mpm_mls_atomic_gpu_solver(p, config, fixed_point_shift=16))
+    try:
+        solver.step_batch(steps, dt, gravity)
+        packed, _ = solver.read_particles_packed()
+    finally:
+        solver.dispose()
+    cfg = dict(config, dt=float(np.float32(dt)))
+    state = OracleState(p, cfg)
+    state.run(cfg, steps)
+    gpu, ref = packed_columns(packed), oracle_columns(state)
+    # src/routes/labs/mpm/kernels/+page.svelte:120-122: position 0.02,
+    # velocity 0.025 + 5e-4 |v|
+    assert np.max(np.abs(gpu["position"] - ref["position"])) <= 0.02
+    excess = np.abs(gpu["velocity"] - ref["velocity"]) - (0.025 + 5e-4 * np.abs(ref["velocity"]))
+    assert np.max(excess) <= 0.0, np.max(excess)
+    # fracture damage of the Neo-Hookean particles (packed word 18)
+    solids = np.nonzero(p.material == 2)[0]
+    assert np.max(np.abs(packed[solids, 18] - state.particles["damage"][solids])) <= 1e-3
+
+
+def _fracture_block(cols=8, rows=4, spacing=5.0):
+    # a bonded Neo-Hookean block whose halves move apart (updateFractureBonds /
+    # applyFractureParticleDamage): bonds strain, gather damage and break
+    n = cols * rows
+    p = ParticleArrays.empty(n)
+    r, c = np.divmod(np.arange(n), cols)
+    p.px[:] = 100 + c * spacing
+    p.py[:] = 100 + r * spacing
+    p.vx[:] = np.where(c < cols // 2, -150.0, 150.0)
+    p.object_id[:] = 1
+    p.volume[:] = spacing * spacing
+    p.plastic_volume[:] = 1.0
+    nh = {"lambda": 2000.0, "mu": 1000.0, "model": "neo-hookean"}
+    p.materials = [nh]
+    p.material[:] = 0
+    bonds = []
+    for k in range(n):
+        rr, cc = divmod(k, cols)
+        if cc + 1 < cols:
+            bonds.append({"firstParticle": k, "secondParticle": k + 1, "restLength": spacing, "failureStrain": 0.12})
+        if rr + 1 < rows:
+            bonds.append({"firstParticle": k, "secondParticle": k + cols, "restLength": spacing,
+                          "failureStrain": 0.12})
+    config = {"grid": {"cellsX": 40, "cellsY": 40, "cellSize": 10}, "particleMass": 0.5, "particleVolume": 25,
+              "material": nh, "fractureBonds": bonds, "gravity": {"x": 0.0, "y": 0.0}}
+    return p, config
+
+
+def test_fracture_damage_matches_the_oracle():
+    p, config = _fracture_block()
+    gravity = config["gravity"]
+    solver = create_mpm_mls_gpu_solver(p, config)
+    try:
+        solver.step_batch(60, 2e-4, gravity)
+        packed, _ = solver.read_particles_packed()
+    finally:
+        solver.dispose()
+    cfg = dict(config, dt=float(np.float32(2e-4)))
+    state = OracleState(p, cfg)
+    state.run(cfg, 60)
+    assert int(state.bonds["broken"].sum()) > 0  # the case reaches broken bonds
+    ref = state.particles["damage"]
+    assert np.max(np.abs(packed[:, 18] - ref)) <= 1e-3
+    gpu = packed_columns(packed)
+    assert np.max(np.abs(gpu["position"] - oracle_columns(state)["position"])) <= 1e-3 * 10
 
 
 def test_multi_material_models_match_the_oracle():
