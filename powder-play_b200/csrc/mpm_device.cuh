@@ -87,7 +87,7 @@ struct alignas(16) StepParams {
     uint32_t cells_x, cells_y, node_w, node_h;
     uint32_t n_particles, n_nodes, tiles_x, tiles_y;
     uint32_t n_bodies, cfl_enabled, n_bonds, fracture_particles;
-    uint32_t pair_cache_enabled, fixed_shift, fracture_incidence, pad0;
+    uint32_t pair_cache_enabled, fixed_shift, fracture_incidence, batch_steps;  // substeps of this batch
     float dx, particle_mass, particle_volume, dt;
     float lambda, mu, stress_scale, gradient_scale;
     float gx, gy, domain_w, domain_h;

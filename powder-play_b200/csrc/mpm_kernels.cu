@@ -2,17 +2,21 @@
 //
 // Substep, default P2G (the role of the reference's gather path,
 // src/lib/mpm/kernels/solver.ts:1465-1570):
-//   k_tile_scan -> k_tile_scatter -> k_p2g_gather
-//   -> k_g2p_tile (grid update + G2P + next substep's tile counts) -> k_commit
-//   (k_tile_count runs once at the start of a batch)
+//   k_tile_scan (starts the substep) -> k_tile_scatter -> k_p2g_gather
+//   -> k_g2p_tile (grid update + G2P + next substep's tile counts)
+//   (k_begin_batch and k_tile_count run once at the start of a batch)
 // The cell sort (k_count, k_scan_*, k_scatter, k_stable_rank) backs the sort
 // probe and the allocation-free cell sort.
 // Substep, fixed-point atomic P2G (createExperimentalMpmMlsAtomicGpuSolver):
-//   k_prepare_scatter -> k_fixed_decode -> k_grid_update -> k_g2p -> k_commit
-// After a CFL-guarded batch: k_speed_max.
+//   k_substep_begin -> k_prepare_scatter -> k_fixed_decode -> k_grid_update
+//   -> k_g2p
+// After a batch: k_end_batch (rollback, maximum particle speed).
 //
 // Every kernel returns early once the persistent status word is non-zero, as
 // every WGSL entry point does (shaders.ts: `atomicLoad(&stateError[0]) != 0u`).
+// A substep that raises it is rolled back (commitParticles,
+// shaders.ts:3067-3080): the batch ends on that substep's input, which no
+// later substep of the batch writes.
 #include <math_constants.h>
 
 #include "mpm_kernels.cuh"
@@ -188,6 +192,44 @@ __device__ bool prepare_particle(const Ctx &c, uint32_t i, float4 &affine, float
     return false;
 }
 
+// Whether the solver takes part in the current substep: no status raised and
+// substeps of this batch left.
+__device__ __forceinline__ bool takes_part(const Ctx &c)
+{
+    return *(volatile uint32_t *)c.status == 0u && c.counters[COUNTER_SUBSTEP] < c.P->batch_steps;
+}
+
+// The start of a substep (one thread): a new tile stamp, the substep index,
+// and, once the state stops taking part, the substeps completed (a status
+// raised in the previous substep leaves that substep's input, the state after
+// the substeps before it, as the result).  Returns whether the substep runs.
+__device__ __forceinline__ bool begin_substep(const Ctx &c)
+{
+    uint32_t *k = c.counters;
+    k[COUNTER_STAMP] += 1u;
+    if (k[COUNTER_FRESH] != 0u)
+        k[COUNTER_FRESH] = 0u;
+    else
+        k[COUNTER_SUBSTEP] += 1u;
+    const uint32_t sub = k[COUNTER_SUBSTEP];
+    const bool failed = *(volatile uint32_t *)c.status != 0u;
+    const bool runs = !failed && sub < c.P->batch_steps;
+    if (!runs && k[COUNTER_STOP] == STOP_NONE) k[COUNTER_STOP] = failed ? (sub == 0u ? 0u : sub - 1u) : c.P->batch_steps;
+    return runs;
+}
+
+// Substeps completed in a batch of `total` substeps, at its end (the same
+// answer however often it is asked).
+__device__ __forceinline__ uint32_t batch_stop(const Ctx &c, uint32_t total)
+{
+    const uint32_t *k = c.counters;
+    const uint32_t stop = k[COUNTER_STOP];
+    if (stop != STOP_NONE) return stop;
+    if (k[COUNTER_FRESH] != 0u) return 0u;  // no substep started
+    // it ran the last substep, total - 1
+    return *(volatile uint32_t *)c.status != 0u ? total - 1u : total;
+}
+
 // Whether the slot of original particle `orig` is tracked (a bonded-triangle
 // vertex or a fracture-bond endpoint).
 __device__ __forceinline__ bool is_tracked(const Ctx &c, uint32_t orig)
@@ -299,6 +341,9 @@ __global__ void k_begin_batch(Ctx c, uint32_t reset_progress)
         if (reset_progress) c.counters[COUNTER_PROGRESS] = 0u;
         c.counters[COUNTER_MAX_SPEED] = 0u;
         for (int k = 0; k < 4; ++k) c.counters[COUNTER_ACTIVE + k] = 0u;
+        c.counters[COUNTER_SUBSTEP] = 0u;
+        c.counters[COUNTER_FRESH] = 1u;
+        c.counters[COUNTER_STOP] = STOP_NONE;
     }
 }
 
@@ -459,6 +504,7 @@ struct NodeVel {
 // P2G sums and the water/oil volumes of its four neighbours (xp, xm, yp, ym;
 // zero outside the halo or where no particle deposited).  Returns false
 // after raising a status.
+template <bool BODIES>
 __device__ __forceinline__ bool node_velocity(const Ctx &c, uint32_t n, int x, int y, float4 S, float4 W, float4 O,
                                               float2 xp, float2 xm, float2 yp, float2 ym, NodeVel &out)
 {
@@ -511,7 +557,7 @@ __device__ __forceinline__ bool node_velocity(const Ctx &c, uint32_t n, int x, i
         }
     }
     float2 impulse = make_float2(0.f, 0.f);
-    if (c.field) {
+    if (BODIES && c.field) {
         // fluid-pebble contact: updateGrid, shaders.ts:1596-1665
         const TriField f = c.field[n];
         if (f.body1 != 0u && f.sd <= P.contact_reach) {
@@ -588,7 +634,7 @@ __device__ bool update_node(const Ctx &c, uint32_t n, int x, int y, float4 S, fl
                             float2 xm, float2 yp, float2 ym)
 {
     NodeVel v;
-    if (!node_velocity(c, n, x, y, S, W, O, xp, xm, yp, ym, v)) return false;
+    if (!node_velocity<true>(c, n, x, y, S, W, O, xp, xm, yp, ym, v)) return false;
     c.g_solid[n] = v.vs;
     c.g_water[n] = v.vw;
     c.g_oil[n] = v.vo;
@@ -616,7 +662,7 @@ __global__ void k_tile_count(Ctx c)
 {
     const StepParams &P = *c.P;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    bool valid = i < P.n_particles && *(volatile uint32_t *)c.status == 0u;
+    bool valid = i < P.n_particles && takes_part(c);
     uint32_t key = 0;
     if (valid) {
         Stencil s;
@@ -639,14 +685,23 @@ __global__ void k_tile_count(Ctx c)
     c.keys[i] = key;
 }
 
-// Exclusive scan of the tile counts in one CTA, 8 consecutive tiles per
-// thread and pass (vector loads and stores), plus the ascending list of
-// tiles holding particles; zeroes the counts for the next substep.  Ignores
-// the status word so counts never leak into a later batch.
+// The first kernel of a substep of the default path: starts the substep
+// (begin_substep), then the exclusive scan of the tile counts in one CTA, 8
+// consecutive tiles per thread and pass (vector loads and stores), plus the
+// ascending list of tiles holding particles; zeroes the counts for the next
+// substep.  A substep that does not run lists no tile (the counts are
+// cleared at the start of every batch).
 __global__ void __launch_bounds__(SCAN_TOP_THREADS) k_tile_scan(Ctx c)
 {
     constexpr int ITEMS = 8;
     constexpr uint32_t PASS = SCAN_TOP_THREADS * ITEMS;
+    __shared__ bool s_runs;
+    if (threadIdx.x == 0) {
+        s_runs = begin_substep(c);
+        if (!s_runs) c.counters[COUNTER_ACTIVE_TILES] = 0u;
+    }
+    __syncthreads();
+    if (!s_runs) return;  // the same answer for every thread of the CTA
     const uint32_t n_tiles = c.n_tiles;
     uint32_t running = 0, running_active = 0;
     for (uint32_t base = 0; base < n_tiles; base += PASS) {
@@ -1337,11 +1392,11 @@ __device__ __forceinline__ ParticleIn load_particle(const Ctx &c, uint32_t s)
 }
 
 // The G2P of one particle with base stencil st: reads `in`, writes slot d.
-// Returns false when the particle raised a status (its output slot is then
-// restored by commit).  When the next substep's tiles are counted, `next`
-// receives the stencil of the new position and the slot's P2G record is
-// written.
-template <class Grid>
+// Returns false when the particle raised a status (the substep is then
+// rolled back).  When the next substep's tiles are counted, `next` receives
+// the stencil of the new position and the slot's P2G record is written.
+// BODIES: the solver may hold bonded-triangle bodies or fracture bonds.
+template <bool BODIES, class Grid>
 __device__ __forceinline__ bool g2p_particle(const Ctx &c, const ParticleIn &in, uint32_t d, const Stencil &st,
                                              const Grid &grid, Stencil &next, bool &count_next)
 {
@@ -1537,7 +1592,7 @@ __device__ __forceinline__ bool g2p_particle(const Ctx &c, const ParticleIn &in,
     const float2 bx = confine_axis(npos.x, vel.x, P.domain_w);
     const float2 by = confine_axis(npos.y, vel.y, P.domain_h);
     float2 projected = make_float2(bx.x, by.x);
-    if (liquid && c.field) {
+    if (BODIES && liquid && c.field) {
         const float radius = sqrtf(in.vol * udet / 3.14159265359f);
         if (!finite_f(radius)) {
             fail_at(c.status, id, ERROR_G2P);
@@ -1564,8 +1619,8 @@ __device__ __forceinline__ bool g2p_particle(const Ctx &c, const ParticleIn &in,
     // next substep's pressure (both evaluate it at the new F)
     float tait_pow = -1.0f;
     if (liquid && m.param > 0.0f && finite_f(m.param)) tait_pow = pow_wgsl(__fdiv_rn(1.0f, udet), m.param);
-    if (P.n_bodies == 0u) validate_cfl(c, id, m, outv, Fn, damage, volume, tait_pow);
-    if (is_tracked(c, id)) {
+    if (!BODIES || P.n_bodies == 0u) validate_cfl(c, id, m, outv, Fn, damage, volume, tait_pow);
+    if (BODIES && is_tracked(c, id)) {
         // a body vertex or fracture particle: its final state comes after the
         // body kernels, which then count its tile and write its record
         c.slot_out[id] = d;
@@ -1598,7 +1653,7 @@ __global__ void k_g2p(Ctx c)
     uint32_t key = 0;
     if (in_range) {
         if (*(volatile uint32_t *)c.status != 0u) {
-            copy_particle(c, d, d);  // identity: perm may be stale once a status is set
+            // the substep is rolled back: the batch ends on its input
         } else {
             const ParticleIn in = load_particle(c, s);
             Stencil st, next;
@@ -1607,7 +1662,7 @@ __global__ void k_g2p(Ctx c)
             } else {
                 const GlobalGrid grid{c.g_solid, c.g_water, c.g_oil, node_index(P, st.bx, st.by), P.node_w};
                 bool count_it;
-                if (g2p_particle(c, in, d, st, grid, next, count_it) && count_it) {
+                if (g2p_particle<true>(c, in, d, st, grid, next, count_it) && count_it) {
                     key = particle_tile(P, next.bx, next.by);
                     counted = true;
                 }
@@ -1662,6 +1717,7 @@ __device__ __forceinline__ void stage_chunk(const Ctx &c, uint32_t base, uint32_
 // whose ring holds a failing node raises the grid status and moves none of
 // its particles (the substep is rolled back); tiles elsewhere still move
 // theirs, so their G2P flags can join the status of that substep.
+template <bool BODIES>
 __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c)
 {
     const StepParams &P = *c.P;
@@ -1731,7 +1787,7 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c)
                 const float4 W = make_float4(sum[3], sum[4], sum[5], sum[6]);
                 const float4 O = make_float4(sum[7], sum[8], sum[9], sum[10]);
                 const uint32_t n = (uint32_t)hy * (uint32_t)node_w + (uint32_t)hx;
-                if (!node_velocity(c, n, hx - 1, hy - 1, S, W, O, s_vol[t + 1], s_vol[t - 1], s_vol[t + VOL_X],
+                if (!node_velocity<BODIES>(c, n, hx - 1, hy - 1, S, W, O, s_vol[t + 1], s_vol[t - 1], s_vol[t + VOL_X],
                                    s_vol[t - VOL_X], v)) {
                     s_fail = 1;
                 } else {
@@ -1751,7 +1807,7 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c)
                         ws += S.x > 0.f;
                         ww += W.x > 0.f;
                         wo += O.x > 0.f;
-                        if (c.field) {  // the body impulse of a node is stored once
+                        if (BODIES && c.field) {  // the body impulse of a node is stored once
                             c.field[n].ix = v.impulse.x;
                             c.field[n].iy = v.impulse.y;
                         }
@@ -1796,7 +1852,7 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c)
                 } else {
                     const RingGrid grid{s_vs, s_vw, s_vo, (uint32_t)(ly * RING_X + lx), RING_X};
                     bool count_it;
-                    if (g2p_particle(c, in, p, st, grid, next, count_it) && count_it) {
+                    if (g2p_particle<BODIES>(c, in, p, st, grid, next, count_it) && count_it) {
                         key = particle_tile(P, next.bx, next.by);
                         counted = true;
                     }
@@ -1819,36 +1875,45 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c)
     }
 }
 
-// commitParticles: shaders.ts:3067-3080.  On a failed substep every slot is
-// restored from the substep's input (whole-substep rollback, keeping the
-// input's slot order); otherwise the committed CFL microstep counter
-// advances.  The substep stamp advances unconditionally.
-__global__ void k_commit(Ctx c)
+// The start of a substep of the fixed-point path (k_tile_scan starts those
+// of the default path).
+__global__ void k_substep_begin(Ctx c)
 {
-    const StepParams &P = *c.P;
-    if (*(volatile uint32_t *)c.status != 0u) {
-        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n_particles; i += gridDim.x * blockDim.x)
-            copy_particle(c, i, i);
-        // the restored output keeps the input's slots
-        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < c.n_tracked; k += gridDim.x * blockDim.x)
-            c.slot_out[c.tracked[k]] = c.slot_in[c.tracked[k]];
-    } else if (blockIdx.x == 0 && threadIdx.x == 0 && P.cfl_enabled) {
-        c.counters[COUNTER_PROGRESS] += 1u;
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) c.counters[COUNTER_STAMP] += 1u;
+    if (blockIdx.x == 0 && threadIdx.x == 0) begin_substep(c);
 }
 
+// The end of a batch of `total` substeps (commitParticles,
+// shaders.ts:3067-3080, once per batch), with `out` the buffer the batch
+// ends in and `in` the other one.  When the substeps completed and `total`
+// differ in parity (a raised status, or fewer substeps than the batch), the
+// state is in `in`: every slot (and the tracked slots) is copied over, the
+// whole-substep rollback.  Then, when `measure_speed` is set,
 // measureParticleSpeedPartials + reduceParticleSpeedPartials
-// (shaders.ts:2463-2533) as one warp-shuffle reduction with an atomic max on
-// the order-preserving bits of the non-negative speed.
-__global__ void k_speed_max(Ctx c)
+// (shaders.ts:2463-2533) of the final state as one warp-shuffle reduction
+// with an atomic max on the order-preserving bits of the non-negative speed.
+// Thread 0 of CTA 0 records the substeps completed and, under a CFL guard,
+// the committed microsteps.
+__global__ void k_end_batch(Ctx c, uint32_t total, uint32_t measure_speed)
 {
-    const StepParams &P = *c.P;
-    float best = 0.0f;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n_particles; i += gridDim.x * blockDim.x) {
-        const float sp = length2(c.in.vel[i]);
-        best = fmaxf(best, finite_f(sp) ? sp : FLOAT_MAX);
+    const uint32_t stop = batch_stop(c, total);
+    const bool restore = ((stop ^ total) & 1u) != 0u;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        c.counters[COUNTER_STOP] = stop;
+        if (c.P->cfl_enabled) c.counters[COUNTER_PROGRESS] = stop;
     }
+    if (restore) {
+        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < c.n_tracked; k += gridDim.x * blockDim.x)
+            c.slot_out[c.tracked[k]] = c.slot_in[c.tracked[k]];
+    }
+    float best = 0.0f;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.n; i += gridDim.x * blockDim.x) {
+        if (restore) copy_particle(c, i, i);
+        if (measure_speed) {
+            const float sp = length2(restore ? c.in.vel[i] : c.out.vel[i]);
+            best = fmaxf(best, finite_f(sp) ? sp : FLOAT_MAX);
+        }
+    }
+    if (!measure_speed) return;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
     if ((threadIdx.x & 31) == 0) atomicMax(c.counters + COUNTER_MAX_SPEED, __float_as_uint(best));
@@ -1861,8 +1926,8 @@ __global__ void __launch_bounds__(TILE_NODES) k_count_active_nodes(Ctx c, uint32
 {
     const StepParams &P = *c.P;
     const int tx = blockIdx.x, ty = blockIdx.y;
-    // the commit of the last substep advanced the stamp by one
-    if (c.tile_stamp[ty * P.tiles_x + tx] + 1u != c.counters[COUNTER_STAMP]) return;
+    // the stamp of the last substep is still current
+    if (c.tile_stamp[ty * P.tiles_x + tx] != c.counters[COUNTER_STAMP]) return;
     const int hx = tx * TILE_X + (threadIdx.x % TILE_X), hy = ty * TILE_Y + (threadIdx.x / TILE_X);
     uint32_t s = 0, w = 0, o = 0;
     if (hx < (int)P.node_w && hy < (int)P.node_h) {
@@ -2496,5 +2561,9 @@ __global__ void k_body_finish(Ctx c)
     const Material m = c.mats[c.out.mat[d]];
     write_record(c, d, m, st, c.out.vel[d], c.out.F[d], c.out.vol[d], c.out.damage[d], c.out.pvol[d], c.out.C[d]);
 }
+
+// the instances the host launches
+template __global__ void k_g2p_tile<false>(Ctx);
+template __global__ void k_g2p_tile<true>(Ctx);
 
 }  // namespace mpm

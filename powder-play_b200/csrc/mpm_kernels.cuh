@@ -134,6 +134,10 @@ static_assert(VOL_X * VOL_Y <= G2P_THREADS && RING_NODES <= G2P_THREADS, "one no
 // device counters beyond the three of mpm_device.cuh
 constexpr int COUNTER_ACTIVE = 4;        // [4..6] active solid/water/oil nodes
 constexpr int COUNTER_ACTIVE_TILES = 7;  // tiles holding particles this substep
+constexpr int COUNTER_SUBSTEP = 8;       // the substep of this batch under way (failed and skipped included)
+constexpr int COUNTER_FRESH = 9;         // 1 from the start of a batch until its first substep starts
+constexpr int COUNTER_STOP = 10;         // substeps completed in this batch (STOP_NONE while running)
+constexpr uint32_t STOP_NONE = 0xffffffffu;
 
 __global__ void k_count(Ctx c);
 __global__ void k_scan_reduce(Ctx c, uint32_t n_chunks);
@@ -145,13 +149,15 @@ __global__ void k_tile_count(Ctx c);
 __global__ void k_tile_scan(Ctx c);
 __global__ void k_tile_scatter(Ctx c);
 __global__ void k_p2g_gather(Ctx c);
+// BODIES: the solver holds bonded-triangle bodies or fracture bonds
+template <bool BODIES>
 __global__ void k_g2p_tile(Ctx c);
 __global__ void k_prepare_scatter(Ctx c);
 __global__ void k_fixed_decode(Ctx c);
 __global__ void k_grid_update(Ctx c);
 __global__ void k_g2p(Ctx c);
-__global__ void k_commit(Ctx c);
-__global__ void k_speed_max(Ctx c);
+__global__ void k_substep_begin(Ctx c);
+__global__ void k_end_batch(Ctx c, uint32_t total_steps, uint32_t measure_speed);
 __global__ void k_begin_batch(Ctx c, uint32_t reset_progress);
 // bodies and fracture
 __global__ void k_triangle_field(Ctx c);

@@ -195,11 +195,11 @@ constexpr unsigned PARTICLE_THREADS = 256;
 // Kernel slots of the profiled substep (mpm_profile_substeps).
 enum KernelSlot {
     K_TILE_COUNT, K_TILE_SCAN, K_TILE_SCATTER, K_P2G_GATHER, K_G2P_TILE, K_PREPARE_SCATTER,
-    K_FIXED_DECODE, K_GRID_UPDATE, K_G2P, K_COMMIT, K_SPEED_MAX, K_SLOTS
+    K_FIXED_DECODE, K_GRID_UPDATE, K_G2P, K_SUBSTEP_BEGIN, K_END_BATCH, K_SLOTS
 };
 const char *const KERNEL_NAMES[K_SLOTS] = {
     "k_tile_count", "k_tile_scan", "k_tile_scatter", "k_p2g_gather", "k_g2p_tile", "k_prepare_scatter",
-    "k_fixed_decode", "k_grid_update", "k_g2p", "k_commit", "k_speed_max"};
+    "k_fixed_decode", "k_grid_update", "k_g2p", "k_substep_begin", "k_end_batch"};
 
 // When set, an event is recorded after every kernel launch so that the
 // kernels of a substep can be timed one by one.  The profiled substeps are
@@ -290,9 +290,14 @@ void enqueue_substep(mpm_solver *s, int parity)
         k_p2g_gather<<<s->p2g_ctas, TILE_CELLS, 0, s->stream>>>(c);
         mark(K_P2G_GATHER);
         if (s->n_bodies) k_triangle_field<<<tiles, TILE_NODES, 0, s->stream>>>(c);
-        k_g2p_tile<<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
+        if (s->n_tracked > 0)
+            k_g2p_tile<true><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
+        else
+            k_g2p_tile<false><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
         mark(K_G2P_TILE);
     } else {
+        k_substep_begin<<<1, 32, 0, s->stream>>>(c);
+        mark(K_SUBSTEP_BEGIN);
         k_prepare_scatter<<<pb, PARTICLE_THREADS, 0, s->stream>>>(c);
         mark(K_PREPARE_SCATTER);
         k_fixed_decode<<<tiles, TILE_NODES, 0, s->stream>>>(c);
@@ -304,10 +309,19 @@ void enqueue_substep(mpm_solver *s, int parity)
         mark(K_G2P);
     }
     enqueue_bodies(s, c);
-    const unsigned cb = std::min(blocks_for(s->n, PARTICLE_THREADS), 592u);
-    k_commit<<<cb, PARTICLE_THREADS, 0, s->stream>>>(c);
-    mark(K_COMMIT);
 }
+
+// The end of a batch of `total` substeps that ended in buffer `parity`.
+void enqueue_end_batch(mpm_solver *s, int parity, uint32_t total, bool measure_speed)
+{
+    const Ctx c = make_ctx(s, 1 - parity);  // out: the buffer the batch ends in
+    k_end_batch<<<std::min(blocks_for(s->n, PARTICLE_THREADS), 1184u), PARTICLE_THREADS, 0, s->stream>>>(
+        c, total, measure_speed ? 1u : 0u);
+    mark(K_END_BATCH);
+}
+
+// Substeps per captured graph: at most 2^MAX_GRAPH_LOG2.
+constexpr int MAX_GRAPH_LOG2 = 9;
 
 int get_graph(mpm_solver *s, int log2_steps, int parity, cudaGraphExec_t *out)
 {
@@ -336,7 +350,7 @@ int get_graph(mpm_solver *s, int log2_steps, int parity, cudaGraphExec_t *out)
 }
 
 void fill_params(mpm_solver *s, StepParams &p, float dt, float gx, float gy, const mpm_cfl_guard *guard,
-                 float bond_reference_dt)
+                 float bond_reference_dt, uint32_t steps)
 {
     std::memset(&p, 0, sizeof p);
     const mpm_config &c = s->cfg;
@@ -354,6 +368,7 @@ void fill_params(mpm_solver *s, StepParams &p, float dt, float gx, float gy, con
     p.fracture_particles = s->fracture_particles;
     p.fracture_incidence = s->fracture_incidence;
     p.pair_cache_enabled = s->pair_cache ? 1u : 0u;
+    p.batch_steps = steps;
     p.fixed_shift = c.fixed_point_shift;
     p.dx = c.cell_size;
     p.inv_dx = 1.0f / c.cell_size;
@@ -389,10 +404,11 @@ void fill_params(mpm_solver *s, StepParams &p, float dt, float gx, float gy, con
     }
 }
 
-int upload_params(mpm_solver *s, float dt, float gx, float gy, const mpm_cfl_guard *guard, float bond_reference_dt)
+int upload_params(mpm_solver *s, float dt, float gx, float gy, const mpm_cfl_guard *guard, float bond_reference_dt,
+                  uint32_t steps)
 {
     CUDA_TRY(cudaEventSynchronize(s->params_copied));
-    fill_params(s, *s->h_params, dt, gx, gy, guard, bond_reference_dt);
+    fill_params(s, *s->h_params, dt, gx, gy, guard, bond_reference_dt, steps);
     CUDA_TRY(cudaMemcpyAsync(s->d_params, s->h_params, sizeof(StepParams), cudaMemcpyHostToDevice, s->stream));
     CUDA_TRY(cudaEventRecord(s->params_copied, s->stream));
     return MPM_OK;
@@ -686,7 +702,8 @@ int create_impl(const mpm_config *config, const float *packed, const uint32_t *o
                 cudaSuccess ||
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_p2g, k_p2g_gather, TILE_CELLS, 0) !=
                 cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_g2p, k_g2p_tile, G2P_THREADS, 0) != cudaSuccess)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_g2p, k_g2p_tile<false>, G2P_THREADS, 0) !=
+                cudaSuccess)
             return fail(set_error(MPM_ERR_CUDA, "occupancy query failed"));
         s->p2g_ctas = (unsigned)std::max<size_t>(1, std::min<size_t>(n_tiles, (size_t)sms * std::max(1, per_sm_p2g)));
         s->g2p_ctas = (unsigned)std::max<size_t>(1, std::min<size_t>(n_tiles, (size_t)sms * std::max(1, per_sm_g2p)));
@@ -797,7 +814,7 @@ int mpm_step_batch(mpm_solver *s, uint32_t step_count, float dt, float gx, float
     if (!(dt > 0.0f) || !std::isfinite(dt)) return set_error(MPM_ERR_INVALID_ARGUMENT, "dt must be greater than zero");
     if (!std::isfinite(gx) || !std::isfinite(gy)) return set_error(MPM_ERR_INVALID_ARGUMENT, "gravity must be finite");
     CUDA_TRY(cudaSetDevice(s->device));
-    int rc = upload_params(s, dt, gx, gy, guard, bond_reference_dt);
+    int rc = upload_params(s, dt, gx, gy, guard, bond_reference_dt, step_count);
     if (rc != MPM_OK) return rc;
     const Ctx c0 = make_ctx(s, s->cur);
     CUDA_TRY(cudaEventRecord(s->batch_start, s->stream));
@@ -806,21 +823,21 @@ int mpm_step_batch(mpm_solver *s, uint32_t step_count, float dt, float gx, float
     if (s->gather() && s->n > 0) enqueue_tile_count(s, c0);
     CUDA_TRY(cudaGetLastError());
     if (s->n > 0) {
+        // graphs of 2^k substeps, k <= MAX_GRAPH_LOG2; the largest repeats
         uint32_t remaining = step_count;
-        for (int k = 30; k >= 0; --k) {
-            if (!(remaining & (1u << k))) continue;
-            cudaGraphExec_t exec;
-            rc = get_graph(s, k, s->cur, &exec);
-            if (rc != MPM_OK) return rc;
-            CUDA_TRY(cudaGraphLaunch(exec, s->stream));
-            if (k == 0) s->cur = 1 - s->cur;  // only an odd substep count flips the buffer
+        for (int k = MAX_GRAPH_LOG2; k >= 0; --k) {
+            while (remaining >= (1u << k)) {
+                cudaGraphExec_t exec;
+                rc = get_graph(s, k, s->cur, &exec);
+                if (rc != MPM_OK) return rc;
+                CUDA_TRY(cudaGraphLaunch(exec, s->stream));
+                if (k == 0) s->cur = 1 - s->cur;  // only an odd substep count flips the buffer
+                remaining -= 1u << k;
+                if (k < MAX_GRAPH_LOG2) break;
+            }
         }
         s->substeps_since_begin = step_count;
-    }
-    if (guard) {
-        const Ctx c1 = make_ctx(s, s->cur);
-        const unsigned blocks = std::min(blocks_for(s->n, PARTICLE_THREADS), 592u);
-        k_speed_max<<<blocks, PARTICLE_THREADS, 0, s->stream>>>(c1);
+        enqueue_end_batch(s, s->cur, step_count, guard != nullptr);
         CUDA_TRY(cudaGetLastError());
     }
     CUDA_TRY(cudaEventRecord(s->batch_stop, s->stream));
@@ -849,7 +866,7 @@ int mpm_profile_substeps(mpm_solver *s, uint32_t step_count, float dt, float gx,
         return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and outputs must not be NULL");
     if (step_count < 1) return set_error(MPM_ERR_INVALID_ARGUMENT, "stepCount must be a positive safe integer.");
     CUDA_TRY(cudaSetDevice(s->device));
-    int rc = upload_params(s, dt, gx, gy, guard, 0.0f);
+    int rc = upload_params(s, dt, gx, gy, guard, 0.0f, step_count);
     if (rc != MPM_OK) return rc;
     for (int k = 0; k < K_SLOTS; ++k) {
         kernel_ms[k] = 0.0;
@@ -869,11 +886,7 @@ int mpm_profile_substeps(mpm_solver *s, uint32_t step_count, float dt, float gx,
         enqueue_substep(s, parity);
         parity = 1 - parity;
     }
-    if (guard) {
-        const Ctx c1 = make_ctx(s, parity);
-        k_speed_max<<<std::min(blocks_for(s->n, PARTICLE_THREADS), 592u), PARTICLE_THREADS, 0, s->stream>>>(c1);
-        mark(K_SPEED_MAX);
-    }
+    if (s->n > 0) enqueue_end_batch(s, parity, step_count, guard != nullptr);
     g_recorder = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -1073,7 +1086,7 @@ int mpm_probe_sort(mpm_solver *s, float dt, uint32_t *keys_out, uint32_t *perm_o
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
     if (!s->gather()) return set_error(MPM_ERR_STATE, "the cell sort runs in gather mode only");
     CUDA_TRY(cudaSetDevice(s->device));
-    int rc = upload_params(s, dt, 0.0f, 0.0f, nullptr, 0.0f);
+    int rc = upload_params(s, dt, 0.0f, 0.0f, nullptr, 0.0f, 1u);
     if (rc != MPM_OK) return rc;
     const Ctx c = make_ctx(s, s->cur);
     enqueue_cell_sort(s, c);
@@ -1104,10 +1117,13 @@ int mpm_probe_triangle_field(mpm_solver *s, float dt, float *field_out)
     if (!s || !field_out) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and field_out must not be NULL");
     if (!s->field) return set_error(MPM_ERR_STATE, "the scene has no bonded triangle bodies");
     CUDA_TRY(cudaSetDevice(s->device));
-    int rc = upload_params(s, dt, 0.0f, 0.0f, nullptr, 0.0f);
+    int rc = upload_params(s, dt, 0.0f, 0.0f, nullptr, 0.0f, 1u);
     if (rc != MPM_OK) return rc;
     const Ctx c = make_ctx(s, s->cur);
-    if (s->gather()) enqueue_tile_count(s, c);  // the tracked slots of the current buffer
+    // the tracked slots of the current buffer, counted as at the start of a
+    // batch of one substep
+    CUDA_TRY(cudaMemsetAsync(s->d_counters + COUNTER_SUBSTEP, 0, sizeof(uint32_t), s->stream));
+    if (s->gather()) enqueue_tile_count(s, c);
     k_triangle_field<<<dim3(s->tiles_x, s->tiles_y), TILE_NODES, 0, s->stream>>>(c);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(field_out, s->field, (size_t)s->node_count * sizeof(TriField), cudaMemcpyDeviceToHost,
@@ -1122,7 +1138,7 @@ int mpm_probe_fixed_point(mpm_solver *s, float dt, int32_t *words_out, float *af
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
     if (s->cfg.p2g_mode != MPM_P2G_FIXED_POINT) return set_error(MPM_ERR_STATE, "the solver was not created in fixed-point mode");
     CUDA_TRY(cudaSetDevice(s->device));
-    int rc = upload_params(s, dt, 0.0f, 0.0f, nullptr, 0.0f);
+    int rc = upload_params(s, dt, 0.0f, 0.0f, nullptr, 0.0f, 1u);
     if (rc != MPM_OK) return rc;
     float4 *aff = nullptr;
     CUDA_TRY(dalloc(&aff, s->n));
