@@ -188,6 +188,39 @@ int mpm_count_active_nodes(mpm_solver *solver, uint32_t counts[3]);
  * work after the solver's. */
 void *mpm_stream(mpm_solver *solver);
 
+/* ---- batched scenes ---- */
+
+/* No counterpart in the reference, which runs one scene per solver
+ * (createMpmMlsGpuSolver, src/lib/mpm/kernels/solver.ts:390-406): one handle
+ * over `scene_count` independent scenes of uneven particle counts and grids,
+ * stepped together (one launch per kernel and substep, every scene's tiles in
+ * one tile list).  Scene k holds particle_counts[k] particles, packed one
+ * scene after another in packed_particles / object_ids (20 words each, as
+ * mpm_create); configs[k] gives its grid and material constants (its
+ * capacity is ignored: a scene holds exactly its particles).  Every scene
+ * runs the default gather P2G; the device comes from configs[0].  No bonded
+ * bodies or fracture bonds.  mpm_read_particles reads all scenes' particles
+ * in this packed order; mpm_clear_status clears every scene. */
+int mpmb_create(const mpm_config *configs, uint32_t scene_count, const uint32_t *particle_counts,
+                const float *packed_particles, const uint32_t *object_ids, mpm_solver **out);
+
+/* One submit of per-scene step batches (stepBatch, src/lib/mpm/kernels/
+ * solver.ts:1407-1498, for every scene at once): scene k runs step_counts[k]
+ * substeps of dts[k] (0: the scene sits the submit out) under gravity
+ * (gravity_xy[2k], gravity_xy[2k+1]) and, when `guards` is not NULL, the CFL
+ * guard guards[k].  A scene whose status is raised stops there, its state
+ * rolled back to the start of the failed substep; the others go on. */
+int mpmb_step_batch(mpm_solver *solver, const uint32_t *step_counts, const float *dts, const float *gravity_xy,
+                    const mpm_cfl_guard *guards);
+
+/* mpm_read_compact for every scene: maximum_speeds[k], completed[k] and the
+ * 8 status words status[8k .. 8k+7], whose particle index (word 1) counts
+ * within the scene (any output may be NULL).  Blocks. */
+int mpmb_read_compact(mpm_solver *solver, float *maximum_speeds, uint32_t *completed_microsteps, uint32_t *status);
+
+/* Scenes of the handle (1 for a handle from mpm_create). */
+uint32_t mpmb_scene_count(const mpm_solver *solver);
+
 /* ---- allocation-free cell sort ---- */
 
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc

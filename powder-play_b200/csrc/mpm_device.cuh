@@ -95,6 +95,9 @@ struct alignas(16) StepParams {
     float cfl_wave_bound, cfl_velocity_limit, bond_reference_dt, wall_friction;
     float fixed_scale, drag_x, drag_y, drag_radius;
     float drag_stiffness, drag_damping, inv_dx, pad1;
+    // the scene's place in a batch of scenes: its first slot and first tile
+    // (its tiles are followed by one sentinel entry) and its tile count
+    uint32_t p_base, tile_base, scene_tiles, pad2;
 };
 
 // Device counters (one 32-word line): stamp of the current substep, committed

@@ -192,7 +192,41 @@ __device__ bool prepare_particle(const Ctx &c, uint32_t i, float4 &affine, float
     return false;
 }
 
-// Whether the solver takes part in the current substep: no status raised and
+// The context of scene s: its parameters, status and counters.
+__device__ __forceinline__ Ctx scene_ctx(const Ctx &c, uint32_t s)
+{
+    Ctx cs = c;
+    cs.P = c.scenes + s;
+    cs.status = c.dyn + (size_t)s * SCENE_WORDS;
+    cs.counters = c.dyn + (size_t)s * SCENE_WORDS + 32;
+    return cs;
+}
+
+// The scene owning slot d (scenes hold contiguous slot ranges).
+__device__ __forceinline__ uint32_t scene_of_slot(const Ctx &c, uint32_t d)
+{
+    uint32_t lo = 0, hi = c.n_scenes;  // scene_p_base[lo] <= d < scene_p_base[hi]
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) / 2u;
+        if (c.scene_p_base[mid] <= d)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// The context of a tile's scene (SCENES: the solver holds several).
+template <bool SCENES>
+__device__ __forceinline__ Ctx tile_ctx(const Ctx &c0, uint32_t tile)
+{
+    if constexpr (SCENES)
+        return scene_ctx(c0, c0.tile_scene[tile]);
+    else
+        return c0;
+}
+
+// Whether the scene takes part in the current substep: no status raised and
 // substeps of this batch left.
 __device__ __forceinline__ bool takes_part(const Ctx &c)
 {
@@ -333,17 +367,23 @@ __device__ __forceinline__ uint32_t warp_count(uint32_t *cell_count, uint32_t ke
 
 // ---------------------------------------------------------------- batch --
 
-// Resets the per-batch counters (reference: cflStepProgress write before the
-// batch, solver.ts:1444-1450; the speed scalar is recomputed after it).
+// Resets every scene's per-batch counters (reference: cflStepProgress write
+// before the batch, solver.ts:1444-1450; the speed scalar is recomputed
+// after it) and the tile lists.
 __global__ void k_begin_batch(Ctx c, uint32_t reset_progress)
 {
-    if (threadIdx.x == 0) {
-        if (reset_progress) c.counters[COUNTER_PROGRESS] = 0u;
-        c.counters[COUNTER_MAX_SPEED] = 0u;
-        for (int k = 0; k < 4; ++k) c.counters[COUNTER_ACTIVE + k] = 0u;
-        c.counters[COUNTER_SUBSTEP] = 0u;
-        c.counters[COUNTER_FRESH] = 1u;
-        c.counters[COUNTER_STOP] = STOP_NONE;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < c.n_scenes; s += gridDim.x * blockDim.x) {
+        uint32_t *counters = c.dyn + (size_t)s * SCENE_WORDS + 32;
+        if (reset_progress) counters[COUNTER_PROGRESS] = 0u;
+        counters[COUNTER_MAX_SPEED] = 0u;
+        for (int k = 0; k < 4; ++k) counters[COUNTER_ACTIVE + k] = 0u;
+        counters[COUNTER_SUBSTEP] = 0u;
+        counters[COUNTER_FRESH] = 1u;
+        counters[COUNTER_STOP] = STOP_NONE;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        c.work[WORK_ACTIVE] = 0u;
+        c.work[WORK_ACTIVE + 1] = 0u;
     }
 }
 
@@ -653,16 +693,17 @@ __device__ bool update_node(const Ctx &c, uint32_t n, int x, int y, float4 S, fl
 // then lies in the tile's 18x10-node ring (tile plus two columns and rows).
 __device__ __forceinline__ uint32_t particle_tile(const StepParams &P, int bx, int by)
 {
-    return tile_of_node(P, (uint32_t)(bx + 1), (uint32_t)(by + 1));
+    return P.tile_base + tile_of_node(P, (uint32_t)(bx + 1), (uint32_t)(by + 1));
 }
 
 // Batch prologue of the default path: tile key, rank within the tile and
 // P2G record of the particle in each slot (later substeps get them from G2P).
-__global__ void k_tile_count(Ctx c)
+__global__ void k_tile_count(Ctx c0)
 {
-    const StepParams &P = *c.P;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    bool valid = i < P.n_particles && takes_part(c);
+    const Ctx c = scene_ctx(c0, c0.n_scenes == 1u || i >= c0.n ? 0u : scene_of_slot(c0, i));
+    const StepParams &P = *c.P;
+    bool valid = i < c0.n && takes_part(c);
     uint32_t key = 0;
     if (valid) {
         Stencil s;
@@ -685,36 +726,46 @@ __global__ void k_tile_count(Ctx c)
     c.keys[i] = key;
 }
 
-// The first kernel of a substep of the default path: starts the substep
-// (begin_substep), then the exclusive scan of the tile counts in one CTA, 8
-// consecutive tiles per thread and pass (vector loads and stores), plus the
-// ascending list of tiles holding particles; zeroes the counts for the next
-// substep.  A substep that does not run lists no tile (the counts are
-// cleared at the start of every batch).
-__global__ void __launch_bounds__(SCAN_TOP_THREADS) k_tile_scan(Ctx c)
+// The first kernel of a substep of the default path, one CTA per scene:
+// starts the scene's substep (begin_substep), then the exclusive scan of its
+// tile counts, 8 consecutive tiles per thread and pass (vector loads and
+// stores), ending in the scene's sentinel entry; the scene's tiles holding
+// particles join the substep's tile list (ascending; with several scenes a
+// range of the list is reserved per pass); zeroes the counts for the next
+// substep.  A scene that does not take part lists no tile (the counts are
+// cleared at the start of every batch).  CTA 0 empties the tile list of the
+// next substep (the other buffer parity).
+__global__ void __launch_bounds__(SCAN_TOP_THREADS) k_tile_scan(Ctx c0)
 {
     constexpr int ITEMS = 8;
     constexpr uint32_t PASS = SCAN_TOP_THREADS * ITEMS;
     __shared__ bool s_runs;
+    __shared__ uint32_t s_list;
+    const Ctx c = scene_ctx(c0, blockIdx.x);
+    uint32_t *list_size = c0.work + WORK_ACTIVE + c0.parity;
     if (threadIdx.x == 0) {
         s_runs = begin_substep(c);
-        if (!s_runs) c.counters[COUNTER_ACTIVE_TILES] = 0u;
+        if (blockIdx.x == 0) c0.work[WORK_ACTIVE + (c0.parity ^ 1u)] = 0u;
     }
     __syncthreads();
     if (!s_runs) return;  // the same answer for every thread of the CTA
-    const uint32_t n_tiles = c.n_tiles;
-    uint32_t running = 0, running_active = 0;
+    const StepParams &P = *c.P;
+    const bool one_scene = c0.n_scenes == 1u;
+    uint32_t *count = c.tile_count + P.tile_base;  // 32-byte aligned: scenes start on 8-tile boundaries
+    uint32_t *start = c.tile_start + P.tile_base;
+    const uint32_t n_tiles = P.scene_tiles;
+    uint32_t running = P.p_base, listed = 0;
     for (uint32_t base = 0; base < n_tiles; base += PASS) {
         const uint32_t first = base + threadIdx.x * ITEMS;
         const bool whole = first + ITEMS <= n_tiles;
         uint32_t v[ITEMS];
         if (whole) {
-            const uint4 a = *reinterpret_cast<const uint4 *>(c.tile_count + first);
-            const uint4 b = *reinterpret_cast<const uint4 *>(c.tile_count + first + 4);
+            const uint4 a = *reinterpret_cast<const uint4 *>(count + first);
+            const uint4 b = *reinterpret_cast<const uint4 *>(count + first + 4);
             v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
         } else {
 #pragma unroll
-            for (int k = 0; k < ITEMS; ++k) v[k] = first + k < n_tiles ? c.tile_count[first + k] : 0u;
+            for (int k = 0; k < ITEMS; ++k) v[k] = first + k < n_tiles ? count[first + k] : 0u;
         }
         uint32_t sum = 0, nonempty = 0;
 #pragma unroll
@@ -724,7 +775,13 @@ __global__ void __launch_bounds__(SCAN_TOP_THREADS) k_tile_scan(Ctx c)
         }
         uint32_t total, total_active;
         const uint32_t offset = running + block_exclusive_scan<SCAN_TOP_THREADS>(sum, total);
-        uint32_t slot = running_active + block_exclusive_scan<SCAN_TOP_THREADS>(nonempty, total_active);
+        const uint32_t rank = block_exclusive_scan<SCAN_TOP_THREADS>(nonempty, total_active);
+        if (!one_scene) {
+            if (threadIdx.x == 0) s_list = total_active ? atomicAdd(list_size, total_active) : 0u;
+            __syncthreads();
+        }
+        uint32_t slot = (one_scene ? listed : s_list) + rank;
+        listed += total_active;
         uint32_t st[ITEMS];
         uint32_t acc = offset;
 #pragma unroll
@@ -733,45 +790,63 @@ __global__ void __launch_bounds__(SCAN_TOP_THREADS) k_tile_scan(Ctx c)
             acc += v[k];
         }
         if (whole) {
-            *reinterpret_cast<uint4 *>(c.tile_start + first) = make_uint4(st[0], st[1], st[2], st[3]);
-            *reinterpret_cast<uint4 *>(c.tile_start + first + 4) = make_uint4(st[4], st[5], st[6], st[7]);
-            *reinterpret_cast<uint4 *>(c.tile_count + first) = make_uint4(0u, 0u, 0u, 0u);
-            *reinterpret_cast<uint4 *>(c.tile_count + first + 4) = make_uint4(0u, 0u, 0u, 0u);
+            *reinterpret_cast<uint4 *>(start + first) = make_uint4(st[0], st[1], st[2], st[3]);
+            *reinterpret_cast<uint4 *>(start + first + 4) = make_uint4(st[4], st[5], st[6], st[7]);
+            *reinterpret_cast<uint4 *>(count + first) = make_uint4(0u, 0u, 0u, 0u);
+            *reinterpret_cast<uint4 *>(count + first + 4) = make_uint4(0u, 0u, 0u, 0u);
         } else {
 #pragma unroll
             for (int k = 0; k < ITEMS; ++k) {
                 if (first + k < n_tiles) {
-                    c.tile_start[first + k] = st[k];
-                    c.tile_count[first + k] = 0u;
+                    start[first + k] = st[k];
+                    count[first + k] = 0u;
                 }
             }
         }
         if (nonempty) {
 #pragma unroll
             for (int k = 0; k < ITEMS; ++k)
-                if (v[k] != 0u) c.active_tiles[slot++] = first + k;
+                if (v[k] != 0u) c.active_tiles[slot++] = P.tile_base + first + k;
         }
         running += total;
-        running_active += total_active;
+        if (!one_scene) __syncthreads();  // s_list is rewritten by the next pass
     }
     if (threadIdx.x == 0) {
-        c.tile_start[n_tiles] = running;
-        c.counters[COUNTER_ACTIVE_TILES] = running_active;
+        start[n_tiles] = running;
+        if (one_scene) *list_size = listed;
     }
 }
 
 // Bucket the slots by tile: perm[tile start + rank] = slot, four slots per
-// thread.  The status word is read along with the keys (no launch in this
-// kernel writes it): keys and ranks of a failed substep may be stale.
+// thread, for the scenes taking part in the substep.  The status word is read
+// along with the keys (no launch in this kernel writes it): keys and ranks of
+// a failed substep may be stale.  With several scenes, a warp whose slots
+// lie in one scene asks once whether that scene takes part.
 __global__ void k_tile_scatter(Ctx c)
 {
     const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) * 4u;
+    if (c.n_scenes > 1u) {
+        const uint32_t first = min(i, c.n - 1u);
+        const uint32_t scene = scene_of_slot(c, first);
+        const uint32_t lead = __shfl_sync(0xffffffffu, scene, 0);
+        const uint32_t end = c.scene_p_base[lead + 1u];
+        const uint32_t warp_last = min(((blockIdx.x * blockDim.x + (threadIdx.x | 31u)) * 4u) + 3u, c.n - 1u);
+        const bool one = __shfl_sync(0xffffffffu, warp_last, 31) < end;
+        if (one && !takes_part(scene_ctx(c, lead))) return;
+        if (i >= c.n) return;
+        for (uint32_t j = i; j < min(i + 4u, c.n); ++j) {
+            if (!one && !takes_part(scene_ctx(c, scene_of_slot(c, j)))) continue;
+            c.perm[c.tile_start[c.keys[j]] + c.ranks[j]] = j;
+        }
+        return;
+    }
     if (i >= c.n) return;
+    const bool runs = __ldcg(c.counters + COUNTER_SUBSTEP) < c.P->batch_steps;
     const uint32_t status = __ldcg(c.status);
     if (i + 4u <= c.n) {
         const uint4 key = __ldcs(reinterpret_cast<const uint4 *>(c.keys + i));
         const uint4 rank = __ldcs(reinterpret_cast<const uint4 *>(c.ranks + i));
-        if (status != 0u) return;
+        if (status != 0u || !runs) return;
         const uint32_t s0 = c.tile_start[key.x], s1 = c.tile_start[key.y], s2 = c.tile_start[key.z],
                        s3 = c.tile_start[key.w];
         c.perm[s0 + rank.x] = i;
@@ -779,7 +854,7 @@ __global__ void k_tile_scatter(Ctx c)
         c.perm[s2 + rank.z] = i + 2u;
         c.perm[s3 + rank.w] = i + 3u;
     } else {
-        if (status != 0u) return;
+        if (status != 0u || !runs) return;
         for (uint32_t j = i; j < c.n; ++j) c.perm[c.tile_start[c.keys[j]] + c.ranks[j]] = j;
     }
 }
@@ -967,13 +1042,15 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, uint32_t begi
 // chunks of the bucket, whose order then decides the rounding of their
 // sums).  The sums go to the tile's own ring record; k_g2p_tile adds
 // the up to four records that cover a node.
-__global__ void __launch_bounds__(TILE_CELLS) k_p2g_gather(Ctx c)
+template <bool SCENES>
+__global__ void __launch_bounds__(TILE_CELLS) k_p2g_gather(Ctx c0)
 {
     __shared__ Stage sm;
-    const uint32_t n_active = c.counters[COUNTER_ACTIVE_TILES];
-    const uint32_t stamp = c.counters[COUNTER_STAMP];
+    const uint32_t n_active = c0.work[WORK_ACTIVE + c0.parity];
     for (uint32_t item = blockIdx.x; item < n_active; item += gridDim.x) {
-        const uint32_t tile = c.active_tiles[item];
+        const uint32_t tile = c0.active_tiles[item];
+        const Ctx c = tile_ctx<SCENES>(c0, tile);
+        const uint32_t stamp = c.counters[COUNTER_STAMP];
         const uint32_t begin = c.tile_start[tile], n_tile = c.tile_start[tile + 1] - begin;
         __syncthreads();  // the previous tile's readers of sm are done
         for (int k = threadIdx.x; k < ACC_WORDS * RING_NODES; k += TILE_CELLS) (&sm.acc[0][0])[k] = 0.f;
@@ -982,7 +1059,7 @@ __global__ void __launch_bounds__(TILE_CELLS) k_p2g_gather(Ctx c)
             sm.mask = 0u;
         }
         __syncthreads();
-        if (sm.failed) return;
+        if (sm.failed) continue;  // the scene's substep is rolled back
         if (n_tile > (uint32_t)STAGE_CAP) {
             if (threadIdx.x < TILE_Y) sm.rows[threadIdx.x] = 0u;
             __syncthreads();
@@ -1019,7 +1096,7 @@ __global__ void __launch_bounds__(TILE_CELLS) k_p2g_gather(Ctx c)
                 i0 = 0;
             }
         }
-        if (!ok) return;
+        if (!ok) continue;
         const uint32_t mask = sm.mask;
         if (threadIdx.x == 0) c.tile_info[tile] = make_uint2(stamp, mask);
         float *out = c.part + (size_t)tile * (ACC_WORDS * RING_NODES);
@@ -1058,7 +1135,7 @@ __device__ __forceinline__ NodeSources node_sources(const StepParams &P, const u
         if (rx >= RING_X || ry >= RING_Y || ox < -1 || ox > 1 || oy < -1 || oy > 1) continue;
         const uint2 in = info[(oy + 1) * 3 + (ox + 1)];
         if (in.x != stamp) continue;
-        ns.base[k] = ((uint32_t)sy * P.tiles_x + (uint32_t)sx) * (uint32_t)(ACC_WORDS * RING_NODES) +
+        ns.base[k] = (P.tile_base + (uint32_t)sy * P.tiles_x + (uint32_t)sx) * (uint32_t)(ACC_WORDS * RING_NODES) +
                      (uint32_t)(ry * RING_X + rx);
         ns.mask[k] = in.y;
     }
@@ -1706,6 +1783,19 @@ __device__ __forceinline__ void stage_chunk(const Ctx &c, uint32_t base, uint32_
 
 }  // namespace
 
+// Adds a warp's counts of active solid / water / oil nodes to the counters
+// and clears them.
+__device__ __forceinline__ void flush_active_nodes(uint32_t *counters, uint32_t &ws, uint32_t &ww, uint32_t &wo)
+{
+    const uint32_t a = warp_sum(ws), b = warp_sum(ww), d = warp_sum(wo);
+    if ((threadIdx.x & 31u) == 0u) {
+        if (a) atomicAdd(counters + COUNTER_ACTIVE, a);
+        if (b) atomicAdd(counters + COUNTER_ACTIVE + 1, b);
+        if (d) atomicAdd(counters + COUNTER_ACTIVE + 2, d);
+    }
+    ws = ww = wo = 0u;
+}
+
 // The grid update and G2P of one tile holding particles (updateGrid,
 // shaders.ts:1485-1746, then g2p as in k_g2p), one tile per CTA iteration.
 // The CTA first evaluates the node update of the tile's 18x10-node ring --
@@ -1717,10 +1807,9 @@ __device__ __forceinline__ void stage_chunk(const Ctx &c, uint32_t base, uint32_
 // whose ring holds a failing node raises the grid status and moves none of
 // its particles (the substep is rolled back); tiles elsewhere still move
 // theirs, so their G2P flags can join the status of that substep.
-template <bool BODIES>
-__global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c)
+template <bool SCENES, bool BODIES>
+__global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
 {
-    const StepParams &P = *c.P;
     __shared__ uint2 s_info[9];
     __shared__ float2 s_vol[VOL_X * VOL_Y];
     __shared__ float2 s_vs[RING_NODES];
@@ -1733,21 +1822,24 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c)
     __shared__ float2 p_pos[G2P_STAGE];
     __shared__ float p_vol[G2P_STAGE], p_pvol[G2P_STAGE], p_damage[G2P_STAGE];
     __shared__ uint32_t p_mat[G2P_STAGE], p_orig[G2P_STAGE];
-    const uint32_t n_active = c.counters[COUNTER_ACTIVE_TILES];
-    const uint32_t stamp = c.counters[COUNTER_STAMP];
-    const int tiles_x = (int)P.tiles_x, tiles_y = (int)P.tiles_y;
-    const int node_w = (int)P.node_w, node_h = (int)P.node_h;
+    const uint32_t n_active = c0.work[WORK_ACTIVE + c0.parity];
     uint32_t ws = 0, ww = 0, wo = 0;
     for (uint32_t item = blockIdx.x; item < n_active; item += gridDim.x) {
-        const uint32_t tile = c.active_tiles[item];
-        const int tx = (int)(tile % P.tiles_x), ty = (int)(tile / P.tiles_x);
+        const uint32_t tile = c0.active_tiles[item];
+        const Ctx c = tile_ctx<SCENES>(c0, tile);
+        const StepParams &P = *c.P;
+        const uint32_t stamp = c.counters[COUNTER_STAMP];
+        const int tiles_x = (int)P.tiles_x, tiles_y = (int)P.tiles_y;
+        const int node_w = (int)P.node_w, node_h = (int)P.node_h;
+        const uint32_t local = tile - P.tile_base;
+        const int tx = (int)(local % P.tiles_x), ty = (int)(local / P.tiles_x);
         const int x0 = tx * TILE_X, y0 = ty * TILE_Y;
         const uint32_t begin = c.tile_start[tile], end = c.tile_start[tile + 1];
         __syncthreads();  // readers of the previous tile's shared data are done
         if (threadIdx.x < 9) {
             const int sx = tx + (int)(threadIdx.x % 3) - 1, sy = ty + (int)(threadIdx.x / 3) - 1;
             s_info[threadIdx.x] = (sx >= 0 && sy >= 0 && sx < tiles_x && sy < tiles_y)
-                                      ? c.tile_info[sy * tiles_x + sx]
+                                      ? c.tile_info[P.tile_base + (uint32_t)(sy * tiles_x + sx)]
                                       : make_uint2(0xffffffffu, 0u);
         }
         if (threadIdx.x == 0) s_fail = *(volatile uint32_t *)c.status != 0u ? 2 : 0;
@@ -1756,8 +1848,8 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c)
                     p_orig);
         __syncthreads();
         if (s_fail) {
-            cp_async_wait_all();  // no copy may land after the CTA has left
-            break;
+            cp_async_wait_all();  // no copy may land after this tile's shared data is reused
+            continue;             // the scene's substep is rolled back
         }
         // node phase: thread t takes node (x0 - 1 + t % VOL_X, y0 - 1 + t / VOL_X)
         // of the region around the ring; ring nodes load their full sums,
@@ -1864,59 +1956,86 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c)
                 c.keys[p] = key;
             }
         }
+        if constexpr (SCENES) flush_active_nodes(c.counters, ws, ww, wo);  // the tile's scene
     }
-    ws = warp_sum(ws);
-    ww = warp_sum(ww);
-    wo = warp_sum(wo);
-    if ((threadIdx.x & 31u) == 0u) {
-        if (ws) atomicAdd(c.counters + COUNTER_ACTIVE, ws);
-        if (ww) atomicAdd(c.counters + COUNTER_ACTIVE + 1, ww);
-        if (wo) atomicAdd(c.counters + COUNTER_ACTIVE + 2, wo);
-    }
+    if constexpr (!SCENES) flush_active_nodes(c0.counters, ws, ww, wo);
 }
 
 // The start of a substep of the fixed-point path (k_tile_scan starts those
-// of the default path).
+// of the default path): begin_substep for every scene.
 __global__ void k_substep_begin(Ctx c)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0) begin_substep(c);
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < c.n_scenes; s += gridDim.x * blockDim.x)
+        begin_substep(scene_ctx(c, s));
 }
 
 // The end of a batch of `total` substeps (commitParticles,
 // shaders.ts:3067-3080, once per batch), with `out` the buffer the batch
-// ends in and `in` the other one.  When the substeps completed and `total`
-// differ in parity (a raised status, or fewer substeps than the batch), the
-// state is in `in`: every slot (and the tracked slots) is copied over, the
-// whole-substep rollback.  Then, when `measure_speed` is set,
+// ends in and `in` the other one.  A scene whose completed substeps and
+// `total` differ in parity (a raised status, or fewer substeps than the
+// batch) has its state in `in`: its slots (and tracked slots) are copied
+// over, the whole-substep rollback.  Then, when `measure_speed` is set,
 // measureParticleSpeedPartials + reduceParticleSpeedPartials
-// (shaders.ts:2463-2533) of the final state as one warp-shuffle reduction
-// with an atomic max on the order-preserving bits of the non-negative speed.
-// Thread 0 of CTA 0 records the substeps completed and, under a CFL guard,
-// the committed microsteps.
-__global__ void k_end_batch(Ctx c, uint32_t total, uint32_t measure_speed)
+// (shaders.ts:2463-2533) of each scene's final state as one warp-shuffle
+// reduction with an atomic max on the order-preserving bits of the
+// non-negative speed.  Thread s of CTA 0 records scene s's completed
+// substeps and, under a CFL guard, its committed microsteps; every thread
+// may ask batch_stop first, which answers the same before and after.
+__global__ void k_end_batch(Ctx c0, uint32_t total, uint32_t measure_speed)
 {
-    const uint32_t stop = batch_stop(c, total);
-    const bool restore = ((stop ^ total) & 1u) != 0u;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        c.counters[COUNTER_STOP] = stop;
-        if (c.P->cfl_enabled) c.counters[COUNTER_PROGRESS] = stop;
-    }
-    if (restore) {
-        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < c.n_tracked; k += gridDim.x * blockDim.x)
-            c.slot_out[c.tracked[k]] = c.slot_in[c.tracked[k]];
-    }
-    float best = 0.0f;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.n; i += gridDim.x * blockDim.x) {
-        if (restore) copy_particle(c, i, i);
-        if (measure_speed) {
-            const float sp = length2(restore ? c.in.vel[i] : c.out.vel[i]);
-            best = fmaxf(best, finite_f(sp) ? sp : FLOAT_MAX);
+    if (blockIdx.x == 0) {
+        for (uint32_t s = threadIdx.x; s < c0.n_scenes; s += blockDim.x) {
+            const Ctx cs = scene_ctx(c0, s);
+            const uint32_t stop = batch_stop(cs, total);
+            cs.counters[COUNTER_STOP] = stop;
+            if (cs.P->cfl_enabled) cs.counters[COUNTER_PROGRESS] = stop;
         }
     }
-    if (!measure_speed) return;
+    // tracked slots: bodies and fracture bonds take a single scene
+    if (c0.n_tracked > 0u && ((batch_stop(c0, total) ^ total) & 1u) != 0u) {
+        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < c0.n_tracked; k += gridDim.x * blockDim.x)
+            c0.slot_out[c0.tracked[k]] = c0.slot_in[c0.tracked[k]];
+    }
+    const bool one_scene = c0.n_scenes == 1u;
+    const bool restore_one = one_scene && ((batch_stop(c0, total) ^ total) & 1u) != 0u;
+    if (one_scene) {
+        float best = 0.0f;
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c0.n; i += gridDim.x * blockDim.x) {
+            if (restore_one) copy_particle(c0, i, i);
+            if (measure_speed) {
+                const float sp = length2(restore_one ? c0.in.vel[i] : c0.out.vel[i]);
+                best = fmaxf(best, finite_f(sp) ? sp : FLOAT_MAX);
+            }
+        }
+        if (!measure_speed) return;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(c.counters + COUNTER_MAX_SPEED, __float_as_uint(best));
+        for (int o = 16; o > 0; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
+        if ((threadIdx.x & 31) == 0) atomicMax(c0.counters + COUNTER_MAX_SPEED, __float_as_uint(best));
+        return;
+    }
+    for (uint32_t base = blockIdx.x * blockDim.x; base < c0.n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        float best = 0.0f;
+        uint32_t scene = 0u;
+        if (i < c0.n) {
+            scene = scene_of_slot(c0, i);
+            const bool restore = ((batch_stop(scene_ctx(c0, scene), total) ^ total) & 1u) != 0u;
+            if (restore) copy_particle(c0, i, i);
+            if (measure_speed) {
+                const float sp = length2(restore ? c0.in.vel[i] : c0.out.vel[i]);
+                best = finite_f(sp) ? sp : FLOAT_MAX;
+            }
+        }
+        if (!measure_speed) continue;
+        if (__all_sync(0xffffffffu, scene == __shfl_sync(0xffffffffu, scene, 0))) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
+            if ((threadIdx.x & 31) == 0)
+                atomicMax(c0.dyn + (size_t)scene * SCENE_WORDS + 32 + COUNTER_MAX_SPEED, __float_as_uint(best));
+        } else if (i < c0.n) {
+            atomicMax(c0.dyn + (size_t)scene * SCENE_WORDS + 32 + COUNTER_MAX_SPEED, __float_as_uint(best));
+        }
+    }
 }
 
 // Counts the nodes of the last fixed-point substep whose solid / water / oil
@@ -2563,7 +2682,10 @@ __global__ void k_body_finish(Ctx c)
 }
 
 // the instances the host launches
-template __global__ void k_g2p_tile<false>(Ctx);
-template __global__ void k_g2p_tile<true>(Ctx);
+template __global__ void k_p2g_gather<false>(Ctx);
+template __global__ void k_p2g_gather<true>(Ctx);
+template __global__ void k_g2p_tile<false, false>(Ctx);
+template __global__ void k_g2p_tile<false, true>(Ctx);
+template __global__ void k_g2p_tile<true, false>(Ctx);
 
 }  // namespace mpm

@@ -49,16 +49,26 @@ struct TriField {
 };
 
 struct Ctx {
-    const StepParams *P;
-    uint32_t n;        // particle count (fixed for a solver; kernels read it from the parameter bank)
-    uint32_t n_tiles;  // 16x8-node tiles of the halo grid
+    const StepParams *P;  // the scene's parameters (scene 0 outside the scene-aware kernels)
+    // a batch of scenes: per scene its parameters and SCENE_WORDS words of
+    // status [0, 32) and counters [32, 64); shared work counters; the scene of
+    // each tile; the first slot of each scene (n_scenes + 1 entries)
+    const StepParams *scenes;
+    uint32_t *dyn;
+    uint32_t *work;
+    const uint32_t *tile_scene;
+    const uint32_t *scene_p_base;
+    uint32_t n_scenes;
+    uint32_t parity;   // the buffer `in` reads (0 / 1): picks the substep's tile list
+    uint32_t n;        // particle count of all scenes
+    uint32_t n_tiles;  // 16x8-node tiles of all scenes' halo grids (with one sentinel each)
     ParticleBuffers in;
     ParticleBuffers out;
     const Material *mats;
     const uint32_t *bonded;  // by original index
     const uint32_t *obj;     // by original index
-    uint32_t *status;
-    uint32_t *counters;
+    uint32_t *status;    // the scene's status words
+    uint32_t *counters;  // the scene's counters
     // cell sort
     uint32_t *keys;
     uint32_t *ranks;
@@ -132,12 +142,13 @@ constexpr int G2P_STAGE = 2 * G2P_THREADS;  // particles of a tile staged at onc
 static_assert(VOL_X * VOL_Y <= G2P_THREADS && RING_NODES <= G2P_THREADS, "one node per thread");
 
 // device counters beyond the three of mpm_device.cuh
-constexpr int COUNTER_ACTIVE = 4;        // [4..6] active solid/water/oil nodes
-constexpr int COUNTER_ACTIVE_TILES = 7;  // tiles holding particles this substep
+constexpr int COUNTER_ACTIVE = 4;        // [4..6] active solid/water/oil nodes (summed over the batch), [7] free
 constexpr int COUNTER_SUBSTEP = 8;       // the substep of this batch under way (failed and skipped included)
 constexpr int COUNTER_FRESH = 9;         // 1 from the start of a batch until its first substep starts
 constexpr int COUNTER_STOP = 10;         // substeps completed in this batch (STOP_NONE while running)
 constexpr uint32_t STOP_NONE = 0xffffffffu;
+constexpr int SCENE_WORDS = 64;  // per scene: status [0, 32), counters [32, 64)
+constexpr int WORK_ACTIVE = 0;   // work[0], work[1]: tiles listed for the substeps from buffer 0 / 1
 
 __global__ void k_count(Ctx c);
 __global__ void k_scan_reduce(Ctx c, uint32_t n_chunks);
@@ -148,9 +159,11 @@ __global__ void k_stable_rank(Ctx c);
 __global__ void k_tile_count(Ctx c);
 __global__ void k_tile_scan(Ctx c);
 __global__ void k_tile_scatter(Ctx c);
+// SCENES: the solver holds several scenes
+template <bool SCENES>
 __global__ void k_p2g_gather(Ctx c);
 // BODIES: the solver holds bonded-triangle bodies or fracture bonds
-template <bool BODIES>
+template <bool SCENES, bool BODIES>
 __global__ void k_g2p_tile(Ctx c);
 __global__ void k_prepare_scatter(Ctx c);
 __global__ void k_fixed_decode(Ctx c);

@@ -67,6 +67,14 @@ float u2f(uint32_t u)
     return v;
 }
 
+// One scene of a solver: its configuration, particle count and place in the
+// shared slot and tile ranges.
+struct SceneHost {
+    mpm_config cfg{};
+    uint32_t n = 0, p_base = 0;
+    uint32_t node_w = 0, node_h = 0, node_count = 0, tiles_x = 0, tiles_y = 0, tiles = 0, tile_base = 0;
+};
+
 }  // namespace
 
 struct mpm_solver {
@@ -79,12 +87,19 @@ struct mpm_solver {
     uint32_t n_bodies = 0, n_bonds = 0;
     int cur = 0;  // buffer holding the current particle state
     uint32_t substeps_since_begin = 0;
+    // scenes: one for mpm_create, several for mpmb_create
+    std::vector<SceneHost> scenes;
+    uint32_t n_scenes = 1, n_tiles_total = 0;
+    uint32_t *dyn = nullptr;           // per scene: 32 status words, 32 counters
+    uint32_t *work = nullptr;          // tile list sizes of the two buffer parities
+    uint32_t *tile_scene = nullptr;    // per tile
+    uint32_t *scene_p_base = nullptr;  // per scene, then the particle count
 
-    StepParams *d_params = nullptr;
-    StepParams *h_params = nullptr;  // pinned staging
+    StepParams *d_params = nullptr;  // per scene
+    StepParams *h_params = nullptr;  // pinned staging, per scene
     cudaEvent_t params_copied = nullptr;
-    uint32_t *d_status = nullptr;
-    uint32_t *d_counters = nullptr;
+    uint32_t *d_status = nullptr;    // scene 0's status words (in dyn)
+    uint32_t *d_counters = nullptr;  // scene 0's counters (in dyn)
     uint32_t *h_readback = nullptr;  // pinned: 2 counters + 8 status words (+ spare)
 
     ParticleBuffers buf[2]{};
@@ -135,8 +150,15 @@ Ctx make_ctx(mpm_solver *s, int parity)
 {
     Ctx c{};
     c.P = s->d_params;
+    c.scenes = s->d_params;
+    c.dyn = s->dyn;
+    c.work = s->work;
+    c.tile_scene = s->tile_scene;
+    c.scene_p_base = s->scene_p_base;
+    c.n_scenes = s->n_scenes;
+    c.parity = (uint32_t)parity;
     c.n = s->n;
-    c.n_tiles = s->tiles_x * s->tiles_y;
+    c.n_tiles = s->n_tiles_total;
     c.in = s->buf[parity];
     c.out = s->buf[1 - parity];
     c.mats = s->d_mats;
@@ -233,7 +255,7 @@ inline void mark(int slot)
 // The first tile count of a batch (later substeps are counted by G2P).
 void enqueue_tile_count(mpm_solver *s, const Ctx &c)
 {
-    cudaMemsetAsync(s->tile_count, 0, (size_t)s->tiles_x * s->tiles_y * sizeof(uint32_t), s->stream);
+    cudaMemsetAsync(s->tile_count, 0, (size_t)s->n_tiles_total * sizeof(uint32_t), s->stream);
     k_tile_count<<<blocks_for(s->n, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c);
     mark(K_TILE_COUNT);
 }
@@ -283,20 +305,25 @@ void enqueue_substep(mpm_solver *s, int parity)
     const unsigned pb = blocks_for(s->n, PARTICLE_THREADS);
     const dim3 tiles(s->tiles_x, s->tiles_y);
     if (s->gather()) {
-        k_tile_scan<<<1, SCAN_TOP_THREADS, 0, s->stream>>>(c);
+        k_tile_scan<<<s->n_scenes, SCAN_TOP_THREADS, 0, s->stream>>>(c);
         mark(K_TILE_SCAN);
         k_tile_scatter<<<blocks_for((s->n + 3) / 4, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c);
         mark(K_TILE_SCATTER);
-        k_p2g_gather<<<s->p2g_ctas, TILE_CELLS, 0, s->stream>>>(c);
+        if (s->n_scenes > 1)
+            k_p2g_gather<true><<<s->p2g_ctas, TILE_CELLS, 0, s->stream>>>(c);
+        else
+            k_p2g_gather<false><<<s->p2g_ctas, TILE_CELLS, 0, s->stream>>>(c);
         mark(K_P2G_GATHER);
         if (s->n_bodies) k_triangle_field<<<tiles, TILE_NODES, 0, s->stream>>>(c);
-        if (s->n_tracked > 0)
-            k_g2p_tile<true><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
+        if (s->n_scenes > 1)
+            k_g2p_tile<true, false><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
+        else if (s->n_tracked > 0)
+            k_g2p_tile<false, true><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
         else
-            k_g2p_tile<false><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
+            k_g2p_tile<false, false><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
         mark(K_G2P_TILE);
     } else {
-        k_substep_begin<<<1, 32, 0, s->stream>>>(c);
+        k_substep_begin<<<blocks_for(s->n_scenes, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c);
         mark(K_SUBSTEP_BEGIN);
         k_prepare_scatter<<<pb, PARTICLE_THREADS, 0, s->stream>>>(c);
         mark(K_PREPARE_SCATTER);
@@ -349,19 +376,23 @@ int get_graph(mpm_solver *s, int log2_steps, int parity, cudaGraphExec_t *out)
     return MPM_OK;
 }
 
-void fill_params(mpm_solver *s, StepParams &p, float dt, float gx, float gy, const mpm_cfl_guard *guard,
-                 float bond_reference_dt, uint32_t steps)
+void fill_params(mpm_solver *s, uint32_t scene, StepParams &p, float dt, float gx, float gy,
+                 const mpm_cfl_guard *guard, float bond_reference_dt, uint32_t steps)
 {
     std::memset(&p, 0, sizeof p);
-    const mpm_config &c = s->cfg;
+    const SceneHost &sc = s->scenes[scene];
+    const mpm_config &c = sc.cfg;
     p.cells_x = c.cells_x;
     p.cells_y = c.cells_y;
-    p.node_w = s->node_w;
-    p.node_h = s->node_h;
-    p.n_particles = s->n;
-    p.n_nodes = s->node_count;
-    p.tiles_x = s->tiles_x;
-    p.tiles_y = s->tiles_y;
+    p.node_w = sc.node_w;
+    p.node_h = sc.node_h;
+    p.n_particles = sc.n;
+    p.n_nodes = sc.node_count;
+    p.tiles_x = sc.tiles_x;
+    p.tiles_y = sc.tiles_y;
+    p.p_base = sc.p_base;
+    p.tile_base = sc.tile_base;
+    p.scene_tiles = sc.tiles;
     p.n_bodies = s->n_bodies;
     p.cfl_enabled = guard ? 1u : 0u;
     p.n_bonds = s->n_bonds;
@@ -404,12 +435,28 @@ void fill_params(mpm_solver *s, StepParams &p, float dt, float gx, float gy, con
     }
 }
 
+// The same step for every scene.
 int upload_params(mpm_solver *s, float dt, float gx, float gy, const mpm_cfl_guard *guard, float bond_reference_dt,
                   uint32_t steps)
 {
     CUDA_TRY(cudaEventSynchronize(s->params_copied));
-    fill_params(s, *s->h_params, dt, gx, gy, guard, bond_reference_dt, steps);
-    CUDA_TRY(cudaMemcpyAsync(s->d_params, s->h_params, sizeof(StepParams), cudaMemcpyHostToDevice, s->stream));
+    for (uint32_t k = 0; k < s->n_scenes; ++k)
+        fill_params(s, k, s->h_params[k], dt, gx, gy, guard, bond_reference_dt, steps);
+    CUDA_TRY(cudaMemcpyAsync(s->d_params, s->h_params, s->n_scenes * sizeof(StepParams), cudaMemcpyHostToDevice,
+                             s->stream));
+    CUDA_TRY(cudaEventRecord(s->params_copied, s->stream));
+    return MPM_OK;
+}
+
+// A step of its own for each scene (steps[k] 0: the scene sits the batch out).
+int upload_scene_params(mpm_solver *s, const uint32_t *steps, const float *dt, const float *gx, const float *gy,
+                        const mpm_cfl_guard *guards)
+{
+    CUDA_TRY(cudaEventSynchronize(s->params_copied));
+    for (uint32_t k = 0; k < s->n_scenes; ++k)
+        fill_params(s, k, s->h_params[k], dt[k], gx[k], gy[k], guards ? guards + k : nullptr, 0.0f, steps[k]);
+    CUDA_TRY(cudaMemcpyAsync(s->d_params, s->h_params, s->n_scenes * sizeof(StepParams), cudaMemcpyHostToDevice,
+                             s->stream));
     CUDA_TRY(cudaEventRecord(s->params_copied, s->stream));
     return MPM_OK;
 }
@@ -535,7 +582,7 @@ void free_solver(mpm_solver *s)
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
     s->graphs.clear();
-    void *ptrs[] = {s->d_params, s->d_status, s->d_counters, s->bonded, s->obj, s->d_mats, s->keys, s->ranks,
+    void *ptrs[] = {s->d_params, s->dyn, s->work, s->tile_scene, s->scene_p_base, s->bonded, s->obj, s->d_mats, s->keys, s->ranks,
                     s->tmp, s->perm, s->cell_count, s->cell_start, s->block_sums, s->p2g_solid, s->p2g_water,
                     s->p2g_oil, s->g_solid, s->g_water, s->g_oil, s->fixed, s->tile_stamp, s->d_active,
                     s->tile_count, s->tile_start, s->active_tiles, s->part, s->tile_info,
@@ -559,15 +606,9 @@ void free_solver(mpm_solver *s)
     delete s;
 }
 
-int create_impl(const mpm_config *config, const float *packed, const uint32_t *object_ids, uint32_t count,
-                const uint32_t *body_starts, uint32_t body_count, const uint32_t *bonds, uint32_t bond_count,
-                const uint32_t *topology, uint32_t topology_words, mpm_solver **out)
+// Validates one scene's configuration for `count` particles.
+int check_config(const mpm_config &c, uint32_t count)
 {
-    if (!config || !out) return set_error(MPM_ERR_INVALID_ARGUMENT, "config and out must not be NULL");
-    *out = nullptr;
-    if (count > 0 && (!packed || !object_ids))
-        return set_error(MPM_ERR_INVALID_ARGUMENT, "packed_particles and object_ids must not be NULL");
-    const mpm_config &c = *config;
     if (c.cells_x < 1 || c.cells_y < 1 || (uint64_t)c.cells_x + 3 > 0xffffffffull || (uint64_t)c.cells_y + 3 > 0xffffffffull)
         return set_error(MPM_ERR_INVALID_ARGUMENT, "grid.cellsX must be a positive safe integer that fits the GPU layout");
     if (!(c.cell_size > 0.0f) || !std::isfinite(c.cell_size))
@@ -586,6 +627,40 @@ int create_impl(const mpm_config *config, const float *packed, const uint32_t *o
         return set_error(MPM_ERR_INVALID_ARGUMENT, "halo grid dimensions exceed the GPU index range");
     if ((uint64_t)c.capacity * 9ull > 0x7fffffffull)
         return set_error(MPM_ERR_INVALID_ARGUMENT, "particle stencil entries exceed the index range");
+    return MPM_OK;
+}
+
+// Creates a solver over `n_scenes` scenes: configs[k] with counts[k]
+// particles, packed one scene after another.  Bonded bodies, fracture bonds
+// and the fixed-point P2G take a single scene; the scenes of a batch hold
+// exactly their particles.
+int create_impl(const mpm_config *configs, uint32_t n_scenes, const uint32_t *counts, const float *packed,
+                const uint32_t *object_ids, const uint32_t *body_starts, uint32_t body_count, const uint32_t *bonds,
+                uint32_t bond_count, const uint32_t *topology, uint32_t topology_words, mpm_solver **out)
+{
+    if (!configs || !counts || !out) return set_error(MPM_ERR_INVALID_ARGUMENT, "configs, counts and out must not be NULL");
+    *out = nullptr;
+    if (n_scenes < 1) return set_error(MPM_ERR_INVALID_ARGUMENT, "a solver needs at least one scene");
+    uint64_t total = 0;
+    for (uint32_t k = 0; k < n_scenes; ++k) {
+        mpm_config ck = configs[k];
+        if (n_scenes > 1) ck.capacity = counts[k];
+        const int rc = check_config(ck, counts[k]);
+        if (rc != MPM_OK) return n_scenes > 1 ? set_error(rc, "scene %u: %s", k, g_last_error.c_str()) : rc;
+        total += counts[k];
+    }
+    if (total * 9ull > 0x7fffffffull)
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "particle stencil entries exceed the index range");
+    const uint32_t count = (uint32_t)total;
+    if (count > 0 && (!packed || !object_ids))
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "packed_particles and object_ids must not be NULL");
+    const mpm_config &c = configs[0];
+    if (n_scenes > 1) {
+        if (c.p2g_mode != MPM_P2G_GATHER)
+            return set_error(MPM_ERR_INVALID_ARGUMENT, "a batch of scenes runs the default P2G only");
+        if (body_count > 0 || bond_count > 0)
+            return set_error(MPM_ERR_INVALID_ARGUMENT, "bonded triangle bodies and fracture bonds take a single scene");
+    }
     if (body_count > 0 && !body_starts) return set_error(MPM_ERR_INVALID_ARGUMENT, "body_starts must not be NULL");
     for (uint32_t b = 0; b < body_count; ++b)
         if ((uint64_t)body_starts[b] + 2u >= count)
@@ -615,7 +690,30 @@ int create_impl(const mpm_config *config, const float *packed, const uint32_t *o
     s->device = c.device;
     s->cfg = c;
     s->n = count;
-    s->capacity = std::max<uint32_t>(c.capacity, 1u);
+    s->capacity = std::max<uint32_t>(n_scenes > 1 ? count : c.capacity, 1u);
+    s->n_scenes = n_scenes;
+    s->scenes.resize(n_scenes);
+    {
+        uint32_t p_base = 0, tile_base = 0;
+        for (uint32_t k = 0; k < n_scenes; ++k) {
+            SceneHost &sc = s->scenes[k];
+            sc.cfg = configs[k];
+            sc.n = counts[k];
+            sc.p_base = p_base;
+            sc.node_w = sc.cfg.cells_x + 3;
+            sc.node_h = sc.cfg.cells_y + 3;
+            sc.node_count = sc.node_w * sc.node_h;
+            sc.tiles_x = (sc.node_w + TILE_X - 1) / TILE_X;
+            sc.tiles_y = (sc.node_h + TILE_Y - 1) / TILE_Y;
+            sc.tiles = sc.tiles_x * sc.tiles_y;
+            sc.tile_base = tile_base;
+            p_base += sc.n;
+            // the scene's tiles, its sentinel, then an 8-tile boundary (the
+            // tile scan reads counts in aligned groups of 8)
+            tile_base = (uint32_t)std::min<uint64_t>(((uint64_t)tile_base + sc.tiles + 1u + 7u) & ~7ull, 0xffffffffull);
+        }
+        s->n_tiles_total = tile_base;
+    }
     s->n_bodies = body_count;
     s->n_bonds = bond_count;
     if (bond_count > 0) {
@@ -624,7 +722,7 @@ int create_impl(const mpm_config *config, const float *packed, const uint32_t *o
     }
     s->node_w = c.cells_x + 3;
     s->node_h = c.cells_y + 3;
-    s->node_count = (uint32_t)nodes;
+    s->node_count = s->node_w * s->node_h;
     s->tiles_x = (s->node_w + TILE_X - 1) / TILE_X;
     s->tiles_y = (s->node_h + TILE_Y - 1) / TILE_Y;
     s->cell_pad = ((s->node_count + SCAN_CHUNK - 1) / SCAN_CHUNK) * SCAN_CHUNK;
@@ -634,6 +732,8 @@ int create_impl(const mpm_config *config, const float *packed, const uint32_t *o
         free_solver(s);
         return code;
     };
+    if ((uint64_t)s->n_tiles_total * (ACC_WORDS * RING_NODES) >= 0xffffffffull)
+        return fail(set_error(MPM_ERR_INVALID_ARGUMENT, "the scenes' halo grids exceed the GPU index range"));
 #define ALLOC(ptr, n)                                                                                          \
     do {                                                                                                       \
         cudaError_t e__ = dalloc(&(ptr), (n));                                                                 \
@@ -645,15 +745,18 @@ int create_impl(const mpm_config *config, const float *packed, const uint32_t *o
     if (cudaEventCreateWithFlags(&s->params_copied, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreate(&s->batch_start) != cudaSuccess || cudaEventCreate(&s->batch_stop) != cudaSuccess)
         return fail(set_error(MPM_ERR_CUDA, "cudaEventCreate failed"));
-    if (cudaMallocHost(reinterpret_cast<void **>(&s->h_params), sizeof(StepParams)) != cudaSuccess ||
+    if (cudaMallocHost(reinterpret_cast<void **>(&s->h_params), n_scenes * sizeof(StepParams)) != cudaSuccess ||
         cudaMallocHost(reinterpret_cast<void **>(&s->h_readback), 16 * sizeof(uint32_t)) != cudaSuccess)
         return fail(set_error(MPM_ERR_CUDA, "cudaMallocHost failed"));
     cudaEventRecord(s->params_copied, s->stream);
 
     const size_t cap = s->capacity;
-    ALLOC(s->d_params, 1);
-    ALLOC(s->d_status, 32);
-    ALLOC(s->d_counters, 32);
+    ALLOC(s->d_params, n_scenes);
+    ALLOC(s->dyn, (size_t)n_scenes * SCENE_WORDS);
+    ALLOC(s->work, 4);
+    ALLOC(s->scene_p_base, (size_t)n_scenes + 1);
+    s->d_status = s->dyn;  // scene 0
+    s->d_counters = s->dyn + 32;
     for (int b = 0; b < 2; ++b) {
         ALLOC(s->buf[b].pos, cap);
         ALLOC(s->buf[b].vel, cap);
@@ -682,9 +785,25 @@ int create_impl(const mpm_config *config, const float *packed, const uint32_t *o
     cudaMemsetAsync(s->g_oil, 0, (size_t)s->node_count * sizeof(float4), s->stream);
     ALLOC(s->tile_stamp, (size_t)s->tiles_x * s->tiles_y);
     ALLOC(s->d_active, 4);
-    const size_t n_tiles = (size_t)s->tiles_x * s->tiles_y;
+    const size_t n_tiles = s->n_tiles_total;
     ALLOC(s->tile_count, n_tiles);
     ALLOC(s->tile_start, n_tiles + 1);
+    ALLOC(s->tile_scene, n_tiles);
+    {
+        std::vector<uint32_t> tile_scene(n_tiles, 0u), p_bases(n_scenes + 1);
+        for (uint32_t k = 0; k < n_scenes; ++k) {
+            const SceneHost &sc = s->scenes[k];
+            const uint32_t end = k + 1 < n_scenes ? s->scenes[k + 1].tile_base : (uint32_t)n_tiles;
+            for (uint32_t t = sc.tile_base; t < end; ++t) tile_scene[t] = k;
+            p_bases[k] = sc.p_base;
+        }
+        p_bases[n_scenes] = count;
+        if (cudaMemcpy(s->tile_scene, tile_scene.data(), n_tiles * sizeof(uint32_t), cudaMemcpyHostToDevice) !=
+                cudaSuccess ||
+            cudaMemcpy(s->scene_p_base, p_bases.data(), (n_scenes + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice) !=
+                cudaSuccess)
+            return fail(set_error(MPM_ERR_CUDA, "scene table upload failed"));
+    }
     if (c.p2g_mode == MPM_P2G_GATHER) {
         ALLOC(s->active_tiles, n_tiles);
         ALLOC(s->part, n_tiles * ACC_WORDS * RING_NODES);
@@ -698,11 +817,13 @@ int create_impl(const mpm_config *config, const float *packed, const uint32_t *o
             return fail(set_error(MPM_ERR_CUDA, "cudaMemset failed"));
         int sms = 0, per_sm_p2g = 0, per_sm_g2p = 0;
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device) != cudaSuccess ||
-            cudaFuncSetAttribute(k_p2g_gather, cudaFuncAttributePreferredSharedMemoryCarveout, 100) !=
+            cudaFuncSetAttribute(k_p2g_gather<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100) !=
                 cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_p2g, k_p2g_gather, TILE_CELLS, 0) !=
+            cudaFuncSetAttribute(k_p2g_gather<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100) !=
                 cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_g2p, k_g2p_tile<false>, G2P_THREADS, 0) !=
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_p2g, k_p2g_gather<false>, TILE_CELLS, 0) !=
+                cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_g2p, k_g2p_tile<false, false>, G2P_THREADS, 0) !=
                 cudaSuccess)
             return fail(set_error(MPM_ERR_CUDA, "occupancy query failed"));
         s->p2g_ctas = (unsigned)std::max<size_t>(1, std::min<size_t>(n_tiles, (size_t)sms * std::max(1, per_sm_p2g)));
@@ -768,11 +889,19 @@ int create_impl(const mpm_config *config, const float *packed, const uint32_t *o
 #undef ALLOC
     cudaMemsetAsync(s->cell_count, 0, (size_t)s->cell_pad * sizeof(uint32_t), s->stream);
     cudaMemsetAsync(s->tile_stamp, 0, (size_t)s->tiles_x * s->tiles_y * sizeof(uint32_t), s->stream);
-    cudaMemsetAsync(s->d_counters, 0, 32 * sizeof(uint32_t), s->stream);
-    const uint32_t init_status[32] = {0, 0xffffffffu};
-    cudaMemcpyAsync(s->d_status, init_status, sizeof init_status, cudaMemcpyHostToDevice, s->stream);
-    const uint32_t one = 1;  // tile stamps start at 0, so the first substep stamp is 1
-    cudaMemcpyAsync(s->d_counters + COUNTER_STAMP, &one, sizeof one, cudaMemcpyHostToDevice, s->stream);
+    {
+        // per scene: status word 1 (the particle index) empty; tile stamps
+        // start at 0 and the counter above them
+        std::vector<uint32_t> dyn((size_t)n_scenes * SCENE_WORDS, 0u);
+        for (uint32_t k = 0; k < n_scenes; ++k) {
+            dyn[(size_t)k * SCENE_WORDS + 1] = 0xffffffffu;
+            dyn[(size_t)k * SCENE_WORDS + 32 + COUNTER_STAMP] = 1u;
+        }
+        const uint32_t zeros[4] = {0, 0, 0, 0};
+        if (cudaMemcpy(s->dyn, dyn.data(), dyn.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(s->work, zeros, sizeof zeros, cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(set_error(MPM_ERR_CUDA, "status upload failed"));
+    }
     if (count > 0) {
         int rc = unpack_and_upload(s, packed, count, 0);
         if (rc != MPM_OK) return fail(rc);
@@ -791,6 +920,8 @@ int create_impl(const mpm_config *config, const float *packed, const uint32_t *o
     return MPM_OK;
 }
 
+int run_batch(mpm_solver *s, uint32_t step_count, bool guarded);
+
 }  // namespace
 
 extern "C" {
@@ -801,8 +932,8 @@ int mpm_create(const mpm_config *config, const float *packed_particles, const ui
                uint32_t fracture_topology_words, mpm_solver **out)
 {
     g_last_error.clear();
-    return create_impl(config, packed_particles, object_ids, particle_count, body_starts, body_count, fracture_bonds,
-                       fracture_bond_count, fracture_topology, fracture_topology_words, out);
+    return create_impl(config, 1u, &particle_count, packed_particles, object_ids, body_starts, body_count,
+                       fracture_bonds, fracture_bond_count, fracture_topology, fracture_topology_words, out);
 }
 
 int mpm_step_batch(mpm_solver *s, uint32_t step_count, float dt, float gx, float gy, const mpm_cfl_guard *guard,
@@ -816,9 +947,78 @@ int mpm_step_batch(mpm_solver *s, uint32_t step_count, float dt, float gx, float
     CUDA_TRY(cudaSetDevice(s->device));
     int rc = upload_params(s, dt, gx, gy, guard, bond_reference_dt, step_count);
     if (rc != MPM_OK) return rc;
+    return run_batch(s, step_count, guard != nullptr);
+}
+
+int mpmb_create(const mpm_config *configs, uint32_t scene_count, const uint32_t *particle_counts,
+                const float *packed_particles, const uint32_t *object_ids, mpm_solver **out)
+{
+    g_last_error.clear();
+    return create_impl(configs, scene_count, particle_counts, packed_particles, object_ids, nullptr, 0u, nullptr,
+                       0u, nullptr, 0u, out);
+}
+
+int mpmb_step_batch(mpm_solver *s, const uint32_t *step_counts, const float *dts, const float *gravity_xy,
+                    const mpm_cfl_guard *guards)
+{
+    g_last_error.clear();
+    if (!s || !step_counts || !dts || !gravity_xy)
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "solver, step_counts, dts and gravity_xy must not be NULL");
+    uint32_t most = 0;
+    std::vector<float> dt(s->n_scenes), gx(s->n_scenes), gy(s->n_scenes);
+    for (uint32_t k = 0; k < s->n_scenes; ++k) {
+        if (step_counts[k] > 0 && (!(dts[k] > 0.0f) || !std::isfinite(dts[k])))
+            return set_error(MPM_ERR_INVALID_ARGUMENT, "scene %u: dt must be greater than zero", k);
+        if (!std::isfinite(gravity_xy[2 * k]) || !std::isfinite(gravity_xy[2 * k + 1]))
+            return set_error(MPM_ERR_INVALID_ARGUMENT, "scene %u: gravity must be finite", k);
+        dt[k] = step_counts[k] > 0 ? dts[k] : 1.0f;  // a scene sitting the batch out keeps finite parameters
+        gx[k] = gravity_xy[2 * k];
+        gy[k] = gravity_xy[2 * k + 1];
+        most = std::max(most, step_counts[k]);
+    }
+    if (most < 1) return set_error(MPM_ERR_INVALID_ARGUMENT, "stepCount must be a positive safe integer.");
+    CUDA_TRY(cudaSetDevice(s->device));
+    int rc = upload_scene_params(s, step_counts, dt.data(), gx.data(), gy.data(), guards);
+    if (rc != MPM_OK) return rc;
+    return run_batch(s, most, guards != nullptr);
+}
+
+int mpmb_read_compact(mpm_solver *s, float *maximum_speeds, uint32_t *completed_microsteps, uint32_t *status)
+{
+    g_last_error.clear();
+    if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
+    CUDA_TRY(cudaSetDevice(s->device));
+    std::vector<uint32_t> dyn((size_t)s->n_scenes * SCENE_WORDS);
+    CUDA_TRY(cudaMemcpyAsync(dyn.data(), s->dyn, dyn.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    for (uint32_t k = 0; k < s->n_scenes; ++k) {
+        const uint32_t *w = dyn.data() + (size_t)k * SCENE_WORDS;
+        if (maximum_speeds) maximum_speeds[k] = u2f(w[32 + COUNTER_MAX_SPEED]);
+        if (completed_microsteps) completed_microsteps[k] = w[32 + COUNTER_PROGRESS];
+        if (status) {
+            std::memcpy(status + (size_t)k * 8, w, 8 * sizeof(uint32_t));
+            // the particle index within the scene
+            const uint32_t base = s->scenes[k].p_base;
+            if (w[1] != 0xffffffffu && w[1] >= base) status[(size_t)k * 8 + 1] = w[1] - base;
+        }
+    }
+    return MPM_OK;
+}
+
+uint32_t mpmb_scene_count(const mpm_solver *s) { return s ? s->n_scenes : 0u; }
+
+}  // extern "C"
+
+namespace {
+
+// Submits one batch of `step_count` substeps (the most any scene takes) with
+// the parameters already uploaded; `guarded`: a CFL guard is on.
+int run_batch(mpm_solver *s, uint32_t step_count, bool guarded)
+{
+    int rc = MPM_OK;
     const Ctx c0 = make_ctx(s, s->cur);
     CUDA_TRY(cudaEventRecord(s->batch_start, s->stream));
-    k_begin_batch<<<1, 32, 0, s->stream>>>(c0, guard ? 1u : 0u);
+    k_begin_batch<<<blocks_for(s->n_scenes, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c0, guarded ? 1u : 0u);
     s->substeps_since_begin = 0;
     if (s->gather() && s->n > 0) enqueue_tile_count(s, c0);
     CUDA_TRY(cudaGetLastError());
@@ -837,13 +1037,17 @@ int mpm_step_batch(mpm_solver *s, uint32_t step_count, float dt, float gx, float
             }
         }
         s->substeps_since_begin = step_count;
-        enqueue_end_batch(s, s->cur, step_count, guard != nullptr);
+        enqueue_end_batch(s, s->cur, step_count, guarded);
         CUDA_TRY(cudaGetLastError());
     }
     CUDA_TRY(cudaEventRecord(s->batch_stop, s->stream));
     s->batch_timed = true;
     return MPM_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 int mpm_last_batch_device_ms(mpm_solver *s, double *milliseconds)
 {
@@ -877,7 +1081,7 @@ int mpm_profile_substeps(mpm_solver *s, uint32_t step_count, float dt, float gx,
     const Ctx c0 = make_ctx(s, s->cur);
     const int start_parity = s->cur;
     CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-    k_begin_batch<<<1, 32, 0, s->stream>>>(c0, guard ? 1u : 0u);
+    k_begin_batch<<<blocks_for(s->n_scenes, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c0, guard ? 1u : 0u);
     rec.mark(-1);
     g_recorder = &rec;
     if (s->gather() && s->n > 0) enqueue_tile_count(s, c0);
@@ -970,8 +1174,11 @@ int mpm_clear_status(mpm_solver *s)
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
     CUDA_TRY(cudaSetDevice(s->device));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
-    const uint32_t init_status[8] = {0, 0xffffffffu, 0, 0, 0, 0, 0, 0};
-    CUDA_TRY(cudaMemcpy(s->d_status, init_status, sizeof init_status, cudaMemcpyHostToDevice));
+    // every scene's status words
+    std::vector<uint32_t> init_status((size_t)s->n_scenes * 8, 0u);
+    for (uint32_t k = 0; k < s->n_scenes; ++k) init_status[(size_t)k * 8 + 1] = 0xffffffffu;
+    CUDA_TRY(cudaMemcpy2D(s->dyn, SCENE_WORDS * sizeof(uint32_t), init_status.data(), 8 * sizeof(uint32_t),
+                          8 * sizeof(uint32_t), s->n_scenes, cudaMemcpyHostToDevice));
     return MPM_OK;
 }
 
@@ -1085,6 +1292,7 @@ int mpm_probe_sort(mpm_solver *s, float dt, uint32_t *keys_out, uint32_t *perm_o
     g_last_error.clear();
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
     if (!s->gather()) return set_error(MPM_ERR_STATE, "the cell sort runs in gather mode only");
+    if (s->n_scenes > 1) return set_error(MPM_ERR_STATE, "the sort probe takes a single-scene solver");
     CUDA_TRY(cudaSetDevice(s->device));
     int rc = upload_params(s, dt, 0.0f, 0.0f, nullptr, 0.0f, 1u);
     if (rc != MPM_OK) return rc;

@@ -7,6 +7,7 @@ from .cfl_bounds import calculate_mpm_cfl_velocity_bound, derive_mpm_mls_gpu_cfl
 from .errors import MpmMlsGpuNumericalError, MpmNativeError, RangeError
 from .layout import ParticleArrays, particles_from_dicts, particles_to_dicts, validate_mpm_mls_gpu_input
 from .solver import (MpmMlsGpuSolver, create_experimental_mpm_mls_atomic_gpu_solver, create_mpm_mls_gpu_solver)
+from .batched import MpmBatchedGpuSolver, create_mpm_batched_gpu_solver
 from .step_scheduler import calculate_mpm_cfl_step_batch, calculate_mpm_step_batch, mean_sinusoidal_acceleration
 
 __all__ = [
@@ -15,5 +16,6 @@ __all__ = [
     "MpmMlsGpuNumericalError", "MpmNativeError", "RangeError", "ParticleArrays", "particles_from_dicts",
     "particles_to_dicts", "validate_mpm_mls_gpu_input", "MpmMlsGpuSolver",
     "create_experimental_mpm_mls_atomic_gpu_solver", "create_mpm_mls_gpu_solver", "calculate_mpm_cfl_step_batch",
-    "calculate_mpm_step_batch", "mean_sinusoidal_acceleration",
+    "calculate_mpm_step_batch", "mean_sinusoidal_acceleration", "MpmBatchedGpuSolver",
+    "create_mpm_batched_gpu_solver",
 ]

@@ -24,6 +24,7 @@ EXPORTED_SYMBOLS = (
     "mpm_particle_count", "mpm_particle_capacity", "mpm_destroy", "mpm_last_error", "mpm_probe_sort",
     "mpm_probe_fixed_point", "mpm_probe_triangle_field", "mpm_node_count", "mpm_last_batch_device_ms", "mpm_profile_substeps",
     "mpm_profile_kernel_name", "mpm_profile_kernel_slots", "mpm_count_active_nodes", "mpm_stream",
+    "mpmb_create", "mpmb_step_batch", "mpmb_read_compact", "mpmb_scene_count",
 )
 
 
@@ -107,6 +108,14 @@ def load_library(path: str = LIBRARY_PATH) -> ctypes.CDLL:
     lib.mpm_count_active_nodes.restype = i32
     lib.mpm_stream.argtypes = [vp]
     lib.mpm_stream.restype = vp
+    lib.mpmb_create.argtypes = [vp, u32, vp, vp, vp, P(vp)]
+    lib.mpmb_create.restype = i32
+    lib.mpmb_step_batch.argtypes = [vp, vp, vp, vp, vp]
+    lib.mpmb_step_batch.restype = i32
+    lib.mpmb_read_compact.argtypes = [vp, vp, vp, vp]
+    lib.mpmb_read_compact.restype = i32
+    lib.mpmb_scene_count.argtypes = [vp]
+    lib.mpmb_scene_count.restype = u32
     _lib = lib
     return lib
 

@@ -9,6 +9,8 @@
   src/lib/mpm/scenes/gate4.ts:134-357 (LCG seeds, draw order, bonds).
 * `create_dam_break_scene` -- the 1,000,000-particle two-phase water/oil dam
   break on a 1024x2048 grid (cellSize 10, gravity 90, Gate-4 liquids).
+* `create_batched_tank_scenes` -- independent SI Tait water tanks of uneven
+  particle counts and grids for the batched solver.
 
 All seeded randomness uses the reference's LCG (gate4.ts:134-144) so that a
 seed names the same scene in every language.
@@ -296,3 +298,63 @@ def create_dam_break_scene(particles_per_phase: int = 500_000, columns: int = 50
     config = {"grid": grid, "particleMass": mass, "particleVolume": spacing * spacing,
               "material": GATE4_WATER_MATERIAL, "wallFriction": 0.0}
     return p, config
+
+
+# ------------------------------------------------------------ batched tanks --
+
+BATCHED_TANK_DOMAIN_M = 0.2
+BATCHED_TANK_GRAVITY = {"x": 0.0, "y": -9.81}
+BATCHED_TANK_MAX_FILL_HEIGHT = 0.6  # of the box
+
+
+def create_batched_tank_scenes(count: int = 512, seed: int = 0x4D504D42, particles=(1_000, 64_000),
+                               sides=(64, 512)):
+    """`count` independent SI Tait water tanks (rho 1000 kg/m^3, gamma 7,
+    c = 20 m/s, 0.02 m extrusion, no-slip walls, at rest under y-up gravity
+    9.81 m/s^2), each a 0.2 m square box.  Scene k draws from the LCG seeded
+    with (seed + k * 0x9E3779B9) mod 2^32: its particle count N log-uniform in
+    `particles`, its grid side S uniform in `sides` (S x S cells, dx = 0.2 m /
+    S), the width of its block (a quarter to 0.6 of the box) and the block's
+    place.  The block is a lattice at dx / 2 (2 x 2 particles per cell) where
+    N of them fit under 0.6 of the box height, else at the finer spacing that
+    fits; each particle is jittered by U(+-0.1) spacing.  Returns
+    [(particles, config), ...]."""
+    depth = MPM_SI_BOX_DOMAIN["extrusionDepthM"]
+    tait = {"referenceDensityKgPerM3": 1000.0, "exponent": 7.0,
+            "pressureCoefficientPa": derive_tait_pressure_coefficient_pa(1000.0, 7.0, 20.0)}
+    material = create_mpm_tait_liquid_material(tait, depth)
+    size = BATCHED_TANK_DOMAIN_M
+    top = BATCHED_TANK_MAX_FILL_HEIGHT * size
+    out = []
+    for k in range(count):
+        rnd = SeededRandom((seed + k * 0x9E3779B9) % UINT32_RANGE)
+        log_lo, log_hi = math.log(particles[0]), math.log(particles[1])
+        n = int(round(math.exp(log_lo + rnd() * (log_hi - log_lo))))
+        side = min(int(sides[0] + math.floor(rnd() * (sides[1] - sides[0] + 1))), sides[1])
+        dx = size / side
+        width = size * (0.25 + 0.35 * rnd())
+
+        def height(spacing):
+            return math.ceil(n / max(1, math.floor(width / spacing))) * spacing
+
+        spacing = dx / 2
+        if height(spacing) > top:
+            spacing = math.sqrt(width * top / n)
+            while height(spacing) > top:
+                spacing *= 0.99
+        columns = max(1, math.floor(width / spacing))
+        rows = math.ceil(n / columns)
+        x0 = (size - columns * spacing) * rnd()
+        y0 = (size - rows * spacing) * 0.5 * rnd()
+        jitter = lcg_sequence(rnd.state, 2 * n)
+        r, c = np.divmod(np.arange(n), columns)
+        p = ParticleArrays.empty(n)
+        p.px[:] = x0 + (c + 0.5) * spacing + (jitter[0::2] * 2 - 1) * 0.1 * spacing
+        p.py[:] = y0 + (r + 0.5) * spacing + (jitter[1::2] * 2 - 1) * 0.1 * spacing
+        area = spacing * spacing
+        p.volume[:] = area
+        config = {"grid": {"cellsX": side, "cellsY": side, "cellSize": dx},
+                  "particleMass": material["density"] * area, "particleVolume": area, "material": material,
+                  "wallFriction": 1.0}
+        out.append((p, config))
+    return out

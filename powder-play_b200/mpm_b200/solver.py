@@ -79,6 +79,28 @@ def validate_cfl_bounds(bounds, state: ValidatedInput, derived):
     return out
 
 
+def native_config(state: ValidatedInput, atomic_p2g: bool, fixed_point_shift: int, device: int):
+    """The mpm_config of a validated input (the float32 values that
+    validateMpmMlsGpuInput, layout.ts:122-607, derives)."""
+    cfg = state.config
+    c = _lib.MpmConfig()
+    c.cells_x, c.cells_y = cfg["grid"]["cellsX"], cfg["grid"]["cellsY"]
+    c.cell_size = state.cell_size_f32
+    c.particle_mass = state.particle_mass_f32
+    c.particle_volume = state.particle_volume_f32
+    c.bond_rest_length = state.bond_rest_length_f32
+    c.bond_stiffness = state.bond_stiffness_f32
+    c.bond_reference_dt = state.bond_reference_dt_f32 or 0.0
+    c.wall_friction = state.wall_friction_f32
+    c.lambda_ = state.lambda_f32
+    c.mu = state.mu_f32
+    c.capacity = state.particle_capacity
+    c.p2g_mode = _lib.MPM_P2G_FIXED_POINT if atomic_p2g else _lib.MPM_P2G_GATHER
+    c.fixed_point_shift = fixed_point_shift
+    c.device = device
+    return c
+
+
 class MpmMlsGpuSolver:
     """MpmMlsGpuSolver, solver.ts:106-144, backed by libmpm_b200.so."""
 
@@ -86,22 +108,7 @@ class MpmMlsGpuSolver:
                  fixed_point_shift: int = DEFAULT_FIXED_POINT_SHIFT):
         self._lib = _lib.load_library()
         self._state = state
-        cfg = state.config
-        c = _lib.MpmConfig()
-        c.cells_x, c.cells_y = cfg["grid"]["cellsX"], cfg["grid"]["cellsY"]
-        c.cell_size = state.cell_size_f32
-        c.particle_mass = state.particle_mass_f32
-        c.particle_volume = state.particle_volume_f32
-        c.bond_rest_length = state.bond_rest_length_f32
-        c.bond_stiffness = state.bond_stiffness_f32
-        c.bond_reference_dt = state.bond_reference_dt_f32 or 0.0
-        c.wall_friction = state.wall_friction_f32
-        c.lambda_ = state.lambda_f32
-        c.mu = state.mu_f32
-        c.capacity = state.particle_capacity
-        c.p2g_mode = _lib.MPM_P2G_FIXED_POINT if atomic_p2g else _lib.MPM_P2G_GATHER
-        c.fixed_point_shift = fixed_point_shift
-        c.device = device
+        c = native_config(state, atomic_p2g, fixed_point_shift, device)
         handle = ctypes.c_void_p()
         packed = np.ascontiguousarray(state.packed_particles, dtype=np.float32)
         ids = np.ascontiguousarray(state.packed_object_ids, dtype=np.uint32)
