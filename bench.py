@@ -225,6 +225,155 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+BATCHED_MAX_MICROSTEPS = 4096
+PLAIN_SAMPLE_SCENES = 16
+
+
+def _batched_bound(velocity, macro_dt, gravity):
+    from mpm_b200.cfl_bounds import calculate_mpm_cfl_velocity_bound
+    return calculate_mpm_cfl_velocity_bound(velocity, macro_dt, math.hypot(gravity["x"], gravity["y"]), 0, 0, 0, 0)
+
+
+def plain_per_scene(scenes, gravity, macro_dt, device):
+    """The plain form on the same scenes: each of the first
+    PLAIN_SAMPLE_SCENES scenes alone in its own solver (one macrostep of warm
+    up, then one timed macrostep through the same adaptive loop)."""
+    from mpm_b200 import calculate_mpm_cfl_microsteps, create_mpm_mls_gpu_solver
+    work = device_ms = 0.0
+    for particles, config in scenes[:PLAIN_SAMPLE_SCENES]:
+        solver = create_mpm_mls_gpu_solver(particles, config, device=device)
+        try:
+            velocity = solver.cfl_bounds["velocityBound"]
+            for timed in (False, True):
+                bound = max(_batched_bound(velocity, macro_dt, gravity), solver._last_scheduled_velocity_bound or 0.0)
+                plan = calculate_mpm_cfl_microsteps(macro_dt, config["grid"]["cellSize"],
+                                                    solver.cfl_bounds["waveSpeedBound"], bound, BATCHED_MAX_MICROSTEPS)
+                solver.device_ms_total = 0.0
+                solver.committed_microsteps_total = 0
+                m = solver.step_cfl_batch_adaptive(1, macro_dt, plan, bound, BATCHED_MAX_MICROSTEPS, gravity)
+                velocity = m["recommendedVelocityBound"]
+            work += len(particles) * solver.committed_microsteps_total
+            device_ms += solver.device_ms_total
+        finally:
+            solver.dispose()
+    return work / (device_ms * 1e-3)
+
+
+def run_b200_batched(args):
+    """The batched form: 512 independent SI Tait water tanks in one solver, one
+    step = one 1/240 s macrostep of every scene through the per-scene
+    adaptive CFL loop (MpmBatchedGpuSolver.step_cfl_batch_adaptive)."""
+    rank, local_rank, world = _rank_info()
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local_rank)
+    from mpm_b200 import create_mpm_batched_gpu_solver
+    from mpm_b200.scenes import BATCHED_TANK_GRAVITY, create_batched_tank_scenes
+    scenes = create_batched_tank_scenes()
+    gravity = BATCHED_TANK_GRAVITY
+    macro_dt = MACRO_DT
+    batch = create_mpm_batched_gpu_solver(scenes, device=local_rank)
+    n_total = int(batch.particle_counts.sum())
+    velocity = [b["velocityBound"] for b in batch.cfl_bounds]
+
+    def one_step():
+        nonlocal velocity
+        bounds = [_batched_bound(v, macro_dt, gravity) for v in velocity]
+        results = batch.step_cfl_batch_adaptive(macro_dt, bounds, BATCHED_MAX_MICROSTEPS, gravity)
+        velocity = [r["recommendedVelocityBound"] for r in results]
+        return results
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    batch.device_ms_total = 0.0
+    batch.committed_particle_substeps = 0
+    wall = 0.0
+    submits = retries = 0
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        results = one_step()
+        wall += time.perf_counter() - t0
+        submits += 1 + max(r["retryCount"] for r in results)
+        retries += sum(r["retryCount"] for r in results)
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    work = batch.committed_particle_substeps
+    times = torch.tensor([batch.device_ms_total / 1e3, wall], dtype=torch.float64, device=f"cuda:{local_rank}")
+    if dist:
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    device_s, wall = float(times[0]), float(times[1])
+    value = world * work / device_s
+    e2e_value = world * work / wall
+
+    # kernel-by-kernel timing of real substeps of every scene at the smallest
+    # microstep dt of the batch, right after the timed region
+    from mpm_b200 import calculate_mpm_cfl_microsteps
+    dt = min(calculate_mpm_cfl_microsteps(macro_dt, c["grid"]["cellSize"], b["waveSpeedBound"],
+                                          _batched_bound(v, macro_dt, gravity), BATCHED_MAX_MICROSTEPS)["microDt"]
+             for (_, c), b, v in zip(scenes, batch.cfl_bounds, velocity))
+    prof_steps = 8
+    prof = batch.profile_substeps(prof_steps, dt, gravity)
+    active = batch.count_active_nodes()
+    total_ms = sum(ms for ms, _ in prof.values())
+    dominant = max(prof, key=lambda k: prof[k][0])
+    dom_ms, dom_launches = prof[dominant]
+    dom_bytes = kernel_bytes(dominant, n_total, active)
+    peak, peak_kind = _peaks()
+    achieved = dom_bytes / (dom_ms / dom_launches * 1e-3) / 1e9
+    substep_bytes = n_total * 104.0 + float(sum(active)) * 64.0
+    substep_ms = total_ms / prof_steps
+    launches_per_substep = sum(l for _, l in prof.values()) / prof_steps
+    plain = plain_per_scene(scenes, gravity, macro_dt, local_rank) if rank == 0 else None
+    counts = batch.particle_counts
+    sides = [c["grid"]["cellsX"] for _, c in scenes]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": device_s * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes, no dataset)",
+        "config": {"workload": "batched: 512 independent SI Tait water tanks (0.2 m box, rho 1000, gamma 7, "
+                               "c 20 m/s), N log-uniform in 1k-64k, S x S grids with S uniform in 64-512, "
+                               "macrostep 1/240 s, per-scene adaptive CFL 0.3",
+                   "scenes": len(scenes), "particles": n_total, "particles_range": [int(counts.min()),
+                                                                                   int(counts.max())],
+                   "grid_sides_range": [min(sides), max(sides)], "macro_dt": macro_dt, "courant": 0.3,
+                   "p2g": "gather", "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (every scene's state, about 0.8 GB)",
+                   "committed_particle_substeps": work, "submits": submits, "retries": retries,
+                   "plain_per_scene": {"value": plain, "unit": UNIT,
+                                       "sample": f"the first {PLAIN_SAMPLE_SCENES} scenes, each alone in its own "
+                                                 "solver, one timed macrostep each"}},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": submits * len(scenes) * 160 // args.steps,
+                "d2h_bytes_per_step": submits * len(scenes) * 256 // args.steps,
+                "path": "Python host MpmBatchedGpuSolver.step_cfl_batch_adaptive -> C ABI"},
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": dram_traffic(dominant + "@batched"),
+                     "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": dom_ms / dom_launches,
+                     "kernel_share": dom_ms / total_ms,
+                     "substep": {"algorithmic_bytes": substep_bytes, "ms": substep_ms,
+                                 "achieved_gbs": substep_bytes / (substep_ms * 1e-3) / 1e9,
+                                 "frac": substep_bytes / (substep_ms * 1e-3) / 1e9 / peak},
+                     "active_channel_nodes": list(active),
+                     "kernels_ms_per_substep": {k: v[0] / prof_steps for k, v in prof.items()}},
+        "clocks": clock_info,
+        "gpu_launches": int(round(launches_per_substep * (work / max(1, n_total)))) if n_total else 0,
+    }
+    batch.dispose()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_b200(args):
     rank, local_rank, world = _rank_info()
     import torch
@@ -344,7 +493,7 @@ def main():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", default="dam-break-1m", choices=["dam-break-1m", "si-tank"])
+    ap.add_argument("--workload", default="dam-break-1m", choices=["dam-break-1m", "si-tank", "batched-512"])
     ap.add_argument("--p2g", choices=["gather", "fixed"], default="gather")
     ap.add_argument("--fixed-shift", type=int, default=16)
     ap.add_argument("--cpu-substeps", type=int, default=12)
@@ -355,6 +504,8 @@ def main():
         raise SystemExit("--warmup must be at least 3")
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batched-512":
+        run_b200_batched(args)
     else:
         run_b200(args)
 

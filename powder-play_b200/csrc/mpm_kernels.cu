@@ -870,12 +870,12 @@ struct Stage {
     float2 momentum[STAGE_CAP];  // m v
     uint32_t orig[STAGE_CAP];
     uint32_t cell[STAGE_CAP];    // local cell | channel << 8 | REC_FAILED
-    uint16_t order[STAGE_CAP];   // arrival rank within the cell
+    uint16_t order[STAGE_CAP];   // arrival rank within the cell, then rank by (channel, original index)
     uint16_t sorted[STAGE_CAP];  // staged indices grouped by cell
     uint32_t count[TILE_CELLS];
     uint32_t start[TILE_CELLS + 1];
     float acc[ACC_WORDS][RING_NODES];
-    uint32_t rows[TILE_Y];
+    uint32_t cells[TILE_CELLS];  // particles per cell of a crowded tile
     uint32_t staged;
     uint32_t mask;
     int failed;
@@ -886,8 +886,8 @@ __device__ __forceinline__ uint32_t sort_key(const Stage &sm, uint32_t k)
     return (((sm.cell[k] >> 8) & 3u) << 30) | sm.orig[k];
 }
 
-// Stages the records of bucket entries [i0, i1) whose local cell row lies in
-// [r0, r1) (all of them when `filtered` is false) with asynchronous copies,
+// Stages the records of bucket entries [i0, i1) whose local cell lies in
+// [q0, q1) (all of them when `filtered` is false) with asynchronous copies,
 // raises the status of failed records and groups the entries by cell.  Then
 // the thread of each cell sums the P2G contributions of its particles of
 // one channel, in original-index order, over the 3x3 stencil nodes in
@@ -896,7 +896,7 @@ __device__ __forceinline__ uint32_t sort_key(const Stage &sm, uint32_t k)
 // node), so every sum has a fixed order.  Returns false once a record had
 // failed.
 __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, uint32_t begin, uint32_t i0, uint32_t i1,
-                                          uint32_t r0, uint32_t r1, bool filtered)
+                                          uint32_t q0, uint32_t q1, bool filtered)
 {
     const StepParams &P = *c.P;
     const uint32_t me = threadIdx.x;  // this thread's cell
@@ -907,8 +907,8 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, uint32_t begi
         const uint32_t s = c.perm[begin + i];
         uint32_t k = i - i0;
         if (filtered) {
-            const uint32_t row = (c.rec_cell[s] & 0xffu) / TILE_X;
-            if (row < r0 || row >= r1) continue;
+            const uint32_t cell = c.rec_cell[s] & 0xffu;
+            if (cell < q0 || cell >= q1) continue;
             k = atomicAdd(&sm.staged, 1u);
         }
         cp_async<16>(&sm.state[k], &c.rec_state[s]);
@@ -959,18 +959,19 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, uint32_t begi
     __syncthreads();
     for (uint32_t k = me; k < n; k += TILE_CELLS) sm.sorted[sm.start[sm.cell[k] & 0xffu] + sm.order[k]] = (uint16_t)k;
     __syncthreads();
-    // each cell orders its own entries by (channel, original index)
-    const uint32_t lo = sm.start[me], hi = sm.start[me + 1];
-    for (uint32_t j = lo + 1; j < hi; ++j) {
-        const uint16_t v = sm.sorted[j];
-        const uint32_t key = sort_key(sm, v);
-        uint32_t q = j;
-        while (q > lo && sort_key(sm, sm.sorted[q - 1]) > key) {
-            sm.sorted[q] = sm.sorted[q - 1];
-            --q;
-        }
-        sm.sorted[q] = v;
+    // order each cell's entries by (channel, original index): every entry
+    // counts the entries of its cell with a smaller key (keys are distinct),
+    // so crowded cells spread over all threads
+    for (uint32_t k = me; k < n; k += TILE_CELLS) {
+        const uint32_t cell = sm.cell[k] & 0xffu, key = sort_key(sm, k);
+        uint32_t rank = 0;
+        for (uint32_t j = sm.start[cell]; j < sm.start[cell + 1]; ++j) rank += sort_key(sm, sm.sorted[j]) < key;
+        sm.order[k] = (uint16_t)rank;
     }
+    __syncthreads();
+    for (uint32_t k = me; k < n; k += TILE_CELLS) sm.sorted[sm.start[sm.cell[k] & 0xffu] + sm.order[k]] = (uint16_t)k;
+    __syncthreads();
+    const uint32_t lo = sm.start[me], hi = sm.start[me + 1];
     const int cx = (int)(me % TILE_X), cy = (int)(me / TILE_X);
     const float dx = P.dx;
     const uint32_t tile_mask = sm.mask;
@@ -1038,9 +1039,9 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, uint32_t begi
 // order (cell-major phases, original particle index within a cell), so
 // they do not depend on the order of the tile buckets and every run is
 // bit-identical.  A tile with more than STAGE_CAP particles is taken in
-// chunks of whole cell rows (rows holding more than STAGE_CAP particles in
-// chunks of the bucket, whose order then decides the rounding of their
-// sums).  The sums go to the tile's own ring record; k_g2p_tile adds
+// chunks of consecutive whole cells (a cell holding more than STAGE_CAP
+// particles in chunks of the bucket, whose order then decides the rounding
+// of its sums).  The sums go to the tile's own ring record; k_g2p_tile adds
 // the up to four records that cover a node.
 template <bool SCENES>
 __global__ void __launch_bounds__(TILE_CELLS) k_p2g_gather(Ctx c0)
@@ -1061,38 +1062,39 @@ __global__ void __launch_bounds__(TILE_CELLS) k_p2g_gather(Ctx c0)
         __syncthreads();
         if (sm.failed) continue;  // the scene's substep is rolled back
         if (n_tile > (uint32_t)STAGE_CAP) {
-            if (threadIdx.x < TILE_Y) sm.rows[threadIdx.x] = 0u;
+            sm.cells[threadIdx.x] = 0u;  // one thread per cell
             __syncthreads();
             for (uint32_t i = threadIdx.x; i < n_tile; i += TILE_CELLS)
-                atomicAdd(&sm.rows[(c.rec_cell[c.perm[begin + i]] & 0xffu) / TILE_X], 1u);
+                atomicAdd(&sm.cells[c.rec_cell[c.perm[begin + i]] & 0xffu], 1u);
             __syncthreads();
         }
-        // chunks: the whole tile; or runs of whole cell rows holding at most
-        // STAGE_CAP particles, a row holding more taken in bucket chunks
+        // chunks: the whole tile; or runs of consecutive whole cells holding
+        // at most STAGE_CAP particles, a cell holding more taken in bucket
+        // chunks
         bool ok = true;
-        uint32_t r = 0, i0 = 0;
-        while (ok && r < (uint32_t)TILE_Y) {
-            uint32_t r1 = TILE_Y, i1 = n_tile;
+        uint32_t q = 0, i0 = 0;
+        while (ok && q < (uint32_t)TILE_CELLS) {
+            uint32_t q1 = TILE_CELLS, i1 = n_tile;
             bool filtered = false;
             if (n_tile > (uint32_t)STAGE_CAP) {
                 filtered = true;
-                if (sm.rows[r] > (uint32_t)STAGE_CAP) {
-                    r1 = r + 1;
+                if (sm.cells[q] > (uint32_t)STAGE_CAP) {
+                    q1 = q + 1;
                     i1 = min(i0 + (uint32_t)STAGE_CAP, n_tile);
                 } else {
                     uint32_t held = 0;
-                    r1 = r;
-                    while (r1 < (uint32_t)TILE_Y && sm.rows[r1] <= (uint32_t)STAGE_CAP &&
-                           held + sm.rows[r1] <= (uint32_t)STAGE_CAP)
-                        held += sm.rows[r1++];
+                    q1 = q;
+                    while (q1 < (uint32_t)TILE_CELLS && sm.cells[q1] <= (uint32_t)STAGE_CAP &&
+                           held + sm.cells[q1] <= (uint32_t)STAGE_CAP)
+                        held += sm.cells[q1++];
                     i0 = 0;
                 }
             }
-            ok = p2g_chunk(c, sm, begin, i0, i1, r, r1, filtered);
-            if (filtered && r1 == r + 1 && i1 < n_tile && sm.rows[r] > (uint32_t)STAGE_CAP) {
-                i0 = i1;  // next bucket chunk of the same crowded row
+            ok = p2g_chunk(c, sm, begin, i0, i1, q, q1, filtered);
+            if (filtered && q1 == q + 1 && i1 < n_tile && sm.cells[q] > (uint32_t)STAGE_CAP) {
+                i0 = i1;  // next bucket chunk of the same crowded cell
             } else {
-                r = r1;
+                q = q1;
                 i0 = 0;
             }
         }

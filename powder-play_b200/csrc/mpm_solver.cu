@@ -1128,12 +1128,18 @@ int mpm_count_active_nodes(mpm_solver *s, uint32_t counts[3])
     if (!s || !counts) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and counts must not be NULL");
     CUDA_TRY(cudaSetDevice(s->device));
     if (s->gather()) {
-        // accumulated by k_p2g_grid since the last batch began: average per substep
-        CUDA_TRY(cudaMemcpyAsync(s->h_readback, s->d_counters + COUNTER_ACTIVE, 3 * sizeof(uint32_t),
-                                 cudaMemcpyDeviceToHost, s->stream));
+        // accumulated by k_g2p_tile since the last batch began, summed over
+        // the scenes: average per substep of the batch
+        std::vector<uint32_t> dyn((size_t)s->n_scenes * SCENE_WORDS);
+        CUDA_TRY(cudaMemcpyAsync(dyn.data(), s->dyn, dyn.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                 s->stream));
         CUDA_TRY(cudaStreamSynchronize(s->stream));
-        const uint32_t steps = std::max(1u, s->substeps_since_begin);
-        for (int k = 0; k < 3; ++k) counts[k] = s->h_readback[k] / steps;
+        const uint64_t steps = std::max(1u, s->substeps_since_begin);
+        for (int k = 0; k < 3; ++k) {
+            uint64_t sum = 0;
+            for (uint32_t sc = 0; sc < s->n_scenes; ++sc) sum += dyn[(size_t)sc * SCENE_WORDS + 32 + COUNTER_ACTIVE + k];
+            counts[k] = (uint32_t)(sum / steps);
+        }
         return MPM_OK;
     }
     CUDA_TRY(cudaMemsetAsync(s->d_active, 0, 4 * sizeof(uint32_t), s->stream));

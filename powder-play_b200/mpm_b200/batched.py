@@ -263,6 +263,27 @@ class MpmBatchedGpuSolver:
                  "committedMicroStepCount": sc["committed"], "attemptedMicroStepCount": sc["consumed"],
                  "retryCount": sc["retries"], "remainingDuration": sc["remaining"]} for sc in scenes]
 
+    def profile_substeps(self, step_count: int, dt: float, gravity: dict) -> dict:
+        """Runs `step_count` real substeps of `dt` in every scene, kernel by
+        kernel with CUDA events between them: {kernel name: (milliseconds,
+        launches)}."""
+        self._assert_active()
+        slots = int(self._lib.mpm_profile_kernel_slots())
+        ms = np.zeros(slots, dtype=np.float64)
+        launches = np.zeros(slots, dtype=np.uint32)
+        _check(self._lib.mpm_profile_substeps(self._handle, step_count, fround(dt), fround(gravity["x"]),
+                                              fround(gravity["y"]), None, _lib.ptr(ms), _lib.ptr(launches)),
+               "profiled substeps failed")
+        return {self._lib.mpm_profile_kernel_name(k).decode(): (float(ms[k]), int(launches[k]))
+                for k in range(slots) if launches[k]}
+
+    def count_active_nodes(self):
+        """Active solid / water / oil nodes per substep of the last batch,
+        summed over the scenes."""
+        counts = np.zeros(3, dtype=np.uint32)
+        _check(self._lib.mpm_count_active_nodes(self._handle, _lib.ptr(counts)), "active node count failed")
+        return tuple(int(c) for c in counts)
+
     # -------------------------------------------------------------- readback --
     def read_particles_packed(self, scene: int):
         """The packed 20-word records and object ids of one scene, in its own

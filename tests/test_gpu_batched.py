@@ -158,3 +158,25 @@ def test_a_batch_of_one_scene_matches_the_plain_solver():
         assert np.array_equal(_bits(got), _bits(want))
     finally:
         batch.dispose()
+
+
+def test_crowded_scenes_match_solo_runs_bit_for_bit():
+    # tens of particles per cell: tiles far above one shared-memory stage,
+    # taken in chunks of whole cells, still sum in a fixed order
+    scenes = create_batched_tank_scenes(3, seed=21, particles=(12_000, 20_000), sides=(20, 28))
+    batch = create_mpm_batched_gpu_solver(scenes)
+    try:
+        dts = [_micro_dt(batch.cfl_bounds[k], scenes[k][1], 0.5) for k in range(3)]
+        steps = [6, 4, 5]
+        batch.step_batch(steps, dts, BATCHED_TANK_GRAVITY)
+        assert all(e is None for e in batch.check_numerical_status())
+        for k, (particles, config) in enumerate(scenes):
+            per_cell = len(particles.px) / (config["grid"]["cellsX"] ** 2)
+            assert per_cell > 10
+            got, _ = batch.read_particles_packed(k)
+            want, status, _ = _solo_state(particles, config, [(steps[k], dts[k])])
+            assert status[0] == 0
+            assert np.array_equal(_bits(got), _bits(want)), f"scene {k} differs from its solo run"
+    finally:
+        batch.dispose()
+
