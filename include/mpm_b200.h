@@ -221,6 +221,50 @@ int mpmb_read_compact(mpm_solver *solver, float *maximum_speeds, uint32_t *compl
 /* Scenes of the handle (1 for a handle from mpm_create). */
 uint32_t mpmb_scene_count(const mpm_solver *solver);
 
+/* ---- differentiable form (adjoint) ---- */
+
+/* No counterpart in the reference, which has no gradients.  An engine over a
+ * batch of scenes of Tait water (model 2 with a Tait exponent) and
+ * fixed-corotated solid (model 5) particles, stepped with the default path's
+ * arithmetic for those models on dense per-scene grids at a fixed dt per
+ * scene, with the loss sum over particles of |x(T) - target|^2 per scene and
+ * its adjoint by checkpoint and recompute.  Particles come as the 20-word
+ * records of mpm_create, scene after scene; a scene's water particles share
+ * one material, as do its solid particles.  The differentiated parameters,
+ * 3 per scene: the water's Tait pressure coefficient (word 14 of a water
+ * record), the solid's lambda and mu (words 14 and 15 of a solid record).
+ * gravity_xy: 2 per scene. */
+typedef struct mpm_adjoint mpm_adjoint;
+int mpma_create(const mpm_config *configs, uint32_t scene_count, const uint32_t *particle_counts,
+                const float *packed_particles, const float *gravity_xy, mpm_adjoint **out);
+
+/* Replaces / reads the parameters (3 per scene, in the order above). */
+int mpma_set_parameters(mpm_adjoint *engine, const float *parameters);
+int mpma_get_parameters(mpm_adjoint *engine, float *parameters);
+
+/* Replaces the initial velocities (2 per particle). */
+int mpma_set_velocities(mpm_adjoint *engine, const float *velocities);
+
+/* Runs `substeps` substeps of dts[k] in scene k from the initial state,
+ * keeping the state at every `checkpoint_every`-th substep, and returns the
+ * loss per scene against `targets` (2 per particle).  Blocks. */
+int mpma_forward(mpm_adjoint *engine, uint32_t substeps, const float *dts, uint32_t checkpoint_every,
+                 const float *targets, double *loss);
+
+/* The gradients of the last forward pass's total loss with respect to the
+ * initial velocities (2 per particle) and the parameters (3 per scene): each
+ * segment of checkpoint_every substeps is recomputed from its checkpoint and
+ * then reversed substep by substep.  Either output may be NULL.  Blocks. */
+int mpma_backward(mpm_adjoint *engine, float *grad_velocities, double *grad_parameters);
+
+/* Final positions of the last forward pass (2 per particle). */
+int mpma_read_positions(mpm_adjoint *engine, float *positions);
+
+/* Device milliseconds of the last forward and backward passes. */
+int mpma_last_ms(mpm_adjoint *engine, double *forward_ms, double *backward_ms);
+
+void mpma_destroy(mpm_adjoint *engine);
+
 /* ---- allocation-free cell sort ---- */
 
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc

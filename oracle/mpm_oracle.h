@@ -118,6 +118,23 @@ int orc_triangle_field(const orc_material *mats, int32_t n_mats, const orc_confi
                        const orc_particle *particles, int32_t n, double *sd, int32_t *body, double *normal,
                        double *bary, char *err, int32_t err_len);
 
+/* The differentiable form in FP64 (adjoint_fp64.c): one scene of Tait water
+ * (liquid[i] = 1) and fixed-corotated solid particles. */
+typedef struct orc_adj_scene {
+    int32_t cells_x, cells_y;
+    double dx, dt, gx, gy, solid_mass, wall_friction;
+    double rho, gamma, tait, lambda_s, mu_s;
+} orc_adj_scene;
+
+/* `steps` substeps from (x0, v0, C0, F0) (2, 2, 4, 4 per particle), the loss
+ * sum |x(T) - target|^2, and its gradients with respect to the initial
+ * velocities (2 per particle) and (tait, lambda_s, mu_s).  x_out (may be NULL)
+ * receives x(T).  Returns 0, -1 when a particle leaves the grid or a value
+ * turns non-finite, -2 when memory runs out. */
+int orc_adjoint_run(const orc_adj_scene *scene, int32_t n, const double *x0, const double *v0, const double *C0,
+                    const double *F0, const double *vol, const int32_t *liquid, const double *target, int32_t steps,
+                    double *loss, double *grad_v0, double *grad_params, double *x_out);
+
 /* Sizes of the structs, so a binding can check its layout. */
 int32_t orc_sizeof_particle(void);
 int32_t orc_sizeof_material(void);

@@ -53,6 +53,12 @@ class OrcDiag(ctypes.Structure):
         "output_my")]
 
 
+class OrcAdjScene(ctypes.Structure):
+    _fields_ = [("cells_x", ctypes.c_int32), ("cells_y", ctypes.c_int32)] + [
+        (k, ctypes.c_double) for k in ("dx", "dt", "gx", "gy", "solid_mass", "wall_friction", "rho", "gamma", "tait",
+                                       "lambda_s", "mu_s")]
+
+
 class OracleError(ValueError):
     """A RangeError/TypeError raised by the restated reference step."""
 
@@ -84,6 +90,8 @@ def load() -> ctypes.CDLL:
     lib.orc_triangle_field.restype = ctypes.c_int
     lib.emu_fixed_point_scatter.argtypes = [ctypes.c_int32] + [vp] * 7 + [ctypes.c_float] * 3 + [ctypes.c_int32] * 3 + [vp]
     lib.emu_fixed_point_scatter.restype = ctypes.c_uint32
+    lib.orc_adjoint_run.argtypes = [ctypes.POINTER(OrcAdjScene), ctypes.c_int32] + [vp] * 7 + [ctypes.c_int32] + [vp] * 4
+    lib.orc_adjoint_run.restype = ctypes.c_int
     for name in ("orc_sizeof_particle", "orc_sizeof_material", "orc_sizeof_bond", "orc_sizeof_config"):
         getattr(lib, name).restype = ctypes.c_int32
     assert lib.orc_sizeof_particle() == PARTICLE_DTYPE.itemsize
@@ -247,3 +255,26 @@ def packed_state(packed: np.ndarray) -> dict:
 
 def js_hypot(x, y):
     return math.hypot(x, y)
+
+
+def adjoint_fp64(scene: dict, x0, v0, C0, F0, vol, liquid, target, steps: int):
+    """The FP64 adjoint of the differentiable form (oracle/adjoint_fp64.c) for
+    one scene: returns (loss, gradient wrt v0 (n, 2), gradient wrt (tait,
+    lambda_s, mu_s), x(T) (n, 2))."""
+    lib = load()
+    s = OrcAdjScene(**scene)
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)  # noqa: E731
+    x0, v0, C0, F0, vol, target = map(f64, (x0, v0, C0, F0, vol, target))
+    liquid = np.ascontiguousarray(liquid, dtype=np.int32)
+    n = len(vol)
+    loss = ctypes.c_double()
+    gv = np.zeros((n, 2), dtype=np.float64)
+    gp = np.zeros(3, dtype=np.float64)
+    xt = np.zeros((n, 2), dtype=np.float64)
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    rc = lib.orc_adjoint_run(ctypes.byref(s), n, p(x0), p(v0), p(C0), p(F0), p(vol), p(liquid), p(target), steps,
+                             ctypes.byref(loss), p(gv), p(gp), p(xt))
+    if rc != 0:
+        raise OracleError(f"the FP64 adjoint stopped ({rc})")
+    return loss.value, gv, gp, xt
+

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUTPUT = os.path.join(HERE, "libmpm_b200.so")
-SOURCES = ["mpm_kernels.cu", "mpm_solver.cu", "mpm_static_sort.cu"]
+SOURCES = ["mpm_kernels.cu", "mpm_solver.cu", "mpm_static_sort.cu", "mpm_adjoint.cu"]
 HEADERS = ["mpm_device.cuh", "mpm_kernels.cuh"]
 
 NVCC_FLAGS = [

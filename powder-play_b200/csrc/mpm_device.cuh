@@ -222,6 +222,10 @@ __device__ __forceinline__ float wall_friction(float vel, int coord, int extent,
     return vel * (1.0f - friction * influence);
 }
 
+// pow as WGSL specifies it: its accuracy is inherited from
+// exp2(y * log2(x)), so the reference's Tait terms are that expression.
+__device__ __forceinline__ float pow_wgsl(float x, float y) { return exp2f(y * log2f(x)); }
+
 __device__ __forceinline__ float length2(float2 v)
 {
     return __fsqrt_rn(__fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y)));

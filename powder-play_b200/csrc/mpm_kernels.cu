@@ -83,9 +83,6 @@ __device__ __forceinline__ bool make_stencil_fast(const StepParams &P, float2 po
     return stencil_from_grid(__fmul_rn(pos.x, P.inv_dx), __fmul_rn(pos.y, P.inv_dx), s);
 }
 
-// pow as WGSL specifies it: its accuracy is inherited from
-// exp2(y * log2(x)), so the reference's Tait terms are that expression.
-__device__ __forceinline__ float pow_wgsl(float x, float y) { return exp2f(y * log2f(x)); }
 
 // prepareParticle: shaders.ts:808-963.  Computes the per-particle stress
 // cache (affine momentum A = m C + (-dt V 4/dx^2) P F^T), mass and current

@@ -924,6 +924,19 @@ int run_batch(mpm_solver *s, uint32_t step_count, bool guarded);
 
 }  // namespace
 
+namespace mpm {
+
+// The last-error channel of the library for its other host sources.
+int host_error(int code, const char *message)
+{
+    g_last_error = message;
+    return code;
+}
+
+void host_clear_error() { g_last_error.clear(); }
+
+}  // namespace mpm
+
 extern "C" {
 
 int mpm_create(const mpm_config *config, const float *packed_particles, const uint32_t *object_ids,

@@ -25,6 +25,8 @@ EXPORTED_SYMBOLS = (
     "mpm_probe_fixed_point", "mpm_probe_triangle_field", "mpm_node_count", "mpm_last_batch_device_ms", "mpm_profile_substeps",
     "mpm_profile_kernel_name", "mpm_profile_kernel_slots", "mpm_count_active_nodes", "mpm_stream",
     "mpmb_create", "mpmb_step_batch", "mpmb_read_compact", "mpmb_scene_count",
+    "mpma_create", "mpma_set_parameters", "mpma_get_parameters", "mpma_set_velocities", "mpma_forward",
+    "mpma_backward", "mpma_read_positions", "mpma_last_ms", "mpma_destroy",
 )
 
 
@@ -116,6 +118,19 @@ def load_library(path: str = LIBRARY_PATH) -> ctypes.CDLL:
     lib.mpmb_read_compact.restype = i32
     lib.mpmb_scene_count.argtypes = [vp]
     lib.mpmb_scene_count.restype = u32
+    lib.mpma_create.argtypes = [vp, u32, vp, vp, vp, P(vp)]
+    lib.mpma_create.restype = i32
+    for name in ("mpma_set_parameters", "mpma_get_parameters", "mpma_set_velocities", "mpma_read_positions"):
+        getattr(lib, name).argtypes = [vp, vp]
+        getattr(lib, name).restype = i32
+    lib.mpma_forward.argtypes = [vp, u32, vp, u32, vp, vp]
+    lib.mpma_forward.restype = i32
+    lib.mpma_backward.argtypes = [vp, vp, vp]
+    lib.mpma_backward.restype = i32
+    lib.mpma_last_ms.argtypes = [vp, P(ctypes.c_double), P(ctypes.c_double)]
+    lib.mpma_last_ms.restype = i32
+    lib.mpma_destroy.argtypes = [vp]
+    lib.mpma_destroy.restype = None
     _lib = lib
     return lib
 

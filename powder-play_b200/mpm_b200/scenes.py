@@ -11,6 +11,9 @@
   break on a 1024x2048 grid (cellSize 10, gravity 90, Gate-4 liquids).
 * `create_batched_tank_scenes` -- independent SI Tait water tanks of uneven
   particle counts and grids for the batched solver.
+* `create_adjoint_scenes` -- water + fixed-corotated solid scenes, their
+  initial velocities and target displacement fields for the differentiable
+  form.
 
 All seeded randomness uses the reference's LCG (gate4.ts:134-144) so that a
 seed names the same scene in every language.
@@ -358,3 +361,78 @@ def create_batched_tank_scenes(count: int = 512, seed: int = 0x4D504D42, particl
                   "wallFriction": 1.0}
         out.append((p, config))
     return out
+
+
+# ------------------------------------------------------- adjoint scenes --
+
+ADJOINT_GRAVITY = {"x": 0.0, "y": 90.0}
+ADJOINT_TAIT_WATER = {"lambda": 22_857.0, "mu": 0.0, "model": "water", "density": 0.02,
+                      "equationOfState": {"model": "tait", "exponent": 7.0}}
+ADJOINT_SOLID = {"lambda": 20.0, "mu": 10.0, "model": "fixed-corotated"}
+
+
+def _normal_pairs(rnd: SeededRandom, count: int) -> np.ndarray:
+    """`count` standard normal draws by Box-Muller over the seeded LCG."""
+    u = lcg_sequence(rnd.state, 2 * ((count + 1) // 2))
+    u1 = np.maximum(u[0::2], 1e-12)
+    r = np.sqrt(-2.0 * np.log(u1))
+    z = np.concatenate([r * np.cos(2 * np.pi * u[1::2]), r * np.sin(2 * np.pi * u[1::2])])
+    return z[:count]
+
+
+def create_adjoint_scenes(count: int = 64, seed: int = 0x4D504D41, water_columns: int = 96, water_rows: int = 128,
+                          solid_side: int = 64, cells: int = 256, velocity_sigma: float = 10.0,
+                          target_amplitude: float = 20.0):
+    """`count` scenes for the differentiable form, in Gate-4 world units
+    (cellSize 10, gravity 90 along +y): a block of water_columns x water_rows
+    Tait water particles (density 0.02, gamma 7, pressure coefficient
+    22,857: the linear EOS's 2,828 sound speed) and a block of solid_side^2
+    fixed-corotated solid particles (lambda 20, mu 10, density 0.02), both at
+    2 x 2 particles per cell (spacing 5, area 25), on a cells x cells grid.
+    Scene k draws from the LCG seeded with (seed + k * 0x9E3779B9) mod 2^32:
+    the blocks' places, initial velocities N(0, velocity_sigma^2) per
+    component, and a target displacement field d(x) = A (sin(2 pi k1 x / L +
+    p1), cos(2 pi k2 y / L + p2)) with A = target_amplitude.  Returns
+    [(particles, config, targets (n, 2))]; the defaults give 64 scenes of
+    12,288 + 4,096 particles on 256 x 256 grids."""
+    dx, spacing = 10.0, 5.0
+    size = cells * dx
+    area = spacing * spacing
+    out = []
+    for k in range(count):
+        rnd = SeededRandom((seed + k * 0x9E3779B9) % UINT32_RANGE)
+        ww, wh = water_columns * spacing, water_rows * spacing
+        sw = solid_side * spacing
+        margin = 4 * dx
+        wx0 = margin + rnd() * (size / 2 - ww - 2 * margin)
+        wy0 = margin + rnd() * (size - wh - 2 * margin)
+        sx0 = size / 2 + margin + rnd() * (size / 2 - sw - 2 * margin)
+        sy0 = margin + rnd() * (size - sw - 2 * margin)
+        nw, ns = water_columns * water_rows, solid_side * solid_side
+        n = nw + ns
+        p = ParticleArrays.empty(n)
+        r, c = np.divmod(np.arange(nw), water_columns)
+        p.px[:nw] = wx0 + (c + 0.5) * spacing
+        p.py[:nw] = wy0 + (r + 0.5) * spacing
+        r, c = np.divmod(np.arange(ns), solid_side)
+        p.px[nw:] = sx0 + (c + 0.5) * spacing
+        p.py[nw:] = sy0 + (r + 0.5) * spacing
+        z = _normal_pairs(rnd, 2 * n) * velocity_sigma
+        rnd.state = (rnd.state * 1_664_525 + 1_013_904_223) & 0xFFFFFFFF  # past the normal draws
+        p.vx[:] = z[:n]
+        p.vy[:] = z[n:]
+        p.volume[:] = area
+        p.materials = [ADJOINT_TAIT_WATER, ADJOINT_SOLID]
+        p.material[:nw] = 0
+        p.material[nw:] = 1
+        p.object_id[:nw] = 1
+        p.object_id[nw:] = 2
+        k1, k2 = 1 + int(rnd() * 3), 1 + int(rnd() * 3)
+        p1, p2 = 2 * np.pi * rnd(), 2 * np.pi * rnd()
+        targets = np.stack([p.px + target_amplitude * np.sin(2 * np.pi * k1 * p.px / size + p1),
+                            p.py + target_amplitude * np.cos(2 * np.pi * k2 * p.py / size + p2)], axis=1)
+        config = {"grid": {"cellsX": cells, "cellsY": cells, "cellSize": dx}, "particleMass": 0.02 * area,
+                  "particleVolume": area, "material": ADJOINT_SOLID, "wallFriction": 0.0}
+        out.append((p, config, targets))
+    return out
+
