@@ -374,6 +374,116 @@ def run_b200_batched(args):
         print(json.dumps(line), flush=True)
 
 
+ADJOINT_SUBSTEPS = 200
+ADJOINT_CHECKPOINT_EVERY = 20
+# algorithmic bytes per particle and backward substep: the segment recompute
+# (P2G reads x, v, C, F: 48 B; G2P reads x, F: 24 B, writes x, v, C, F: 48 B),
+# the G2P adjoint (reads x, F and the output adjoint: 72 B, writes the G2P
+# parts: 24 B) and the fused grid + P2G adjoint (reads x, v, C, F and the G2P
+# parts: 72 B, writes the input adjoint: 48 B)
+ADJOINT_BYTES_PER_PARTICLE = 48 + 24 + 48 + 72 + 24 + 72 + 48
+
+
+def run_b200_adjoint(args):
+    """The differentiable form: 64 scenes of 12,288 Tait water + 4,096
+    fixed-corotated particles on 256x256 grids, 200 substeps at each scene's
+    fixed CFL dt, checkpoints every 20; one step = one forward pass (loss)
+    and one backward pass (gradients wrt initial velocities and the scenes'
+    Tait coefficient, lambda, mu)."""
+    rank, local_rank, world = _rank_info()
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local_rank)
+    from mpm_b200 import create_mpm_batched_gpu_solver
+    from mpm_b200.adjoint import create_mpm_adjoint_engine, fixed_cfl_dt
+    from mpm_b200.scenes import ADJOINT_GRAVITY, create_adjoint_scenes
+    scenes = create_adjoint_scenes()
+    gravity = ADJOINT_GRAVITY
+    steps = ADJOINT_SUBSTEPS
+    dts = []
+    for p, c, _ in scenes:
+        dt = fixed_cfl_dt(p, c, 90.0, 0.0)
+        dts.append(float(np.float32(fixed_cfl_dt(p, c, 90.0, steps * dt))))
+    targets = np.concatenate([t for _, _, t in scenes]).astype(np.float32)
+    engine = create_mpm_adjoint_engine([(p, c) for p, c, _ in scenes], gravity, device=local_rank)
+    n = int(engine.particle_counts.sum())
+
+    def one_step():
+        loss = engine.forward(steps, dts, targets, ADJOINT_CHECKPOINT_EVERY)
+        gv, gp = engine.backward()
+        return loss, gv, gp
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    fwd = bwd = wall = 0.0
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        loss, gv, gp = one_step()
+        wall += time.perf_counter() - t0
+        f, b = engine.last_ms()
+        fwd += f
+        bwd += b
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    engine.dispose()
+    times = torch.tensor([fwd / 1e3, bwd / 1e3, wall], dtype=torch.float64, device=f"cuda:{local_rank}")
+    if dist:
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    fwd_s, bwd_s, wall = (float(v) for v in times)
+    # the default solver stepping the same scenes with the same dt
+    batch = create_mpm_batched_gpu_solver([(p, c) for p, c, _ in scenes], device=local_rank)
+    batch.step_batch([steps] * len(scenes), dts, gravity)
+    batch.last_batch_device_ms()
+    batch.step_batch([steps] * len(scenes), dts, gravity)
+    plain_ms = batch.last_batch_device_ms()
+    batch.dispose()
+    work = world * n * steps * args.steps
+    value = work / bwd_s
+    peak, peak_kind = _peaks()
+    achieved = ADJOINT_BYTES_PER_PARTICLE * n * steps * args.steps / bwd_s / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "particle-substeps/s (adjoint)", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": (fwd_s + bwd_s) * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded scenes, no dataset)",
+        "config": {"workload": "differentiable form: 64 scenes of 12,288 Tait water + 4,096 fixed-corotated "
+                               "(lambda 20, mu 10) particles on 256x256 grids (cellSize 10, gravity 90), initial "
+                               "velocities N(0, 10^2), 200 substeps at each scene's fixed CFL dt, checkpoints every "
+                               "20, loss sum |x(T) - target|^2 against a seeded displacement field",
+                   "scenes": len(scenes), "particles": n, "substeps": steps,
+                   "checkpoint_every": ADJOINT_CHECKPOINT_EVERY, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (1M particles' state and 64 grids of 67,081 nodes)",
+                   "adjoint_forward_ratio": bwd_s / fwd_s,
+                   "adjoint_over_default_forward": (bwd_s / args.steps) / (plain_ms * 1e-3),
+                   "forward_ms": fwd_s * 1e3 / args.steps, "backward_ms": bwd_s * 1e3 / args.steps,
+                   "default_solver_forward_ms": plain_ms},
+        "e2e": {"value": work / wall, "unit": "particle-substeps/s (forward + adjoint)",
+                "h2d_bytes_per_step": n * 8 + len(scenes) * 4,
+                "d2h_bytes_per_step": n * 8 + len(scenes) * (3 * 8 + 8),
+                "path": "Python host MpmAdjointEngine.forward + backward -> C ABI"},
+        "roofline": {"bound": "hbm", "kernel": "backward pass (segment recompute + G2P adjoint + grid/P2G adjoint)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_particle_substep": ADJOINT_BYTES_PER_PARTICLE},
+        "clocks": clock_info,
+        "gpu_launches": int(args.steps * (2 * steps + 4 * steps + 1)),
+    }
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_b200(args):
     rank, local_rank, world = _rank_info()
     import torch
@@ -493,7 +603,8 @@ def main():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", default="dam-break-1m", choices=["dam-break-1m", "si-tank", "batched-512"])
+    ap.add_argument("--workload", default="dam-break-1m",
+                    choices=["dam-break-1m", "si-tank", "batched-512", "adjoint-64"])
     ap.add_argument("--p2g", choices=["gather", "fixed"], default="gather")
     ap.add_argument("--fixed-shift", type=int, default=16)
     ap.add_argument("--cpu-substeps", type=int, default=12)
@@ -506,6 +617,8 @@ def main():
         run_reference(args)
     elif args.workload == "batched-512":
         run_b200_batched(args)
+    elif args.workload == "adjoint-64":
+        run_b200_adjoint(args)
     else:
         run_b200(args)
 

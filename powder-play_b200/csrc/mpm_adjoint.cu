@@ -399,24 +399,38 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_g2p(AdjCtx c)
     c.out.F[i] = Fn;
 }
 
-// Loss sum |x - target|^2 per scene and its adjoint seeds.
+// Loss sum |x - target|^2 per scene (one atomic per warp whose particles
+// share a scene) and its adjoint seeds.
 __global__ void __launch_bounds__(ADJ_THREADS) k_adj_loss(AdjCtx c)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.n) return;
-    const float2 x = c.in.x[i], t = c.target[i];
-    const float dx = x.x - t.x, dy = x.y - t.y;
-    atomicAdd(&c.loss[c.scene_of[i]], (double)dx * dx + (double)dy * dy);
-    c.xb_next[i] = make_float2(2.0f * dx, 2.0f * dy);
-    c.vb_next[i] = make_float2(0.f, 0.f);
-    c.Cb_next[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    c.Fb_next[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const bool valid = i < c.n;
+    const uint32_t scene = valid ? c.scene_of[i] : 0u;
+    double term = 0.0;
+    if (valid) {
+        const float2 x = c.in.x[i], t = c.target[i];
+        const float dx = x.x - t.x, dy = x.y - t.y;
+        term = (double)dx * dx + (double)dy * dy;
+        c.xb_next[i] = make_float2(2.0f * dx, 2.0f * dy);
+        c.vb_next[i] = make_float2(0.f, 0.f);
+        c.Cb_next[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        c.Fb_next[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    const unsigned full = 0xffffffffu;
+    const uint32_t lead = __shfl_sync(full, scene, 0);
+    if (__all_sync(full, !valid || scene == lead)) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) term += __shfl_xor_sync(full, term, o);
+        if ((threadIdx.x & 31u) == 0u) atomicAdd(&c.loss[lead], term);
+    } else if (valid) {
+        atomicAdd(&c.loss[scene], term);
+    }
 }
 
 // The G2P adjoint of one substep: from the adjoints of the substep's outputs
 // (x, v, C, F) to the node-velocity adjoints (scattered) and the G2P parts of
 // the input position and F adjoints.
-__global__ void __launch_bounds__(ADJ_THREADS) k_adj_g2p_bwd(AdjCtx c)
+__global__ void __launch_bounds__(ADJ_THREADS, 3) k_adj_g2p_bwd(AdjCtx c)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
@@ -547,7 +561,7 @@ __device__ __forceinline__ void add_param_grads(double *grad, uint32_t scene, fl
 // reversed), then reverses its own P2G contribution and stress; adds the G2P
 // parts; writes the adjoints of the substep's inputs and the parameter
 // gradients.
-__global__ void __launch_bounds__(ADJ_THREADS) k_adj_p2g_bwd(AdjCtx c)
+__global__ void __launch_bounds__(ADJ_THREADS, 3) k_adj_p2g_bwd(AdjCtx c)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = i < c.n;
