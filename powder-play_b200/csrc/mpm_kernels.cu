@@ -872,8 +872,7 @@ struct Stage {
     uint32_t count[TILE_CELLS];
     uint32_t start[TILE_CELLS + 1];
     float acc[ACC_WORDS][RING_NODES];
-    uint32_t cells[TILE_CELLS];  // particles per cell of a crowded tile
-    uint32_t staged;
+    uint32_t cells[TILE_CELLS + 1];  // a crowded tile: its cells' first entries in the cell-ordered list
     uint32_t mask;
     int failed;
 };
@@ -883,8 +882,7 @@ __device__ __forceinline__ uint32_t sort_key(const Stage &sm, uint32_t k)
     return (((sm.cell[k] >> 8) & 3u) << 30) | sm.orig[k];
 }
 
-// Stages the records of bucket entries [i0, i1) whose local cell lies in
-// [q0, q1) (all of them when `filtered` is false) with asynchronous copies,
+// Stages the records of the slots src[i0 .. i1) with asynchronous copies,
 // raises the status of failed records and groups the entries by cell.  Then
 // the thread of each cell sums the P2G contributions of its particles of
 // one channel, in original-index order, over the 3x3 stencil nodes in
@@ -892,22 +890,15 @@ __device__ __forceinline__ uint32_t sort_key(const Stage &sm, uint32_t k)
 // phases, one stencil offset per phase (no two cells of a phase share a
 // node), so every sum has a fixed order.  Returns false once a record had
 // failed.
-__device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, uint32_t begin, uint32_t i0, uint32_t i1,
-                                          uint32_t q0, uint32_t q1, bool filtered)
+__device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, const uint32_t *src, uint32_t i0, uint32_t i1)
 {
     const StepParams &P = *c.P;
     const uint32_t me = threadIdx.x;  // this thread's cell
     sm.count[me] = 0u;
-    if (me == 0) sm.staged = 0u;
     __syncthreads();
     for (uint32_t i = i0 + me; i < i1; i += TILE_CELLS) {
-        const uint32_t s = c.perm[begin + i];
-        uint32_t k = i - i0;
-        if (filtered) {
-            const uint32_t cell = c.rec_cell[s] & 0xffu;
-            if (cell < q0 || cell >= q1) continue;
-            k = atomicAdd(&sm.staged, 1u);
-        }
+        const uint32_t s = src[i];
+        const uint32_t k = i - i0;
         cp_async<16>(&sm.state[k], &c.rec_state[s]);
         cp_async<16>(&sm.affine[k], &c.rec_affine[s]);
         cp_async<8>(&sm.momentum[k], &c.rec_mom[s]);
@@ -916,7 +907,7 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, uint32_t begi
     }
     cp_async_wait_all();
     __syncthreads();
-    const uint32_t n = filtered ? sm.staged : i1 - i0;
+    const uint32_t n = i1 - i0;
     uint32_t mask = 0;
     for (uint32_t k = me; k < n; k += TILE_CELLS) {
         const uint32_t cell = sm.cell[k];
@@ -1058,38 +1049,81 @@ __global__ void __launch_bounds__(TILE_CELLS) k_p2g_gather(Ctx c0)
         }
         __syncthreads();
         if (sm.failed) continue;  // the scene's substep is rolled back
+        // a tile above one stage: its entries are first ordered by cell into
+        // the scratch list tmp[begin .. begin + n_tile) (arrival order within
+        // a cell), then taken in chunks of consecutive whole cells holding at
+        // most STAGE_CAP particles in all; a cell holding more is taken in
+        // chunks of its list, whose arrival order then decides the rounding
+        const uint32_t *src = c.perm + begin;
         if (n_tile > (uint32_t)STAGE_CAP) {
-            sm.cells[threadIdx.x] = 0u;  // one thread per cell
+            sm.count[threadIdx.x] = 0u;  // one thread per cell
             __syncthreads();
-            for (uint32_t i = threadIdx.x; i < n_tile; i += TILE_CELLS)
-                atomicAdd(&sm.cells[c.rec_cell[c.perm[begin + i]] & 0xffu], 1u);
+            for (uint32_t i = threadIdx.x; i < n_tile; i += 4 * TILE_CELLS) {
+                uint32_t s[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) s[u] = i + u * TILE_CELLS < n_tile ? src[i + u * TILE_CELLS] : 0xffffffffu;
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (s[u] != 0xffffffffu) atomicAdd(&sm.count[c.rec_cell[s[u]] & 0xffu], 1u);
+            }
             __syncthreads();
+            if (threadIdx.x < 32) {
+                const uint32_t me = threadIdx.x;
+                const uint32_t a = sm.count[4 * me], b = sm.count[4 * me + 1], d = sm.count[4 * me + 2],
+                               e = sm.count[4 * me + 3];
+                const uint32_t t = a + b + d + e;
+                uint32_t inc = t;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t up = __shfl_up_sync(0xffffffffu, inc, o);
+                    if (me >= (uint32_t)o) inc += up;
+                }
+                const uint32_t ex = inc - t;
+                sm.cells[4 * me] = ex;
+                sm.cells[4 * me + 1] = ex + a;
+                sm.cells[4 * me + 2] = ex + a + b;
+                sm.cells[4 * me + 3] = ex + a + b + d;
+                if (me == 31) sm.cells[TILE_CELLS] = inc;
+                // cursors for the placement below
+                sm.start[4 * me] = ex;
+                sm.start[4 * me + 1] = ex + a;
+                sm.start[4 * me + 2] = ex + a + b;
+                sm.start[4 * me + 3] = ex + a + b + d;
+            }
+            __syncthreads();
+            uint32_t *list = c.tmp + begin;
+            for (uint32_t i = threadIdx.x; i < n_tile; i += 4 * TILE_CELLS) {
+                uint32_t s[4], cell[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) s[u] = i + u * TILE_CELLS < n_tile ? src[i + u * TILE_CELLS] : 0xffffffffu;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) cell[u] = s[u] != 0xffffffffu ? c.rec_cell[s[u]] & 0xffu : 0u;
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (s[u] != 0xffffffffu) list[atomicAdd(&sm.start[cell[u]], 1u)] = s[u];
+            }
+            __syncthreads();  // the list is written (global, read back by this CTA)
+            src = list;
         }
-        // chunks: the whole tile; or runs of consecutive whole cells holding
-        // at most STAGE_CAP particles, a cell holding more taken in bucket
-        // chunks
         bool ok = true;
         uint32_t q = 0, i0 = 0;
         while (ok && q < (uint32_t)TILE_CELLS) {
-            uint32_t q1 = TILE_CELLS, i1 = n_tile;
-            bool filtered = false;
+            uint32_t q1 = TILE_CELLS, lo = 0, hi = n_tile;
             if (n_tile > (uint32_t)STAGE_CAP) {
-                filtered = true;
-                if (sm.cells[q] > (uint32_t)STAGE_CAP) {
+                if (sm.cells[q + 1] - sm.cells[q] > (uint32_t)STAGE_CAP) {
                     q1 = q + 1;
-                    i1 = min(i0 + (uint32_t)STAGE_CAP, n_tile);
+                    lo = sm.cells[q] + i0;
+                    hi = min(lo + (uint32_t)STAGE_CAP, sm.cells[q + 1]);
                 } else {
-                    uint32_t held = 0;
                     q1 = q;
-                    while (q1 < (uint32_t)TILE_CELLS && sm.cells[q1] <= (uint32_t)STAGE_CAP &&
-                           held + sm.cells[q1] <= (uint32_t)STAGE_CAP)
-                        held += sm.cells[q1++];
-                    i0 = 0;
+                    while (q1 < (uint32_t)TILE_CELLS && sm.cells[q1 + 1] - sm.cells[q] <= (uint32_t)STAGE_CAP) ++q1;
+                    lo = sm.cells[q];
+                    hi = sm.cells[q1];
                 }
             }
-            ok = p2g_chunk(c, sm, begin, i0, i1, q, q1, filtered);
-            if (filtered && q1 == q + 1 && i1 < n_tile && sm.cells[q] > (uint32_t)STAGE_CAP) {
-                i0 = i1;  // next bucket chunk of the same crowded cell
+            ok = p2g_chunk(c, sm, src, lo, hi);
+            if (n_tile > (uint32_t)STAGE_CAP && q1 == q + 1 && hi < sm.cells[q + 1]) {
+                i0 += (uint32_t)STAGE_CAP;  // next chunk of the same crowded cell
             } else {
                 q = q1;
                 i0 = 0;
