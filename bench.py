@@ -50,6 +50,19 @@ def _rank_info():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
 
 
+def reduce_over_ranks(dist, device, maxima, sums):
+    """The maximum over ranks of each of `maxima` (times) and the sum over
+    ranks of each of `sums` (work); one collective each, the same on every
+    rank, no collective without a process group."""
+    import torch
+    t_max = torch.tensor(list(maxima), dtype=torch.float64, device=device)
+    t_sum = torch.tensor(list(sums), dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t_sum, op=dist.ReduceOp.SUM)
+    return [float(v) for v in t_max], [float(v) for v in t_sum]
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -272,7 +285,7 @@ def run_b200_batched(args):
     torch.cuda.set_device(local_rank)
     from mpm_b200 import create_mpm_batched_gpu_solver
     from mpm_b200.scenes import BATCHED_TANK_GRAVITY, create_batched_tank_scenes
-    scenes = create_batched_tank_scenes()
+    scenes = create_batched_tank_scenes(first=rank * 512)  # each rank its own shard of scenes
     gravity = BATCHED_TANK_GRAVITY
     macro_dt = MACRO_DT
     batch = create_mpm_batched_gpu_solver(scenes, device=local_rank)
@@ -306,13 +319,10 @@ def run_b200_batched(args):
         retries += sum(r["retryCount"] for r in results)
     torch.cuda.synchronize()
     clock_info = clocks.stop()
-    work = batch.committed_particle_substeps
-    times = torch.tensor([batch.device_ms_total / 1e3, wall], dtype=torch.float64, device=f"cuda:{local_rank}")
-    if dist:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    device_s, wall = float(times[0]), float(times[1])
-    value = world * work / device_s
-    e2e_value = world * work / wall
+    (device_s, wall), (work,) = reduce_over_ranks(dist, f"cuda:{local_rank}", [batch.device_ms_total / 1e3, wall],
+                                                  [batch.committed_particle_substeps])
+    value = work / device_s
+    e2e_value = work / wall
 
     # kernel-by-kernel timing of real substeps of every scene at the smallest
     # microstep dt of the batch, right after the timed region
@@ -345,7 +355,7 @@ def run_b200_batched(args):
                    "scenes": len(scenes), "particles": n_total, "particles_range": [int(counts.min()),
                                                                                    int(counts.max())],
                    "grid_sides_range": [min(sides), max(sides)], "macro_dt": macro_dt, "courant": 0.3,
-                   "p2g": "gather", "parallelism": f"replicas x{world}",
+                   "p2g": "gather", "parallelism": f"scene shards x{world} (512 different scenes per GPU)",
                    "l2": "inputs larger than L2 (every scene's state, about 0.8 GB)",
                    "committed_particle_substeps": work, "submits": submits, "retries": retries,
                    "plain_per_scene": {"value": plain, "unit": UNIT,
@@ -400,7 +410,7 @@ def run_b200_adjoint(args):
     from mpm_b200 import create_mpm_batched_gpu_solver
     from mpm_b200.adjoint import create_mpm_adjoint_engine, fixed_cfl_dt
     from mpm_b200.scenes import ADJOINT_GRAVITY, create_adjoint_scenes
-    scenes = create_adjoint_scenes()
+    scenes = create_adjoint_scenes(first=rank * 64)  # each rank its own shard of scenes
     gravity = ADJOINT_GRAVITY
     steps = ADJOINT_SUBSTEPS
     dts = []
@@ -435,10 +445,7 @@ def run_b200_adjoint(args):
     torch.cuda.synchronize()
     clock_info = clocks.stop()
     engine.dispose()
-    times = torch.tensor([fwd / 1e3, bwd / 1e3, wall], dtype=torch.float64, device=f"cuda:{local_rank}")
-    if dist:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    fwd_s, bwd_s, wall = (float(v) for v in times)
+    (fwd_s, bwd_s, wall), _ = reduce_over_ranks(dist, f"cuda:{local_rank}", [fwd / 1e3, bwd / 1e3, wall], [])
     # the default solver stepping the same scenes with the same dt
     batch = create_mpm_batched_gpu_solver([(p, c) for p, c, _ in scenes], device=local_rank)
     batch.step_batch([steps] * len(scenes), dts, gravity)
@@ -460,7 +467,8 @@ def run_b200_adjoint(args):
                                "velocities N(0, 10^2), 200 substeps at each scene's fixed CFL dt, checkpoints every "
                                "20, loss sum |x(T) - target|^2 against a seeded displacement field",
                    "scenes": len(scenes), "particles": n, "substeps": steps,
-                   "checkpoint_every": ADJOINT_CHECKPOINT_EVERY, "parallelism": f"replicas x{world}",
+                   "checkpoint_every": ADJOINT_CHECKPOINT_EVERY,
+                   "parallelism": f"scene shards x{world} (64 different scenes per GPU)",
                    "l2": "inputs larger than L2 (1M particles' state and 64 grids of 67,081 nodes)",
                    "adjoint_forward_ratio": bwd_s / fwd_s,
                    "adjoint_over_default_forward": (bwd_s / args.steps) / (plain_ms * 1e-3),
@@ -538,10 +546,7 @@ def run_b200(args):
     clock_info = clocks.stop()
     device_s = solver.device_ms_total / 1e3
     substeps = solver.committed_microsteps_total
-    times = torch.tensor([device_s, wall], dtype=torch.float64, device=f"cuda:{local_rank}")
-    if dist:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    device_s, wall = float(times[0]), float(times[1])
+    (device_s, wall), _ = reduce_over_ranks(dist, f"cuda:{local_rank}", [device_s, wall], [])
     value = world * n * substeps / device_s
     e2e_value = world * n * substeps / wall
 

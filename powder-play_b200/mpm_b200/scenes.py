@@ -311,11 +311,12 @@ BATCHED_TANK_MAX_FILL_HEIGHT = 0.6  # of the box
 
 
 def create_batched_tank_scenes(count: int = 512, seed: int = 0x4D504D42, particles=(1_000, 64_000),
-                               sides=(64, 512)):
+                               sides=(64, 512), first: int = 0):
     """`count` independent SI Tait water tanks (rho 1000 kg/m^3, gamma 7,
     c = 20 m/s, 0.02 m extrusion, no-slip walls, at rest under y-up gravity
-    9.81 m/s^2), each a 0.2 m square box.  Scene k draws from the LCG seeded
-    with (seed + k * 0x9E3779B9) mod 2^32: its particle count N log-uniform in
+    9.81 m/s^2), each a 0.2 m square box.  Scene k (k = first, ..., first +
+    count - 1) draws from the LCG seeded with (seed + k * 0x9E3779B9) mod
+    2^32: its particle count N log-uniform in
     `particles`, its grid side S uniform in `sides` (S x S cells, dx = 0.2 m /
     S), the width of its block (a quarter to 0.6 of the box) and the block's
     place.  The block is a lattice at dx / 2 (2 x 2 particles per cell) where
@@ -329,7 +330,7 @@ def create_batched_tank_scenes(count: int = 512, seed: int = 0x4D504D42, particl
     size = BATCHED_TANK_DOMAIN_M
     top = BATCHED_TANK_MAX_FILL_HEIGHT * size
     out = []
-    for k in range(count):
+    for k in range(first, first + count):
         rnd = SeededRandom((seed + k * 0x9E3779B9) % UINT32_RANGE)
         log_lo, log_hi = math.log(particles[0]), math.log(particles[1])
         n = int(round(math.exp(log_lo + rnd() * (log_hi - log_lo))))
@@ -382,15 +383,15 @@ def _normal_pairs(rnd: SeededRandom, count: int) -> np.ndarray:
 
 def create_adjoint_scenes(count: int = 64, seed: int = 0x4D504D41, water_columns: int = 96, water_rows: int = 128,
                           solid_side: int = 64, cells: int = 256, velocity_sigma: float = 10.0,
-                          target_amplitude: float = 20.0):
+                          target_amplitude: float = 20.0, first: int = 0):
     """`count` scenes for the differentiable form, in Gate-4 world units
     (cellSize 10, gravity 90 along +y): a block of water_columns x water_rows
     Tait water particles (density 0.02, gamma 7, pressure coefficient
     22,857: the linear EOS's 2,828 sound speed) and a block of solid_side^2
     fixed-corotated solid particles (lambda 20, mu 10, density 0.02), both at
     2 x 2 particles per cell (spacing 5, area 25), on a cells x cells grid.
-    Scene k draws from the LCG seeded with (seed + k * 0x9E3779B9) mod 2^32:
-    the blocks' places, initial velocities N(0, velocity_sigma^2) per
+    Scene k (k = first, ..., first + count - 1) draws from the LCG seeded with
+    (seed + k * 0x9E3779B9) mod 2^32: the blocks' places, initial velocities N(0, velocity_sigma^2) per
     component, and a target displacement field d(x) = A (sin(2 pi k1 x / L +
     p1), cos(2 pi k2 y / L + p2)) with A = target_amplitude.  Returns
     [(particles, config, targets (n, 2))]; the defaults give 64 scenes of
@@ -399,7 +400,7 @@ def create_adjoint_scenes(count: int = 64, seed: int = 0x4D504D41, water_columns
     size = cells * dx
     area = spacing * spacing
     out = []
-    for k in range(count):
+    for k in range(first, first + count):
         rnd = SeededRandom((seed + k * 0x9E3779B9) % UINT32_RANGE)
         ww, wh = water_columns * spacing, water_rows * spacing
         sw = solid_side * spacing
