@@ -131,9 +131,44 @@ int mpm_set_drag(mpm_solver *solver, const mpm_drag *drag);
  * handle's queued work completes.  Blocks. */
 int mpm_queue_completion_ms(mpm_solver *solver, double *milliseconds);
 
-/* particleCount / particleCapacity (solver.ts:108-110). */
+/* particleCount / particleCapacity (solver.ts:108-110); allocatedParticleCount
+ * (:109): original indices handed out, particles removed by an outlet
+ * included. */
 uint32_t mpm_particle_count(const mpm_solver *solver);
 uint32_t mpm_particle_capacity(const mpm_solver *solver);
+uint32_t mpm_allocated_particle_count(const mpm_solver *solver);
+
+/* ---- interaction (single-scene solvers) ---- */
+
+/* appendParticles (solver.ts:2108-2278): `count` validated packed particles
+ * (no bonded-triangle markers) become original indices
+ * allocated .. allocated + count - 1 (*first_index = the first) under their
+ * object ids.  The caller applies the reference's refusal rules (pending
+ * readbacks, capacity split into accepted / dropped) before calling. */
+int mpm_append_particles(mpm_solver *solver, const float *packed_particles, const uint32_t *object_ids,
+                         uint32_t count, uint32_t *first_index);
+
+/* removeParticlesInOutlet (solver.ts:2280-2386, shaders.ts:3041-3065): water
+ * and oil particles inside the bounds leave the simulation; their original
+ * indices stay allocated and read back with material model 0xffffffff and
+ * their last state.  Blocks. */
+int mpm_remove_particles_in_outlet(mpm_solver *solver, float min_x, float min_y, float max_x, float max_y,
+                                   uint32_t *removed_count);
+
+/* pick (solver.ts:2733-2815, shaders.ts:3082-3116): the active particle
+ * nearest to (x, y) within `radius` (lowest index among equally near ones):
+ * its original index (0xffffffff: none), position and object id.  Blocks. */
+int mpm_pick(mpm_solver *solver, float x, float y, float radius, uint32_t *particle_index, float *anchor_xy,
+             uint32_t *object_id);
+
+/* clone (solver.ts:2852-2940, shaders.ts:3118-3147): the particles with
+ * original indices start .. start + count - 1 (an object's range) are copied
+ * as new original indices (*first_index = the first), moved by the offset
+ * and clamped to the domain, under `object_id`.  Refused (MPM_ERR_STATE)
+ * after an outlet removal and in scenes with bonded bodies or fracture
+ * bonds. */
+int mpm_clone_range(mpm_solver *solver, uint32_t start, uint32_t count, float offset_x, float offset_y,
+                    uint32_t object_id, uint32_t *first_index);
 
 /* dispose (solver.ts:143). */
 void mpm_destroy(mpm_solver *solver);

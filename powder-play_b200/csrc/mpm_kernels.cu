@@ -2714,6 +2714,88 @@ __global__ void k_body_finish(Ctx c)
     write_record(c, d, m, st, c.out.vel[d], c.out.F[d], c.out.vol[d], c.out.damage[d], c.out.pvol[d], c.out.C[d]);
 }
 
+// --------------------------------------------------------- interaction --
+
+// removeParticlesInOutlet (shaders.ts:3041-3065): water and oil particles of
+// the current state inside `bounds` (min x, min y, max x, max y) leave the
+// slot range.  Kept particles are packed into `out` (slot order free: every
+// sum of the default path has a fixed order regardless), removed ones into
+// `removed` with their original index; counters[0] / [1] count them.
+__global__ void k_outlet_compact(Ctx c, float4 bounds, ParticleBuffers removed, uint32_t *counters)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const Material m = c.mats[c.in.mat[i]];
+    const float2 p = c.in.pos[i];
+    const bool liquid = m.model == MODEL_WATER || m.model == MODEL_OIL;
+    if (liquid && p.x >= bounds.x && p.y >= bounds.y && p.x <= bounds.z && p.y <= bounds.w) {
+        const uint32_t j = atomicAdd(counters + 1, 1u);
+        removed.pos[j] = p;
+        removed.vel[j] = c.in.vel[i];
+        removed.C[j] = c.in.C[i];
+        removed.F[j] = c.in.F[i];
+        removed.pvol[j] = c.in.pvol[i];
+        removed.damage[j] = c.in.damage[i];
+        removed.vol[j] = c.in.vol[i];
+        removed.mat[j] = c.in.mat[i];
+        removed.orig[j] = c.in.orig[i];
+        return;
+    }
+    const uint32_t j = atomicAdd(counters, 1u);
+    copy_particle(c, i, j);
+    const uint32_t orig = c.in.orig[i];
+    if (is_tracked(c, orig)) c.slot_out[orig] = j;
+}
+
+// pickParticle (shaders.ts:3082-3116): the particle nearest to (px, py)
+// within sqrt(r2), the lowest original index among equally near ones, as the
+// minimum of (squared distance bits << 32 | original index).
+__global__ void k_pick(Ctx c, float px, float py, float r2, unsigned long long *best)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long key = ~0ull;
+    if (i < c.n) {
+        const float2 p = c.in.pos[i];
+        const float ox = __fsub_rn(p.x, px), oy = __fsub_rn(p.y, py);
+        const float d2 = __fadd_rn(__fmul_rn(ox, ox), __fmul_rn(oy, oy));
+        if (d2 <= r2) key = ((unsigned long long)__float_as_uint(d2) << 32) | c.in.orig[i];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+        key = other < key ? other : key;
+    }
+    if ((threadIdx.x & 31u) == 0u && key != ~0ull) atomicMin(best, key);
+}
+
+// cloneObject (shaders.ts:3118-3147): the particles with original indices
+// [start, start + count) of the current state are copied to the new slots
+// n .. n + count - 1 as original indices orig_base .. orig_base + count - 1,
+// moved by `offset` and clamped to the domain [0, domain.x] x [0, domain.y],
+// under `object_id`.
+__global__ void k_clone(Ctx c, uint32_t start, uint32_t count, float2 offset, float2 domain, uint32_t orig_base,
+                        uint32_t object_id)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const uint32_t orig = c.in.orig[i];
+    if (orig < start || orig - start >= count) return;
+    const uint32_t k = orig - start, j = c.n + k;
+    const float2 p = c.in.pos[i];
+    c.in.pos[j] = make_float2(fminf(fmaxf(__fadd_rn(p.x, offset.x), 0.0f), domain.x),
+                              fminf(fmaxf(__fadd_rn(p.y, offset.y), 0.0f), domain.y));
+    c.in.vel[j] = c.in.vel[i];
+    c.in.C[j] = c.in.C[i];
+    c.in.F[j] = c.in.F[i];
+    c.in.pvol[j] = c.in.pvol[i];
+    c.in.damage[j] = c.in.damage[i];
+    c.in.vol[j] = c.in.vol[i];
+    c.in.mat[j] = c.in.mat[i];
+    c.in.orig[j] = orig_base + k;
+    const_cast<uint32_t *>(c.obj)[orig_base + k] = object_id;
+    const_cast<uint32_t *>(c.bonded)[orig_base + k] = 0u;
+}
+
 // the instances the host launches
 template __global__ void k_p2g_gather<false>(Ctx);
 template __global__ void k_p2g_gather<true>(Ctx);

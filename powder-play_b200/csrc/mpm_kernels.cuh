@@ -184,5 +184,10 @@ __global__ void k_fracture_bonds(Ctx c);
 __global__ void k_fracture_damage(Ctx c);
 __global__ void k_body_finish(Ctx c);
 __global__ void k_count_active_nodes(Ctx c, uint32_t *counts);
+// interaction
+__global__ void k_outlet_compact(Ctx c, float4 bounds, ParticleBuffers removed, uint32_t *counters);
+__global__ void k_pick(Ctx c, float px, float py, float r2, unsigned long long *best);
+__global__ void k_clone(Ctx c, uint32_t start, uint32_t count, float2 offset, float2 domain, uint32_t orig_base,
+                        uint32_t object_id);
 
 }  // namespace mpm

@@ -81,7 +81,12 @@ struct mpm_solver {
     int device = 0;
     cudaStream_t stream = nullptr;
     mpm_config cfg{};
-    uint32_t n = 0, capacity = 0;
+    uint32_t n = 0, capacity = 0;  // particles in device slots, slots allocated
+    // original indices handed out (appends and clones add some); particles
+    // removed by an outlet keep theirs, with their last state kept here
+    uint32_t allocated = 0;
+    std::vector<float> removed_words;   // 20 per original index (valid where removed)
+    std::vector<uint8_t> removed;       // per original index
     uint32_t node_w = 0, node_h = 0, node_count = 0, tiles_x = 0, tiles_y = 0;
     uint32_t cell_pad = 0, n_chunks = 0;
     uint32_t n_bodies = 0, n_bonds = 0;
@@ -482,7 +487,10 @@ uint32_t intern_material(std::vector<Material> &table, const float *w)
 }
 
 // Uploads packed records in original order: slot i holds particle i.
-int unpack_and_upload(mpm_solver *s, const float *packed, uint32_t count, int target)
+// Uploads `count` packed particles into slots slot_base.. of buffer `target`
+// as original indices orig_base..
+int unpack_and_upload(mpm_solver *s, const float *packed, uint32_t count, int target, uint32_t slot_base = 0,
+                      uint32_t orig_base = 0)
 {
     std::vector<float2> pos(count), vel(count);
     std::vector<float4> C(count), F(count);
@@ -503,7 +511,7 @@ int unpack_and_upload(mpm_solver *s, const float *packed, uint32_t count, int ta
         vol[i] = w[17];
         mat[i] = intern_material(s->mats, w);
         bonded[i] = f2u(w[19]);
-        orig[i] = i;
+        orig[i] = orig_base + i;
         if (bonded[i] > 3u) return set_error(MPM_ERR_INVALID_ARGUMENT, "particle %u has an invalid bonded triangle marker", i);
     }
     if (s->mats.size() > 65536) return set_error(MPM_ERR_INVALID_ARGUMENT, "more than 65536 distinct materials");
@@ -519,20 +527,25 @@ int unpack_and_upload(mpm_solver *s, const float *packed, uint32_t count, int ta
         s->graphs.clear();
     }
     ParticleBuffers &b = s->buf[target];
-    CUDA_TRY(cudaMemcpyAsync(b.pos, pos.data(), count * sizeof(float2), cudaMemcpyHostToDevice, s->stream));
-    CUDA_TRY(cudaMemcpyAsync(b.vel, vel.data(), count * sizeof(float2), cudaMemcpyHostToDevice, s->stream));
-    CUDA_TRY(cudaMemcpyAsync(b.C, C.data(), count * sizeof(float4), cudaMemcpyHostToDevice, s->stream));
-    CUDA_TRY(cudaMemcpyAsync(b.F, F.data(), count * sizeof(float4), cudaMemcpyHostToDevice, s->stream));
-    CUDA_TRY(cudaMemcpyAsync(b.pvol, pvol.data(), count * sizeof(float), cudaMemcpyHostToDevice, s->stream));
-    CUDA_TRY(cudaMemcpyAsync(b.damage, damage.data(), count * sizeof(float), cudaMemcpyHostToDevice, s->stream));
-    CUDA_TRY(cudaMemcpyAsync(b.vol, vol.data(), count * sizeof(float), cudaMemcpyHostToDevice, s->stream));
-    CUDA_TRY(cudaMemcpyAsync(b.mat, mat.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
-    CUDA_TRY(cudaMemcpyAsync(b.orig, orig.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
-    CUDA_TRY(cudaMemcpyAsync(s->bonded, bonded.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+    const size_t d = slot_base;
+    CUDA_TRY(cudaMemcpyAsync(b.pos + d, pos.data(), count * sizeof(float2), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(b.vel + d, vel.data(), count * sizeof(float2), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(b.C + d, C.data(), count * sizeof(float4), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(b.F + d, F.data(), count * sizeof(float4), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(b.pvol + d, pvol.data(), count * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(b.damage + d, damage.data(), count * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(b.vol + d, vol.data(), count * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(b.mat + d, mat.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(b.orig + d, orig.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->bonded + orig_base, bonded.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                             s->stream));
     if (s->slot_of[target]) {
         // the uploaded slots are in original order
-        CUDA_TRY(cudaMemcpyAsync(s->slot_of[target], orig.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice,
-                                 s->stream));
+        std::vector<uint32_t> slots(count);
+        for (uint32_t i = 0; i < count; ++i) slots[i] = slot_base + i;
+        CUDA_TRY(cudaMemcpyAsync(s->slot_of[target] + orig_base, slots.data(), count * sizeof(uint32_t),
+                                 cudaMemcpyHostToDevice, s->stream));
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
     }
     // the copies above read pageable host vectors; wait before they go away
     CUDA_TRY(cudaStreamSynchronize(s->stream));
@@ -690,6 +703,7 @@ int create_impl(const mpm_config *configs, uint32_t n_scenes, const uint32_t *co
     s->device = c.device;
     s->cfg = c;
     s->n = count;
+    s->allocated = count;
     s->capacity = std::max<uint32_t>(n_scenes > 1 ? count : c.capacity, 1u);
     s->n_scenes = n_scenes;
     s->scenes.resize(n_scenes);
@@ -852,10 +866,12 @@ int create_impl(const mpm_config *configs, uint32_t n_scenes, const uint32_t *co
         }
         s->n_tracked = (uint32_t)tracked.size();
         s->n_endpoints = (uint32_t)endpoints.size();
-        ALLOC(s->track_flag, count);
+        ALLOC(s->track_flag, cap);
+        if (cudaMemset(s->track_flag, 0, cap * sizeof(uint32_t)) != cudaSuccess)
+            return fail(set_error(MPM_ERR_CUDA, "cudaMemset failed"));
         ALLOC(s->tracked, tracked.size());
         ALLOC(s->endpoints, endpoints.size());
-        for (int b = 0; b < 2; ++b) ALLOC(s->slot_of[b], count);
+        for (int b = 0; b < 2; ++b) ALLOC(s->slot_of[b], cap);
         if (body_count > 0) {
             ALLOC(s->field, s->node_count);
             ALLOC(s->body_starts, body_count);
@@ -921,6 +937,18 @@ int create_impl(const mpm_config *configs, uint32_t n_scenes, const uint32_t *co
 }
 
 int run_batch(mpm_solver *s, uint32_t step_count, bool guarded);
+
+// After the particle count of a single-scene solver changed: its parameters
+// and scene table follow, and the captured graphs (launch sizes) are dropped.
+int refresh_count(mpm_solver *s)
+{
+    s->scenes[0].n = s->n;
+    const uint32_t bounds[2] = {0u, s->n};
+    CUDA_TRY(cudaMemcpy(s->scene_p_base, bounds, sizeof bounds, cudaMemcpyHostToDevice));
+    for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    s->graphs.clear();
+    return MPM_OK;
+}
 
 }  // namespace
 
@@ -1207,28 +1235,37 @@ int mpm_read_particles(mpm_solver *s, const uint32_t *indices, uint32_t count, f
     g_last_error.clear();
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
     if (!packed_out) return set_error(MPM_ERR_INVALID_ARGUMENT, "packed_out must not be NULL");
-    if (!indices && count != s->n) return set_error(MPM_ERR_INVALID_ARGUMENT, "count must equal the particle count");
+    const uint32_t total = s->allocated;  // original indices, removed ones included
+    if (!indices && count != total) return set_error(MPM_ERR_INVALID_ARGUMENT, "count must equal the particle count");
     for (uint32_t k = 0; indices && k < count; ++k)
-        if (indices[k] >= s->n) return set_error(MPM_ERR_INVALID_ARGUMENT, "particleIndices must identify active GPU particles.");
+        if (indices[k] >= total) return set_error(MPM_ERR_INVALID_ARGUMENT, "particleIndices must identify active GPU particles.");
     CUDA_TRY(cudaSetDevice(s->device));
     const uint32_t n = s->n;
     HostState h;
     int rc = download_state(s, h);
     if (rc != MPM_OK) return rc;
-    std::vector<uint32_t> bonded(n), obj(n), slot_of(n);
-    if (n > 0) {
-        CUDA_TRY(cudaMemcpyAsync(bonded.data(), s->bonded, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
-        CUDA_TRY(cudaMemcpyAsync(obj.data(), s->obj, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    std::vector<uint32_t> bonded(total), obj(total), slot_of(total, 0xffffffffu);
+    if (total > 0) {
+        CUDA_TRY(cudaMemcpyAsync(bonded.data(), s->bonded, total * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(obj.data(), s->obj, total * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
         CUDA_TRY(cudaStreamSynchronize(s->stream));
     }
     for (uint32_t d = 0; d < n; ++d) {
-        if (h.orig[d] >= n) return set_error(MPM_ERR_CUDA, "corrupt particle slot map");
+        if (h.orig[d] >= total) return set_error(MPM_ERR_CUDA, "corrupt particle slot map");
         slot_of[h.orig[d]] = d;
     }
     for (uint32_t k = 0; k < count; ++k) {
         const uint32_t i = indices ? indices[k] : k;
         const uint32_t d = slot_of[i];
         float *w = packed_out + (size_t)k * MPM_PARTICLE_WORDS;
+        if (object_ids_out) object_ids_out[k] = obj[i];
+        if (d == 0xffffffffu) {
+            // removed by an outlet: its last state, material model 0xffffffff
+            // (MODEL_REMOVED, shaders.ts:195)
+            if (i >= s->removed.size() || !s->removed[i]) return set_error(MPM_ERR_CUDA, "corrupt particle slot map");
+            std::memcpy(w, s->removed_words.data() + (size_t)i * MPM_PARTICLE_WORDS, MPM_PARTICLE_WORDS * sizeof(float));
+            continue;
+        }
         const Material &m = s->mats[h.mat[d]];
         w[0] = h.pos[d].x;
         w[1] = h.pos[d].y;
@@ -1250,7 +1287,6 @@ int mpm_read_particles(mpm_solver *s, const uint32_t *indices, uint32_t count, f
         w[17] = h.vol[d];
         w[18] = m.model == MODEL_NEO_HOOKEAN ? h.damage[d] : m.param;
         w[19] = u2f(bonded[i]);
-        if (object_ids_out) object_ids_out[k] = obj[i];
     }
     return MPM_OK;
 }
@@ -1260,6 +1296,7 @@ int mpm_write_particles(mpm_solver *s, const float *packed, uint32_t count)
     g_last_error.clear();
     if (!s || !packed) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and packed_particles must not be NULL");
     if (count != s->n) return set_error(MPM_ERR_INVALID_ARGUMENT, "count must equal the particle count");
+    if (s->allocated != s->n) return set_error(MPM_ERR_STATE, "particles were removed; the state cannot be overwritten");
     CUDA_TRY(cudaSetDevice(s->device));
     return unpack_and_upload(s, packed, count, s->cur);
 }
@@ -1297,6 +1334,180 @@ int mpm_queue_completion_ms(mpm_solver *s, double *ms)
     if (ms) *ms = elapsed;
     return MPM_OK;
 }
+
+int mpm_append_particles(mpm_solver *s, const float *packed, const uint32_t *object_ids, uint32_t count,
+                         uint32_t *first_index)
+{
+    g_last_error.clear();
+    if (!s || (count > 0 && (!packed || !object_ids)))
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "solver, packed_particles and object_ids must not be NULL");
+    if (s->n_scenes > 1) return set_error(MPM_ERR_STATE, "particles are appended to a single-scene solver");
+    if ((uint64_t)s->allocated + count > s->capacity)
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "particle slot capacity %u is full", s->capacity);
+    for (uint32_t k = 0; k < count; ++k)
+        if (f2u(packed[(size_t)k * MPM_PARTICLE_WORDS + 19]) != 0u)
+            return set_error(MPM_ERR_INVALID_ARGUMENT,
+                             "triangle-bonded particles cannot be appended without a complete object topology");
+    if (first_index) *first_index = s->allocated;
+    if (count == 0) return MPM_OK;
+    CUDA_TRY(cudaSetDevice(s->device));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    int rc = unpack_and_upload(s, packed, count, s->cur, s->n, s->allocated);
+    if (rc != MPM_OK) return rc;
+    CUDA_TRY(cudaMemcpy(s->obj + s->allocated, object_ids, count * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    s->allocated += count;
+    s->n += count;
+    return refresh_count(s);
+}
+
+int mpm_remove_particles_in_outlet(mpm_solver *s, float min_x, float min_y, float max_x, float max_y,
+                                   uint32_t *removed_count)
+{
+    g_last_error.clear();
+    if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
+    if (s->n_scenes > 1) return set_error(MPM_ERR_STATE, "outlets act on a single-scene solver");
+    if (!(min_x <= max_x) || !(min_y <= max_y))
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "outlet minimum coordinates must not exceed the maximum.");
+    if (removed_count) *removed_count = 0;
+    if (s->n == 0) return MPM_OK;
+    CUDA_TRY(cudaSetDevice(s->device));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    const uint32_t n = s->n;
+    ParticleBuffers r{};
+    uint32_t *counters = nullptr;
+    cudaError_t e = dalloc(&r.pos, n);
+    if (e == cudaSuccess) e = dalloc(&r.vel, n);
+    if (e == cudaSuccess) e = dalloc(&r.C, n);
+    if (e == cudaSuccess) e = dalloc(&r.F, n);
+    if (e == cudaSuccess) e = dalloc(&r.pvol, n);
+    if (e == cudaSuccess) e = dalloc(&r.damage, n);
+    if (e == cudaSuccess) e = dalloc(&r.vol, n);
+    if (e == cudaSuccess) e = dalloc(&r.mat, n);
+    if (e == cudaSuccess) e = dalloc(&r.orig, n);
+    if (e == cudaSuccess) e = dalloc(&counters, 2);
+    uint32_t h_counts[2] = {0, 0};
+    if (e == cudaSuccess) e = cudaMemsetAsync(counters, 0, 2 * sizeof(uint32_t), s->stream);
+    if (e == cudaSuccess) {
+        const Ctx c = make_ctx(s, s->cur);
+        k_outlet_compact<<<blocks_for(n, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(
+            c, make_float4(min_x, min_y, max_x, max_y), r, counters);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_counts, counters, sizeof h_counts, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    const uint32_t removed = h_counts[1];
+    std::vector<float2> pos(removed), vel(removed);
+    std::vector<float4> C(removed), F(removed);
+    std::vector<float> pvol(removed), vol(removed);
+    std::vector<uint32_t> mat(removed), orig(removed);
+    if (e == cudaSuccess && removed > 0) {
+        e = cudaMemcpy(pos.data(), r.pos, removed * sizeof(float2), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(vel.data(), r.vel, removed * sizeof(float2), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(C.data(), r.C, removed * sizeof(float4), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(F.data(), r.F, removed * sizeof(float4), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(pvol.data(), r.pvol, removed * sizeof(float), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(vol.data(), r.vol, removed * sizeof(float), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(mat.data(), r.mat, removed * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(orig.data(), r.orig, removed * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    }
+    void *ptrs[] = {r.pos, r.vel, r.C, r.F, r.pvol, r.damage, r.vol, r.mat, r.orig, counters};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (e != cudaSuccess) return set_error(MPM_ERR_CUDA, "outlet removal failed: %s", cudaGetErrorString(e));
+    if (h_counts[0] + removed != n) return set_error(MPM_ERR_CUDA, "outlet removal lost particles");
+    // the kept particles are in the other buffer now
+    s->cur = 1 - s->cur;
+    s->n = h_counts[0];
+    if (removed > 0) {
+        if (s->removed.size() < s->allocated) {
+            s->removed.resize(s->allocated, 0u);
+            s->removed_words.resize((size_t)s->allocated * MPM_PARTICLE_WORDS, 0.0f);
+        }
+        for (uint32_t k = 0; k < removed; ++k) {
+            const uint32_t i = orig[k];
+            const Material &m = s->mats[mat[k]];
+            float *w = s->removed_words.data() + (size_t)i * MPM_PARTICLE_WORDS;
+            const float words[MPM_PARTICLE_WORDS] = {pos[k].x, pos[k].y, vel[k].x, vel[k].y, C[k].x, C[k].y,
+                                                     C[k].z, C[k].w, F[k].x, F[k].y, F[k].z, F[k].w, pvol[k],
+                                                     u2f(0xffffffffu), m.lambda, m.mu, m.density, vol[k], m.param,
+                                                     0.0f};
+            std::memcpy(w, words, sizeof words);
+            s->removed[i] = 1u;
+        }
+    }
+    if (removed_count) *removed_count = removed;
+    return refresh_count(s);
+}
+
+int mpm_pick(mpm_solver *s, float x, float y, float radius, uint32_t *particle_index, float *anchor_xy,
+             uint32_t *object_id)
+{
+    g_last_error.clear();
+    if (!s || !particle_index) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and particle_index must not be NULL");
+    if (s->n_scenes > 1) return set_error(MPM_ERR_STATE, "picking acts on a single-scene solver");
+    if (!(radius >= 0.0f) || !std::isfinite(radius))
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "pick radius must be non-negative");
+    *particle_index = 0xffffffffu;
+    if (s->n == 0) return MPM_OK;
+    CUDA_TRY(cudaSetDevice(s->device));
+    unsigned long long *best = nullptr, h_best = ~0ull;
+    CUDA_TRY(dalloc(&best, 1));
+    cudaError_t e = cudaMemcpyAsync(best, &h_best, sizeof h_best, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) {
+        const Ctx c = make_ctx(s, s->cur);
+        k_pick<<<blocks_for(s->n, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c, x, y, radius * radius, best);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h_best, best, sizeof h_best, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    cudaFree(best);
+    if (e != cudaSuccess) return set_error(MPM_ERR_CUDA, "particle pick failed: %s", cudaGetErrorString(e));
+    if (h_best == ~0ull) return MPM_OK;
+    const uint32_t index = (uint32_t)(h_best & 0xffffffffull);
+    float packed[MPM_PARTICLE_WORDS];
+    uint32_t id = 0;
+    const int rc = mpm_read_particles(s, &index, 1, packed, &id);
+    if (rc != MPM_OK) return rc;
+    *particle_index = index;
+    if (anchor_xy) {
+        anchor_xy[0] = packed[0];
+        anchor_xy[1] = packed[1];
+    }
+    if (object_id) *object_id = id;
+    return MPM_OK;
+}
+
+int mpm_clone_range(mpm_solver *s, uint32_t start, uint32_t count, float offset_x, float offset_y,
+                    uint32_t object_id, uint32_t *first_index)
+{
+    g_last_error.clear();
+    if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
+    if (s->n_scenes > 1) return set_error(MPM_ERR_STATE, "cloning acts on a single-scene solver");
+    if (!std::isfinite(offset_x) || !std::isfinite(offset_y))
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "clone offset must be finite");
+    if ((uint64_t)start + count > s->allocated)
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "the cloned range must hold allocated particles");
+    if (s->allocated != s->n) return set_error(MPM_ERR_STATE, "objects are not cloned after an outlet removed particles");
+    if ((uint64_t)s->allocated + count > s->capacity)
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "particle slot capacity %u is full", s->capacity);
+    if (s->n_bodies > 0 || s->n_bonds > 0)
+        return set_error(MPM_ERR_STATE, "scenes with bonded triangle bodies or fracture bonds are not cloned");
+    if (first_index) *first_index = s->allocated;
+    if (count == 0) return MPM_OK;
+    CUDA_TRY(cudaSetDevice(s->device));
+    const Ctx c = make_ctx(s, s->cur);
+    const float2 domain = make_float2((float)((double)s->cfg.cells_x * (double)s->cfg.cell_size),
+                                      (float)((double)s->cfg.cells_y * (double)s->cfg.cell_size));
+    k_clone<<<blocks_for(s->n, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(
+        c, start, count, make_float2(offset_x, offset_y), domain, s->allocated, object_id);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->allocated += count;
+    s->n += count;
+    return refresh_count(s);
+}
+
+uint32_t mpm_allocated_particle_count(const mpm_solver *s) { return s ? s->allocated : 0u; }
 
 uint32_t mpm_particle_count(const mpm_solver *s) { return s ? s->n : 0u; }
 uint32_t mpm_particle_capacity(const mpm_solver *s) { return s ? s->capacity : 0u; }

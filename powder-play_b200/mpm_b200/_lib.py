@@ -25,6 +25,8 @@ EXPORTED_SYMBOLS = (
     "mpm_probe_fixed_point", "mpm_probe_triangle_field", "mpm_node_count", "mpm_last_batch_device_ms", "mpm_profile_substeps",
     "mpm_profile_kernel_name", "mpm_profile_kernel_slots", "mpm_count_active_nodes", "mpm_stream",
     "mpmb_create", "mpmb_step_batch", "mpmb_read_compact", "mpmb_scene_count",
+    "mpm_allocated_particle_count", "mpm_append_particles", "mpm_remove_particles_in_outlet", "mpm_pick",
+    "mpm_clone_range",
     "mpma_create", "mpma_set_parameters", "mpma_get_parameters", "mpma_set_velocities", "mpma_forward",
     "mpma_backward", "mpma_read_positions", "mpma_last_ms", "mpma_destroy",
 )
@@ -118,6 +120,16 @@ def load_library(path: str = LIBRARY_PATH) -> ctypes.CDLL:
     lib.mpmb_read_compact.restype = i32
     lib.mpmb_scene_count.argtypes = [vp]
     lib.mpmb_scene_count.restype = u32
+    lib.mpm_allocated_particle_count.argtypes = [vp]
+    lib.mpm_allocated_particle_count.restype = u32
+    lib.mpm_append_particles.argtypes = [vp, vp, vp, u32, P(u32)]
+    lib.mpm_append_particles.restype = i32
+    lib.mpm_remove_particles_in_outlet.argtypes = [vp, f32, f32, f32, f32, P(u32)]
+    lib.mpm_remove_particles_in_outlet.restype = i32
+    lib.mpm_pick.argtypes = [vp, f32, f32, f32, P(u32), vp, P(u32)]
+    lib.mpm_pick.restype = i32
+    lib.mpm_clone_range.argtypes = [vp, u32, u32, f32, f32, u32, P(u32)]
+    lib.mpm_clone_range.restype = i32
     lib.mpma_create.argtypes = [vp, u32, vp, vp, vp, P(vp)]
     lib.mpma_create.restype = i32
     for name in ("mpma_set_parameters", "mpma_get_parameters", "mpma_set_velocities", "mpma_read_positions"):

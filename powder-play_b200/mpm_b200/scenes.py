@@ -9,6 +9,8 @@
   src/lib/mpm/scenes/gate4.ts:134-357 (LCG seeds, draw order, bonds).
 * `create_dam_break_scene` -- the 1,000,000-particle two-phase water/oil dam
   break on a 1024x2048 grid (cellSize 10, gravity 90, Gate-4 liquids).
+* `create_mpm_emitter_particles` -- src/lib/mpm/scenes/emitter.ts:49-129 (the
+  particles of an interactive emitter batch).
 * `create_batched_tank_scenes` -- independent SI Tait water tanks of uneven
   particle counts and grids for the batched solver.
 * `create_adjoint_scenes` -- water + fixed-corotated solid scenes, their
@@ -435,5 +437,86 @@ def create_adjoint_scenes(count: int = 64, seed: int = 0x4D504D41, water_columns
         config = {"grid": {"cellsX": cells, "cellsY": cells, "cellSize": dx}, "particleMass": 0.02 * area,
                   "particleVolume": area, "material": ADJOINT_SOLID, "wallFriction": 0.0}
         out.append((p, config, targets))
+    return out
+
+
+# ---------------------------------------------------------------- emitter --
+
+MAX_MPM_EMITTER_PARTICLES = 100_000
+_GOLDEN_ANGLE = math.pi * (3 - math.sqrt(5))
+_EMITTER_MATERIALS = {
+    "water": {"lambda": 40_000 * 4, "mu": 0.0, "model": "water", "density": 0.02},
+    "oil": {"lambda": 30_000 * 4, "mu": 0.0, "model": "oil", "density": 0.016},
+    "neo-hookean": {"lambda": 20.0, "mu": 10.0, "model": "neo-hookean"},
+}
+
+
+def create_mpm_emitter_particles(config: dict) -> list:
+    """createMpmEmitterParticles, emitter.ts:49-129: `count` particles in a
+    jittered rectangle lattice or a golden-angle disc around `center`, with
+    the seeded LCG's draws in the reference's order."""
+    count = config.get("count")
+    if not isinstance(count, int) or isinstance(count, bool) or count < 1:
+        raise RangeError("count must be a positive safe integer")
+    if count > MAX_MPM_EMITTER_PARTICLES:
+        raise RangeError(f"count must not exceed {MAX_MPM_EMITTER_PARTICLES}")
+    seed = config.get("seed")
+    if not isinstance(seed, int) or isinstance(seed, bool) or seed < 0 or seed > 0xFFFFFFFF:
+        raise RangeError("seed must be an unsigned 32-bit integer")
+    shape = config.get("shape")
+    if shape not in ("rectangle", "circle"):
+        raise RangeError("shape must be rectangle or circle")
+    material = config.get("material")
+    if material not in _EMITTER_MATERIALS:
+        raise RangeError("material must be water, oil, or neo-hookean")
+
+    def vector(v, name):
+        if not isinstance(v, dict):
+            raise TypeError(f"{name} must be a vector")
+        if not all(isinstance(v.get(k), (int, float)) and math.isfinite(v.get(k)) for k in ("x", "y")):
+            raise RangeError(f"{name} components must be finite")
+        return float(v["x"]), float(v["y"])
+
+    def positive(v, name):
+        if not isinstance(v, (int, float)) or not math.isfinite(v) or v <= 0:
+            raise RangeError(f"{name} must be a positive finite number")
+        return float(v)
+
+    cx, cy = vector(config.get("center"), "center")
+    vx, vy = vector(config.get("velocity"), "velocity")
+    grid = config.get("grid")
+    if not isinstance(grid, dict):
+        raise TypeError("grid must be an object")
+    if not all(isinstance(grid.get(k), int) and grid.get(k) >= 1 for k in ("cellsX", "cellsY")):
+        raise RangeError("grid cell counts must be positive safe integers")
+    cell = positive(grid.get("cellSize"), "grid.cellSize")
+    spacing = positive(config.get("spacing"), "spacing")
+    volume = positive(config.get("particleVolume", 25), "particleVolume")
+    width, height = grid["cellsX"] * cell, grid["cellsY"] * cell
+    if cx < 0 or cx > width or cy < 0 or cy > height:
+        raise RangeError("center must be inside the simulation domain")
+    random = SeededRandom(seed)
+    columns = math.ceil(math.sqrt(count))
+    rows = math.ceil(count / columns)
+    radius = spacing * math.sqrt(count / math.pi)
+    angular_offset = random() * math.pi * 2
+    out = []
+    for index in range(count):
+        if shape == "circle":
+            radial = math.sqrt((index + 0.5) / count)
+            angle = angular_offset + index * _GOLDEN_ANGLE
+            jitter = (random() - 0.5) * spacing * 0.12
+            distance = max(0.0, radial * radius + jitter)
+            x, y = cx + math.cos(angle) * distance, cy + math.sin(angle) * distance
+        else:
+            column, row = index % columns, index // columns
+            x = cx + (column - (columns - 1) * 0.5) * spacing + (random() - 0.5) * spacing * 0.12
+            y = cy + (row - (rows - 1) * 0.5) * spacing + (random() - 0.5) * spacing * 0.12
+        if x < 0 or x > width or y < 0 or y > height:
+            raise RangeError(f"emitted particle {index} would be outside the simulation domain")
+        out.append({"position": {"x": x, "y": y}, "velocity": {"x": vx, "y": vy},
+                    "C": {"m00": 0.0, "m01": 0.0, "m10": 0.0, "m11": 0.0},
+                    "F": {"m00": 1.0, "m01": 0.0, "m10": 0.0, "m11": 1.0}, "plasticVolume": 1.0,
+                    "volume": volume, "material": dict(_EMITTER_MATERIALS[material])})
     return out
 

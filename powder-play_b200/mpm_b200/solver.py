@@ -23,8 +23,8 @@ from .cfl import calculate_mpm_cfl_microsteps, calculate_mpm_cfl_safe_dt, calcul
 from .cfl_bounds import derive_mpm_mls_gpu_cfl_bounds
 from .errors import (MpmMlsGpuNumericalError, MpmNativeError, RangeError, decode_numerical_error,
                      is_recoverable_cfl_error)
-from .layout import (PARTICLE_FLOATS, ValidatedInput, fround, pack_step_parameters, unpack_particles,
-                     validate_mpm_mls_gpu_input, _is_safe_integer)
+from .layout import (PARTICLE_FLOATS, ValidatedInput, fround, pack_step_parameters, particles_from_dicts,
+                     unpack_particles, validate_mpm_mls_gpu_input, _is_safe_integer)
 
 CFL_RECOVERY_BOUND_SAFETY_FACTOR = 1.25
 MPM_MLS_GPU_DRAG_STIFFNESS = 20.0
@@ -32,6 +32,16 @@ MPM_MLS_GPU_DRAG_DAMPING = 8.0
 EPSILON = 2.220446049250313e-16
 MIN_VALUE = 5e-324
 DEFAULT_FIXED_POINT_SHIFT = 24
+
+
+def _interaction_float32(value, name: str) -> float:
+    """finiteInteractionFloat32, solver.ts:3268-3277."""
+    if isinstance(value, bool) or not isinstance(value, (int, float)) or not math.isfinite(value):
+        raise TypeError(f"{name} must be a finite number.")
+    result = fround(value)
+    if not math.isfinite(result):
+        raise RangeError(f"{name} is outside the supported float32 range.")
+    return result
 
 
 def _is_capacity_error(error) -> bool:
@@ -126,7 +136,11 @@ class MpmMlsGpuSolver:
         self.atomic_p2g = atomic_p2g
         self.fixed_point_shift = fixed_point_shift
         self._disposed = False
-        self._slot_count = state.particle_count
+        self._slot_count = state.particle_count      # particleSlotCount (allocated original indices)
+        self._active_count = state.particle_count    # activeParticleCount
+        self._has_removed = False
+        self._object_ranges = {r["objectId"]: (r["start"], r["count"]) for r in state.object_ranges}
+        self._next_object_id = max([r["objectId"] + 1 for r in state.object_ranges] + [0])
         self._cfl_speed_measurement_submitted = False
         self._cfl_state_usable = cfl_bounds is not None
         self._last_scheduled_velocity_bound = None if cfl_bounds is None else cfl_bounds["velocityBound"]
@@ -140,7 +154,7 @@ class MpmMlsGpuSolver:
     # ---------------------------------------------------------------- props --
     @property
     def particle_count(self) -> int:
-        return self._slot_count
+        return self._active_count
 
     @property
     def allocated_particle_count(self) -> int:
@@ -501,18 +515,210 @@ class MpmMlsGpuSolver:
         _check(self._lib.mpm_queue_completion_ms(self._handle, ctypes.byref(out)), "Failed to measure the queue.")
         return float(out.value)
 
-    def begin_drag(self, target: dict, radius: float) -> None:
-        """beginDrag/updateDrag (solver.ts:2700-2790): grid-node spring and damping."""
+    # ----------------------------------------------------------- interaction --
+    def _world_point(self, point, name: str) -> tuple:
+        """validateMpmWorldPoint, solver.ts:3228-3242."""
+        if not isinstance(point, dict):
+            raise TypeError(f"{name} must be a vector.")
+        x, y = _interaction_float32(point.get("x"), f"{name}.x"), _interaction_float32(point.get("y"), f"{name}.y")
+        if x < 0 or x > self._state.domain_width_f32 or y < 0 or y > self._state.domain_height_f32:
+            raise RangeError(f"{name} must be inside the MLS-MPM domain.")
+        return x, y
+
+    def _pick_radius(self, radius) -> float:
+        """validateMpmPickRadius, solver.ts:3244-3250."""
+        value = _interaction_float32(radius, "pick radius")
+        if value < 0 or value > max(self._state.domain_width_f32, self._state.domain_height_f32):
+            raise RangeError("pick radius must be non-negative and within the MLS-MPM domain extent.")
+        return value
+
+    def _resolve_selection(self, selection) -> tuple:
+        """resolveSelection, solver.ts:1363-1387 -> (start, count)."""
+        if not isinstance(selection, dict):
+            raise TypeError("selection must identify an MPM particle.")
+        index, oid = selection.get("particleIndex"), selection.get("objectId")
+        if (not _is_safe_integer(index) or index < 0 or index >= self._slot_count or not _is_safe_integer(oid)
+                or oid < 0 or oid > 0xFFFFFFFF):
+            raise RangeError("selection must identify an active MPM particle.")
+        self._world_point(selection.get("anchor"), "selection anchor")
+        rng = self._object_ranges.get(oid)
+        if rng is None or not rng[0] <= index < rng[0] + rng[1]:
+            raise RangeError("selection objectId does not match the selected particle.")
+        return rng
+
+    def pick(self, point, radius):
+        """pick, solver.ts:2733-2815: the nearest active particle within
+        `radius` as {particleIndex, objectId, anchor}, or None."""
         self._assert_active()
-        drag = _lib.MpmDrag(fround(target["x"]), fround(target["y"]), fround(radius), MPM_MLS_GPU_DRAG_STIFFNESS,
-                            MPM_MLS_GPU_DRAG_DAMPING)
-        _check(self._lib.mpm_set_drag(self._handle, ctypes.byref(drag)), "Failed to set the drag target.")
-        self._active_drag = {"radius": radius}
+        x, y = self._world_point(point, "pick point")
+        r = self._pick_radius(radius)
+        if self._active_count == 0:
+            return None
+        index, oid = ctypes.c_uint32(), ctypes.c_uint32()
+        anchor = np.zeros(2, dtype=np.float32)
+        _check(self._lib.mpm_pick(self._handle, x, y, r, ctypes.byref(index), _lib.ptr(anchor), ctypes.byref(oid)),
+               "Failed to pick an MLS-MPM particle from GPU state.")
+        if index.value == 0xFFFFFFFF:
+            return None
+        rng = self._object_ranges.get(oid.value)
+        if rng is None or not rng[0] <= index.value < rng[0] + rng[1]:
+            raise RuntimeError("GPU returned an object id inconsistent with the selected particle.")
+        return {"particleIndex": int(index.value), "objectId": int(oid.value),
+                "anchor": {"x": float(anchor[0]), "y": float(anchor[1])}}
+
+    def begin_drag(self, selection, target, radius) -> None:
+        """beginDrag (solver.ts:2817-2829): a grid-node spring toward `target`
+        within `radius` (finishGridVelocity, shaders.ts:1757-1775)."""
+        self._assert_active()
+        self._resolve_selection(selection)
+        x, y = self._world_point(target, "drag target")
+        r = self._pick_radius(radius)
+        if r <= 0:
+            raise RangeError("drag radius must be greater than zero.")
+        self._write_drag(x, y, r)
+        self._active_drag = {"radius": r}
+
+    def update_drag(self, target) -> None:
+        """updateDrag (solver.ts:2831-2836)."""
+        self._assert_active()
+        if self._active_drag is None:
+            return
+        x, y = self._world_point(target, "drag target")
+        self._write_drag(x, y, self._active_drag["radius"])
 
     def end_drag(self) -> None:
-        self._assert_active()
-        _check(self._lib.mpm_set_drag(self._handle, None), "Failed to end the drag.")
+        """endDrag (solver.ts:2838-2843)."""
+        if self._active_drag is None:
+            return
         self._active_drag = None
+        if not self._disposed:
+            _check(self._lib.mpm_set_drag(self._handle, None), "Failed to end the drag.")
+
+    def _write_drag(self, x: float, y: float, radius: float) -> None:
+        drag = _lib.MpmDrag(x, y, radius, MPM_MLS_GPU_DRAG_STIFFNESS, MPM_MLS_GPU_DRAG_DAMPING)
+        _check(self._lib.mpm_set_drag(self._handle, ctypes.byref(drag)), "Failed to set the drag target.")
+
+    def append_particles(self, particles) -> dict:
+        """appendParticles, solver.ts:2108-2278: an emitter batch as a new
+        object; returns the reference's MpmMlsGpuAppendResult."""
+        self._assert_active()
+        if not isinstance(particles, (list, tuple)) and not hasattr(particles, "px"):
+            raise TypeError("particles must be an array of emitter particles.")
+        requested = len(particles)
+
+        def result(accepted, refused, dropped, velocity_bound=0.0, reason=None):
+            out = {"requested": requested, "accepted": accepted, "refused": refused, "dropped": dropped,
+                   "activeParticleCount": self._active_count, "allocatedParticleCount": self._slot_count,
+                   "capacity": self.particle_capacity, "velocityBound": velocity_bound}
+            if reason is not None:
+                out["reason"] = reason
+            return out
+
+        if requested == 0:
+            return result(0, 0, 0)
+        if self._cfl_speed_measurement_submitted:
+            return result(0, requested, 0, 0.0,
+                          "wait for the submitted CFL speed readback before emitting particles")
+        available = self.particle_capacity - self._slot_count
+        if available <= 0:
+            return result(0, 0, requested, 0.0, f"particle slot capacity {self.particle_capacity} is full")
+        if self._next_object_id > 0xFFFFFFFF:
+            return result(0, requested, 0, 0.0, "no object ids remain for a new emitter group")
+        object_id = self._next_object_id
+        arrays = particles if hasattr(particles, "px") else particles_from_dicts(particles)
+        if np.any(arrays.bonded_vertex >= 0):
+            return result(0, requested, 0, 0.0,
+                          "triangle-bonded particles cannot be appended without a complete object topology")
+        arrays = arrays.copy()
+        arrays.object_id[:] = object_id
+        cfg = dict(self._state.config, capacity=requested, fractureBonds=[])
+        try:
+            candidate = validate_mpm_mls_gpu_input(arrays, cfg)
+        except Exception as error:  # noqa: BLE001 - the reference reports any validation failure as a refusal
+            reason = str(error).strip() or "emitter particles failed GPU input validation"
+            return result(0, requested, 0, 0.0, reason)
+        if len(candidate.bonded_body_starts) > 0:
+            return result(0, requested, 0, 0.0,
+                          "triangle-bonded particles cannot be appended without a complete object topology")
+        accepted = min(requested, available)
+        additions = derive_mpm_mls_gpu_cfl_bounds(arrays.take(np.arange(accepted)), candidate.config)
+        if self.cfl_bounds is not None and additions is None:
+            return result(0, requested, 0, 0.0, "appended material has no safely derived CFL wave-speed bound")
+        packed = np.ascontiguousarray(candidate.packed_particles[:accepted], dtype=np.float32)
+        ids = np.full(accepted, object_id, dtype=np.uint32)
+        first = ctypes.c_uint32()
+        try:
+            _check(self._lib.mpm_append_particles(self._handle, _lib.ptr(packed), _lib.ptr(ids), accepted,
+                                                  ctypes.byref(first)),
+                   "Failed to append a validated GPU MLS-MPM emitter batch.")
+        except Exception:
+            self._cfl_state_usable = False
+            raise
+        self._object_ranges[object_id] = (int(first.value), accepted)
+        self._slot_count += accepted
+        self._active_count += accepted
+        self._next_object_id += 1
+        if additions is not None and self.cfl_bounds is not None:
+            self.cfl_bounds = dict(self.cfl_bounds,
+                                   waveSpeedBound=max(self.cfl_bounds["waveSpeedBound"], additions["waveSpeedBound"]),
+                                   velocityBound=max(self.cfl_bounds["velocityBound"], additions["velocityBound"]))
+            self._last_scheduled_velocity_bound = max(self._last_scheduled_velocity_bound or 0.0,
+                                                      additions["velocityBound"])
+        velocity_bound = additions["velocityBound"] if additions is not None else 0.0
+        return result(accepted, 0, requested - accepted, velocity_bound,
+                      None if requested == accepted else
+                      f"accepted only {accepted} of {requested}; GPU slot capacity is exhausted")
+
+    def remove_particles_in_outlet(self, bounds) -> int:
+        """removeParticlesInOutlet, solver.ts:2280-2386: removes the water and
+        oil particles inside the bounds; returns how many."""
+        self._assert_active()
+        if not isinstance(bounds, dict):
+            raise TypeError("outlet bounds must be an object.")
+        x0, y0 = self._world_point({"x": bounds.get("minX"), "y": bounds.get("minY")}, "outlet minimum")
+        x1, y1 = self._world_point({"x": bounds.get("maxX"), "y": bounds.get("maxY")}, "outlet maximum")
+        if x0 > x1 or y0 > y1:
+            raise RangeError("outlet minimum coordinates must not exceed the maximum.")
+        if self._slot_count == 0 or self._active_count == 0:
+            return 0
+        removed = ctypes.c_uint32()
+        try:
+            _check(self._lib.mpm_remove_particles_in_outlet(self._handle, x0, y0, x1, y1, ctypes.byref(removed)),
+                   "Failed to remove liquid particles from the GPU outlet region.")
+        except Exception:
+            self._cfl_state_usable = False
+            raise
+        if removed.value > self._active_count:
+            raise RuntimeError("GPU reported an outlet removal count above the active particle count.")
+        self._active_count -= removed.value
+        self._has_removed = self._has_removed or removed.value > 0
+        return int(removed.value)
+
+    def clone(self, selection, offset) -> bool:
+        """clone, solver.ts:2852-2940: a copy of the selected object moved by
+        `offset`; False when it cannot be placed."""
+        self._assert_active()
+        start, count = self._resolve_selection(selection)
+        if not isinstance(offset, dict):
+            raise TypeError("clone offset must be a vector.")
+        ox = _interaction_float32(offset.get("x"), "clone offset.x")
+        oy = _interaction_float32(offset.get("y"), "clone offset.y")
+        if self._has_removed or self._state.fracture_bond_count > 0 or len(self._state.bonded_body_starts) > 0:
+            return False
+        if count > self.particle_capacity - self._slot_count:
+            return False
+        if self._next_object_id > 0xFFFFFFFF:
+            raise RangeError("No unsigned 32-bit object ids remain for MLS-MPM cloning.")
+        object_id = self._next_object_id
+        self.end_drag()
+        first = ctypes.c_uint32()
+        _check(self._lib.mpm_clone_range(self._handle, start, count, ox, oy, object_id, ctypes.byref(first)),
+               "Failed to clone the selected MLS-MPM object on the GPU.")
+        self._object_ranges[object_id] = (int(first.value), count)
+        self._slot_count += count
+        self._active_count += count
+        self._next_object_id += 1
+        return True
 
     # ---------------------------------------------------------------- probes --
     def probe_sort(self, dt: float):
