@@ -216,6 +216,19 @@ int mpm_profile_substeps(mpm_solver *solver, uint32_t step_count, float dt, floa
 const char *mpm_profile_kernel_name(uint32_t slot);
 uint32_t mpm_profile_kernel_slots(void);
 
+/* Launch shape of the default path: the persistent grids (CTAs) of its P2G
+ * and G2P kernels; 0 keeps a value.  Results do not depend on it (every sum
+ * has a fixed order). */
+int mpm_set_launch_shape(mpm_solver *solver, uint32_t p2g_ctas, uint32_t g2p_ctas);
+int mpm_get_launch_shape(mpm_solver *solver, uint32_t *p2g_ctas, uint32_t *g2p_ctas, uint32_t *sm_count);
+
+/* The autotuner: times `substeps` real substeps of the last submit's
+ * parameters for each candidate grid (1 .. occupancy-limit CTAs per SM, and
+ * one CTA per tile), P2G first, then G2P with the best P2G, keeps the
+ * fastest, and restores the particle state and counters it started from.
+ * Needs one submitted batch.  Blocks. */
+int mpm_autotune(mpm_solver *solver, uint32_t substeps, uint32_t *p2g_ctas, uint32_t *g2p_ctas, double *best_ms);
+
 /* Nodes of the last substep with positive solid / water / oil mass. */
 int mpm_count_active_nodes(mpm_solver *solver, uint32_t counts[3]);
 

@@ -936,6 +936,58 @@ int create_impl(const mpm_config *configs, uint32_t n_scenes, const uint32_t *co
     return MPM_OK;
 }
 
+// Runs `step_count` real substeps with the uploaded parameters, captured in
+// one graph with an event after every kernel, and sums each kernel slot's
+// milliseconds and launches.
+int profile_run(mpm_solver *s, uint32_t step_count, bool guarded, double *kernel_ms, uint32_t *kernel_launches)
+{
+    for (int k = 0; k < K_SLOTS; ++k) {
+        kernel_ms[k] = 0.0;
+        kernel_launches[k] = 0;
+    }
+    Recorder rec;
+    rec.stream = s->stream;
+    const Ctx c0 = make_ctx(s, s->cur);
+    const int start_parity = s->cur;
+    CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    k_begin_batch<<<blocks_for(s->n_scenes, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c0, guarded ? 1u : 0u);
+    rec.mark(-1);
+    g_recorder = &rec;
+    if (s->gather() && s->n > 0) enqueue_tile_count(s, c0);
+    int parity = start_parity;
+    for (uint32_t k = 0; k < step_count; ++k) {
+        enqueue_substep(s, parity);
+        parity = 1 - parity;
+    }
+    if (s->n > 0) enqueue_end_batch(s, parity, step_count, guarded);
+    g_recorder = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+    if (e == cudaSuccess) e = rec.error;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e == cudaSuccess) {
+        s->cur = parity;
+        s->substeps_since_begin = step_count;
+    }
+    for (size_t k = 1; e == cudaSuccess && k < rec.events.size(); ++k) {
+        float ms = 0.0f;
+        e = cudaEventElapsedTime(&ms, rec.events[k - 1], rec.events[k]);
+        if (rec.slots[k] >= 0) {
+            kernel_ms[rec.slots[k]] += ms;
+            kernel_launches[rec.slots[k]] += 1;
+        }
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (cudaEvent_t ev : rec.events) cudaEventDestroy(ev);
+    if (e != cudaSuccess) return set_error(MPM_ERR_CUDA, "profiled substeps failed: %s", cudaGetErrorString(e));
+    return MPM_OK;
+}
+
+
 int run_batch(mpm_solver *s, uint32_t step_count, bool guarded);
 
 // After the particle count of a single-scene solver changed: its parameters
@@ -1113,49 +1165,147 @@ int mpm_profile_substeps(mpm_solver *s, uint32_t step_count, float dt, float gx,
     CUDA_TRY(cudaSetDevice(s->device));
     int rc = upload_params(s, dt, gx, gy, guard, 0.0f, step_count);
     if (rc != MPM_OK) return rc;
-    for (int k = 0; k < K_SLOTS; ++k) {
-        kernel_ms[k] = 0.0;
-        kernel_launches[k] = 0;
-    }
-    Recorder rec;
-    rec.stream = s->stream;
-    const Ctx c0 = make_ctx(s, s->cur);
-    const int start_parity = s->cur;
-    CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-    k_begin_batch<<<blocks_for(s->n_scenes, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c0, guard ? 1u : 0u);
-    rec.mark(-1);
-    g_recorder = &rec;
-    if (s->gather() && s->n > 0) enqueue_tile_count(s, c0);
-    int parity = start_parity;
-    for (uint32_t k = 0; k < step_count; ++k) {
-        enqueue_substep(s, parity);
-        parity = 1 - parity;
-    }
-    if (s->n > 0) enqueue_end_batch(s, parity, step_count, guard != nullptr);
-    g_recorder = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
-    if (e == cudaSuccess) e = rec.error;
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-    if (e == cudaSuccess) e = cudaGraphLaunch(exec, s->stream);
+    return profile_run(s, step_count, guard != nullptr, kernel_ms, kernel_launches);
+}
+
+int mpm_set_launch_shape(mpm_solver *s, uint32_t p2g_ctas, uint32_t g2p_ctas)
+{
+    g_last_error.clear();
+    if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
+    if (!s->gather()) return set_error(MPM_ERR_STATE, "launch shapes apply to the default P2G path");
+    if (p2g_ctas) s->p2g_ctas = p2g_ctas;
+    if (g2p_ctas) s->g2p_ctas = g2p_ctas;
+    for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    s->graphs.clear();
+    return MPM_OK;
+}
+
+int mpm_get_launch_shape(mpm_solver *s, uint32_t *p2g_ctas, uint32_t *g2p_ctas, uint32_t *sm_count)
+{
+    g_last_error.clear();
+    if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
+    int sms = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+    if (p2g_ctas) *p2g_ctas = s->p2g_ctas;
+    if (g2p_ctas) *g2p_ctas = s->g2p_ctas;
+    if (sm_count) *sm_count = (uint32_t)sms;
+    return MPM_OK;
+}
+
+int mpm_autotune(mpm_solver *s, uint32_t substeps, uint32_t *p2g_ctas, uint32_t *g2p_ctas, double *best_ms)
+{
+    g_last_error.clear();
+    if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
+    if (!s->gather()) return set_error(MPM_ERR_STATE, "launch shapes apply to the default P2G path");
+    if (!s->batch_timed) return set_error(MPM_ERR_STATE, "tune after a first batch (its parameters are reused)");
+    if (substeps < 1 || substeps > 64) return set_error(MPM_ERR_INVALID_ARGUMENT, "substeps must lie in [1, 64]");
+    if (s->n == 0) return set_error(MPM_ERR_STATE, "there are no particles to time");
+    CUDA_TRY(cudaSetDevice(s->device));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    // the state the trials start from, restored before each and at the end
+    const uint32_t n = s->n;
+    const int start = s->cur;
+    ParticleBuffers save{};
+    std::vector<uint32_t> dyn((size_t)s->n_scenes * SCENE_WORDS);
+    uint32_t *slots = nullptr;
+    cudaError_t e = dalloc(&save.pos, n);
+    if (e == cudaSuccess) e = dalloc(&save.vel, n);
+    if (e == cudaSuccess) e = dalloc(&save.C, n);
+    if (e == cudaSuccess) e = dalloc(&save.F, n);
+    if (e == cudaSuccess) e = dalloc(&save.pvol, n);
+    if (e == cudaSuccess) e = dalloc(&save.damage, n);
+    if (e == cudaSuccess) e = dalloc(&save.vol, n);
+    if (e == cudaSuccess) e = dalloc(&save.mat, n);
+    if (e == cudaSuccess) e = dalloc(&save.orig, n);
+    if (e == cudaSuccess && s->slot_of[0]) e = dalloc(&slots, s->allocated);
+    auto copy_buffers = [&](const ParticleBuffers &dst, const ParticleBuffers &src) {
+        const std::pair<void *, const void *> pairs[] = {{dst.pos, src.pos}, {dst.vel, src.vel}, {dst.C, src.C},
+                                                         {dst.F, src.F}, {dst.pvol, src.pvol},
+                                                         {dst.damage, src.damage}, {dst.vol, src.vol},
+                                                         {dst.mat, src.mat}, {dst.orig, src.orig}};
+        const size_t bytes[] = {sizeof(float2), sizeof(float2), sizeof(float4), sizeof(float4), sizeof(float),
+                                sizeof(float), sizeof(float), sizeof(uint32_t), sizeof(uint32_t)};
+        cudaError_t r = cudaSuccess;
+        for (int k = 0; k < 9 && r == cudaSuccess; ++k)
+            r = cudaMemcpyAsync(pairs[k].first, pairs[k].second, n * bytes[k], cudaMemcpyDeviceToDevice, s->stream);
+        return r;
+    };
+    auto restore = [&]() {
+        cudaError_t r = copy_buffers(s->buf[start], save);
+        if (r == cudaSuccess)
+            r = cudaMemcpyAsync(s->dyn, dyn.data(), dyn.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream);
+        if (r == cudaSuccess && slots)
+            r = cudaMemcpyAsync(s->slot_of[start], slots, s->allocated * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                                s->stream);
+        if (r == cudaSuccess) r = cudaStreamSynchronize(s->stream);
+        s->cur = start;
+        return r;
+    };
+    if (e == cudaSuccess) e = copy_buffers(save, s->buf[start]);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dyn.data(), s->dyn, dyn.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess && slots)
+        e = cudaMemcpyAsync(slots, s->slot_of[start], s->allocated * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                            s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
-    if (e == cudaSuccess) {
-        s->cur = parity;
-        s->substeps_since_begin = step_count;
+    // the last submit's parameters, `substeps` for every scene that took part
+    for (uint32_t k = 0; k < s->n_scenes; ++k)
+        if (s->h_params[k].batch_steps > 0) s->h_params[k].batch_steps = substeps;
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->d_params, s->h_params, s->n_scenes * sizeof(StepParams), cudaMemcpyHostToDevice,
+                            s->stream);
+    int sms = 0, per_sm_p2g = 1, per_sm_g2p = 1;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_p2g, k_p2g_gather<false>, TILE_CELLS, 0);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_g2p, k_g2p_tile<false, false>, G2P_THREADS, 0);
+    int rc = e == cudaSuccess ? MPM_OK : set_error(MPM_ERR_CUDA, "autotune set-up failed: %s", cudaGetErrorString(e));
+    const bool guarded = s->h_params[0].cfl_enabled != 0u;
+    auto trial = [&](unsigned p, unsigned g, double &p_ms, double &g_ms) {
+        s->p2g_ctas = p;
+        s->g2p_ctas = g;
+        const cudaError_t r = restore();
+        if (r != cudaSuccess) return set_error(MPM_ERR_CUDA, "autotune restore failed: %s", cudaGetErrorString(r));
+        double ms[K_SLOTS];
+        uint32_t launches[K_SLOTS];
+        const int prc = profile_run(s, substeps, guarded, ms, launches);
+        p_ms = ms[K_P2G_GATHER];
+        g_ms = ms[K_G2P_TILE];
+        return prc;
+    };
+    const unsigned p0 = s->p2g_ctas, g0 = s->g2p_ctas;
+    unsigned best_p = p0, best_g = g0;
+    double best_p_ms = 1e300, best_g_ms = 1e300;
+    // P2G and G2P are separate launches, tuned one after the other: persistent
+    // grids of 1 .. (occupancy limit) CTAs per SM, and one CTA per tile
+    const unsigned tiles = std::max(1u, s->n_tiles_total);
+    for (int k = 1; rc == MPM_OK && k <= std::max(1, per_sm_p2g) + 1; ++k) {
+        const unsigned p = k <= per_sm_p2g ? std::min(tiles, (unsigned)(sms * k)) : tiles;
+        double pm = 0, gm = 0;
+        rc = trial(p, g0, pm, gm);
+        if (rc == MPM_OK && pm < best_p_ms) best_p_ms = pm, best_p = p;
     }
-    for (size_t k = 1; e == cudaSuccess && k < rec.events.size(); ++k) {
-        float ms = 0.0f;
-        e = cudaEventElapsedTime(&ms, rec.events[k - 1], rec.events[k]);
-        if (rec.slots[k] >= 0) {
-            kernel_ms[rec.slots[k]] += ms;
-            kernel_launches[rec.slots[k]] += 1;
-        }
+    for (int k = 1; rc == MPM_OK && k <= std::max(1, per_sm_g2p) + 1; ++k) {
+        const unsigned g = k <= per_sm_g2p ? std::min(tiles, (unsigned)(sms * k)) : tiles;
+        double pm = 0, gm = 0;
+        rc = trial(best_p, g, pm, gm);
+        if (rc == MPM_OK && gm < best_g_ms) best_g_ms = gm, best_g = g;
     }
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
-    for (cudaEvent_t ev : rec.events) cudaEventDestroy(ev);
-    if (e != cudaSuccess) return set_error(MPM_ERR_CUDA, "profiled substeps failed: %s", cudaGetErrorString(e));
+    const cudaError_t r = restore();
+    if (rc == MPM_OK && r != cudaSuccess) rc = set_error(MPM_ERR_CUDA, "autotune restore failed: %s", cudaGetErrorString(r));
+    void *ptrs[] = {save.pos, save.vel, save.C, save.F, save.pvol, save.damage, save.vol, save.mat, save.orig, slots};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    s->p2g_ctas = rc == MPM_OK ? best_p : p0;
+    s->g2p_ctas = rc == MPM_OK ? best_g : g0;
+    for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    s->graphs.clear();
+    s->batch_timed = false;  // the batch events now time the trials
+    if (rc != MPM_OK) return rc;
+    if (p2g_ctas) *p2g_ctas = best_p;
+    if (g2p_ctas) *g2p_ctas = best_g;
+    if (best_ms) *best_ms = (best_p_ms + best_g_ms) / substeps;
     return MPM_OK;
 }
 

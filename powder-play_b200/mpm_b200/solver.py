@@ -754,6 +754,23 @@ class MpmMlsGpuSolver:
                 "normal": raw[:, 2:4].reshape(h, w, 2),
                 "bary": np.stack([1.0 - b1 - b2, b1, b2], axis=1).reshape(h, w, 3)}
 
+    def launch_shape(self) -> dict:
+        """The persistent grids of the default path's P2G and G2P kernels."""
+        p, g, sms = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        _check(self._lib.mpm_get_launch_shape(self._handle, ctypes.byref(p), ctypes.byref(g), ctypes.byref(sms)),
+               "launch shape read failed")
+        return {"p2gCtas": int(p.value), "g2pCtas": int(g.value), "smCount": int(sms.value)}
+
+    def autotune(self, substeps: int = 8) -> dict:
+        """Picks the fastest persistent grids for P2G and G2P on this
+        workload (mpm_autotune: real substeps timed per candidate, the state
+        restored); call after a first batch."""
+        self._assert_active()
+        p, g, ms = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_double()
+        _check(self._lib.mpm_autotune(self._handle, int(substeps), ctypes.byref(p), ctypes.byref(g), ctypes.byref(ms)),
+               "autotune failed")
+        return {"p2gCtas": int(p.value), "g2pCtas": int(g.value), "transferMsPerSubstep": float(ms.value)}
+
     def dispose(self) -> None:
         if self._disposed:
             return

@@ -180,3 +180,28 @@ def test_crowded_scenes_match_solo_runs_bit_for_bit():
     finally:
         batch.dispose()
 
+
+
+def test_autotuned_launch_shape_changes_no_result():
+    scenes = _small_scenes(4, seed=13)
+    dts = None
+    results = []
+    for tune in (False, True):
+        batch = create_mpm_batched_gpu_solver(scenes)
+        try:
+            dts = [_micro_dt(batch.cfl_bounds[k], scenes[k][1], 0.5) for k in range(batch.scene_count)]
+            batch.step_batch([3] * batch.scene_count, dts, BATCHED_TANK_GRAVITY)
+            if tune:
+                before = [batch.read_particles_packed(k)[0] for k in range(batch.scene_count)]
+                shape = batch.autotune(substeps=4)
+                assert shape["p2gCtas"] >= 1 and shape["g2pCtas"] >= 1
+                assert batch.launch_shape()["p2gCtas"] == shape["p2gCtas"]
+                # the tuner restored the state it started from
+                for k in range(batch.scene_count):
+                    assert np.array_equal(_bits(batch.read_particles_packed(k)[0]), _bits(before[k]))
+            batch.step_batch([5] * batch.scene_count, dts, BATCHED_TANK_GRAVITY)
+            results.append([batch.read_particles_packed(k)[0] for k in range(batch.scene_count)])
+        finally:
+            batch.dispose()
+    for a, b in zip(*results):
+        assert np.array_equal(_bits(a), _bits(b))
