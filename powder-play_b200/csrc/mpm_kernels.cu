@@ -2,7 +2,7 @@
 //
 // Substep, default P2G (the role of the reference's gather path,
 // src/lib/mpm/kernels/solver.ts:1465-1570):
-//   k_tile_scan (starts the substep) -> k_tile_scatter -> k_p2g_gather
+//   k_tile_alloc (starts the substep) -> k_tile_scatter -> k_p2g_gather
 //   -> k_g2p_tile (grid update + G2P + next substep's tile counts)
 //   (k_begin_batch and k_tile_count run once at the start of a batch)
 // The cell sort (k_count, k_scan_*, k_scatter, k_stable_rank) backs the sort
@@ -249,6 +249,15 @@ __device__ __forceinline__ bool begin_substep(const Ctx &c)
     return runs;
 }
 
+// begin_substep's answer without its effects: whether the scene runs the
+// substep about to start, from the counters and status as they are before it.
+__device__ __forceinline__ bool substep_runs(const Ctx &c)
+{
+    const uint32_t *k = c.counters;
+    const uint32_t sub = k[COUNTER_FRESH] != 0u ? k[COUNTER_SUBSTEP] : k[COUNTER_SUBSTEP] + 1u;
+    return *(volatile uint32_t *)c.status == 0u && sub < c.P->batch_steps;
+}
+
 // Substeps completed in a batch of `total` substeps, at its end (the same
 // answer however often it is asked).
 __device__ __forceinline__ uint32_t batch_stop(const Ctx &c, uint32_t total)
@@ -314,32 +323,32 @@ __device__ __forceinline__ uint32_t warp_sum(uint32_t v)
 }
 
 // Block-wide exclusive scan of one value per thread (blockDim multiple of 32).
-template <int THREADS>
-__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t &total)
+template <int THREADS, class T = uint32_t>
+__device__ __forceinline__ T block_exclusive_scan(T v, T &total)
 {
-    __shared__ uint32_t warp_totals[THREADS / 32];
-    __shared__ uint32_t s_total;
+    __shared__ T warp_totals[THREADS / 32];
+    __shared__ T s_total;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t inc = v;
+    T inc = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        uint32_t n = __shfl_up_sync(0xffffffffu, inc, o);
+        T n = __shfl_up_sync(0xffffffffu, inc, o);
         if (lane >= o) inc += n;
     }
     if (lane == 31) warp_totals[warp] = inc;
     __syncthreads();
     if (warp == 0) {
-        uint32_t w = lane < THREADS / 32 ? warp_totals[lane] : 0u;
-        uint32_t wi = w;
+        T w = lane < THREADS / 32 ? warp_totals[lane] : T(0);
+        T wi = w;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            uint32_t n = __shfl_up_sync(0xffffffffu, wi, o);
+            T n = __shfl_up_sync(0xffffffffu, wi, o);
             if (lane >= o) wi += n;
         }
         if (lane < THREADS / 32) warp_totals[lane] = wi - w;
     }
     __syncthreads();
-    const uint32_t warp_offset = warp_totals[warp];
+    const T warp_offset = warp_totals[warp];
     if (threadIdx.x == THREADS - 1) s_total = warp_offset + inc;
     __syncthreads();
     total = s_total;
@@ -377,6 +386,7 @@ __global__ void k_begin_batch(Ctx c, uint32_t reset_progress)
         counters[COUNTER_SUBSTEP] = 0u;
         counters[COUNTER_FRESH] = 1u;
         counters[COUNTER_STOP] = STOP_NONE;
+        counters[COUNTER_CURSOR] = c.scenes[s].p_base;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         c.work[WORK_ACTIVE] = 0u;
@@ -723,104 +733,132 @@ __global__ void k_tile_count(Ctx c0)
     c.keys[i] = key;
 }
 
-// The first kernel of a substep of the default path, one CTA per scene:
-// starts the scene's substep (begin_substep), then the exclusive scan of its
-// tile counts, 8 consecutive tiles per thread and pass (vector loads and
-// stores), ending in the scene's sentinel entry; the scene's tiles holding
-// particles join the substep's tile list (ascending; with several scenes a
-// range of the list is reserved per pass); zeroes the counts for the next
-// substep.  A scene that does not take part lists no tile (the counts are
-// cleared at the start of every batch).  CTA 0 empties the tile list of the
-// next substep (the other buffer parity).
-__global__ void __launch_bounds__(SCAN_TOP_THREADS) k_tile_scan(Ctx c0)
+// The scene of allocation CTA b: scene_chunk[scene] <= b < scene_chunk[scene + 1].
+__device__ __forceinline__ uint32_t scene_of_chunk(const Ctx &c, uint32_t b)
 {
-    constexpr int ITEMS = 8;
-    constexpr uint32_t PASS = SCAN_TOP_THREADS * ITEMS;
+    uint32_t lo = 0, hi = c.n_scenes;
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) / 2u;
+        if (c.scene_chunk[mid] <= b)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Whether scene `scene` takes part in the substep under way, as k_tile_alloc
+// found it (read while k_tile_scatter starts the substep).
+__device__ __forceinline__ bool runs_flag(const Ctx &c, uint32_t scene)
+{
+    return __ldcg(c.dyn + (size_t)scene * SCENE_WORDS + 32 + COUNTER_RUNS) != 0u;
+}
+
+// The first kernel of a substep of the default path: each CTA takes 1024
+// consecutive tiles of one scene (4 per thread, vector loads and stores),
+// and, when the scene runs the substep, gives each of its tiles holding
+// particles a range of the scene's bucket entries -- one atomic per CTA on
+// the scene's cursor, so the ranges of different CTAs lie in the order the
+// CTAs got there -- and a place in the substep's tile list (one atomic per
+// CTA on the list size), and zeroes the counts for the next substep.  Every
+// CTA reads whether the scene runs (substep_runs) and stores the answer in
+// the scene's counters; k_tile_scatter then starts the substep
+// (begin_substep) and resets the cursor.  A scene that does not take part
+// lists no tile (the counts are cleared at the start of every batch).  CTA
+// 0 empties the tile list of the next substep (the other buffer parity).
+// Neither the order of the bucket ranges nor that of the list changes any
+// sum: P2G orders each tile's particles by cell, channel and original index.
+__global__ void __launch_bounds__(ALLOC_THREADS) k_tile_alloc(Ctx c0)
+{
+    __shared__ uint32_t s_base[2];
     __shared__ bool s_runs;
-    __shared__ uint32_t s_list;
-    const Ctx c = scene_ctx(c0, blockIdx.x);
-    uint32_t *list_size = c0.work + WORK_ACTIVE + c0.parity;
+    const bool one_scene = c0.n_scenes == 1u;
+    const uint32_t scene = one_scene ? 0u : scene_of_chunk(c0, blockIdx.x);
+    const uint32_t chunk = one_scene ? blockIdx.x : blockIdx.x - c0.scene_chunk[scene];
+    const Ctx c = scene_ctx(c0, scene);
+    const StepParams &P = *c.P;
     if (threadIdx.x == 0) {
-        s_runs = begin_substep(c);
+        const bool runs = substep_runs(c);
+        s_runs = runs;
+        c.counters[COUNTER_RUNS] = runs ? 1u : 0u;  // the same value from every CTA of the scene
         if (blockIdx.x == 0) c0.work[WORK_ACTIVE + (c0.parity ^ 1u)] = 0u;
     }
-    __syncthreads();
-    if (!s_runs) return;  // the same answer for every thread of the CTA
-    const StepParams &P = *c.P;
-    const bool one_scene = c0.n_scenes == 1u;
+    // the counts are read before the answer is known (they exist either way)
     uint32_t *count = c.tile_count + P.tile_base;  // 32-byte aligned: scenes start on 8-tile boundaries
-    uint32_t *start = c.tile_start + P.tile_base;
     const uint32_t n_tiles = P.scene_tiles;
-    uint32_t running = P.p_base, listed = 0;
-    for (uint32_t base = 0; base < n_tiles; base += PASS) {
-        const uint32_t first = base + threadIdx.x * ITEMS;
-        const bool whole = first + ITEMS <= n_tiles;
-        uint32_t v[ITEMS];
-        if (whole) {
-            const uint4 a = *reinterpret_cast<const uint4 *>(count + first);
-            const uint4 b = *reinterpret_cast<const uint4 *>(count + first + 4);
-            v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
-        } else {
+    const uint32_t first = chunk * ALLOC_TILES + threadIdx.x * ALLOC_ITEMS;
+    const bool whole = first + ALLOC_ITEMS <= n_tiles;
+    uint32_t v[ALLOC_ITEMS];
+    if (whole) {
+        const uint4 a = *reinterpret_cast<const uint4 *>(count + first);
+        v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w;
+    } else {
 #pragma unroll
-            for (int k = 0; k < ITEMS; ++k) v[k] = first + k < n_tiles ? count[first + k] : 0u;
-        }
+        for (int k = 0; k < ALLOC_ITEMS; ++k) v[k] = first + k < n_tiles ? count[first + k] : 0u;
+    }
+    __syncthreads();
+    if (s_runs) {
+        uint2 *range = c.tile_range + P.tile_base;
         uint32_t sum = 0, nonempty = 0;
 #pragma unroll
-        for (int k = 0; k < ITEMS; ++k) {
+        for (int k = 0; k < ALLOC_ITEMS; ++k) {
             sum += v[k];
             nonempty += v[k] != 0u;
         }
-        uint32_t total, total_active;
-        const uint32_t offset = running + block_exclusive_scan<SCAN_TOP_THREADS>(sum, total);
-        const uint32_t rank = block_exclusive_scan<SCAN_TOP_THREADS>(nonempty, total_active);
-        if (!one_scene) {
-            if (threadIdx.x == 0) s_list = total_active ? atomicAdd(list_size, total_active) : 0u;
-            __syncthreads();
+        // particles in the high word, listed tiles (at most 1024) in the low
+        unsigned long long total;
+        const unsigned long long offset =
+            block_exclusive_scan<ALLOC_THREADS, unsigned long long>(((unsigned long long)sum << 32) | nonempty, total);
+        if (threadIdx.x == 0) {
+            const uint32_t particles = (uint32_t)(total >> 32), listed = (uint32_t)total;
+            s_base[0] = particles ? atomicAdd(c.counters + COUNTER_CURSOR, particles) : 0u;
+            s_base[1] = listed ? atomicAdd(c0.work + WORK_ACTIVE + c0.parity, listed) : 0u;
         }
-        uint32_t slot = (one_scene ? listed : s_list) + rank;
-        listed += total_active;
-        uint32_t st[ITEMS];
-        uint32_t acc = offset;
+        __syncthreads();
+        uint32_t at = s_base[0] + (uint32_t)(offset >> 32);
+        uint32_t slot = s_base[1] + (uint32_t)offset;
+        uint2 r[ALLOC_ITEMS];
 #pragma unroll
-        for (int k = 0; k < ITEMS; ++k) {
-            st[k] = acc;
-            acc += v[k];
+        for (int k = 0; k < ALLOC_ITEMS; ++k) {
+            r[k] = make_uint2(at, v[k]);
+            at += v[k];
         }
         if (whole) {
-            *reinterpret_cast<uint4 *>(start + first) = make_uint4(st[0], st[1], st[2], st[3]);
-            *reinterpret_cast<uint4 *>(start + first + 4) = make_uint4(st[4], st[5], st[6], st[7]);
+            *reinterpret_cast<uint4 *>(range + first) = make_uint4(r[0].x, r[0].y, r[1].x, r[1].y);
+            *reinterpret_cast<uint4 *>(range + first + 2) = make_uint4(r[2].x, r[2].y, r[3].x, r[3].y);
             *reinterpret_cast<uint4 *>(count + first) = make_uint4(0u, 0u, 0u, 0u);
-            *reinterpret_cast<uint4 *>(count + first + 4) = make_uint4(0u, 0u, 0u, 0u);
         } else {
 #pragma unroll
-            for (int k = 0; k < ITEMS; ++k) {
+            for (int k = 0; k < ALLOC_ITEMS; ++k) {
                 if (first + k < n_tiles) {
-                    start[first + k] = st[k];
+                    range[first + k] = r[k];
                     count[first + k] = 0u;
                 }
             }
         }
         if (nonempty) {
 #pragma unroll
-            for (int k = 0; k < ITEMS; ++k)
+            for (int k = 0; k < ALLOC_ITEMS; ++k)
                 if (v[k] != 0u) c.active_tiles[slot++] = P.tile_base + first + k;
         }
-        running += total;
-        if (!one_scene) __syncthreads();  // s_list is rewritten by the next pass
-    }
-    if (threadIdx.x == 0) {
-        start[n_tiles] = running;
-        if (one_scene) *list_size = listed;
     }
 }
 
-// Bucket the slots by tile: perm[tile start + rank] = slot, four slots per
-// thread, for the scenes taking part in the substep.  The status word is read
-// along with the keys (no launch in this kernel writes it): keys and ranks of
-// a failed substep may be stale.  With several scenes, a warp whose slots
-// lie in one scene asks once whether that scene takes part.
+// Bucket the slots by tile: perm[first entry of the tile + rank] = slot,
+// four slots per thread, for the scenes taking part in the substep (the
+// answer k_tile_alloc stored).  The first threads of CTA 0 start the substep
+// of every scene (begin_substep) and reset the scenes' bucket cursors.  With
+// several scenes, a warp whose slots lie in one scene asks once whether that
+// scene takes part.
 __global__ void k_tile_scatter(Ctx c)
 {
+    if (blockIdx.x == 0) {
+        for (uint32_t s = threadIdx.x; s < c.n_scenes; s += blockDim.x) {
+            const Ctx cs = scene_ctx(c, s);
+            begin_substep(cs);
+            cs.counters[COUNTER_CURSOR] = cs.P->p_base;
+        }
+    }
     const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) * 4u;
     if (c.n_scenes > 1u) {
         const uint32_t first = min(i, c.n - 1u);
@@ -829,30 +867,29 @@ __global__ void k_tile_scatter(Ctx c)
         const uint32_t end = c.scene_p_base[lead + 1u];
         const uint32_t warp_last = min(((blockIdx.x * blockDim.x + (threadIdx.x | 31u)) * 4u) + 3u, c.n - 1u);
         const bool one = __shfl_sync(0xffffffffu, warp_last, 31) < end;
-        if (one && !takes_part(scene_ctx(c, lead))) return;
+        if (one && !runs_flag(c, lead)) return;
         if (i >= c.n) return;
         for (uint32_t j = i; j < min(i + 4u, c.n); ++j) {
-            if (!one && !takes_part(scene_ctx(c, scene_of_slot(c, j)))) continue;
-            c.perm[c.tile_start[c.keys[j]] + c.ranks[j]] = j;
+            if (!one && !runs_flag(c, scene_of_slot(c, j))) continue;
+            c.perm[c.tile_range[c.keys[j]].x + c.ranks[j]] = j;
         }
         return;
     }
     if (i >= c.n) return;
-    const bool runs = __ldcg(c.counters + COUNTER_SUBSTEP) < c.P->batch_steps;
-    const uint32_t status = __ldcg(c.status);
+    const bool runs = runs_flag(c, 0u);
     if (i + 4u <= c.n) {
         const uint4 key = __ldcs(reinterpret_cast<const uint4 *>(c.keys + i));
         const uint4 rank = __ldcs(reinterpret_cast<const uint4 *>(c.ranks + i));
-        if (status != 0u || !runs) return;
-        const uint32_t s0 = c.tile_start[key.x], s1 = c.tile_start[key.y], s2 = c.tile_start[key.z],
-                       s3 = c.tile_start[key.w];
+        if (!runs) return;
+        const uint32_t s0 = c.tile_range[key.x].x, s1 = c.tile_range[key.y].x, s2 = c.tile_range[key.z].x,
+                       s3 = c.tile_range[key.w].x;
         c.perm[s0 + rank.x] = i;
         c.perm[s1 + rank.y] = i + 1u;
         c.perm[s2 + rank.z] = i + 2u;
         c.perm[s3 + rank.w] = i + 3u;
     } else {
-        if (status != 0u || !runs) return;
-        for (uint32_t j = i; j < c.n; ++j) c.perm[c.tile_start[c.keys[j]] + c.ranks[j]] = j;
+        if (!runs) return;
+        for (uint32_t j = i; j < c.n; ++j) c.perm[c.tile_range[c.keys[j]].x + c.ranks[j]] = j;
     }
 }
 
@@ -1040,7 +1077,8 @@ __global__ void __launch_bounds__(TILE_CELLS) k_p2g_gather(Ctx c0)
         const uint32_t tile = c0.active_tiles[item];
         const Ctx c = tile_ctx<SCENES>(c0, tile);
         const uint32_t stamp = c.counters[COUNTER_STAMP];
-        const uint32_t begin = c.tile_start[tile], n_tile = c.tile_start[tile + 1] - begin;
+        const uint2 range = c.tile_range[tile];
+        const uint32_t begin = range.x, n_tile = range.y;
         __syncthreads();  // the previous tile's readers of sm are done
         for (int k = threadIdx.x; k < ACC_WORDS * RING_NODES; k += TILE_CELLS) (&sm.acc[0][0])[k] = 0.f;
         if (threadIdx.x == 0) {
@@ -1867,7 +1905,8 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
         const uint32_t local = tile - P.tile_base;
         const int tx = (int)(local % P.tiles_x), ty = (int)(local / P.tiles_x);
         const int x0 = tx * TILE_X, y0 = ty * TILE_Y;
-        const uint32_t begin = c.tile_start[tile], end = c.tile_start[tile + 1];
+        const uint2 range = c.tile_range[tile];
+        const uint32_t begin = range.x, end = range.x + range.y;
         __syncthreads();  // readers of the previous tile's shared data are done
         if (threadIdx.x < 9) {
             const int sx = tx + (int)(threadIdx.x % 3) - 1, sy = ty + (int)(threadIdx.x / 3) - 1;
@@ -1994,7 +2033,7 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
     if constexpr (!SCENES) flush_active_nodes(c0.counters, ws, ww, wo);
 }
 
-// The start of a substep of the fixed-point path (k_tile_scan starts those
+// The start of a substep of the fixed-point path (k_tile_alloc starts those
 // of the default path): begin_substep for every scene.
 __global__ void k_substep_begin(Ctx c)
 {

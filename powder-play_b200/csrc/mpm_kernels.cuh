@@ -81,8 +81,9 @@ struct Ctx {
     uint32_t count_next;  // G2P also counts the next substep's tiles
     // tile buckets and the per-tile partial node sums of the default P2G
     uint32_t *tile_count;
-    uint32_t *tile_start;    // n_tiles + 1
-    uint32_t *active_tiles;  // tiles holding particles this substep, ascending
+    uint2 *tile_range;       // per tile listed this substep: first bucket entry, particles
+    uint32_t *active_tiles;  // tiles holding particles this substep
+    const uint32_t *scene_chunk;  // per scene: its first CTA of k_tile_alloc, then the CTA total
     float *part;             // per tile: ACC_WORDS x RING_NODES sums, word-major
     uint2 *tile_info;        // per tile: (substep stamp of the sums, channel mask)
     // P2G records of the particles in the input slots, written by the batch
@@ -121,6 +122,9 @@ constexpr int SCAN_THREADS = 512;
 constexpr int SCAN_ITEMS = 8;
 constexpr int SCAN_CHUNK = SCAN_THREADS * SCAN_ITEMS;
 constexpr int SCAN_TOP_THREADS = 1024;
+constexpr int ALLOC_THREADS = 256;  // k_tile_alloc: 4 tiles per thread, 1024 per CTA
+constexpr int ALLOC_ITEMS = 4;
+constexpr uint32_t ALLOC_TILES = ALLOC_THREADS * ALLOC_ITEMS;
 
 // default P2G: the particles whose base node lies in one 16x8-node tile reach
 // the 18x10 nodes of its ring (the tile plus two columns and two rows)
@@ -146,6 +150,8 @@ constexpr int COUNTER_ACTIVE = 4;        // [4..6] active solid/water/oil nodes 
 constexpr int COUNTER_SUBSTEP = 8;       // the substep of this batch under way (failed and skipped included)
 constexpr int COUNTER_FRESH = 9;         // 1 from the start of a batch until its first substep starts
 constexpr int COUNTER_STOP = 10;         // substeps completed in this batch (STOP_NONE while running)
+constexpr int COUNTER_CURSOR = 11;       // the next free bucket entry of the scene (k_tile_alloc)
+constexpr int COUNTER_RUNS = 12;         // the scene takes part in the substep under way (k_tile_alloc)
 constexpr uint32_t STOP_NONE = 0xffffffffu;
 constexpr int SCENE_WORDS = 64;  // per scene: status [0, 32), counters [32, 64)
 constexpr int WORK_ACTIVE = 0;   // work[0], work[1]: tiles listed for the substeps from buffer 0 / 1
@@ -157,7 +163,7 @@ __global__ void k_scan_apply(Ctx c, uint32_t n_chunks);
 __global__ void k_scatter(Ctx c);
 __global__ void k_stable_rank(Ctx c);
 __global__ void k_tile_count(Ctx c);
-__global__ void k_tile_scan(Ctx c);
+__global__ void k_tile_alloc(Ctx c);
 __global__ void k_tile_scatter(Ctx c);
 // SCENES: the solver holds several scenes
 template <bool SCENES>

@@ -119,7 +119,10 @@ struct mpm_solver {
     float4 *g_water = nullptr, *g_oil = nullptr;
     int32_t *fixed = nullptr;
     uint32_t *tile_stamp = nullptr;
-    uint32_t *tile_count = nullptr, *tile_start = nullptr, *active_tiles = nullptr;
+    uint32_t *tile_count = nullptr, *active_tiles = nullptr;
+    uint2 *tile_range = nullptr;
+    uint32_t *scene_chunk = nullptr;  // per scene: first CTA of k_tile_alloc, then the total
+    uint32_t alloc_ctas = 1;
     float *part = nullptr;
     uint2 *tile_info = nullptr;
     float4 *rec_state = nullptr, *rec_affine = nullptr;
@@ -189,7 +192,8 @@ Ctx make_ctx(mpm_solver *s, int parity)
     c.fixed = s->fixed;
     c.tile_stamp = s->tile_stamp;
     c.tile_count = s->tile_count;
-    c.tile_start = s->tile_start;
+    c.tile_range = s->tile_range;
+    c.scene_chunk = s->scene_chunk;
     c.active_tiles = s->active_tiles;
     c.part = s->part;
     c.tile_info = s->tile_info;
@@ -221,11 +225,11 @@ constexpr unsigned PARTICLE_THREADS = 256;
 
 // Kernel slots of the profiled substep (mpm_profile_substeps).
 enum KernelSlot {
-    K_TILE_COUNT, K_TILE_SCAN, K_TILE_SCATTER, K_P2G_GATHER, K_G2P_TILE, K_PREPARE_SCATTER,
+    K_TILE_COUNT, K_TILE_ALLOC, K_TILE_SCATTER, K_P2G_GATHER, K_G2P_TILE, K_PREPARE_SCATTER,
     K_FIXED_DECODE, K_GRID_UPDATE, K_G2P, K_SUBSTEP_BEGIN, K_END_BATCH, K_SLOTS
 };
 const char *const KERNEL_NAMES[K_SLOTS] = {
-    "k_tile_count", "k_tile_scan", "k_tile_scatter", "k_p2g_gather", "k_g2p_tile", "k_prepare_scatter",
+    "k_tile_count", "k_tile_alloc", "k_tile_scatter", "k_p2g_gather", "k_g2p_tile", "k_prepare_scatter",
     "k_fixed_decode", "k_grid_update", "k_g2p", "k_substep_begin", "k_end_batch"};
 
 // When set, an event is recorded after every kernel launch so that the
@@ -310,8 +314,8 @@ void enqueue_substep(mpm_solver *s, int parity)
     const unsigned pb = blocks_for(s->n, PARTICLE_THREADS);
     const dim3 tiles(s->tiles_x, s->tiles_y);
     if (s->gather()) {
-        k_tile_scan<<<s->n_scenes, SCAN_TOP_THREADS, 0, s->stream>>>(c);
-        mark(K_TILE_SCAN);
+        k_tile_alloc<<<s->alloc_ctas, ALLOC_THREADS, 0, s->stream>>>(c);
+        mark(K_TILE_ALLOC);
         k_tile_scatter<<<blocks_for((s->n + 3) / 4, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c);
         mark(K_TILE_SCATTER);
         if (s->n_scenes > 1)
@@ -598,7 +602,7 @@ void free_solver(mpm_solver *s)
     void *ptrs[] = {s->d_params, s->dyn, s->work, s->tile_scene, s->scene_p_base, s->bonded, s->obj, s->d_mats, s->keys, s->ranks,
                     s->tmp, s->perm, s->cell_count, s->cell_start, s->block_sums, s->p2g_solid, s->p2g_water,
                     s->p2g_oil, s->g_solid, s->g_water, s->g_oil, s->fixed, s->tile_stamp, s->d_active,
-                    s->tile_count, s->tile_start, s->active_tiles, s->part, s->tile_info,
+                    s->tile_count, s->tile_range, s->scene_chunk, s->active_tiles, s->part, s->tile_info,
                     s->rec_state, s->rec_affine, s->rec_mom, s->rec_cell, s->field, s->body_starts,
                     s->slot_of[0], s->slot_of[1], s->track_flag, s->tracked, s->pair_cache, s->contact_count,
                     s->body_vel, s->bonds, s->topology, s->endpoints};
@@ -801,20 +805,28 @@ int create_impl(const mpm_config *configs, uint32_t n_scenes, const uint32_t *co
     ALLOC(s->d_active, 4);
     const size_t n_tiles = s->n_tiles_total;
     ALLOC(s->tile_count, n_tiles);
-    ALLOC(s->tile_start, n_tiles + 1);
+    ALLOC(s->tile_range, n_tiles);
     ALLOC(s->tile_scene, n_tiles);
+    ALLOC(s->scene_chunk, (size_t)n_scenes + 1);
     {
-        std::vector<uint32_t> tile_scene(n_tiles, 0u), p_bases(n_scenes + 1);
+        std::vector<uint32_t> tile_scene(n_tiles, 0u), p_bases(n_scenes + 1), chunks(n_scenes + 1);
+        uint32_t chunk = 0;
         for (uint32_t k = 0; k < n_scenes; ++k) {
             const SceneHost &sc = s->scenes[k];
             const uint32_t end = k + 1 < n_scenes ? s->scenes[k + 1].tile_base : (uint32_t)n_tiles;
             for (uint32_t t = sc.tile_base; t < end; ++t) tile_scene[t] = k;
             p_bases[k] = sc.p_base;
+            chunks[k] = chunk;
+            chunk += (sc.tiles + ALLOC_TILES - 1) / ALLOC_TILES;
         }
         p_bases[n_scenes] = count;
+        chunks[n_scenes] = chunk;
+        s->alloc_ctas = chunk;
         if (cudaMemcpy(s->tile_scene, tile_scene.data(), n_tiles * sizeof(uint32_t), cudaMemcpyHostToDevice) !=
                 cudaSuccess ||
             cudaMemcpy(s->scene_p_base, p_bases.data(), (n_scenes + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice) !=
+                cudaSuccess ||
+            cudaMemcpy(s->scene_chunk, chunks.data(), (n_scenes + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice) !=
                 cudaSuccess)
             return fail(set_error(MPM_ERR_CUDA, "scene table upload failed"));
     }
