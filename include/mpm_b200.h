@@ -223,8 +223,8 @@ int mpm_set_launch_shape(mpm_solver *solver, uint32_t p2g_ctas, uint32_t g2p_cta
 int mpm_get_launch_shape(mpm_solver *solver, uint32_t *p2g_ctas, uint32_t *g2p_ctas, uint32_t *sm_count);
 
 /* The autotuner: times `substeps` real substeps of the last submit's
- * parameters for each candidate grid (1 .. occupancy-limit CTAs per SM, and
- * one CTA per tile), P2G first, then G2P with the best P2G, keeps the
+ * parameters for each candidate persistent grid (1 .. occupancy-limit CTAs
+ * per SM), P2G first, then G2P with the best P2G, keeps the
  * fastest, and restores the particle state and counters it started from.
  * Needs one submitted batch.  Blocks. */
 int mpm_autotune(mpm_solver *solver, uint32_t substeps, uint32_t *p2g_ctas, uint32_t *g2p_ctas, double *best_ms);

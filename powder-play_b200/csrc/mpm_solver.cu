@@ -1290,16 +1290,17 @@ int mpm_autotune(mpm_solver *s, uint32_t substeps, uint32_t *p2g_ctas, uint32_t 
     unsigned best_p = p0, best_g = g0;
     double best_p_ms = 1e300, best_g_ms = 1e300;
     // P2G and G2P are separate launches, tuned one after the other: persistent
-    // grids of 1 .. (occupancy limit) CTAs per SM, and one CTA per tile
+    // grids of 1 .. (occupancy limit) CTAs per SM (a grid of one CTA per tile
+    // would pay for every tile of every scene in substeps that list few)
     const unsigned tiles = std::max(1u, s->n_tiles_total);
-    for (int k = 1; rc == MPM_OK && k <= std::max(1, per_sm_p2g) + 1; ++k) {
-        const unsigned p = k <= per_sm_p2g ? std::min(tiles, (unsigned)(sms * k)) : tiles;
+    for (int k = 1; rc == MPM_OK && k <= std::max(1, per_sm_p2g); ++k) {
+        const unsigned p = std::min(tiles, (unsigned)(sms * k));
         double pm = 0, gm = 0;
         rc = trial(p, g0, pm, gm);
         if (rc == MPM_OK && pm < best_p_ms) best_p_ms = pm, best_p = p;
     }
-    for (int k = 1; rc == MPM_OK && k <= std::max(1, per_sm_g2p) + 1; ++k) {
-        const unsigned g = k <= per_sm_g2p ? std::min(tiles, (unsigned)(sms * k)) : tiles;
+    for (int k = 1; rc == MPM_OK && k <= std::max(1, per_sm_g2p); ++k) {
+        const unsigned g = std::min(tiles, (unsigned)(sms * k));
         double pm = 0, gm = 0;
         rc = trial(best_p, g, pm, gm);
         if (rc == MPM_OK && gm < best_g_ms) best_g_ms = gm, best_g = g;
