@@ -170,6 +170,24 @@ int mpm_pick(mpm_solver *solver, float x, float y, float radius, uint32_t *parti
 int mpm_clone_range(mpm_solver *solver, uint32_t start, uint32_t count, float offset_x, float offset_y,
                     uint32_t object_id, uint32_t *first_index);
 
+/* The water/oil free-surface field of render('surface') without the
+ * renderer (solver.ts:2043-2066: clearSurfaceOccupancy, buildBuckets,
+ * gatherSurfaceOccupancy; shaders.ts:700-806): per halo node, row-major
+ * (node_w x node_h, node (x, y) at (y + 1) * node_w + x + 1), the water and
+ * oil display area 2 V det(F) w / cellSize^2 of the liquid particles of the
+ * current state.  The sums are 64-bit fixed point (2^40 per unit), so the
+ * field is bit-identical from run to run.  field_out (2 floats per node)
+ * and surface_flags_out (status word 7: 1 bucket / stencil, 2 particle
+ * area, 4 accumulation; decodeSurfaceError, solver.ts:208-224, 286-294) may
+ * be NULL.  Nothing is gathered (the field is zero) while a numerical status
+ * or surface flag is pending.  Single-scene solvers.  Blocks. */
+int mpm_gather_surface_occupancy(mpm_solver *solver, float *field_out, uint32_t *surface_flags_out);
+
+/* The device buffer of the last gathered surface field (2 floats per halo
+ * node, owned by the solver, valid until the next gather or mpm_destroy),
+ * for consumers that read it on the GPU; node_w / node_h may be NULL. */
+int mpm_surface_field_device(mpm_solver *solver, const float **device_field, uint32_t *node_w, uint32_t *node_h);
+
 /* dispose (solver.ts:143). */
 void mpm_destroy(mpm_solver *solver);
 

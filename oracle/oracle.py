@@ -278,3 +278,54 @@ def adjoint_fp64(scene: dict, x0, v0, C0, F0, vol, liquid, target, steps: int):
         raise OracleError(f"the FP64 adjoint stopped ({rc})")
     return loss.value, gv, gp, xt
 
+
+
+def current_area_fp64(px, py, F, volume, phase, cells_x: int, cells_y: int, cell_size: float) -> np.ndarray:
+    """FP64 restatement of gatherCurrentArea (src/lib/mpm/reference/occupancy.ts:70-128,
+    particleStencil / quadraticWeights :283-303) on a dense halo field.
+
+    phase: 0 water, 1 oil, anything else ignored (occupancy.ts:223).  Returns
+    (cells_y + 3, cells_x + 3, 2): node (x, y) at [y + 1, x + 1], its water
+    and oil current area V det(F) w / cellSize^2, added particle by particle
+    in stencil order (oy, then ox) like the reference's loop.  The GPU field
+    of gatherSurfaceOccupancy (shaders.ts:770-772) is the display area, twice
+    this.  Raises OracleError for the inputs the reference rejects
+    (occupancy.ts:178-230)."""
+    px = np.asarray(px, np.float64)
+    py = np.asarray(py, np.float64)
+    F = np.asarray(F, np.float64).reshape(-1, 4)
+    volume = np.asarray(volume, np.float64)
+    phase = np.asarray(phase)
+    if not (cell_size > 0):
+        raise OracleError("grid.cellSize must be greater than zero")
+    width, height = cells_x * cell_size, cells_y * cell_size
+    if np.any((px < 0) | (px > width) | (py < 0) | (py > height)):
+        raise OracleError("position must be inside the grid domain")
+    jac = F[:, 0] * F[:, 3] - F[:, 1] * F[:, 2]
+    if np.any(~np.isfinite(jac) | (jac <= 0)):
+        raise OracleError("F must have a finite positive determinant")
+    liquid = (phase == 0) | (phase == 1)
+    area = volume * jac
+    field = np.zeros(((cells_y + 3) * (cells_x + 3), 2), np.float64)
+    if not np.any(liquid):
+        return field.reshape(cells_y + 3, cells_x + 3, 2)
+    gx, gy = px[liquid] / cell_size, py[liquid] / cell_size
+    bx, by = np.floor(gx - 0.5), np.floor(gy - 0.5)
+    fx, fy = gx - bx, gy - by
+
+    def weights(f):
+        return np.stack([0.5 * (1.5 - f) ** 2, 0.75 - (f - 1) ** 2, 0.5 * (f - 0.5) ** 2], axis=1)
+
+    wx, wy = weights(fx), weights(fy)
+    cell_area = cell_size * cell_size
+    node_w = cells_x + 3
+    index, value = [], []
+    for oy in range(3):
+        for ox in range(3):
+            index.append((by + oy + 1) * node_w + (bx + ox + 1))
+            value.append(wx[:, ox] * wy[:, oy] * area[liquid] / cell_area)
+    index = np.stack(index, axis=1).astype(np.int64)  # particle-major, then oy, ox
+    value = np.stack(value, axis=1)
+    channel = np.repeat(phase[liquid].astype(np.int64)[:, None], 9, axis=1)
+    np.add.at(field, (index.ravel(), channel.ravel()), value.ravel())
+    return field.reshape(cells_y + 3, cells_x + 3, 2)

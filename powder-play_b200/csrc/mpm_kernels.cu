@@ -2835,6 +2835,90 @@ __global__ void k_clone(Ctx c, uint32_t start, uint32_t count, float2 offset, fl
     const_cast<uint32_t *>(c.bonded)[orig_base + k] = 0u;
 }
 
+// ------------------------------------------------ surface occupancy --
+
+// gatherSurfaceOccupancy (shaders.ts:710-806): the water and oil display
+// area of the liquid particles in the current slots spread over their 3x3
+// stencils, 2 V det(F) w / dx^2 per node, one thread per slot.  Each
+// contribution is added as a 64-bit fixed-point integer (SURFACE_SCALE
+// units per unit of area), so the sums do not depend on the order of the
+// atomics and every run is bit-identical (the reference adds floats in the
+// order of its node buckets).  Nothing is gathered while a numerical status
+// or surface flag is pending (status words 0 and 7).  Flags go to status
+// word 7 as in the reference: SURFACE_ERROR_BUCKET when the stencil leaves
+// the halo, SURFACE_ERROR_PARTICLE_AREA for a non-finite position or an
+// invalid area, determinant or weight, SURFACE_ERROR_ACCUMULATION when a
+// sum leaves the fixed-point range.  The geometry comes as arguments: the
+// solver's step parameters need not be uploaded yet.
+__global__ void k_surface_gather(Ctx c, SurfaceGeometry g, unsigned long long *acc)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    if (*(volatile uint32_t *)c.status != 0u || *(volatile uint32_t *)(c.status + 7) != 0u) return;
+    const Material m = c.mats[c.in.mat[i]];
+    const uint32_t phase = m.model == MODEL_WATER ? 0u : (m.model == MODEL_OIL ? 1u : 2u);
+    if (phase == 2u) return;
+    Stencil s;
+    const float2 pos = c.in.pos[i];
+    if (!stencil_from_grid(__fdiv_rn(pos.x, g.dx), __fdiv_rn(pos.y, g.dx), s)) {
+        fail(c.status + 7, SURFACE_ERROR_PARTICLE_AREA);
+        return;
+    }
+    if (s.bx < -1 || s.by < -1 || s.bx + 2 > (int)g.cells_x + 1 || s.by + 2 > (int)g.cells_y + 1) {
+        fail(c.status + 7, SURFACE_ERROR_BUCKET);
+        return;
+    }
+    const float det = det2(c.in.F[i]);
+    const float volume = c.in.vol[i];
+    const float area = __fmul_rn(volume, det);
+    const float display = __fmul_rn(area, 2.0f);
+    const float cell = __fmul_rn(g.dx, g.dx);
+    if (!finite_f(det) || det <= 0.0f || !finite_f(volume) || volume <= 0.0f || !finite_f(area) || area <= 0.0f) {
+        fail(c.status + 7, SURFACE_ERROR_PARTICLE_AREA);
+        return;
+    }
+    unsigned long long units[9];
+#pragma unroll
+    for (int oy = 0; oy < 3; ++oy) {
+#pragma unroll
+        for (int ox = 0; ox < 3; ++ox) {
+            const float w = __fmul_rn(quad_weight(s.fx, ox), quad_weight(s.fy, oy));
+            const float a = __fdiv_rn(__fmul_rn(display, w), cell);
+            if (!finite_f(w) || w < 0.0f || !finite_f(a) || a < 0.0f) {
+                fail(c.status + 7, SURFACE_ERROR_PARTICLE_AREA);
+                return;
+            }
+            const double scaled = rint((double)a * SURFACE_SCALE);
+            if (scaled >= SURFACE_LIMIT) {
+                fail(c.status + 7, SURFACE_ERROR_ACCUMULATION);
+                return;
+            }
+            units[oy * 3 + ox] = (unsigned long long)scaled;
+        }
+    }
+    const uint32_t n00 = (uint32_t)(s.by + 1) * g.node_w + (uint32_t)(s.bx + 1);
+#pragma unroll
+    for (int oy = 0; oy < 3; ++oy) {
+#pragma unroll
+        for (int ox = 0; ox < 3; ++ox) {
+            const unsigned long long u = units[oy * 3 + ox];
+            if (u == 0ull) continue;
+            const uint32_t n = n00 + (uint32_t)oy * g.node_w + (uint32_t)ox;
+            const unsigned long long prev = atomicAdd(acc + 2u * n + phase, u);
+            if (prev + u < prev) fail(c.status + 7, SURFACE_ERROR_ACCUMULATION);
+        }
+    }
+}
+
+// The fixed-point sums of k_surface_gather as (water, oil) areas per node.
+__global__ void k_surface_decode(const unsigned long long *acc, float2 *field, uint32_t nodes)
+{
+    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= nodes) return;
+    const ulonglong2 v = reinterpret_cast<const ulonglong2 *>(acc)[n];
+    field[n] = make_float2((float)((double)v.x / SURFACE_SCALE), (float)((double)v.y / SURFACE_SCALE));
+}
+
 // the instances the host launches
 template __global__ void k_p2g_gather<false>(Ctx);
 template __global__ void k_p2g_gather<true>(Ctx);

@@ -190,6 +190,18 @@ __global__ void k_fracture_bonds(Ctx c);
 __global__ void k_fracture_damage(Ctx c);
 __global__ void k_body_finish(Ctx c);
 __global__ void k_count_active_nodes(Ctx c, uint32_t *counts);
+// surface occupancy (status word 7 flags: shaders.ts:187-189)
+constexpr uint32_t SURFACE_ERROR_BUCKET = 1u;
+constexpr uint32_t SURFACE_ERROR_PARTICLE_AREA = 2u;
+constexpr uint32_t SURFACE_ERROR_ACCUMULATION = 4u;
+constexpr double SURFACE_SCALE = 1099511627776.0;  // 2^40 fixed-point units per unit of area
+constexpr double SURFACE_LIMIT = 4611686018427387904.0;  // 2^62: the largest single contribution
+struct SurfaceGeometry {
+    float dx;
+    uint32_t cells_x, cells_y, node_w;
+};
+__global__ void k_surface_gather(Ctx c, SurfaceGeometry g, unsigned long long *acc);
+__global__ void k_surface_decode(const unsigned long long *acc, float2 *field, uint32_t nodes);
 // interaction
 __global__ void k_outlet_compact(Ctx c, float4 bounds, ParticleBuffers removed, uint32_t *counters);
 __global__ void k_pick(Ctx c, float px, float py, float r2, unsigned long long *best);

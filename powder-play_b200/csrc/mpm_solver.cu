@@ -142,6 +142,10 @@ struct mpm_solver {
     mpm_drag drag{};
     bool drag_active = false;
 
+    // surface occupancy (allocated at the first gather)
+    unsigned long long *surface_acc = nullptr;  // per halo node: water, oil fixed-point sums
+    float2 *surface_field = nullptr;            // per halo node: water, oil area
+
     cudaEvent_t batch_start = nullptr, batch_stop = nullptr;
     bool batch_timed = false;
     uint32_t *d_active = nullptr;
@@ -605,7 +609,7 @@ void free_solver(mpm_solver *s)
                     s->tile_count, s->tile_range, s->scene_chunk, s->active_tiles, s->part, s->tile_info,
                     s->rec_state, s->rec_affine, s->rec_mom, s->rec_cell, s->field, s->body_starts,
                     s->slot_of[0], s->slot_of[1], s->track_flag, s->tracked, s->pair_cache, s->contact_count,
-                    s->body_vel, s->bonds, s->topology, s->endpoints};
+                    s->body_vel, s->bonds, s->topology, s->endpoints, s->surface_acc, s->surface_field};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (int b = 0; b < 2; ++b) {
@@ -1637,6 +1641,48 @@ int mpm_pick(mpm_solver *s, float x, float y, float radius, uint32_t *particle_i
         anchor_xy[1] = packed[1];
     }
     if (object_id) *object_id = id;
+    return MPM_OK;
+}
+
+int mpm_gather_surface_occupancy(mpm_solver *s, float *field_out, uint32_t *surface_flags_out)
+{
+    g_last_error.clear();
+    if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
+    if (s->n_scenes > 1) return set_error(MPM_ERR_STATE, "the surface field belongs to a single-scene solver");
+    CUDA_TRY(cudaSetDevice(s->device));
+    const uint32_t nodes = s->node_count;
+    if (!s->surface_acc) {
+        CUDA_TRY(dalloc(&s->surface_acc, 2 * (size_t)nodes));
+        CUDA_TRY(dalloc(&s->surface_field, nodes));
+    }
+    CUDA_TRY(cudaMemsetAsync(s->surface_acc, 0, 2 * (size_t)nodes * sizeof(unsigned long long), s->stream));
+    const SurfaceGeometry g{s->cfg.cell_size, s->cfg.cells_x, s->cfg.cells_y, s->node_w};
+    if (s->n > 0) {
+        const Ctx c = make_ctx(s, s->cur);
+        k_surface_gather<<<blocks_for(s->n, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c, g, s->surface_acc);
+        CUDA_TRY(cudaGetLastError());
+    }
+    k_surface_decode<<<blocks_for(nodes, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(s->surface_acc,
+                                                                                           s->surface_field, nodes);
+    CUDA_TRY(cudaGetLastError());
+    if (field_out)
+        CUDA_TRY(cudaMemcpyAsync(field_out, s->surface_field, (size_t)nodes * sizeof(float2), cudaMemcpyDeviceToHost,
+                                 s->stream));
+    if (surface_flags_out)
+        CUDA_TRY(cudaMemcpyAsync(surface_flags_out, s->d_status + 7, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                 s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return MPM_OK;
+}
+
+int mpm_surface_field_device(mpm_solver *s, const float **device_field, uint32_t *node_w, uint32_t *node_h)
+{
+    g_last_error.clear();
+    if (!s || !device_field) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and device_field must not be NULL");
+    if (!s->surface_field) return set_error(MPM_ERR_STATE, "no surface field has been gathered");
+    *device_field = reinterpret_cast<const float *>(s->surface_field);
+    if (node_w) *node_w = s->node_w;
+    if (node_h) *node_h = s->node_h;
     return MPM_OK;
 }
 

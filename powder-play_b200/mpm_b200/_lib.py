@@ -27,6 +27,7 @@ EXPORTED_SYMBOLS = (
     "mpmb_create", "mpmb_step_batch", "mpmb_read_compact", "mpmb_scene_count",
     "mpm_allocated_particle_count", "mpm_append_particles", "mpm_remove_particles_in_outlet", "mpm_pick",
     "mpm_clone_range", "mpm_set_launch_shape", "mpm_get_launch_shape", "mpm_autotune",
+    "mpm_gather_surface_occupancy", "mpm_surface_field_device",
     "mpma_create", "mpma_set_parameters", "mpma_get_parameters", "mpma_set_velocities", "mpma_forward",
     "mpma_backward", "mpma_read_positions", "mpma_last_ms", "mpma_destroy",
 )
@@ -130,6 +131,10 @@ def load_library(path: str = LIBRARY_PATH) -> ctypes.CDLL:
     lib.mpm_pick.restype = i32
     lib.mpm_clone_range.argtypes = [vp, u32, u32, f32, f32, u32, P(u32)]
     lib.mpm_clone_range.restype = i32
+    lib.mpm_gather_surface_occupancy.argtypes = [vp, vp, P(u32)]
+    lib.mpm_gather_surface_occupancy.restype = i32
+    lib.mpm_surface_field_device.argtypes = [vp, P(vp), P(u32), P(u32)]
+    lib.mpm_surface_field_device.restype = i32
     lib.mpm_set_launch_shape.argtypes = [vp, u32, u32]
     lib.mpm_set_launch_shape.restype = i32
     lib.mpm_get_launch_shape.argtypes = [vp, P(u32), P(u32), P(u32)]

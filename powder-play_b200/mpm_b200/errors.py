@@ -117,3 +117,26 @@ def is_recoverable_cfl_error(error: MpmMlsGpuNumericalError) -> bool:
             "particleSpeed", "waveSpeed", "velocityLimit", "waveSpeedLimit"))
     return (error.flags in (ERROR_DEFORMATION, ERROR_DEFORMATION_SUBSTEP_LIMIT)
             and error.measured_maximum_speed is not None and math.isfinite(error.measured_maximum_speed))
+
+
+_SURFACE_FLAG_DETAILS = (
+    (1, "invalid free-surface bucket state"),
+    (2, "invalid particle area or deformation determinant"),
+    (4, "non-finite free-surface occupancy accumulation"),
+)
+
+
+class MpmMlsGpuSurfaceError(Exception):
+    """MpmMlsGpuSurfaceError, src/lib/mpm/kernels/solver.ts:208-224."""
+
+    def __init__(self, flags):
+        self.flags = flags
+        message = "; ".join(text for flag, text in _SURFACE_FLAG_DETAILS if flags & flag)
+        body = message or f"status 0x{flags:x}"
+        super().__init__(f"GPU free-surface occupancy generation failed ({body}); particle state was not modified.")
+
+
+def decode_surface_error(status):
+    """decodeSurfaceError, src/lib/mpm/kernels/solver.ts:286-294: status word 7."""
+    flags = int(status[7])
+    return None if flags == 0 else MpmMlsGpuSurfaceError(flags)

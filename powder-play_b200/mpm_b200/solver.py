@@ -22,7 +22,7 @@ from . import _lib
 from .cfl import calculate_mpm_cfl_microsteps, calculate_mpm_cfl_safe_dt, calculate_mpm_cfl_velocity_limit
 from .cfl_bounds import derive_mpm_mls_gpu_cfl_bounds
 from .errors import (MpmMlsGpuNumericalError, MpmNativeError, RangeError, decode_numerical_error,
-                     is_recoverable_cfl_error)
+                     decode_surface_error, is_recoverable_cfl_error)
 from .layout import (PARTICLE_FLOATS, ValidatedInput, fround, pack_step_parameters, particles_from_dicts,
                      unpack_particles, validate_mpm_mls_gpu_input, _is_safe_integer)
 
@@ -419,9 +419,9 @@ class MpmMlsGpuSolver:
             error = decode_numerical_error(status, completed, speed)
             if error is not None:
                 raise error
-            if status[7] != 0:
-                raise RuntimeError(f"GPU free-surface occupancy generation failed (status 0x{int(status[7]):x}); "
-                                   "particle state was not modified.")
+            surface_error = decode_surface_error(status)
+            if surface_error is not None:
+                raise surface_error
             if not math.isfinite(speed) or speed < 0:
                 raise RangeError("GPU returned an invalid maximum-particle-speed scalar.")
             if sequence >= self._latest_completed_cfl_measurement_sequence:
@@ -469,6 +469,9 @@ class MpmMlsGpuSolver:
         error = decode_numerical_error(status)
         if error is not None:
             raise error
+        surface_error = decode_surface_error(status)
+        if surface_error is not None:
+            raise surface_error
 
     def read_status_words(self) -> np.ndarray:
         self._assert_active()
@@ -693,6 +696,35 @@ class MpmMlsGpuSolver:
         self._active_count -= removed.value
         self._has_removed = self._has_removed or removed.value > 0
         return int(removed.value)
+
+    def gather_surface_occupancy(self) -> np.ndarray:
+        """The water/oil free-surface field that render('surface') draws
+        (solver.ts:2043-2066; gatherSurfaceOccupancy, shaders.ts:700-806),
+        gathered on the GPU from the current state without the renderer:
+        (node_h, node_w, 2) float32, halo node (x, y) at [y + 1, x + 1], the
+        water and oil display area 2 V det(F) w / cellSize^2.  The device copy
+        stays in the solver (surface_field_device).  Raises
+        MpmMlsGpuSurfaceError when the gather set a surface flag."""
+        self._assert_active()
+        nodes = int(self._lib.mpm_node_count(self._handle))
+        field = np.zeros((nodes, 2), dtype=np.float32)
+        flags = ctypes.c_uint32()
+        _check(self._lib.mpm_gather_surface_occupancy(self._handle, _lib.ptr(field), ctypes.byref(flags)),
+               "GPU free-surface occupancy gather failed")
+        error = decode_surface_error([0] * 7 + [flags.value])
+        if error is not None:
+            raise error
+        grid = self._state.config["grid"]
+        return field.reshape(grid["cellsY"] + 3, grid["cellsX"] + 3, 2)
+
+    def surface_field_device(self):
+        """(device pointer, node_w, node_h) of the last gathered surface field
+        (two float32 per halo node, owned by the solver)."""
+        self._assert_active()
+        ptr, w, h = ctypes.c_void_p(), ctypes.c_uint32(), ctypes.c_uint32()
+        _check(self._lib.mpm_surface_field_device(self._handle, ctypes.byref(ptr), ctypes.byref(w), ctypes.byref(h)),
+               "no surface field")
+        return int(ptr.value), int(w.value), int(h.value)
 
     def clone(self, selection, offset) -> bool:
         """clone, solver.ts:2852-2940: a copy of the selected object moved by
