@@ -26,6 +26,7 @@ import math
 
 import numpy as np
 
+from .errors import RangeError
 from .layout import ParticleArrays
 from .materials import MPM_SI_BOX_DOMAIN
 
@@ -249,6 +250,61 @@ def create_mpm_gate4_scene(seed: int = GATE4_SCENE_SEED, liquid_particle_diamete
     p.material[:] = arr[:, 7].astype(np.int32)
     p.materials = mats
     return p, bonds, probes
+
+
+def create_mpm_cpu_parity_sample(particles, probe_indices, grid_cell_size: float) -> dict:
+    """createMpmCpuParitySample (src/lib/mpm/scenes/gate4.ts:359-467): the
+    particles a CPU step needs to reproduce the probes' step -- every
+    particle within 20 cells of a probe, every bonded triangle whose box lies
+    within 22 cells of a probe with the particles within 20 cells of that box,
+    and the whole triangle of every bonded vertex taken -- in source order.
+    Returns {"particles": ParticleArrays, "sourceIndices": [...],
+    "probeSampleIndices": [...]} with the reference's errors."""
+    probes = list(probe_indices)
+    if not probes:
+        raise RangeError("At least one CPU/GPU parity probe is required.")
+    if not (math.isfinite(grid_cell_size) and grid_cell_size > 0):
+        raise RangeError("gridCellSize must be a positive finite number.")
+    n = len(particles)
+    for index in probes:
+        if not isinstance(index, (int, np.integer)) or index < 0 or index >= n:
+            raise RangeError("CPU/GPU parity probe indices must identify input particles.")
+    px, py = np.asarray(particles.px, np.float64), np.asarray(particles.py, np.float64)
+    vertex = np.asarray(particles.bonded_vertex, np.int64)  # -1: not a bonded vertex
+    qx, qy = px[probes], py[probes]
+    radius = grid_cell_size * 20
+    source = np.zeros(n, bool)
+    for x, y in zip(qx, qy):
+        source |= (np.abs(px - x) <= radius) & (np.abs(py - y) <= radius)
+    contact = radius + 2 * grid_cell_size
+
+    def body_ok(start):
+        return start + 3 <= n and all(vertex[start + v] == v for v in range(3))
+
+    for start in np.flatnonzero(vertex == 0):
+        start = int(start)
+        if not body_ok(start):
+            raise RangeError(f"Bonded triangle at particle {start} is incomplete.")
+        bx, by = px[start:start + 3], py[start:start + 3]
+        x0, x1, y0, y1 = bx.min(), bx.max(), by.min(), by.max()
+        if not np.any((qx >= x0 - contact) & (qx <= x1 + contact) & (qy >= y0 - contact) & (qy <= y1 + contact)):
+            continue
+        source[start:start + 3] = True
+        source |= (px >= x0 - radius) & (px <= x1 + radius) & (py >= y0 - radius) & (py <= y1 + radius)
+    for index in np.flatnonzero(source & (vertex >= 0)):
+        start = int(index - vertex[index])
+        if start < 0 or not body_ok(start):
+            raise RangeError(f"Bonded triangle at particle {start} is incomplete.")
+        source[start:start + 3] = True
+    ordered = np.flatnonzero(source)
+    position = {int(s): k for k, s in enumerate(ordered)}
+    probe_samples = []
+    for index in probes:
+        if int(index) not in position:
+            raise RuntimeError(f"CPU/GPU parity probe {index} is missing from its local sample.")
+        probe_samples.append(position[int(index)])
+    return {"particles": particles.take(ordered), "sourceIndices": [int(s) for s in ordered],
+            "probeSampleIndices": probe_samples}
 
 
 def create_mpm_gate4_step_config(gravity=None, dt=GATE4_FIXED_STEP_SECONDS, fracture_bonds=None, grid=None):
