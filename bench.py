@@ -18,7 +18,9 @@ compact readback.
   sample of the same scene, single-threaded like the reference's worker.
 
 `--impl reference` times that CPU restatement alone (the reference is
-TypeScript; no JavaScript runtime exists on this image).  Multi-GPU runs are
+TypeScript; no JavaScript runtime exists on this image), one single-threaded
+process per host core (replicas of the scene for the plain form, shares of
+the scenes for the batched and differentiable forms).  Multi-GPU runs are
 replicas: each rank steps its own copy of the scene (weak scaling).
 """
 from __future__ import annotations
@@ -210,31 +212,190 @@ def dram_traffic(kernel: str):
     return None
 
 
+# ------------------------------------------------------------ reference arm
+#
+# The reference's CPU step is single-threaded (a JavaScript worker), so the
+# arm runs one copy of the FP64 restatement per host core, in processes
+# started with `spawn` (no GPU is touched): replicas of the whole scene for
+# the plain form, a share of the scenes per process for the batched and
+# differentiable forms.  Throughput = the work of all processes / the wall
+# time of the step in which they all run.
+
+def _reference_plan(workload: str):
+    """(jobs, meta): jobs = [(kind, payload)] of the whole workload, built
+    identically in every process."""
+    from mpm_b200 import calculate_mpm_cfl_microsteps, derive_mpm_mls_gpu_cfl_bounds
+    if workload in ("dam-break-1m", "si-tank"):
+        particles, config, gravity, meta = build_workload(workload)
+        bounds = derive_mpm_mls_gpu_cfl_bounds(particles, config)
+        plan = calculate_mpm_cfl_microsteps(meta["macro_dt"], config["grid"]["cellSize"], bounds["waveSpeedBound"],
+                                            max(bounds["velocityBound"], 5.0), BATCHED_MAX_MICROSTEPS)
+        micro = float(np.float32(plan["microDt"]))
+        return [("step", (particles, dict(config, dt=micro, gravity=gravity)))], dict(meta, micro_dt=micro)
+    if workload == "batched-512":
+        from mpm_b200.scenes import BATCHED_TANK_GRAVITY, create_batched_tank_scenes
+        scenes = create_batched_tank_scenes()
+        jobs = []
+        for particles, config in scenes:
+            bounds = derive_mpm_mls_gpu_cfl_bounds(particles, config)
+            plan = calculate_mpm_cfl_microsteps(MACRO_DT, config["grid"]["cellSize"], bounds["waveSpeedBound"],
+                                                _batched_bound(bounds["velocityBound"], MACRO_DT, BATCHED_TANK_GRAVITY),
+                                                BATCHED_MAX_MICROSTEPS)
+            jobs.append(("step", (particles, dict(config, dt=float(np.float32(plan["microDt"])),
+                                                  gravity=BATCHED_TANK_GRAVITY))))
+        return jobs, {"workload": "batched: 512 independent SI Tait water tanks (see the b200 arm)",
+                      "scenes": len(scenes), "particles": int(sum(len(p) for p, _ in scenes))}
+    if workload == "adjoint-64":
+        from mpm_b200.adjoint import fixed_cfl_dt
+        from mpm_b200.scenes import ADJOINT_GRAVITY, create_adjoint_scenes
+        jobs = []
+        for particles, config, target in create_adjoint_scenes():
+            dt = fixed_cfl_dt(particles, config, 90.0, 0.0)
+            dt = float(np.float32(fixed_cfl_dt(particles, config, 90.0, ADJOINT_SUBSTEPS * dt)))
+            jobs.append(("adjoint", (particles, config, target, dt)))
+        return jobs, {"workload": "differentiable form: 64 scenes (see the b200 arm)", "scenes": len(jobs)}
+    raise SystemExit(f"unknown workload {workload}")
+
+
+def _reference_share(workload: str, worker: int, workers: int):
+    """The jobs of process `worker`: the whole scene for the plain form (a
+    replica), every workers-th scene otherwise."""
+    jobs, _ = _reference_plan(workload)
+    from oracle import OracleState
+    mine = []
+    picked = jobs if len(jobs) == 1 else jobs[worker::workers]
+    for kind, payload in picked:
+        if kind == "step":
+            particles, cfg = payload
+            mine.append((kind, (OracleState(particles, cfg), cfg, len(particles))))
+        else:
+            mine.append((kind, payload))
+    return mine
+
+
+def _adjoint_inputs(particles, config, target, dt):
+    from mpm_b200.layout import validate_mpm_mls_gpu_input
+    from mpm_b200.scenes import ADJOINT_GRAVITY
+    pk = validate_mpm_mls_gpu_input(particles, config).packed_particles
+    liquid = pk[:, 13].view(np.uint32) == 2
+    pk64 = pk.astype(np.float64)
+    water, solid = pk64[liquid][0], pk64[~liquid][0]
+    scene = {"cells_x": config["grid"]["cellsX"], "cells_y": config["grid"]["cellsY"],
+             "dx": config["grid"]["cellSize"], "dt": dt, "gx": ADJOINT_GRAVITY["x"], "gy": ADJOINT_GRAVITY["y"],
+             "solid_mass": float(np.float32(config["particleMass"])), "wall_friction": config["wallFriction"],
+             "rho": float(water[16]), "gamma": float(water[18]), "tait": float(water[14]),
+             "lambda_s": float(solid[14]), "mu_s": float(solid[15])}
+    return (scene, pk64[:, 0:2], pk64[:, 2:4], pk64[:, 4:8], pk64[:, 8:12], pk64[:, 17], liquid.astype(np.int32),
+            np.asarray(target, np.float32).astype(np.float64))
+
+
+def _reference_sample(share, substeps: int):
+    """One timed sample of a process's share: (seconds, particle-substeps)."""
+    from oracle import adjoint_fp64
+    work, t0 = 0, time.perf_counter()
+    for kind, payload in share:
+        if kind == "step":
+            state, cfg, n = payload
+            state.run(cfg, substeps)
+            work += n * substeps
+        else:
+            particles, config, target, dt = payload
+            adjoint_fp64(*_adjoint_inputs(particles, config, target, dt), substeps)
+            work += len(particles) * substeps
+    return time.perf_counter() - t0, work
+
+
+def _reference_process(conn, workload: str, worker: int, workers: int):
+    """A reference process: builds its share, then answers each step request
+    (substeps) with (seconds, work) until it receives None."""
+    try:
+        share = _reference_share(workload, worker, workers)
+        conn.send("ready")
+        while True:
+            substeps = conn.recv()
+            if substeps is None:
+                break
+            conn.send(_reference_sample(share, substeps))
+    except Exception as exc:  # reported to the parent, which fails the run
+        conn.send(("error", repr(exc)))
+    finally:
+        conn.close()
+
+
+def _reference_workers(workload: str, jobs: int) -> int:
+    """One process per host core (at most one per scene when the workload
+    has several), within the host memory (about 1 GB per replica of the
+    1M-particle scene)."""
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    workers = min(cores, jobs) if jobs > 1 else cores
+    if workload == "dam-break-1m":
+        try:
+            import psutil
+            workers = min(workers, max(1, int(psutil.virtual_memory().available // (1 << 30)) - 4))
+        except ImportError:
+            pass
+    return max(1, workers)
+
+
 def run_reference(args):
     rank, _, world = _rank_info()
     if rank != 0:
         return
-    particles, config, gravity, meta = build_workload(args.workload)
-    from mpm_b200 import calculate_mpm_cfl_microsteps, derive_mpm_mls_gpu_cfl_bounds
-    bounds = derive_mpm_mls_gpu_cfl_bounds(particles, config)
-    plan = calculate_mpm_cfl_microsteps(meta["macro_dt"], config["grid"]["cellSize"], bounds["waveSpeedBound"],
-                                        max(bounds["velocityBound"], 5.0), MAX_MICROSTEPS)
-    micro = float(np.float32(plan["microDt"]))
-    total_sub, total_s, samples = 0, 0.0, []
-    for step in range(args.warmup + args.steps):
-        res = cpu_baseline(particles, config, gravity, micro, args.reference_substeps)
-        if step >= args.warmup:
-            total_sub += args.reference_substeps
-            total_s += len(particles) * args.reference_substeps / res["value"]
-            samples.append(res["sample"])
-    value = len(particles) * total_sub / total_s
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+    import multiprocessing
+    jobs, meta = _reference_plan(args.workload)
+    workers = _reference_workers(args.workload, len(jobs))
+    substeps = args.reference_substeps
+    ctx = multiprocessing.get_context("spawn")
+    pipes, procs = [], []
+    for k in range(workers):
+        parent, child = ctx.Pipe()
+        proc = ctx.Process(target=_reference_process, args=(child, args.workload, k, workers), daemon=True)
+        proc.start()
+        child.close()
+        pipes.append(parent)
+        procs.append(proc)
+    total_work, total_s = 0, 0.0
+    try:
+        for conn in pipes:
+            msg = conn.recv()
+            if msg != "ready":
+                raise SystemExit(f"reference process failed: {msg}")
+        for step in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            for conn in pipes:
+                conn.send(substeps)
+            results = [conn.recv() for conn in pipes]
+            wall = time.perf_counter() - t0
+            for r in results:
+                if not isinstance(r, tuple) or r[0] == "error":
+                    raise SystemExit(f"reference process failed: {r}")
+            if step >= args.warmup:
+                total_work += sum(w for _, w in results)
+                total_s += wall
+    finally:
+        for conn in pipes:
+            try:
+                conn.send(None)
+            except OSError:
+                pass
+        for proc in procs:
+            proc.join(timeout=30)
+    value = total_work / total_s
+    adjoint = args.workload == "adjoint-64"
+    unit = "particle-substeps/s (adjoint)" if adjoint else UNIT
+    what = {"dam-break-1m": f"{workers} replicas of the full scene, {substeps} substeps each per step",
+            "si-tank": f"{workers} replicas of the full scene, {substeps} substeps each per step",
+            "batched-512": f"the 512 scenes shared by {workers} processes, {substeps} substeps of each scene per step",
+            "adjoint-64": f"the 64 scenes shared by {workers} processes, {substeps} forward + adjoint substeps of "
+                          "each scene per step (FP64 adjoint, oracle/adjoint_fp64.c)"}[args.workload]
+    sample = (f"{what}; C FP64 restatement (oracle/), one single-threaded process per host core, "
+              f"{total_s:.1f} s timed")
+    line = {"metric": METRIC, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scene)",
-            "impl": "reference", "config": dict(meta, p2g="CPU scatter (stepMpm restatement)"),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
-                             "sample": f"{args.reference_substeps} substeps per step; {samples[0] if samples else ''}"},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scenes)",
+            "impl": "reference", "config": dict(meta, p2g="CPU scatter (stepMpm restatement)", processes=workers),
+            "cpu_baseline": {"value": value, "unit": unit, "cores": workers, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
