@@ -910,9 +910,25 @@ struct Stage {
     uint32_t start[TILE_CELLS + 1];
     float acc[ACC_WORDS][RING_NODES];
     uint32_t cells[TILE_CELLS + 1];  // a crowded tile: its cells' first entries in the cell-ordered list
+    uint8_t active[TILE_CELLS];      // the chunk's cells holding entries, ascending
+    uint32_t warp_active[TILE_CELLS / 32];
     uint32_t mask;
     int failed;
 };
+
+// First sorted entry of channel >= ch in the cell's entries [lo, hi) (they
+// are ordered by channel, then original index).
+__device__ __forceinline__ uint32_t channel_start(const Stage &sm, uint32_t lo, uint32_t hi, uint32_t ch)
+{
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) / 2u;
+        if (((sm.cell[sm.sorted[mid]] >> 8) & 3u) < ch)
+            lo = mid + 1u;
+        else
+            hi = mid;
+    }
+    return lo;
+}
 
 __device__ __forceinline__ uint32_t sort_key(const Stage &sm, uint32_t k)
 {
@@ -996,20 +1012,45 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, const uint32_
     __syncthreads();
     for (uint32_t k = me; k < n; k += TILE_CELLS) sm.sorted[sm.start[sm.cell[k] & 0xffu] + sm.order[k]] = (uint16_t)k;
     __syncthreads();
-    const uint32_t lo = sm.start[me], hi = sm.start[me + 1];
-    const int cx = (int)(me % TILE_X), cy = (int)(me / TILE_X);
+    // the cells holding entries, compacted; each gets a group of `share`
+    // consecutive threads of one warp (a power of two up to 32, so that the
+    // groups fill the CTA): a crowded chunk of few cells spreads each cell's
+    // particles over its group, which adds their sums in a fixed tree order
+    // (with more than 64 such cells every thread takes its own cell)
+    const bool has = sm.start[me + 1] > sm.start[me];
+    const uint32_t n_cells = (uint32_t)__syncthreads_count(has);
+    uint32_t share = 1;
+    while (share < 32u && n_cells * share * 2u <= (uint32_t)TILE_CELLS) share *= 2u;
+    if (share > 1u) {
+        const unsigned ballot = __ballot_sync(0xffffffffu, has);
+        const uint32_t lane = me & 31u, warp = me >> 5;
+        if (lane == 0u) sm.warp_active[warp] = __popc(ballot);
+        __syncthreads();
+        uint32_t before = 0;
+        for (uint32_t w = 0; w < warp; ++w) before += sm.warp_active[w];
+        if (has) sm.active[before + __popc(ballot & ((1u << lane) - 1u))] = (uint8_t)me;
+        __syncthreads();
+    }
+    const uint32_t group = me / share, part = me % share;
+    const bool mine = share == 1u || group < n_cells;
+    const uint32_t cell = share == 1u ? me : (mine ? sm.active[group] : 0u);
+    const uint32_t lo = mine ? sm.start[cell] : 0u, hi = mine ? sm.start[cell + 1] : 0u;
+    const int cx = (int)(cell % TILE_X), cy = (int)(cell / TILE_X);
     const float dx = P.dx;
     const uint32_t tile_mask = sm.mask;
-    uint32_t j = lo;
+    uint32_t lo_ch = lo;
 #pragma unroll 1
     for (uint32_t ch = 0; ch < 3u; ++ch) {
         if (!(tile_mask & (1u << ch))) continue;
         float m[9], px[9], py[9], vl[9];
 #pragma unroll
         for (int o = 0; o < 9; ++o) m[o] = px[o] = py[o] = vl[o] = 0.f;
-        for (; j < hi; ++j) {
+        // this channel's entries of the cell: [a, b)
+        const uint32_t a = lo_ch;
+        const uint32_t b = ch == 2u ? hi : channel_start(sm, a, hi, ch + 1u);
+        lo_ch = b;
+        for (uint32_t j = a + part; j < b; j += share) {
             const uint32_t k = sm.sorted[j];
-            if (((sm.cell[k] >> 8) & 3u) != ch) break;
             const float4 q = sm.state[k];
             const float4 A = sm.affine[k];
             const float2 mv = sm.momentum[k];
@@ -1036,6 +1077,19 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, const uint32_
                 }
             }
         }
+        if (share > 1u) {
+            // the group's partial sums, added pairwise (lane + off into lane)
+            for (uint32_t off = share / 2u; off > 0u; off /= 2u) {
+#pragma unroll
+                for (int o = 0; o < 9; ++o) {
+                    m[o] += __shfl_down_sync(0xffffffffu, m[o], off, (int)share);
+                    px[o] += __shfl_down_sync(0xffffffffu, px[o], off, (int)share);
+                    py[o] += __shfl_down_sync(0xffffffffu, py[o], off, (int)share);
+                    vl[o] += __shfl_down_sync(0xffffffffu, vl[o], off, (int)share);
+                }
+            }
+        }
+        const bool adds = mine && part == 0u;
         const int word = ch == 0u ? 0 : (ch == 1u ? 3 : 7);
 #pragma unroll
         for (int oy = 0; oy < 3; ++oy) {
@@ -1043,11 +1097,13 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, const uint32_
             for (int ox = 0; ox < 3; ++ox) {
                 const int o = oy * 3 + ox;
                 __syncthreads();  // the previous phase's adds are done
-                const int r = (cy + oy) * RING_X + cx + ox;
-                sm.acc[word][r] += m[o];
-                sm.acc[word + 1][r] += px[o];
-                sm.acc[word + 2][r] += py[o];
-                if (ch != 0u) sm.acc[word + 3][r] += vl[o];
+                if (adds) {
+                    const int r = (cy + oy) * RING_X + cx + ox;
+                    sm.acc[word][r] += m[o];
+                    sm.acc[word + 1][r] += px[o];
+                    sm.acc[word + 2][r] += py[o];
+                    if (ch != 0u) sm.acc[word + 3][r] += vl[o];
+                }
             }
         }
     }
