@@ -313,7 +313,10 @@ int mpma_set_velocities(mpm_adjoint *engine, const float *velocities);
 
 /* Runs `substeps` substeps of dts[k] in scene k from the initial state,
  * keeping the state at every `checkpoint_every`-th substep, and returns the
- * loss per scene against `targets` (2 per particle).  Blocks. */
+ * loss per scene against `targets` (2 per particle).  With
+ * checkpoint_every >= substeps the pass keeps every substep's state and node
+ * sums (48 B per particle and 32 B per node, per substep) and
+ * mpma_backward recomputes nothing.  Blocks. */
 int mpma_forward(mpm_adjoint *engine, uint32_t substeps, const float *dts, uint32_t checkpoint_every,
                  const float *targets, double *loss);
 

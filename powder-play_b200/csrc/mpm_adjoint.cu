@@ -668,6 +668,7 @@ struct mpm_adjoint {
     uint32_t steps = 0, every = 0;
     int final_buffer = 0;
     bool forward_done = false;
+    bool taped = false;  // the forward kept every substep's state and sums (one segment)
     cudaEvent_t ev[4]{};
     float forward_ms = 0.f, backward_ms = 0.f;
 };
@@ -1021,11 +1022,23 @@ int mpma_forward(mpm_adjoint *a, uint32_t substeps, const float *dts, uint32_t c
     ADJ_TRY(cudaMemsetAsync(a->loss, 0, a->n_scenes * sizeof(double), a->stream));
     ADJ_TRY(cudaEventRecord(a->ev[0], a->stream));
     int cur = 0;
-    ADJ_TRY(copy_state(a->ping[0], a->init, a->n, a->stream));
-    for (uint32_t k = 0; k < substeps; ++k) {
-        if (k % checkpoint_every == 0) ADJ_TRY(copy_state(a->checkpoints[k / checkpoint_every], a->ping[cur], a->n, a->stream));
-        ADJ_TRY(forward_substep(a, a->ping[cur], a->ping[1 - cur], a->sum_s, a->sum_w));
-        cur = 1 - cur;
+    a->taped = n_check == 1;
+    if (a->taped) {
+        // one segment: the forward runs on the recompute tape itself (every
+        // substep's input state and node sums stay in HBM), so the backward
+        // pass recomputes nothing; the final state lands in ping[0]
+        ADJ_TRY(copy_state(a->tape[0], a->init, a->n, a->stream));
+        for (uint32_t k = 0; k < substeps; ++k)
+            ADJ_TRY(forward_substep(a, a->tape[k], k + 1 < substeps ? a->tape[k + 1] : a->ping[0], a->tape_s[k],
+                                    a->tape_w[k]));
+    } else {
+        ADJ_TRY(copy_state(a->ping[0], a->init, a->n, a->stream));
+        for (uint32_t k = 0; k < substeps; ++k) {
+            if (k % checkpoint_every == 0)
+                ADJ_TRY(copy_state(a->checkpoints[k / checkpoint_every], a->ping[cur], a->n, a->stream));
+            ADJ_TRY(forward_substep(a, a->ping[cur], a->ping[1 - cur], a->sum_s, a->sum_w));
+            cur = 1 - cur;
+        }
     }
     ADJ_TRY(cudaEventRecord(a->ev[1], a->stream));
     a->final_buffer = cur;
@@ -1054,8 +1067,8 @@ int mpma_backward(mpm_adjoint *a, float *grad_velocities, double *grad_parameter
     const uint32_t K = a->every;
     for (int seg = (int)a->checkpoints.size() - 1; seg >= 0; --seg) {
         const uint32_t start = (uint32_t)seg * K, len = std::min(K, a->steps - start);
-        ADJ_TRY(copy_state(a->tape[0], a->checkpoints[seg], a->n, a->stream));
-        for (uint32_t j = 0; j < len; ++j) {
+        if (!a->taped) ADJ_TRY(copy_state(a->tape[0], a->checkpoints[seg], a->n, a->stream));
+        for (uint32_t j = 0; j < len && !a->taped; ++j) {
             ADJ_TRY(cudaMemsetAsync(a->tape_s[j], 0, (size_t)a->n_nodes * sizeof(float4), a->stream));
             ADJ_TRY(cudaMemsetAsync(a->tape_w[j], 0, (size_t)a->n_nodes * sizeof(float4), a->stream));
             const AdjCtx c = make_adj_ctx(a, a->tape[j], j + 1 < len ? a->tape[j + 1] : a->ping[0], a->tape_s[j],
