@@ -773,6 +773,17 @@ def run_b200(args):
         "clocks": clock_info,
         "gpu_launches": gpu_launches,
     }
+    if args.p2g == "fixed" and "k_prepare_scatter" in prof:
+        # the fixed-point scatter's int32 atomics: 9 nodes x 4 words per
+        # liquid particle (mass, momentum, volume), 9 x 3 per solid one
+        packed, _ = solver.read_particles_packed()
+        model = packed[:, 13].view(np.uint32)
+        liquid = int(np.count_nonzero((model == 2) | (model == 3)))
+        per_substep = 36 * liquid + 27 * (len(model) - liquid)
+        ms, launches = prof["k_prepare_scatter"]
+        line["atomics"] = {"kernel": "k_prepare_scatter", "per_substep": per_substep,
+                           "per_s": per_substep / (ms / launches * 1e-3),
+                           "per_particle": {"liquid": 36, "solid": 27}}
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(particles, config, gravity, float(np.float32(plan["microDt"])),
                                             args.cpu_substeps)
