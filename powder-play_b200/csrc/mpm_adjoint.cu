@@ -278,8 +278,13 @@ struct G2pFwd {
     float2 xn;       // new position before confinement
 };
 
+// With `keep_u` / `keep_mv` (shared memory, [stencil node][ADJ_THREADS]) it
+// also keeps each stencil node's velocity and, for a liquid, its liquid mass
+// and volume, for this thread's adjoint.
+template <bool KEEP = false>
 __device__ __forceinline__ bool g2p_forward(const AdjCtx &c, const AdjScene &S, bool liquid, const AdjStencil &st,
-                                            float2 x, float4 F0, G2pFwd &g)
+                                            float2 x, float4 F0, G2pFwd &g, float2 (*keep_u)[ADJ_THREADS] = nullptr,
+                                            float2 (*keep_mv)[ADJ_THREADS] = nullptr)
 {
     g.vp = make_float2(0.f, 0.f);
     g.B = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -295,6 +300,10 @@ __device__ __forceinline__ bool g2p_forward(const AdjCtx &c, const AdjScene &S, 
             const float4 sum = liquid ? c.sum_w[n] : c.sum_s[n];
             float2 D;
             const float2 u = node_velocity_adj(S, sum, st.bx + ox, st.by + oy, D);
+            if constexpr (KEEP) {
+                keep_u[oy * 3 + ox][threadIdx.x] = u;
+                keep_mv[oy * 3 + ox][threadIdx.x] = make_float2(sum.x, sum.w);
+            }
             g.vp.x += w * u.x;
             g.vp.y += w * u.y;
             g.B.x += w * u.x * dpx;
@@ -432,6 +441,10 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_loss(AdjCtx c)
 // the input position and F adjoints.
 __global__ void __launch_bounds__(ADJ_THREADS, 3) k_adj_g2p_bwd(AdjCtx c)
 {
+    // this thread's stencil node velocities and liquid sums from the forward
+    // recompute, read again by the adjoint's scatter
+    __shared__ float2 s_u[9][ADJ_THREADS];
+    __shared__ float2 s_mv[9][ADJ_THREADS];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const AdjScene &S = c.scenes[c.scene_of[i]];
@@ -440,7 +453,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) k_adj_g2p_bwd(AdjCtx c)
     const float4 F0 = c.in.F[i];
     AdjStencil st;
     G2pFwd g;
-    if (!adj_stencil(S, x, st) || !g2p_forward(c, S, liquid, st, x, F0, g)) {
+    if (!adj_stencil(S, x, st) || !g2p_forward<true>(c, S, liquid, st, x, F0, g, s_u, s_mv)) {
         adj_fail(c, ADJ_ERR_NONFINITE);
         return;
     }
@@ -506,9 +519,8 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) k_adj_g2p_bwd(AdjCtx c)
             const float w = st.wx[ox] * st.wy[oy];
             const float dpx = ((float)ox - st.fx) * S.dx;
             const uint32_t n = adj_node(S, st.bx + ox, st.by + oy);
-            const float4 sum = liquid ? c.sum_w[n] : c.sum_s[n];
-            float2 D;
-            const float2 u = node_velocity_adj(S, sum, st.bx + ox, st.by + oy, D);
+            const float2 u = s_u[oy * 3 + ox][threadIdx.x];
+            const float2 mv = s_mv[oy * 3 + ox][threadIdx.x];  // liquid mass and volume
             // node velocity adjoint: w vpb + w Bb dp
             const float ubx = w * (vpb.x + Bb.x * dpx + Bb.y * dpy);
             const float uby = w * (vpb.y + Bb.z * dpx + Bb.w * dpy);
@@ -519,7 +531,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) k_adj_g2p_bwd(AdjCtx c)
             // d/dx of w: (dwx wy, wx dwy) / dx
             const float gwx = st.dwx[ox] * st.wy[oy] * S.inv_dx, gwy = st.wx[ox] * st.dwy[oy] * S.inv_dx;
             float sval = u.x * (vpb.x + Bb.x * dpx + Bb.y * dpy) + u.y * (vpb.y + Bb.z * dpx + Bb.w * dpy);
-            if (liquid) sval += pm_b * sum.x + pv_b * sum.w;
+            if (liquid) sval += pm_b * mv.x + pv_b * mv.y;
             // dp = (k - f) dx: d/dx = -1 per axis
             xb.x += gwx * sval - w * (u.x * Bb.x + u.y * Bb.z);
             xb.y += gwy * sval - w * (u.x * Bb.y + u.y * Bb.w);
