@@ -30,6 +30,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -55,7 +56,7 @@ constexpr unsigned ADJ_THREADS = 256;
 // material parameters.
 struct AdjScene {
     uint32_t n, p_base, node_base, node_w;
-    uint32_t cells_x, cells_y, pad0, pad1;
+    uint32_t cells_x, cells_y, tile_base, tiles_x;  // 16x16-node tiles of the halo grid, row-major
     float dx, inv_dx, gs, dt;
     float gx, gy, domain_w, domain_h;
     float solid_mass, wall_friction, rho, gamma;
@@ -86,7 +87,10 @@ struct AdjCtx {
     double *param_grad;    // per scene: tait, lambda_s, mu_s
     const float2 *target;  // per particle
     double *loss;          // per scene
+    uint8_t *mark_out;     // per tile: marked when a new position's stencil reaches it (k_adj_g2p), or NULL
 };
+
+constexpr int ADJ_TILE = 16;  // nodes per side of a clearing tile
 
 constexpr uint32_t ADJ_ERR_STENCIL = 1u, ADJ_ERR_NONFINITE = 2u, ADJ_ERR_DETERMINANT = 4u;
 
@@ -350,6 +354,22 @@ __device__ __forceinline__ float4 project_liquid(float4 T)
 
 }  // namespace
 
+// Marks the clearing tiles that the stencil with base (bx, by) reaches (its
+// corner nodes lie in at most four); the lanes of a warp marking the same
+// tile store once.
+__device__ __forceinline__ void mark_tiles(uint8_t *mark, const AdjScene &S, int bx, int by)
+{
+    const unsigned active = __activemask();
+    const uint32_t x0 = (uint32_t)(bx + 1) / ADJ_TILE, x1 = (uint32_t)(bx + 3) / ADJ_TILE;
+    const uint32_t y0 = (uint32_t)(by + 1) / ADJ_TILE, y1 = (uint32_t)(by + 3) / ADJ_TILE;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t t = S.tile_base + ((k & 2) ? y1 : y0) * S.tiles_x + ((k & 1) ? x1 : x0);
+        const unsigned same = __match_any_sync(active, t);
+        if ((threadIdx.x & 31u) == (uint32_t)(__ffs(same) - 1)) mark[t] = 1u;
+    }
+}
+
 // ------------------------------------------------------------- kernels ----
 
 __global__ void __launch_bounds__(ADJ_THREADS) k_adj_p2g(AdjCtx c)
@@ -402,6 +422,10 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_g2p(AdjCtx c)
     const float4 Fn = liquid ? project_liquid(g.trial) : g.trial;
     const float2 bx = confine_axis(g.xn.x, g.vp.x, S.domain_w);
     const float2 by = confine_axis(g.xn.y, g.vp.y, S.domain_h);
+    if (c.mark_out) {
+        AdjStencil next;
+        if (adj_stencil(S, make_float2(bx.x, by.x), next)) mark_tiles(c.mark_out, S, next.bx, next.by);
+    }
     c.out.x[i] = make_float2(bx.x, by.x);
     c.out.v[i] = make_float2(bx.y, by.y);
     c.out.C[i] = g.Cn;
@@ -410,6 +434,40 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_g2p(AdjCtx c)
 
 // Loss sum |x - target|^2 per scene (one atomic per warp whose particles
 // share a scene) and its adjoint seeds.
+// Marks the clearing tiles the stencils of the particles in c.in reach (the
+// first substep's; later substeps' marks come from k_adj_g2p).
+__global__ void __launch_bounds__(ADJ_THREADS) k_adj_mark(AdjCtx c, uint8_t *mark)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const AdjScene &S = c.scenes[c.scene_of[i]];
+    AdjStencil st;
+    if (adj_stencil(S, c.in.x[i], st)) mark_tiles(mark, S, st.bx, st.by);
+}
+
+// Zeroes the nodes of the marked tiles in up to three node arrays (NULL:
+// skipped), one tile per CTA iteration and one node per thread: every node a
+// substep adds to or reads lies in a tile its particles mark.  The rest of
+// the grid keeps stale values that no stencil reads.  tile_scene gives each
+// tile's scene.
+__global__ void __launch_bounds__(ADJ_TILE * ADJ_TILE) k_adj_clear(const AdjScene *scenes, const uint32_t *tile_scene,
+                                                                   uint32_t n_tiles, const uint8_t *mark, float4 *a,
+                                                                   float4 *b, float2 *c2)
+{
+    for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        if (!mark[t]) continue;  // the same answer for the whole CTA
+        const AdjScene &S = scenes[tile_scene[t]];
+        const uint32_t local = t - S.tile_base;
+        const uint32_t hx = (local % S.tiles_x) * ADJ_TILE + threadIdx.x % ADJ_TILE;
+        const uint32_t hy = (local / S.tiles_x) * ADJ_TILE + threadIdx.x / ADJ_TILE;
+        if (hx >= S.node_w || hy >= S.cells_y + 3u) continue;
+        const uint32_t n = S.node_base + hy * S.node_w + hx;
+        if (a) a[n] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (b) b[n] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (c2) c2[n] = make_float2(0.f, 0.f);
+    }
+}
+
 __global__ void __launch_bounds__(ADJ_THREADS) k_adj_loss(AdjCtx c)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -672,6 +730,11 @@ struct mpm_adjoint {
     AdjState init{}, ping[2]{};
     std::vector<AdjState> checkpoints, tape;
     float4 *sum_s = nullptr, *sum_w = nullptr;   // forward scratch
+    uint8_t *mark = nullptr;                     // per substep (0 .. steps) and clearing tile
+    size_t mark_count = 0;
+    uint32_t *tile_scene = nullptr;              // per clearing tile
+    uint32_t n_tiles = 0;
+    unsigned clear_ctas = 1;
     std::vector<float4 *> tape_s, tape_w;       // per recomputed substep
     float2 *xb[2]{}, *vb[2]{}, *xg = nullptr, *ub_s = nullptr;
     float4 *Cb[2]{}, *Fb[2]{}, *Fg = nullptr, *ub_w = nullptr;
@@ -731,7 +794,7 @@ void free_engine(mpm_adjoint *a)
     for (auto &s : a->tape) free_state(s);
     for (float4 *p : a->tape_s) cudaFree(p);
     for (float4 *p : a->tape_w) cudaFree(p);
-    void *ptrs[] = {a->d_scenes, a->scene_of, a->liquid, a->status, a->vol, a->sum_s, a->sum_w, a->xb[0], a->xb[1],
+    void *ptrs[] = {a->mark, a->tile_scene, a->d_scenes, a->scene_of, a->liquid, a->status, a->vol, a->sum_s, a->sum_w, a->xb[0], a->xb[1],
                     a->vb[0], a->vb[1], a->xg, a->ub_s, a->Cb[0], a->Cb[1], a->Fb[0], a->Fb[1], a->Fg, a->ub_w,
                     a->param_grad, a->loss, a->target, a->final_x};
     for (void *p : ptrs)
@@ -792,14 +855,28 @@ AdjCtx make_adj_ctx(mpm_adjoint *a, const AdjState &in, const AdjState &out, flo
 unsigned blocks(uint32_t n) { return std::max(1u, (n + ADJ_THREADS - 1) / ADJ_THREADS); }
 
 // One forward substep from `in` to `out` with the sums in (ss, sw).
-cudaError_t forward_substep(mpm_adjoint *a, const AdjState &in, const AdjState &out, float4 *ss, float4 *sw)
+// The clearing-tile marks of substep k (its input positions).
+uint8_t *marks_of(mpm_adjoint *a, uint32_t k) { return a->mark + (size_t)k * a->n_tiles; }
+
+// Zeroes the node arrays over the marked tiles of one substep (NULL arrays are skipped).
+void clear_marked(mpm_adjoint *a, const uint8_t *mark, float4 *x, float4 *y, float2 *z)
 {
-    cudaError_t e = cudaMemsetAsync(ss, 0, (size_t)a->n_nodes * sizeof(float4), a->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(sw, 0, (size_t)a->n_nodes * sizeof(float4), a->stream);
-    if (e != cudaSuccess) return e;
-    const AdjCtx c = make_adj_ctx(a, in, out, ss, sw, 0);
+    k_adj_clear<<<a->clear_ctas, ADJ_TILE * ADJ_TILE, 0, a->stream>>>(a->d_scenes, a->tile_scene, a->n_tiles, mark, x,
+                                                                        y, z);
+}
+
+// One forward substep k from `in` into `out`, its node sums in ss / sw: they
+// are zeroed over the substep's marked tiles first, and the new positions
+// mark substep k + 1's tiles (adding to the marks when a segment is
+// recomputed: float atomics may move a position by its last bits).
+cudaError_t forward_substep(mpm_adjoint *a, uint32_t k, const AdjState &in, const AdjState &out, float4 *ss, float4 *sw,
+                            bool run_g2p = true)
+{
+    clear_marked(a, marks_of(a, k), ss, sw, nullptr);
+    AdjCtx c = make_adj_ctx(a, in, out, ss, sw, 0);
+    c.mark_out = marks_of(a, k + 1);
     k_adj_p2g<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(c);
-    k_adj_g2p<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(c);
+    if (run_g2p) k_adj_g2p<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(c);
     return cudaGetLastError();
 }
 
@@ -833,6 +910,7 @@ int mpma_create(const mpm_config *configs, uint32_t scene_count, const uint32_t 
     std::vector<float2> x, v;
     std::vector<float4> C, F;
     uint64_t total = 0, nodes = 0;
+    std::vector<uint32_t> tile_scene;  // per clearing tile
     for (uint32_t k = 0; k < scene_count; ++k) {
         const mpm_config &cfg = configs[k];
         if (cfg.cells_x < 1 || cfg.cells_y < 1 || cfg.cells_x > 65536 || cfg.cells_y > 65536 || !(cfg.cell_size > 0.f))
@@ -889,6 +967,9 @@ int mpma_create(const mpm_config *configs, uint32_t scene_count, const uint32_t 
         }
         total += S.n;
         nodes += (uint64_t)(cfg.cells_x + 3) * (cfg.cells_y + 3);
+        S.tile_base = (uint32_t)tile_scene.size();
+        S.tiles_x = (cfg.cells_x + 3 + ADJ_TILE - 1) / ADJ_TILE;
+        tile_scene.insert(tile_scene.end(), (size_t)S.tiles_x * ((cfg.cells_y + 3 + ADJ_TILE - 1) / ADJ_TILE), k);
         if (total > 0x7fffffffull || nodes > 0x7fffffffull)
             return err(MPM_ERR_INVALID_ARGUMENT, "the batch exceeds the GPU index range");
     }
@@ -940,7 +1021,15 @@ int mpma_create(const mpm_config *configs, uint32_t scene_count, const uint32_t 
     ADJ_ALLOC(a->loss, scene_count);
     ADJ_ALLOC(a->target, n);
     ADJ_ALLOC(a->final_x, n);
+    a->n_tiles = (uint32_t)tile_scene.size();
+    ADJ_ALLOC(a->tile_scene, tile_scene.size());
 #undef ADJ_ALLOC
+    {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+            return fail(err(MPM_ERR_CUDA, "device query failed"));
+        a->clear_ctas = (unsigned)std::max<size_t>(1, std::min<size_t>(tile_scene.size(), (size_t)sms * 8));
+    }
     bool ok = cudaMemcpy(a->d_scenes, scenes.data(), scene_count * sizeof(AdjScene), cudaMemcpyHostToDevice) == cudaSuccess;
     ok = ok && cudaMemcpy(a->scene_of, scene_of.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice) == cudaSuccess;
     ok = ok && cudaMemcpy(a->liquid, liquid.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice) == cudaSuccess;
@@ -950,6 +1039,8 @@ int mpma_create(const mpm_config *configs, uint32_t scene_count, const uint32_t 
     ok = ok && cudaMemcpy(a->init.C, C.data(), n * sizeof(float4), cudaMemcpyHostToDevice) == cudaSuccess;
     ok = ok && cudaMemcpy(a->init.F, F.data(), n * sizeof(float4), cudaMemcpyHostToDevice) == cudaSuccess;
     ok = ok && cudaMemset(a->status, 0, sizeof(uint32_t)) == cudaSuccess;
+    ok = ok && cudaMemcpy(a->tile_scene, tile_scene.data(), tile_scene.size() * sizeof(uint32_t),
+                          cudaMemcpyHostToDevice) == cudaSuccess;
     if (!ok) return fail(err(MPM_ERR_CUDA, "upload failed"));
     *out = a;
     return MPM_OK;
@@ -1030,6 +1121,15 @@ int mpma_forward(mpm_adjoint *a, uint32_t substeps, const float *dts, uint32_t c
     }
     a->steps = substeps;
     a->every = checkpoint_every;
+    const size_t marks = ((size_t)substeps + 1) * a->n_tiles;
+    if (a->mark_count < marks) {
+        cudaFree(a->mark);
+        a->mark = nullptr;
+        a->mark_count = 0;
+        if (adj_alloc(&a->mark, marks) != cudaSuccess) return err(MPM_ERR_CUDA, "tile mark allocation failed");
+        a->mark_count = marks;
+    }
+    ADJ_TRY(cudaMemsetAsync(a->mark, 0, marks, a->stream));
     ADJ_TRY(cudaMemsetAsync(a->status, 0, sizeof(uint32_t), a->stream));
     ADJ_TRY(cudaMemsetAsync(a->loss, 0, a->n_scenes * sizeof(double), a->stream));
     ADJ_TRY(cudaEventRecord(a->ev[0], a->stream));
@@ -1040,15 +1140,19 @@ int mpma_forward(mpm_adjoint *a, uint32_t substeps, const float *dts, uint32_t c
         // substep's input state and node sums stay in HBM), so the backward
         // pass recomputes nothing; the final state lands in ping[0]
         ADJ_TRY(copy_state(a->tape[0], a->init, a->n, a->stream));
+        k_adj_mark<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(
+            make_adj_ctx(a, a->tape[0], a->tape[0], nullptr, nullptr, 0), marks_of(a, 0));
         for (uint32_t k = 0; k < substeps; ++k)
-            ADJ_TRY(forward_substep(a, a->tape[k], k + 1 < substeps ? a->tape[k + 1] : a->ping[0], a->tape_s[k],
+            ADJ_TRY(forward_substep(a, k, a->tape[k], k + 1 < substeps ? a->tape[k + 1] : a->ping[0], a->tape_s[k],
                                     a->tape_w[k]));
     } else {
         ADJ_TRY(copy_state(a->ping[0], a->init, a->n, a->stream));
+        k_adj_mark<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(
+            make_adj_ctx(a, a->ping[0], a->ping[0], nullptr, nullptr, 0), marks_of(a, 0));
         for (uint32_t k = 0; k < substeps; ++k) {
             if (k % checkpoint_every == 0)
                 ADJ_TRY(copy_state(a->checkpoints[k / checkpoint_every], a->ping[cur], a->n, a->stream));
-            ADJ_TRY(forward_substep(a, a->ping[cur], a->ping[1 - cur], a->sum_s, a->sum_w));
+            ADJ_TRY(forward_substep(a, k, a->ping[cur], a->ping[1 - cur], a->sum_s, a->sum_w));
             cur = 1 - cur;
         }
     }
@@ -1080,17 +1184,11 @@ int mpma_backward(mpm_adjoint *a, float *grad_velocities, double *grad_parameter
     for (int seg = (int)a->checkpoints.size() - 1; seg >= 0; --seg) {
         const uint32_t start = (uint32_t)seg * K, len = std::min(K, a->steps - start);
         if (!a->taped) ADJ_TRY(copy_state(a->tape[0], a->checkpoints[seg], a->n, a->stream));
-        for (uint32_t j = 0; j < len && !a->taped; ++j) {
-            ADJ_TRY(cudaMemsetAsync(a->tape_s[j], 0, (size_t)a->n_nodes * sizeof(float4), a->stream));
-            ADJ_TRY(cudaMemsetAsync(a->tape_w[j], 0, (size_t)a->n_nodes * sizeof(float4), a->stream));
-            const AdjCtx c = make_adj_ctx(a, a->tape[j], j + 1 < len ? a->tape[j + 1] : a->ping[0], a->tape_s[j],
-                                          a->tape_w[j], adj);
-            k_adj_p2g<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(c);
-            if (j + 1 < len) k_adj_g2p<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(c);
-        }
+        for (uint32_t j = 0; j < len && !a->taped; ++j)
+            ADJ_TRY(forward_substep(a, start + j, a->tape[j], j + 1 < len ? a->tape[j + 1] : a->ping[0], a->tape_s[j],
+                                    a->tape_w[j], j + 1 < len));
         for (int j = (int)len - 1; j >= 0; --j) {
-            ADJ_TRY(cudaMemsetAsync(a->ub_s, 0, (size_t)a->n_nodes * sizeof(float2), a->stream));
-            ADJ_TRY(cudaMemsetAsync(a->ub_w, 0, (size_t)a->n_nodes * sizeof(float4), a->stream));
+            clear_marked(a, marks_of(a, start + (uint32_t)j), a->ub_w, nullptr, a->ub_s);
             const AdjCtx c = make_adj_ctx(a, a->tape[j], a->tape[j], a->tape_s[j], a->tape_w[j], adj);
             k_adj_g2p_bwd<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(c);
             k_adj_p2g_bwd<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(c);
