@@ -355,18 +355,18 @@ __device__ __forceinline__ float4 project_liquid(float4 T)
 }  // namespace
 
 // Marks the clearing tiles that the stencil with base (bx, by) reaches (its
-// corner nodes lie in at most four); the lanes of a warp marking the same
-// tile store once.
+// corner nodes lie in at most four).  Lanes of a warp storing to the same
+// mark byte in one instruction make one memory transaction.
 __device__ __forceinline__ void mark_tiles(uint8_t *mark, const AdjScene &S, int bx, int by)
 {
-    const unsigned active = __activemask();
     const uint32_t x0 = (uint32_t)(bx + 1) / ADJ_TILE, x1 = (uint32_t)(bx + 3) / ADJ_TILE;
     const uint32_t y0 = (uint32_t)(by + 1) / ADJ_TILE, y1 = (uint32_t)(by + 3) / ADJ_TILE;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const uint32_t t = S.tile_base + ((k & 2) ? y1 : y0) * S.tiles_x + ((k & 1) ? x1 : x0);
-        const unsigned same = __match_any_sync(active, t);
-        if ((threadIdx.x & 31u) == (uint32_t)(__ffs(same) - 1)) mark[t] = 1u;
+    uint8_t *row0 = mark + S.tile_base + y0 * S.tiles_x, *row1 = mark + S.tile_base + y1 * S.tiles_x;
+    row0[x0] = 1u;
+    if (x1 != x0) row0[x1] = 1u;
+    if (y1 != y0) {
+        row1[x0] = 1u;
+        if (x1 != x0) row1[x1] = 1u;
     }
 }
 
