@@ -1937,7 +1937,12 @@ __device__ __forceinline__ void flush_active_nodes(uint32_t *counters, uint32_t 
 template <bool SCENES, bool BODIES>
 __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
 {
-    __shared__ uint2 s_info[9];
+    // per buffer parity: the tile, its bucket range and its 3x3 neighbours'
+    // (stamp, mask); with one scene the next tile's are copied in while this
+    // one's particles move, and the index of the one after it
+    __shared__ uint32_t s_tile[2];
+    __shared__ uint2 s_range[2];
+    __shared__ uint2 s_infos[2][9];
     __shared__ float2 s_vol[VOL_X * VOL_Y];
     __shared__ float2 s_vs[RING_NODES];
     __shared__ float4 s_vw[RING_NODES];
@@ -1951,8 +1956,16 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
     __shared__ uint32_t p_mat[G2P_STAGE], p_orig[G2P_STAGE];
     const uint32_t n_active = c0.work[WORK_ACTIVE + c0.parity];
     uint32_t ws = 0, ww = 0, wo = 0;
-    for (uint32_t item = blockIdx.x; item < n_active; item += gridDim.x) {
-        const uint32_t tile = c0.active_tiles[item];
+    if constexpr (!SCENES) {
+        // visible after the first iteration's barrier
+        if (threadIdx.x == 0 && blockIdx.x + gridDim.x < n_active) s_tile[1] = c0.active_tiles[blockIdx.x + gridDim.x];
+    }
+    uint32_t it = 0;
+    for (uint32_t item = blockIdx.x; item < n_active; item += gridDim.x, ++it) {
+        const uint32_t buf = it & 1u;
+        const bool fetched = !SCENES && it > 0u;  // copied in during the previous tile
+        uint2 *const info = s_infos[buf];
+        const uint32_t tile = fetched ? s_tile[buf] : c0.active_tiles[item];
         const Ctx c = tile_ctx<SCENES>(c0, tile);
         const StepParams &P = *c.P;
         const uint32_t stamp = c.counters[COUNTER_STAMP];
@@ -1961,20 +1974,42 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
         const uint32_t local = tile - P.tile_base;
         const int tx = (int)(local % P.tiles_x), ty = (int)(local / P.tiles_x);
         const int x0 = tx * TILE_X, y0 = ty * TILE_Y;
-        const uint2 range = c.tile_range[tile];
+        const uint2 range = fetched ? s_range[buf] : c.tile_range[tile];
         const uint32_t begin = range.x, end = range.x + range.y;
         __syncthreads();  // readers of the previous tile's shared data are done
-        if (threadIdx.x < 9) {
+        if (!fetched && threadIdx.x < 9) {
             const int sx = tx + (int)(threadIdx.x % 3) - 1, sy = ty + (int)(threadIdx.x / 3) - 1;
-            s_info[threadIdx.x] = (sx >= 0 && sy >= 0 && sx < tiles_x && sy < tiles_y)
-                                      ? c.tile_info[P.tile_base + (uint32_t)(sy * tiles_x + sx)]
-                                      : make_uint2(0xffffffffu, 0u);
+            info[threadIdx.x] = (sx >= 0 && sy >= 0 && sx < tiles_x && sy < tiles_y)
+                                    ? c.tile_info[P.tile_base + (uint32_t)(sy * tiles_x + sx)]
+                                    : make_uint2(0xffffffffu, 0u);
         }
         if (threadIdx.x == 0) s_fail = *(volatile uint32_t *)c.status != 0u ? 2 : 0;
         // the first chunk of particles, copied in while the node phase runs
         stage_chunk(c, begin, min(end - begin, (uint32_t)G2P_STAGE), p_pos, p_F, p_vol, p_pvol, p_damage, p_mat,
                     p_orig);
         __syncthreads();
+        if constexpr (!SCENES) {
+            // the next tile's range and neighbour records (its index came in
+            // during the previous tile) and the index of the tile after it;
+            // every copy has landed by this tile's cp.async waits
+            const uint32_t nb = buf ^ 1u;
+            if (item + gridDim.x < n_active && threadIdx.x < 10) {
+                const uint32_t tn = s_tile[nb];
+                if (threadIdx.x == 9) {
+                    cp_async<8>(&s_range[nb], &c.tile_range[tn]);
+                } else {
+                    const uint32_t ln = tn - P.tile_base;
+                    const int sx = (int)(ln % P.tiles_x) + (int)(threadIdx.x % 3) - 1;
+                    const int sy = (int)(ln / P.tiles_x) + (int)(threadIdx.x / 3) - 1;
+                    if (sx >= 0 && sy >= 0 && sx < tiles_x && sy < tiles_y)
+                        cp_async<8>(&s_infos[nb][threadIdx.x], &c.tile_info[P.tile_base + (uint32_t)(sy * tiles_x + sx)]);
+                    else
+                        s_infos[nb][threadIdx.x] = make_uint2(0xffffffffu, 0u);
+                }
+            }
+            if (threadIdx.x == 10 && item + 2u * gridDim.x < n_active)
+                cp_async<4>(&s_tile[buf], &c0.active_tiles[item + 2u * gridDim.x]);
+        }
         if (s_fail) {
             cp_async_wait_all();  // no copy may land after this tile's shared data is reused
             continue;             // the scene's substep is rolled back
@@ -1992,7 +2027,7 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
 #pragma unroll
         for (int k = 0; k < ACC_WORDS; ++k) sum[k] = 0.f;
         if (in_grid) {
-            const NodeSources ns = node_sources(P, s_info, tx, ty, hx, hy, stamp);
+            const NodeSources ns = node_sources(P, info, tx, ty, hx, hy, stamp);
             add_sources(c, ns, ring_node, sum);
         }
         if (in_region) s_vol[t] = make_float2(sum[6], sum[10]);
@@ -2015,10 +2050,10 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
                     // tile, left, below, below-left)
                     const int dx = rx >= TILE_X ? 1 : 0, dy = ry >= TILE_Y ? 1 : 0;
                     int ox = dx, oy = dy;
-                    if (s_info[(dy + 1) * 3 + dx + 1].x != stamp) {
-                        if (s_info[(dy + 1) * 3 + dx].x == stamp)
+                    if (info[(dy + 1) * 3 + dx + 1].x != stamp) {
+                        if (info[(dy + 1) * 3 + dx].x == stamp)
                             ox = dx - 1;
-                        else if (s_info[dy * 3 + dx + 1].x == stamp)
+                        else if (info[dy * 3 + dx + 1].x == stamp)
                             oy = dy - 1;
                         else
                             ox = dx - 1, oy = dy - 1;
