@@ -1965,6 +1965,8 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
         const uint32_t buf = it & 1u;
         const bool fetched = !SCENES && it > 0u;  // copied in during the previous tile
         uint2 *const info = s_infos[buf];
+        // (the copies read here landed, and were made visible by a barrier,
+        // during the previous tile)
         const uint32_t tile = fetched ? s_tile[buf] : c0.active_tiles[item];
         const Ctx c = tile_ctx<SCENES>(c0, tile);
         const StepParams &P = *c.P;
@@ -2012,6 +2014,7 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
         }
         if (s_fail) {
             cp_async_wait_all();  // no copy may land after this tile's shared data is reused
+            __syncthreads();      // and the copies are visible to the next tile
             continue;             // the scene's substep is rolled back
         }
         // node phase: thread t takes node (x0 - 1 + t % VOL_X, y0 - 1 + t / VOL_X)
