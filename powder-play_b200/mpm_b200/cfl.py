@@ -97,9 +97,35 @@ def calculate_mpm_cfl_safe_dt(cellSize, waveSpeedBound, velocityBound, courantLi
     return safe
 
 
+_PLAN_CACHE: dict = {}
+_PLAN_CACHE_LIMIT = 4096
+
+
 def calculate_mpm_cfl_microsteps(macroDt, cellSize, waveSpeedBound, velocityBound, maxMicrosteps,
                                  minimumStepCount=1, courantLimit=DEFAULT_MPM_COURANT_LIMIT) -> dict:
-    """calculateMpmCflMicrosteps, cfl.ts:151-232 -> {stepCount, microDt, safeDt}."""
+    """calculateMpmCflMicrosteps, cfl.ts:151-232 -> {stepCount, microDt, safeDt}.
+
+    A pure function of its arguments; the adaptive stepping loop asks for the
+    same plan several times per macrostep (the caller's plan, then the
+    solver's certification of it), so successful plans are remembered by the
+    arguments' types and values (errors are raised afresh every time)."""
+    args = (macroDt, cellSize, waveSpeedBound, velocityBound, maxMicrosteps, minimumStepCount, courantLimit)
+    try:
+        key = tuple((type(a), a) for a in args)
+        plan = _PLAN_CACHE.get(key)
+    except TypeError:  # an unhashable argument: no caching
+        key, plan = None, None
+    if plan is None:
+        plan = _calculate_mpm_cfl_microsteps(*args)
+        if key is not None:
+            if len(_PLAN_CACHE) >= _PLAN_CACHE_LIMIT:
+                _PLAN_CACHE.clear()
+            _PLAN_CACHE[key] = plan
+    return dict(plan)
+
+
+def _calculate_mpm_cfl_microsteps(macroDt, cellSize, waveSpeedBound, velocityBound, maxMicrosteps,
+                                  minimumStepCount=1, courantLimit=DEFAULT_MPM_COURANT_LIMIT) -> dict:
     if courantLimit is None:
         courantLimit = DEFAULT_MPM_COURANT_LIMIT
     if minimumStepCount is None:
