@@ -902,7 +902,7 @@ struct Stage {
     float4 state[STAGE_CAP];     // fx, fy, mass, liquid volume
     float4 affine[STAGE_CAP];    // A = m C + (-dt V 4/dx^2) P F^T
     float2 momentum[STAGE_CAP];  // m v
-    uint32_t orig[STAGE_CAP];
+    uint32_t orig[STAGE_CAP];    // original index; after the count pass channel << 30 | original index
     uint32_t cell[STAGE_CAP];    // local cell | channel << 8 | REC_FAILED
     uint16_t order[STAGE_CAP];   // arrival rank within the cell, then rank by (channel, original index)
     uint16_t sorted[STAGE_CAP];  // staged indices grouped by cell
@@ -932,7 +932,7 @@ __device__ __forceinline__ uint32_t channel_start(const Stage &sm, uint32_t lo, 
 
 __device__ __forceinline__ uint32_t sort_key(const Stage &sm, uint32_t k)
 {
-    return (((sm.cell[k] >> 8) & 3u) << 30) | sm.orig[k];
+    return sm.orig[k];  // channel << 30 | original index, set by p2g_chunk's count pass
 }
 
 // Stages the records of the slots src[i0 .. i1) with asynchronous copies,
@@ -975,6 +975,10 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, const uint32_
         }
         sm.order[k] = (uint16_t)atomicAdd(&sm.count[cell & 0xffu], 1u);
         mask |= 1u << ((cell >> 8) & 3u);
+        // from here on the entry's word holds its sort key: channel in the top
+        // two bits over the original index (below 2^30: far more particles
+        // than the device memory holds)
+        sm.orig[k] |= ((cell >> 8) & 3u) << 30;
     }
     if (mask) atomicOr(&sm.mask, mask);
     __syncthreads();
