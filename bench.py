@@ -453,9 +453,11 @@ def run_b200_batched(args):
     n_total = int(batch.particle_counts.sum())
     velocity = [b["velocityBound"] for b in batch.cfl_bounds]
 
+    batch.recovery_bound_factor = args.cfl_recovery_factor
+
     def one_step():
         nonlocal velocity
-        bounds = [_batched_bound(v, macro_dt, gravity) for v in velocity]
+        bounds = [_batched_bound(v, macro_dt, gravity) * args.cfl_plan_margin for v in velocity]
         results = batch.step_cfl_batch_adaptive(macro_dt, bounds, BATCHED_MAX_MICROSTEPS, gravity)
         velocity = [r["recommendedVelocityBound"] for r in results]
         return results
@@ -522,6 +524,8 @@ def run_b200_batched(args):
                    "l2": "inputs larger than L2 (every scene's state, about 0.8 GB)",
                    "committed_particle_substeps": work, "submits": submits, "retries": retries,
                    "launch_shape": shape,
+                   "cfl_policy": {"recovery_factor": args.cfl_recovery_factor, "plan_margin": args.cfl_plan_margin,
+                                  "scene_macrosteps_per_device_s": world * len(scenes) * args.steps / device_s},
                    "plain_per_scene": {"value": plain, "unit": UNIT,
                                        "sample": f"the first {PLAIN_SAMPLE_SCENES} scenes, each alone in its own "
                                                  "solver, one timed macrostep each"}},
@@ -808,6 +812,9 @@ def main():
     ap.add_argument("--cpu-substeps", type=int, default=12)
     ap.add_argument("--reference-substeps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # the batched workload's adaptive CFL policy (the reference's: 1.25 and no margin)
+    ap.add_argument("--cfl-recovery-factor", type=float, default=1.25)
+    ap.add_argument("--cfl-plan-margin", type=float, default=1.0)
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be at least 3")

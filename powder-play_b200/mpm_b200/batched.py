@@ -54,6 +54,9 @@ class MpmBatchedGpuSolver:
         self._counts = counts
         self._bases = np.concatenate([[0], np.cumsum(counts, dtype=np.int64)])
         self._disposed = False
+        # the factor a failed batch's observed speed and wave speed are raised by
+        # before the retry (solver.ts:73 fixes it at 1.25); callers may study others
+        self.recovery_bound_factor = CFL_RECOVERY_BOUND_SAFETY_FACTOR
         self.device_ms_total = 0.0
         self.committed_particle_substeps = 0
 
@@ -207,9 +210,9 @@ class MpmBatchedGpuSolver:
                     self.committed_particle_substeps += completed * int(self._counts[k])
                     observed = max(error.measured_maximum_speed or 0.0,
                                    (error.cfl_details or {}).get("particleSpeed", 0.0))
-                    retry_velocity = max(sc["velocity"], observed * CFL_RECOVERY_BOUND_SAFETY_FACTOR)
+                    retry_velocity = max(sc["velocity"], observed * self.recovery_bound_factor)
                     if error.cfl_details is not None:
-                        wave = error.cfl_details["waveSpeed"] * CFL_RECOVERY_BOUND_SAFETY_FACTOR
+                        wave = error.cfl_details["waveSpeed"] * self.recovery_bound_factor
                         self.cfl_bounds[k] = b = dict(b, waveSpeedBound=max(b["waveSpeedBound"], wave))
                     sc["velocity"], sc["speed"] = retry_velocity, observed
                     cleared = True

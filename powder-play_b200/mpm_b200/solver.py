@@ -136,6 +136,9 @@ class MpmMlsGpuSolver:
         self.atomic_p2g = atomic_p2g
         self.fixed_point_shift = fixed_point_shift
         self._disposed = False
+        # the factor a failed batch's observed speed and wave speed are raised by
+        # before the retry (solver.ts:73 fixes it at 1.25); callers may study others
+        self.recovery_bound_factor = CFL_RECOVERY_BOUND_SAFETY_FACTOR
         self._slot_count = state.particle_count      # particleSlotCount (allocated original indices)
         self._active_count = state.particle_count    # activeParticleCount
         self._has_removed = False
@@ -323,13 +326,13 @@ class MpmMlsGpuSolver:
                 observed = max(error.measured_maximum_speed or 0.0,
                                (error.cfl_details or {}).get("particleSpeed", 0.0))
                 retry_velocity = max(attempt_velocity, self._last_scheduled_velocity_bound or 0.0,
-                                     observed * CFL_RECOVERY_BOUND_SAFETY_FACTOR)
+                                     observed * self.recovery_bound_factor)
                 if not math.isfinite(retry_velocity):
                     raise RuntimeError(f"Adaptive CFL recovery stopped after {retry_count} retry attempt(s) "
                                        f"(non-finite velocity bound); last GPU error: {error}") from error
                 self._last_scheduled_velocity_bound = retry_velocity
                 if error.cfl_details is not None:
-                    retry_wave = error.cfl_details["waveSpeed"] * CFL_RECOVERY_BOUND_SAFETY_FACTOR
+                    retry_wave = error.cfl_details["waveSpeed"] * self.recovery_bound_factor
                     if not math.isfinite(retry_wave):
                         raise RuntimeError(f"Adaptive CFL recovery stopped after {retry_count} retry attempt(s) "
                                            f"(non-finite wave-speed bound); last GPU error: {error}") from error
