@@ -810,7 +810,7 @@ def main():
     ap.add_argument("--p2g", choices=["gather", "fixed"], default="gather")
     ap.add_argument("--fixed-shift", type=int, default=16)
     ap.add_argument("--cpu-substeps", type=int, default=12)
-    ap.add_argument("--reference-substeps", type=int, default=2)
+    ap.add_argument("--reference-substeps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # the batched workload's adaptive CFL policy (the reference's: 1.25 and no margin)
     ap.add_argument("--cfl-recovery-factor", type=float, default=1.25)
