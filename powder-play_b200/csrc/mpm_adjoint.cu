@@ -82,7 +82,7 @@ struct AdjCtx {
     float4 *Cb_next, *Fb_next, *Cb, *Fb;
     float2 *xg;            // the G2P part of the input position adjoint
     float4 *Fg;            // the G2P part of the input F adjoint
-    float2 *ub_s;          // per node: solid velocity adjoint
+    float4 *ub_s;          // per node: solid velocity adjoint (x, y), then (Qx, Qy, M) adjoints, 0
     float4 *ub_w;          // per node: water velocity, liquid mass, liquid volume adjoints
     double *param_grad;    // per scene: tait, lambda_s, mu_s
     const float2 *target;  // per particle
@@ -468,6 +468,43 @@ __global__ void __launch_bounds__(ADJ_TILE * ADJ_TILE) k_adj_clear(const AdjScen
     }
 }
 
+// The grid-update adjoint of the marked tiles' nodes, in place: the node
+// velocity adjoints that k_adj_g2p_bwd scattered become the adjoints of the
+// node sums (u = D (q / m + dt g): momentum q, mass m; the liquid volume's
+// passes through), once per node instead of once per particle reaching it.
+// One tile per CTA iteration, one node per thread.
+__global__ void __launch_bounds__(ADJ_TILE * ADJ_TILE) k_adj_grid_bwd(AdjCtx c, const uint32_t *tile_scene,
+                                                                      uint32_t n_tiles, const uint8_t *mark)
+{
+    for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        if (!mark[t]) continue;  // the same answer for the whole CTA
+        const AdjScene &S = c.scenes[tile_scene[t]];
+        const uint32_t local = t - S.tile_base;
+        const uint32_t hx = (local % S.tiles_x) * ADJ_TILE + threadIdx.x % ADJ_TILE;
+        const uint32_t hy = (local / S.tiles_x) * ADJ_TILE + threadIdx.x / ADJ_TILE;
+        if (hx >= S.node_w || hy >= S.cells_y + 3u) continue;
+        const uint32_t n = S.node_base + hy * S.node_w + hx;
+        const int ix = (int)hx - 1, iy = (int)hy - 1;
+#pragma unroll
+        for (int channel = 0; channel < 2; ++channel) {
+            float4 *ub = channel ? c.ub_w : c.ub_s;
+            const float4 sum = channel ? c.sum_w[n] : c.sum_s[n];
+            const float4 b = ub[n];  // velocity (x, y), liquid mass, liquid volume adjoints
+            float M_b = channel ? b.z : 0.f, Qx_b = 0.f, Qy_b = 0.f;
+            if (sum.x > 0.0f) {
+                float2 D;
+                node_velocity_adj(S, sum, ix, iy, D);
+                const float inv = 1.0f / sum.x;
+                const float udx = D.x * b.x, udy = D.y * b.y;
+                Qx_b = udx * inv;
+                Qy_b = udy * inv;
+                M_b -= (udx * sum.y + udy * sum.z) * inv * inv;
+            }
+            ub[n] = make_float4(Qx_b, Qy_b, M_b, channel ? b.w : 0.f);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(ADJ_THREADS) k_adj_loss(AdjCtx c)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -585,7 +622,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) k_adj_g2p_bwd(AdjCtx c)
             if (liquid)
                 atomicAdd(&c.ub_w[n], make_float4(ubx, uby, w * pm_b, w * pv_b));
             else
-                atomicAdd(&c.ub_s[n], make_float2(ubx, uby));
+                atomicAdd(reinterpret_cast<float2 *>(&c.ub_s[n]), make_float2(ubx, uby));
             // d/dx of w: (dwx wy, wx dwy) / dx
             const float gwx = st.dwx[ox] * st.wy[oy] * S.inv_dx, gwy = st.wx[ox] * st.dwy[oy] * S.inv_dx;
             float sval = u.x * (vpb.x + Bb.x * dpx + Bb.y * dpy) + u.y * (vpb.y + Bb.z * dpx + Bb.w * dpy);
@@ -660,29 +697,9 @@ __global__ void __launch_bounds__(ADJ_THREADS, 3) k_adj_p2g_bwd(AdjCtx c)
                     const float dpx = ((float)ox - st.fx) * S.dx;
                     const int ix = st.bx + ox, iy = st.by + oy;
                     const uint32_t n = adj_node(S, ix, iy);
-                    const float4 sum = liquid ? c.sum_w[n] : c.sum_s[n];
-                    float2 ub;
-                    float lm_b = 0.f, lv_b = 0.f;
-                    if (liquid) {
-                        const float4 t = c.ub_w[n];
-                        ub = make_float2(t.x, t.y);
-                        lm_b = t.z;
-                        lv_b = t.w;
-                    } else {
-                        ub = c.ub_s[n];
-                    }
-                    // grid update adjoint: u = D (q / m + dt g)
-                    float M_b = lm_b, Qx_b = 0.f, Qy_b = 0.f;
-                    if (sum.x > 0.0f) {
-                        float2 D;
-                        node_velocity_adj(S, sum, ix, iy, D);
-                        const float inv = 1.0f / sum.x;
-                        const float udx = D.x * ub.x, udy = D.y * ub.y;
-                        Qx_b = udx * inv;
-                        Qy_b = udy * inv;
-                        M_b -= (udx * sum.y + udy * sum.z) * inv * inv;
-                    }
-                    const float V_b = lv_b;
+                    // the node's sum adjoints (k_adj_grid_bwd): momentum, mass, liquid volume
+                    const float4 g = liquid ? c.ub_w[n] : c.ub_s[n];
+                    const float Qx_b = g.x, Qy_b = g.y, M_b = g.z, V_b = g.w;
                     // P2G adjoint of M += w m, Q += w (m v + A dp), V += w vliq
                     vb.x += w * p.m * Qx_b;
                     vb.y += w * p.m * Qy_b;
@@ -736,8 +753,8 @@ struct mpm_adjoint {
     uint32_t n_tiles = 0;
     unsigned clear_ctas = 1;
     std::vector<float4 *> tape_s, tape_w;       // per recomputed substep
-    float2 *xb[2]{}, *vb[2]{}, *xg = nullptr, *ub_s = nullptr;
-    float4 *Cb[2]{}, *Fb[2]{}, *Fg = nullptr, *ub_w = nullptr;
+    float2 *xb[2]{}, *vb[2]{}, *xg = nullptr;
+    float4 *Cb[2]{}, *Fb[2]{}, *Fg = nullptr, *ub_w = nullptr, *ub_s = nullptr;
     double *param_grad = nullptr, *loss = nullptr;
     float2 *target = nullptr, *final_x = nullptr;
     uint32_t steps = 0, every = 0;
@@ -1188,9 +1205,11 @@ int mpma_backward(mpm_adjoint *a, float *grad_velocities, double *grad_parameter
             ADJ_TRY(forward_substep(a, start + j, a->tape[j], j + 1 < len ? a->tape[j + 1] : a->ping[0], a->tape_s[j],
                                     a->tape_w[j], j + 1 < len));
         for (int j = (int)len - 1; j >= 0; --j) {
-            clear_marked(a, marks_of(a, start + (uint32_t)j), a->ub_w, nullptr, a->ub_s);
+            const uint8_t *marks = marks_of(a, start + (uint32_t)j);
+            clear_marked(a, marks, a->ub_w, a->ub_s, nullptr);
             const AdjCtx c = make_adj_ctx(a, a->tape[j], a->tape[j], a->tape_s[j], a->tape_w[j], adj);
             k_adj_g2p_bwd<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(c);
+            k_adj_grid_bwd<<<a->clear_ctas, ADJ_TILE * ADJ_TILE, 0, a->stream>>>(c, a->tile_scene, a->n_tiles, marks);
             k_adj_p2g_bwd<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(c);
             adj = 1 - adj;
         }
