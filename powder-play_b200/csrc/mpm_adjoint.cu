@@ -77,6 +77,8 @@ struct AdjCtx {
     uint32_t *status;
     AdjState in, out;
     float4 *sum_s, *sum_w;  // per node: solid (m, qx, qy, 0), water (m, qx, qy, V)
+    float2 *gv_s;           // per node: solid velocity (k_adj_grid_fwd)
+    float4 *gv_w;           // per node: water velocity (x, y), liquid mass, liquid volume
     // adjoints: of the substep's outputs (next) and inputs (cur)
     float2 *xb_next, *vb_next, *xb, *vb;
     float4 *Cb_next, *Fb_next, *Cb, *Fb;
@@ -301,9 +303,16 @@ __device__ __forceinline__ bool g2p_forward(const AdjCtx &c, const AdjScene &S, 
             const float w = st.wx[ox] * st.wy[oy];
             const float dpx = ((float)ox - st.fx) * S.dx;
             const uint32_t n = adj_node(S, st.bx + ox, st.by + oy);
-            const float4 sum = liquid ? c.sum_w[n] : c.sum_s[n];
-            float2 D;
-            const float2 u = node_velocity_adj(S, sum, st.bx + ox, st.by + oy, D);
+            float2 u;
+            float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);  // liquid mass in x, liquid volume in w
+            if (liquid) {
+                const float4 gw = c.gv_w[n];
+                u = make_float2(gw.x, gw.y);
+                sum.x = gw.z;
+                sum.w = gw.w;
+            } else {
+                u = c.gv_s[n];
+            }
             if constexpr (KEEP) {
                 keep_u[oy * 3 + ox][threadIdx.x] = u;
                 keep_mv[oy * 3 + ox][threadIdx.x] = make_float2(sum.x, sum.w);
@@ -465,6 +474,30 @@ __global__ void __launch_bounds__(ADJ_TILE * ADJ_TILE) k_adj_clear(const AdjScen
         if (a) a[n] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (b) b[n] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (c2) c2[n] = make_float2(0.f, 0.f);
+    }
+}
+
+// The grid update of the marked tiles' nodes (finishGridVelocity with the
+// wall factors, node_velocity_adj): each node's velocity from its sums, once
+// per node, for the G2P kernels; the water record also carries the node's
+// liquid mass and volume.  One tile per CTA iteration, one node per thread.
+__global__ void __launch_bounds__(ADJ_TILE * ADJ_TILE) k_adj_grid_fwd(AdjCtx c, const uint32_t *tile_scene,
+                                                                      uint32_t n_tiles, const uint8_t *mark)
+{
+    for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        if (!mark[t]) continue;  // the same answer for the whole CTA
+        const AdjScene &S = c.scenes[tile_scene[t]];
+        const uint32_t local = t - S.tile_base;
+        const uint32_t hx = (local % S.tiles_x) * ADJ_TILE + threadIdx.x % ADJ_TILE;
+        const uint32_t hy = (local / S.tiles_x) * ADJ_TILE + threadIdx.x / ADJ_TILE;
+        if (hx >= S.node_w || hy >= S.cells_y + 3u) continue;
+        const uint32_t n = S.node_base + hy * S.node_w + hx;
+        const int ix = (int)hx - 1, iy = (int)hy - 1;
+        float2 D;
+        c.gv_s[n] = node_velocity_adj(S, c.sum_s[n], ix, iy, D);
+        const float4 w = c.sum_w[n];
+        const float2 u = node_velocity_adj(S, w, ix, iy, D);
+        c.gv_w[n] = make_float4(u.x, u.y, w.x, w.w);
     }
 }
 
@@ -755,6 +788,8 @@ struct mpm_adjoint {
     std::vector<float4 *> tape_s, tape_w;       // per recomputed substep
     float2 *xb[2]{}, *vb[2]{}, *xg = nullptr;
     float4 *Cb[2]{}, *Fb[2]{}, *Fg = nullptr, *ub_w = nullptr, *ub_s = nullptr;
+    float2 *gv_s = nullptr;  // node velocities of the substep at hand
+    float4 *gv_w = nullptr;
     double *param_grad = nullptr, *loss = nullptr;
     float2 *target = nullptr, *final_x = nullptr;
     uint32_t steps = 0, every = 0;
@@ -812,7 +847,7 @@ void free_engine(mpm_adjoint *a)
     for (float4 *p : a->tape_s) cudaFree(p);
     for (float4 *p : a->tape_w) cudaFree(p);
     void *ptrs[] = {a->mark, a->tile_scene, a->d_scenes, a->scene_of, a->liquid, a->status, a->vol, a->sum_s, a->sum_w, a->xb[0], a->xb[1],
-                    a->vb[0], a->vb[1], a->xg, a->ub_s, a->Cb[0], a->Cb[1], a->Fb[0], a->Fb[1], a->Fg, a->ub_w,
+                    a->vb[0], a->vb[1], a->xg, a->ub_s, a->Cb[0], a->Cb[1], a->Fb[0], a->Fb[1], a->Fg, a->ub_w, a->gv_s, a->gv_w,
                     a->param_grad, a->loss, a->target, a->final_x};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -862,6 +897,8 @@ AdjCtx make_adj_ctx(mpm_adjoint *a, const AdjState &in, const AdjState &out, flo
     c.xg = a->xg;
     c.Fg = a->Fg;
     c.ub_s = a->ub_s;
+    c.gv_s = a->gv_s;
+    c.gv_w = a->gv_w;
     c.ub_w = a->ub_w;
     c.param_grad = a->param_grad;
     c.target = a->target;
@@ -893,7 +930,11 @@ cudaError_t forward_substep(mpm_adjoint *a, uint32_t k, const AdjState &in, cons
     AdjCtx c = make_adj_ctx(a, in, out, ss, sw, 0);
     c.mark_out = marks_of(a, k + 1);
     k_adj_p2g<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(c);
-    if (run_g2p) k_adj_g2p<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(c);
+    if (run_g2p) {
+        k_adj_grid_fwd<<<a->clear_ctas, ADJ_TILE * ADJ_TILE, 0, a->stream>>>(c, a->tile_scene, a->n_tiles,
+                                                                             marks_of(a, k));
+        k_adj_g2p<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(c);
+    }
     return cudaGetLastError();
 }
 
@@ -1034,6 +1075,8 @@ int mpma_create(const mpm_config *configs, uint32_t scene_count, const uint32_t 
     ADJ_ALLOC(a->Fg, n);
     ADJ_ALLOC(a->ub_s, nodes);
     ADJ_ALLOC(a->ub_w, nodes);
+    ADJ_ALLOC(a->gv_s, nodes);
+    ADJ_ALLOC(a->gv_w, nodes);
     ADJ_ALLOC(a->param_grad, 3 * (size_t)scene_count);
     ADJ_ALLOC(a->loss, scene_count);
     ADJ_ALLOC(a->target, n);
@@ -1208,6 +1251,7 @@ int mpma_backward(mpm_adjoint *a, float *grad_velocities, double *grad_parameter
             const uint8_t *marks = marks_of(a, start + (uint32_t)j);
             clear_marked(a, marks, a->ub_w, a->ub_s, nullptr);
             const AdjCtx c = make_adj_ctx(a, a->tape[j], a->tape[j], a->tape_s[j], a->tape_w[j], adj);
+            k_adj_grid_fwd<<<a->clear_ctas, ADJ_TILE * ADJ_TILE, 0, a->stream>>>(c, a->tile_scene, a->n_tiles, marks);
             k_adj_g2p_bwd<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(c);
             k_adj_grid_bwd<<<a->clear_ctas, ADJ_TILE * ADJ_TILE, 0, a->stream>>>(c, a->tile_scene, a->n_tiles, marks);
             k_adj_p2g_bwd<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(c);
