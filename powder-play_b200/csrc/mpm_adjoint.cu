@@ -454,17 +454,35 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_mark(AdjCtx c, uint8_t *mar
     if (adj_stencil(S, c.in.x[i], st)) mark_tiles(mark, S, st.bx, st.by);
 }
 
-// Zeroes the nodes of the marked tiles in up to three node arrays (NULL:
-// skipped), one tile per CTA iteration and one node per thread: every node a
-// substep adds to or reads lies in a tile its particles mark.  The rest of
-// the grid keeps stale values that no stencil reads.  tile_scene gives each
-// tile's scene.
-__global__ void __launch_bounds__(ADJ_TILE * ADJ_TILE) k_adj_clear(const AdjScene *scenes, const uint32_t *tile_scene,
-                                                                   uint32_t n_tiles, const uint8_t *mark, float4 *a,
-                                                                   float4 *b, float2 *c2)
+constexpr int COMPACT_THREADS = 256;
+
+// Appends the marked tiles of one substep to its list (list[0], zeroed before,
+// counts them; list[1 ..] holds them in no particular order: each tile is
+// cleared and updated on its own).  One tile per thread, one atomic per warp.
+__global__ void __launch_bounds__(COMPACT_THREADS) k_adj_compact(const uint8_t *mark, uint32_t n_tiles, uint32_t *list)
 {
-    for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
-        if (!mark[t]) continue;  // the same answer for the whole CTA
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool marked = t < n_tiles && mark[t] != 0u;
+    const unsigned ballot = __ballot_sync(0xffffffffu, marked);
+    if (!ballot) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t base = 0;
+    if (lane == 0u) base = atomicAdd(list, (uint32_t)__popc(ballot));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (marked) list[1 + base + __popc(ballot & ((1u << lane) - 1u))] = t;
+}
+
+// Zeroes the nodes of the listed (marked) tiles in up to three node arrays
+// (NULL: skipped), one tile per CTA iteration and one node per thread: every
+// node a substep adds to or reads lies in a tile its particles mark.  The rest
+// of the grid keeps stale values that no stencil reads.  tile_scene gives each
+// tile's scene; list[0] counts the tiles in list[1 ..].
+__global__ void __launch_bounds__(ADJ_TILE * ADJ_TILE) k_adj_clear(const AdjScene *scenes, const uint32_t *tile_scene,
+                                                                   const uint32_t *list, float4 *a, float4 *b, float2 *c2)
+{
+    const uint32_t count = list[0];
+    for (uint32_t i = blockIdx.x; i < count; i += gridDim.x) {
+        const uint32_t t = list[1 + i];
         const AdjScene &S = scenes[tile_scene[t]];
         const uint32_t local = t - S.tile_base;
         const uint32_t hx = (local % S.tiles_x) * ADJ_TILE + threadIdx.x % ADJ_TILE;
@@ -482,10 +500,11 @@ __global__ void __launch_bounds__(ADJ_TILE * ADJ_TILE) k_adj_clear(const AdjScen
 // per node, for the G2P kernels; the water record also carries the node's
 // liquid mass and volume.  One tile per CTA iteration, one node per thread.
 __global__ void __launch_bounds__(ADJ_TILE * ADJ_TILE) k_adj_grid_fwd(AdjCtx c, const uint32_t *tile_scene,
-                                                                      uint32_t n_tiles, const uint8_t *mark)
+                                                                      const uint32_t *list)
 {
-    for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
-        if (!mark[t]) continue;  // the same answer for the whole CTA
+    const uint32_t count = list[0];
+    for (uint32_t i = blockIdx.x; i < count; i += gridDim.x) {
+        const uint32_t t = list[1 + i];
         const AdjScene &S = c.scenes[tile_scene[t]];
         const uint32_t local = t - S.tile_base;
         const uint32_t hx = (local % S.tiles_x) * ADJ_TILE + threadIdx.x % ADJ_TILE;
@@ -507,10 +526,11 @@ __global__ void __launch_bounds__(ADJ_TILE * ADJ_TILE) k_adj_grid_fwd(AdjCtx c, 
 // passes through), once per node instead of once per particle reaching it.
 // One tile per CTA iteration, one node per thread.
 __global__ void __launch_bounds__(ADJ_TILE * ADJ_TILE) k_adj_grid_bwd(AdjCtx c, const uint32_t *tile_scene,
-                                                                      uint32_t n_tiles, const uint8_t *mark)
+                                                                      const uint32_t *list)
 {
-    for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
-        if (!mark[t]) continue;  // the same answer for the whole CTA
+    const uint32_t count = list[0];
+    for (uint32_t i = blockIdx.x; i < count; i += gridDim.x) {
+        const uint32_t t = list[1 + i];
         const AdjScene &S = c.scenes[tile_scene[t]];
         const uint32_t local = t - S.tile_base;
         const uint32_t hx = (local % S.tiles_x) * ADJ_TILE + threadIdx.x % ADJ_TILE;
@@ -782,6 +802,7 @@ struct mpm_adjoint {
     float4 *sum_s = nullptr, *sum_w = nullptr;   // forward scratch
     uint8_t *mark = nullptr;                     // per substep (0 .. steps) and clearing tile
     size_t mark_count = 0;
+    uint32_t *lists = nullptr;                   // per substep: marked-tile count, then the tiles
     uint32_t *tile_scene = nullptr;              // per clearing tile
     uint32_t n_tiles = 0;
     unsigned clear_ctas = 1;
@@ -846,7 +867,7 @@ void free_engine(mpm_adjoint *a)
     for (auto &s : a->tape) free_state(s);
     for (float4 *p : a->tape_s) cudaFree(p);
     for (float4 *p : a->tape_w) cudaFree(p);
-    void *ptrs[] = {a->mark, a->tile_scene, a->d_scenes, a->scene_of, a->liquid, a->status, a->vol, a->sum_s, a->sum_w, a->xb[0], a->xb[1],
+    void *ptrs[] = {a->mark, a->lists, a->tile_scene, a->d_scenes, a->scene_of, a->liquid, a->status, a->vol, a->sum_s, a->sum_w, a->xb[0], a->xb[1],
                     a->vb[0], a->vb[1], a->xg, a->ub_s, a->Cb[0], a->Cb[1], a->Fb[0], a->Fb[1], a->Fg, a->ub_w, a->gv_s, a->gv_w,
                     a->param_grad, a->loss, a->target, a->final_x};
     for (void *p : ptrs)
@@ -912,11 +933,21 @@ unsigned blocks(uint32_t n) { return std::max(1u, (n + ADJ_THREADS - 1) / ADJ_TH
 // The clearing-tile marks of substep k (its input positions).
 uint8_t *marks_of(mpm_adjoint *a, uint32_t k) { return a->mark + (size_t)k * a->n_tiles; }
 
-// Zeroes the node arrays over the marked tiles of one substep (NULL arrays are skipped).
-void clear_marked(mpm_adjoint *a, const uint8_t *mark, float4 *x, float4 *y, float2 *z)
+// The marked-tile list of substep k.
+uint32_t *list_of(mpm_adjoint *a, uint32_t k) { return a->lists + (size_t)k * (a->n_tiles + 1u); }
+
+// Lists the marked tiles of substep k.
+void compact_marks(mpm_adjoint *a, uint32_t k)
 {
-    k_adj_clear<<<a->clear_ctas, ADJ_TILE * ADJ_TILE, 0, a->stream>>>(a->d_scenes, a->tile_scene, a->n_tiles, mark, x,
-                                                                        y, z);
+    cudaMemsetAsync(list_of(a, k), 0, sizeof(uint32_t), a->stream);
+    k_adj_compact<<<blocks(a->n_tiles), COMPACT_THREADS, 0, a->stream>>>(marks_of(a, k), a->n_tiles, list_of(a, k));
+}
+
+// Zeroes the node arrays over the marked tiles of substep k (NULL arrays are skipped).
+void clear_marked(mpm_adjoint *a, uint32_t k, float4 *x, float4 *y, float2 *z)
+{
+    k_adj_clear<<<a->clear_ctas, ADJ_TILE * ADJ_TILE, 0, a->stream>>>(a->d_scenes, a->tile_scene, list_of(a, k), x, y,
+                                                                        z);
 }
 
 // One forward substep k from `in` into `out`, its node sums in ss / sw: they
@@ -926,14 +957,14 @@ void clear_marked(mpm_adjoint *a, const uint8_t *mark, float4 *x, float4 *y, flo
 cudaError_t forward_substep(mpm_adjoint *a, uint32_t k, const AdjState &in, const AdjState &out, float4 *ss, float4 *sw,
                             bool run_g2p = true)
 {
-    clear_marked(a, marks_of(a, k), ss, sw, nullptr);
+    clear_marked(a, k, ss, sw, nullptr);
     AdjCtx c = make_adj_ctx(a, in, out, ss, sw, 0);
     c.mark_out = marks_of(a, k + 1);
     k_adj_p2g<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(c);
     if (run_g2p) {
-        k_adj_grid_fwd<<<a->clear_ctas, ADJ_TILE * ADJ_TILE, 0, a->stream>>>(c, a->tile_scene, a->n_tiles,
-                                                                             marks_of(a, k));
+        k_adj_grid_fwd<<<a->clear_ctas, ADJ_TILE * ADJ_TILE, 0, a->stream>>>(c, a->tile_scene, list_of(a, k));
         k_adj_g2p<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(c);
+        compact_marks(a, k + 1);
     }
     return cudaGetLastError();
 }
@@ -1186,7 +1217,11 @@ int mpma_forward(mpm_adjoint *a, uint32_t substeps, const float *dts, uint32_t c
         cudaFree(a->mark);
         a->mark = nullptr;
         a->mark_count = 0;
-        if (adj_alloc(&a->mark, marks) != cudaSuccess) return err(MPM_ERR_CUDA, "tile mark allocation failed");
+        cudaFree(a->lists);
+        a->lists = nullptr;
+        if (adj_alloc(&a->mark, marks) != cudaSuccess ||
+            adj_alloc(&a->lists, ((size_t)substeps + 1) * (a->n_tiles + 1u)) != cudaSuccess)
+            return err(MPM_ERR_CUDA, "tile mark allocation failed");
         a->mark_count = marks;
     }
     ADJ_TRY(cudaMemsetAsync(a->mark, 0, marks, a->stream));
@@ -1202,6 +1237,7 @@ int mpma_forward(mpm_adjoint *a, uint32_t substeps, const float *dts, uint32_t c
         ADJ_TRY(copy_state(a->tape[0], a->init, a->n, a->stream));
         k_adj_mark<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(
             make_adj_ctx(a, a->tape[0], a->tape[0], nullptr, nullptr, 0), marks_of(a, 0));
+        compact_marks(a, 0);
         for (uint32_t k = 0; k < substeps; ++k)
             ADJ_TRY(forward_substep(a, k, a->tape[k], k + 1 < substeps ? a->tape[k + 1] : a->ping[0], a->tape_s[k],
                                     a->tape_w[k]));
@@ -1209,6 +1245,7 @@ int mpma_forward(mpm_adjoint *a, uint32_t substeps, const float *dts, uint32_t c
         ADJ_TRY(copy_state(a->ping[0], a->init, a->n, a->stream));
         k_adj_mark<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(
             make_adj_ctx(a, a->ping[0], a->ping[0], nullptr, nullptr, 0), marks_of(a, 0));
+        compact_marks(a, 0);
         for (uint32_t k = 0; k < substeps; ++k) {
             if (k % checkpoint_every == 0)
                 ADJ_TRY(copy_state(a->checkpoints[k / checkpoint_every], a->ping[cur], a->n, a->stream));
@@ -1248,12 +1285,12 @@ int mpma_backward(mpm_adjoint *a, float *grad_velocities, double *grad_parameter
             ADJ_TRY(forward_substep(a, start + j, a->tape[j], j + 1 < len ? a->tape[j + 1] : a->ping[0], a->tape_s[j],
                                     a->tape_w[j], j + 1 < len));
         for (int j = (int)len - 1; j >= 0; --j) {
-            const uint8_t *marks = marks_of(a, start + (uint32_t)j);
-            clear_marked(a, marks, a->ub_w, a->ub_s, nullptr);
+            const uint32_t k = start + (uint32_t)j;
+            clear_marked(a, k, a->ub_w, a->ub_s, nullptr);
             const AdjCtx c = make_adj_ctx(a, a->tape[j], a->tape[j], a->tape_s[j], a->tape_w[j], adj);
-            k_adj_grid_fwd<<<a->clear_ctas, ADJ_TILE * ADJ_TILE, 0, a->stream>>>(c, a->tile_scene, a->n_tiles, marks);
+            k_adj_grid_fwd<<<a->clear_ctas, ADJ_TILE * ADJ_TILE, 0, a->stream>>>(c, a->tile_scene, list_of(a, k));
             k_adj_g2p_bwd<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(c);
-            k_adj_grid_bwd<<<a->clear_ctas, ADJ_TILE * ADJ_TILE, 0, a->stream>>>(c, a->tile_scene, a->n_tiles, marks);
+            k_adj_grid_bwd<<<a->clear_ctas, ADJ_TILE * ADJ_TILE, 0, a->stream>>>(c, a->tile_scene, list_of(a, k));
             k_adj_p2g_bwd<<<blocks(a->n), ADJ_THREADS, 0, a->stream>>>(c);
             adj = 1 - adj;
         }
