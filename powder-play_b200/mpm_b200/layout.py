@@ -13,6 +13,7 @@ in the reference's order so the message names the same particle and field.
 from __future__ import annotations
 
 import math
+import struct
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -31,10 +32,17 @@ MAX_FLOAT32 = 3.4028234663852886e38
 MAX_SAFE_INTEGER = 2 ** 53 - 1
 
 
+_F32 = struct.Struct("<f")
+
+
 def fround(value: float) -> float:
-    """Math.fround."""
-    with np.errstate(over="ignore"):
-        return float(np.float32(value))
+    """Math.fround: round to the nearest float32 (ties to even); beyond the
+    float32 range, to an infinity."""
+    try:
+        return _F32.unpack(_F32.pack(value))[0]
+    except (OverflowError, TypeError, struct.error):
+        with np.errstate(over="ignore"):
+            return float(np.float32(value))
 
 
 def finite_float32(value: float, name: str, positive: bool = False) -> float:
