@@ -83,6 +83,29 @@ def test_batched_scenes_match_solo_runs_bit_for_bit():
         batch.dispose()
 
 
+def test_tiny_scenes_among_larger_ones_match_solo_runs_bit_for_bit():
+    # scenes of 2 to 4 particles (a few lanes of one warp, one tile each)
+    # between tanks of hundreds, some sitting a batch out
+    tiny = create_batched_tank_scenes(4, seed=3, particles=(1, 40), sides=(16, 24))
+    scenes = [tiny[0]] + _small_scenes(2, seed=9) + tiny[1:3] + _small_scenes(1, seed=11) + [tiny[3]]
+    batch = create_mpm_batched_gpu_solver(scenes)
+    try:
+        s = batch.scene_count
+        dts = [_micro_dt(batch.cfl_bounds[k], scenes[k][1], 0.5) for k in range(s)]
+        submits = [[(2 + k % 3, dts[k]) for k in range(s)],
+                   [(0 if k % 2 else 3, dts[k]) for k in range(s)]]
+        for sub in submits:
+            batch.step_batch([st for st, _ in sub], [dt for _, dt in sub], BATCHED_TANK_GRAVITY)
+        assert all(e is None for e in batch.check_numerical_status())
+        for k, (particles, config) in enumerate(scenes):
+            got, _ = batch.read_particles_packed(k)
+            want, status, _ = _solo_state(particles, config, [sub[k] for sub in submits])
+            assert status[0] == 0
+            assert np.array_equal(_bits(got), _bits(want)), f"scene {k} differs from its solo run"
+    finally:
+        batch.dispose()
+
+
 def test_a_failing_scene_rolls_back_alone():
     scenes = _small_scenes(5, seed=11)
     bounds = [_wide_bounds(p, c) for p, c in scenes]
