@@ -1496,11 +1496,13 @@ __device__ void validate_cfl(const Ctx &c, uint32_t id, const Material &m, float
 {
     const StepParams &P = *c.P;
     if (!P.cfl_enabled) return;
-    if (*(volatile uint32_t *)c.status != 0u) return;
     const float speed = length2(vel);
     const float wave = wave_speed_bound(c, m, F, damage, volume, tait_pow);
     if (!finite2(vel) || !finite_f(speed) || !finite_f(wave) || speed > P.cfl_velocity_limit ||
         wave > P.cfl_wave_bound) {
+        // the reference reads the status word before the bounds; a particle
+        // within them records nothing either way, so only a violation reads it
+        if (*(volatile uint32_t *)c.status != 0u) return;
         const uint32_t prev = atomicOr(c.status + 6, 3u);
         if (prev == 0u) {
             atomicExch(c.status + 1, id);
