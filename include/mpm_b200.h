@@ -216,6 +216,18 @@ int mpm_probe_fixed_point(mpm_solver *solver, float dt, int32_t *words_out, floa
  * counterpart: the reference keeps this buffer internal. */
 int mpm_probe_triangle_field(mpm_solver *solver, float dt, float *field_out);
 
+/* Evaluates G2P's deformation-gradient trial on `device` for `count` (F, C)
+ * pairs (4 floats each, row-major m00 m01 m10 m11) at step `dt`: the
+ * increment dt * max row sum |C|, the substep count n = ceil(increment /
+ * 0.25) doubled while det <= 0 (at most 64), the trial F of n fused products
+ * and its compensated determinant; `flags_out` holds 0, or 32 (more than 64
+ * substeps) / 16 (a non-finite product).  The same device function G2P runs
+ * (integrateDeformation and its retries, src/lib/mpm/kernels/shaders.ts:1459-1483,
+ * :2249-2298); the reference pins it with the float32 known answer of
+ * src/lib/mpm/kernels/solver.spec.ts:197-278. */
+int mpm_probe_deformation(int device, const float *F, const float *C, uint32_t count, float dt, float *trial_out,
+                          float *increment_out, float *determinant_out, uint32_t *substeps_out, uint32_t *flags_out);
+
 /* Halo node count ((cells_x + 3) * (cells_y + 3)). */
 uint32_t mpm_node_count(const mpm_solver *solver);
 

@@ -193,6 +193,40 @@ __device__ __forceinline__ float4 integrate_deformation(float4 f, float4 c, floa
     return r;
 }
 
+// The trial deformation of G2P (shaders.ts:2249-2298): the increment
+// dt * max row sum |C|, n = max(1, ceil(increment / 0.25)) fused products of
+// integrateDeformation, n doubled (at most 64) while det F <= 0.
+struct DeformationTrial {
+    float4 F;
+    float increment, det;
+    uint32_t substeps;
+};
+
+// Returns 0, ERROR_DEFORMATION_SUBSTEP_LIMIT when n would exceed 64, or
+// ERROR_G2P when a product is not finite.  A finite det <= 0 after the
+// retries is left to the caller (recordDeformationFailure).
+__device__ __forceinline__ uint32_t deformation_trial(float4 F0, float4 Cn, float dt, DeformationTrial &t)
+{
+    const float row = fmaxf(fabsf(Cn.x) + fabsf(Cn.y), fabsf(Cn.z) + fabsf(Cn.w));
+    t.increment = dt * row;
+    const float req = ceilf(t.increment * (1.0f / MAX_DEFORMATION_INCREMENT));  // exact: the increment is 2^-2
+    if (!finite_f(req) || req > MAX_DEFORMATION_SUBSTEPS) return ERROR_DEFORMATION_SUBSTEP_LIMIT;
+    uint32_t sub = max(1u, (uint32_t)req);
+    float4 trial = integrate_deformation(F0, Cn, dt, sub);
+    if (!finite4(trial)) return ERROR_G2P;
+    float tdet = det2(trial);
+    while (finite_f(tdet) && tdet <= 0.f && sub < 64u) {
+        sub = min(sub * 2u, 64u);
+        trial = integrate_deformation(F0, Cn, dt, sub);
+        if (!finite4(trial)) return ERROR_G2P;
+        tdet = det2(trial);
+    }
+    t.F = trial;
+    t.det = tdet;
+    t.substeps = sub;
+    return 0u;
+}
+
 // confineAxis: shaders.ts:522-534 -> (position, velocity)
 __device__ __forceinline__ float2 confine_axis(float next, float vel, float maximum)
 {

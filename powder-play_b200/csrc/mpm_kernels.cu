@@ -1688,29 +1688,18 @@ __device__ __forceinline__ bool g2p_particle(const Ctx &c, const ParticleIn &in,
         fail(c.status, ERROR_G2P);
         return false;
     }
-    const float row = fmaxf(fabsf(Cn.x) + fabsf(Cn.y), fabsf(Cn.z) + fabsf(Cn.w));
-    const float inc = dt * row;
-    const float req = ceilf(inc * (1.0f / MAX_DEFORMATION_INCREMENT));  // exact: the increment is 2^-2
-    if (!finite_f(req) || req > MAX_DEFORMATION_SUBSTEPS) {
+    DeformationTrial dtr;
+    const uint32_t dflags = deformation_trial(F0, Cn, dt, dtr);
+    if (dflags == ERROR_DEFORMATION_SUBSTEP_LIMIT) {
         fail_at(c.status, id, ERROR_DEFORMATION_SUBSTEP_LIMIT);
         return false;
     }
-    uint32_t sub = max(1u, (uint32_t)req);
-    float4 trial = integrate_deformation(F0, Cn, dt, sub);
-    if (!finite4(trial)) {
-        fail(c.status, ERROR_G2P);
+    if (dflags != 0u) {
+        fail(c.status, dflags);
         return false;
     }
-    float tdet = det2(trial);
-    while (finite_f(tdet) && tdet <= 0.f && sub < 64u) {
-        sub = min(sub * 2u, 64u);
-        trial = integrate_deformation(F0, Cn, dt, sub);
-        if (!finite4(trial)) {
-            fail(c.status, ERROR_G2P);
-            return false;
-        }
-        tdet = det2(trial);
-    }
+    const float4 trial = dtr.F;
+    const float tdet = dtr.det, inc = dtr.increment;
     float4 Fn = trial;
     float pv = in.pvol;
     if (!finite_f(tdet) || tdet <= 0.f) {
@@ -3020,6 +3009,24 @@ __global__ void k_surface_decode(const unsigned long long *acc, float2 *field, u
 }
 
 // the instances the host launches
+// The trial deformation G2P computes (deformation_trial) for `n` given
+// (F, C) pairs: trial F, increment, determinant and substep count, or the
+// flags of a failed integration in `flags`.
+__global__ void k_probe_deformation(const float4 *F, const float4 *C, float dt, uint32_t n, float4 *trial,
+                                    float2 *increment_det, uint32_t *substeps, uint32_t *flags)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    DeformationTrial t;
+    t.F = make_float4(0.f, 0.f, 0.f, 0.f);
+    t.increment = t.det = 0.f;
+    t.substeps = 0u;
+    flags[i] = deformation_trial(F[i], C[i], dt, t);
+    trial[i] = t.F;
+    increment_det[i] = make_float2(t.increment, t.det);
+    substeps[i] = t.substeps;
+}
+
 template __global__ void k_p2g_gather<false>(Ctx);
 template __global__ void k_p2g_gather<true>(Ctx);
 template __global__ void k_g2p_tile<false, false>(Ctx);

@@ -190,6 +190,8 @@ __global__ void k_fracture_bonds(Ctx c);
 __global__ void k_fracture_damage(Ctx c);
 __global__ void k_body_finish(Ctx c);
 __global__ void k_count_active_nodes(Ctx c, uint32_t *counts);
+__global__ void k_probe_deformation(const float4 *F, const float4 *C, float dt, uint32_t n, float4 *trial,
+                                    float2 *increment_det, uint32_t *substeps, uint32_t *flags);
 // surface occupancy (status word 7 flags: shaders.ts:187-189)
 constexpr uint32_t SURFACE_ERROR_BUCKET = 1u;
 constexpr uint32_t SURFACE_ERROR_PARTICLE_AREA = 2u;

@@ -1779,6 +1779,49 @@ int mpm_probe_triangle_field(mpm_solver *s, float dt, float *field_out)
     return MPM_OK;
 }
 
+int mpm_probe_deformation(int device, const float *F, const float *C, uint32_t count, float dt, float *trial_out,
+                          float *increment_out, float *determinant_out, uint32_t *substeps_out, uint32_t *flags_out)
+{
+    g_last_error.clear();
+    if (count == 0) return MPM_OK;
+    if (!F || !C || !trial_out || !increment_out || !determinant_out || !substeps_out || !flags_out)
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "every array must be given");
+    if (!std::isfinite(dt) || dt <= 0.0f) return set_error(MPM_ERR_INVALID_ARGUMENT, "dt must be positive and finite");
+    CUDA_TRY(cudaSetDevice(device));
+    float4 *dF = nullptr, *dC = nullptr, *dT = nullptr;
+    float2 *dI = nullptr;
+    uint32_t *dS = nullptr, *dFl = nullptr;
+    cudaError_t e = dalloc(&dF, count);
+    if (e == cudaSuccess) e = dalloc(&dC, count);
+    if (e == cudaSuccess) e = dalloc(&dT, count);
+    if (e == cudaSuccess) e = dalloc(&dI, count);
+    if (e == cudaSuccess) e = dalloc(&dS, count);
+    if (e == cudaSuccess) e = dalloc(&dFl, count);
+    if (e == cudaSuccess) e = cudaMemcpy(dF, F, count * sizeof(float4), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dC, C, count * sizeof(float4), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_probe_deformation<<<(count + 127u) / 128u, 128>>>(dF, dC, dt, count, dT, dI, dS, dFl);
+        e = cudaGetLastError();
+    }
+    std::vector<float2> inc(count);
+    if (e == cudaSuccess) e = cudaMemcpy(trial_out, dT, count * sizeof(float4), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(inc.data(), dI, count * sizeof(float2), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(substeps_out, dS, count * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(flags_out, dFl, count * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    cudaFree(dF);
+    cudaFree(dC);
+    cudaFree(dT);
+    cudaFree(dI);
+    cudaFree(dS);
+    cudaFree(dFl);
+    if (e != cudaSuccess) return set_error(MPM_ERR_CUDA, "deformation probe failed: %s", cudaGetErrorString(e));
+    for (uint32_t i = 0; i < count; ++i) {
+        increment_out[i] = inc[i].x;
+        determinant_out[i] = inc[i].y;
+    }
+    return MPM_OK;
+}
+
 int mpm_probe_fixed_point(mpm_solver *s, float dt, int32_t *words_out, float *affine_out)
 {
     g_last_error.clear();

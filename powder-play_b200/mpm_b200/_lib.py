@@ -22,7 +22,7 @@ EXPORTED_SYMBOLS = (
     "mpm_create", "mpm_step_batch", "mpm_read_compact", "mpm_read_status", "mpm_clear_status",
     "mpm_read_particles", "mpm_write_particles", "mpm_set_drag", "mpm_queue_completion_ms",
     "mpm_particle_count", "mpm_particle_capacity", "mpm_destroy", "mpm_last_error", "mpm_probe_sort",
-    "mpm_probe_fixed_point", "mpm_probe_triangle_field", "mpm_node_count", "mpm_last_batch_device_ms", "mpm_profile_substeps",
+    "mpm_probe_fixed_point", "mpm_probe_triangle_field", "mpm_probe_deformation", "mpm_node_count", "mpm_last_batch_device_ms", "mpm_profile_substeps",
     "mpm_profile_kernel_name", "mpm_profile_kernel_slots", "mpm_count_active_nodes", "mpm_stream",
     "mpmb_create", "mpmb_step_batch", "mpmb_read_compact", "mpmb_scene_count",
     "mpm_allocated_particle_count", "mpm_append_particles", "mpm_remove_particles_in_outlet", "mpm_pick",
@@ -101,6 +101,8 @@ def load_library(path: str = LIBRARY_PATH) -> ctypes.CDLL:
     lib.mpm_probe_triangle_field.restype = i32
     lib.mpm_probe_fixed_point.argtypes = [vp, f32, vp, vp]
     lib.mpm_probe_fixed_point.restype = i32
+    lib.mpm_probe_deformation.argtypes = [i32, vp, vp, u32, f32, vp, vp, vp, vp, vp]
+    lib.mpm_probe_deformation.restype = i32
     lib.mpm_last_batch_device_ms.argtypes = [vp, P(ctypes.c_double)]
     lib.mpm_last_batch_device_ms.restype = i32
     lib.mpm_profile_substeps.argtypes = [vp, u32, f32, f32, f32, P(MpmCflGuard), vp, vp]

@@ -29,6 +29,7 @@ import numpy as np
 from .errors import RangeError
 from .layout import ParticleArrays
 from .materials import MPM_SI_BOX_DOMAIN
+from .tait_eos import create_mpm_tait_liquid_material, derive_tait_pressure_coefficient_pa
 
 UINT32_RANGE = 0x1_0000_0000
 
@@ -68,25 +69,6 @@ def lcg_sequence(seed: int, count: int) -> np.ndarray:
         out[start:start + n] = states.astype(np.float64) / UINT32_RANGE
         state = states[n - 1]
     return out
-
-
-# ------------------------------------------------------------------ tait --
-
-def derive_tait_pressure_coefficient_pa(reference_density, exponent, sound_speed):
-    """deriveTaitPressureCoefficientPa, src/lib/mpm/reference/tait-eos.ts:73-86."""
-    for name, v in (("referenceDensityKgPerM3", reference_density), ("exponent", exponent),
-                    ("soundSpeedMPerS", sound_speed)):
-        if not math.isfinite(v) or v <= 0:
-            raise ValueError(f"{name} must be a finite positive number.")
-    return (reference_density * sound_speed * sound_speed) / exponent
-
-
-def create_mpm_tait_liquid_material(parameters: dict, extrusion_depth_m: float, model: str = "water") -> dict:
-    """createMpmTaitLiquidMaterial, tait-eos.ts:26-44."""
-    density = parameters["referenceDensityKgPerM3"] * extrusion_depth_m
-    lam = parameters["pressureCoefficientPa"] * extrusion_depth_m
-    return {"model": model, "lambda": lam, "mu": 0.0, "density": density,
-            "equationOfState": {"model": "tait", "exponent": parameters["exponent"]}}
 
 
 SI_FLUID_GRID_CELLS = 40

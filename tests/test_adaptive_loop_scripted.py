@@ -1,0 +1,404 @@
+"""The adaptive CFL loop's host logic with scripted device status words (CPU).
+
+A fake native library stands in for libmpm_b200.so: it records the batches
+submitted and answers each compact readback (maximum speed, committed
+microsteps, 8 status words) from a script, as the reference's tests map
+scripted bytes into the readback buffer (src/lib/mpm/kernels/solver.spec.ts:
+570-840).  Restated cases: compact readback without particle reads, a CFL
+violation surfaced, rollback and retry, more than four retries while budget
+remains, partial progress and its continuation.  The remaining exits of
+MpmMlsGpuSolver.step_cfl_batch_adaptive and of the batched solver's scene loop
+(budget exhausted, non-recoverable errors, invalid progress reports) are
+driven the same way.
+"""
+import ctypes
+import math
+import struct
+
+import numpy as np
+import pytest
+
+import mpm_b200._lib as native
+from mpm_b200 import (MpmMlsGpuNumericalError, RangeError, calculate_mpm_cfl_microsteps, create_mpm_batched_gpu_solver,
+                      create_mpm_mls_gpu_solver)
+
+CONFIG = {"grid": {"cellsX": 16, "cellsY": 8, "cellSize": 1}, "particleMass": 0.1, "particleVolume": 0.01,
+          "material": {"lambda": 20, "mu": 10}, "capacity": 4}
+PARTICLE = {"position": {"x": 8, "y": 4}, "velocity": {"x": 0, "y": 0},
+            "C": {"m00": 0, "m01": 0, "m10": 0, "m11": 0}, "F": {"m00": 1, "m01": 0, "m10": 0, "m11": 1}}
+GRAVITY = {"x": 0, "y": 0}
+BOUNDS = {"waveSpeedBound": 25, "velocityBound": 1}
+
+
+def f32_bits(value: float) -> int:
+    return struct.unpack("<I", struct.pack("<f", value))[0]
+
+
+def snapshot(speed=0.0, completed=0, status=None):
+    words = [0] * 8
+    for k, v in (status or {}).items():
+        words[k] = v
+    return speed, completed, words
+
+
+def cfl_violation(speed, completed, wave=25.0, particle=0, particle_speed=None):
+    """The compact bytes of a CFL violation: status 16384, claim kind 3 and the
+    (particle speed, wave speed, velocity limit, wave limit) diagnostics."""
+    ps = speed if particle_speed is None else particle_speed
+    return snapshot(speed, completed, {0: 16384, 1: particle, 6: 3, 2: f32_bits(ps), 3: f32_bits(wave),
+                                       4: f32_bits(40.0), 5: f32_bits(wave)})
+
+
+class FakeLibrary:
+    """The entry points the host mirror calls, with scripted readbacks."""
+
+    def __init__(self, script):
+        self.script = script
+        self.readbacks = 0
+        self.batches = []  # (step counts, dts, velocity limits)
+        self.clears = 0
+        self.particle_reads = 0
+
+    # single-scene solver
+    def mpm_create(self, config, packed, ids, n, starts, n_starts, bonds, n_bonds, topo, n_topo, handle):
+        handle._obj.value = 1
+        return native.MPM_OK
+
+    def mpm_step_batch(self, handle, steps, dt, gx, gy, guard, bref):
+        limit = None if guard is None else guard._obj.velocity_limit
+        self.batches.append(([int(steps)], [float(dt)], [limit]))
+        return native.MPM_OK
+
+    def _next(self):
+        entry = self.script(self.readbacks) if callable(self.script) else self.script[self.readbacks]
+        self.readbacks += 1
+        return entry
+
+    def mpm_read_compact(self, handle, speed, completed, status):
+        s, done, words = self._next()
+        speed._obj.value = s
+        completed._obj.value = done
+        arr = np.asarray(words, dtype=np.uint32)
+        ctypes.memmove(status.value, arr.ctypes.data, 32)
+        return native.MPM_OK
+
+    def mpm_clear_status(self, handle):
+        self.clears += 1
+        return native.MPM_OK
+
+    def mpm_last_batch_device_ms(self, handle, out):
+        out._obj.value = 0.0
+        return native.MPM_OK
+
+    def mpm_read_particles(self, *args):
+        self.particle_reads += 1
+        return native.MPM_OK
+
+    def mpm_destroy(self, handle):
+        return None
+
+    def mpm_last_error(self):
+        return b""
+
+    # batched solver: one script entry per readback, a list of per-scene snapshots
+    def mpmb_create(self, configs, count, counts, packed, ids, handle):
+        handle._obj.value = 1
+        return native.MPM_OK
+
+    def mpmb_step_batch(self, handle, steps, dts, gravity, guards):
+        n = len(self._scene_counts)
+        s = np.ctypeslib.as_array(ctypes.cast(steps.value, ctypes.POINTER(ctypes.c_uint32)), (n,)).tolist()
+        d = np.ctypeslib.as_array(ctypes.cast(dts.value, ctypes.POINTER(ctypes.c_float)), (n,)).tolist()
+        self.batches.append((s, d, None))
+        return native.MPM_OK
+
+    def mpmb_read_compact(self, handle, speeds, done, status):
+        n = len(self._scene_counts)
+        entries = self._next()
+        sp = np.ctypeslib.as_array(ctypes.cast(speeds.value, ctypes.POINTER(ctypes.c_float)), (n,))
+        dn = np.ctypeslib.as_array(ctypes.cast(done.value, ctypes.POINTER(ctypes.c_uint32)), (n,))
+        st = np.ctypeslib.as_array(ctypes.cast(status.value, ctypes.POINTER(ctypes.c_uint32)), (n, 8))
+        for k, (s, c, words) in enumerate(entries):
+            sp[k], dn[k], st[k] = s, c, words
+        return native.MPM_OK
+
+
+@pytest.fixture
+def fake(monkeypatch):
+    holder = {}
+
+    def install(script, scene_counts=(1,)):
+        lib = FakeLibrary(script)
+        lib._scene_counts = scene_counts
+        monkeypatch.setattr(native, "load_library", lambda *a, **k: lib)
+        holder["lib"] = lib
+        return lib
+
+    return install
+
+
+def plan_for(solver, velocity, max_micro, macro=0.001):
+    b = solver.cfl_bounds
+    return calculate_mpm_cfl_microsteps(macro, CONFIG["grid"]["cellSize"], b["waveSpeedBound"], velocity, max_micro,
+                                        courantLimit=b.get("courantLimit"))
+
+
+def submitted(lib):
+    return sum(sum(s) for s, _, _ in lib.batches)
+
+
+# ------------------------------------------------ solver.spec.ts:570-840 --
+
+def test_reads_the_compact_speed_and_status_without_particle_reads(fake):
+    lib = fake([snapshot(0.0, 1)])
+    solver = create_mpm_mls_gpu_solver([PARTICLE], CONFIG)
+    plan = plan_for(solver, 0, 1)
+    solver.step_cfl_batch(1, 0.001, plan, 0, 1, GRAVITY)
+    with pytest.raises(RuntimeError, match=r"queue measureMaximumParticleSpeed\(\).*before submitting another"):
+        solver.step_cfl_batch(1, 0.001, plan, 0, 1, GRAVITY)
+    assert solver.measure_maximum_particle_speed() == {"maximumSpeed": 0.0, "sequence": 1}
+    assert lib.readbacks == 1 and lib.particle_reads == 0
+    assert len(lib.batches) == 1
+
+
+def test_surfaces_a_cfl_violation_from_the_compact_status(fake):
+    wave = None
+
+    def script(k):
+        return cfl_violation(50.0, 0, wave=wave)
+
+    lib = fake(script)
+    solver = create_mpm_mls_gpu_solver([PARTICLE], CONFIG)
+    wave = solver.cfl_bounds["waveSpeedBound"]
+    plan = plan_for(solver, 1, 1)
+    solver.step_cfl_batch(1, 0.001, plan, 1, 1, GRAVITY)
+    with pytest.raises(MpmMlsGpuNumericalError,
+                       match="particle exceeded the enforced CFL wave-speed or velocity bound at particle 0"):
+        solver.measure_maximum_particle_speed()
+    with pytest.raises(RuntimeError, match="failed CFL measurement invalidated the tracked velocity bound"):
+        solver.step_cfl_batch(1, 0.001, plan, 1, 1, GRAVITY)
+    assert lib.readbacks == 1
+
+
+def test_recovers_a_rejected_microstep_at_a_finer_resolution(fake):
+    def script(k):
+        if k == 0:
+            return cfl_violation(50.0, 1)
+        return snapshot(50.0, 2 if k == 1 else 1)
+
+    lib = fake(script)
+    solver = create_mpm_mls_gpu_solver([PARTICLE], CONFIG, BOUNDS)
+    plan = plan_for(solver, 1, 8)
+    m = solver.step_cfl_batch_adaptive(3, 0.001, plan, 1, 8, GRAVITY)
+    assert m["maximumSpeed"] == 50 and m["sequence"] == 3
+    assert m["attemptedMicroStepCount"] == 7 and m["retryCount"] == 1
+    assert submitted(lib) == 7  # every encoded microstep (the reference counts its commit passes)
+    assert lib.clears == 1      # the failed status is cleared before the retry
+    assert m["remainingDuration"] == 0
+
+
+def test_continues_beyond_four_retries_while_budget_remains(fake):
+    lib = fake(lambda k: cfl_violation(50.0, 0) if k < 5 else snapshot(50.0, 0))
+    solver = create_mpm_mls_gpu_solver([PARTICLE], CONFIG, BOUNDS)
+    plan = plan_for(solver, 1, 64)
+    m = solver.step_cfl_batch_adaptive(1, 0.001, plan, 1, 64, GRAVITY)
+    assert m["retryCount"] == 5
+    assert m["remainingDuration"] == 0
+    assert lib.clears == 5
+
+
+def test_returns_partial_progress_then_resumes_the_remainder(fake):
+    lib = fake(lambda k: cfl_violation(50.0, 1) if k == 0 else snapshot(0.5, 2))
+    solver = create_mpm_mls_gpu_solver([PARTICLE], CONFIG, BOUNDS)
+    plan = plan_for(solver, 1, 4)
+    partial = solver.step_cfl_batch_adaptive(3, 0.001, plan, 1, 4, GRAVITY)
+    assert partial["maximumSpeed"] == 50 and partial["sequence"] == 1
+    assert partial["recommendedVelocityBound"] == 62.5
+    assert partial["attemptedMicroStepCount"] == 3 and partial["retryCount"] == 0
+    assert math.isclose(partial["simulatedDuration"], 0.001, rel_tol=1e-12)
+    assert math.isclose(partial["remainingDuration"], 0.002, rel_tol=1e-12)
+    velocity = partial["recommendedVelocityBound"]
+    b = solver.cfl_bounds
+    cont_plan = calculate_mpm_cfl_microsteps(0.001, 1, b["waveSpeedBound"], velocity, 8,
+                                             courantLimit=b.get("courantLimit"))
+    cont = solver.step_cfl_batch_adaptive(2, 0.001, cont_plan, velocity, 8, GRAVITY)
+    assert cont["attemptedMicroStepCount"] == 2
+    assert math.isclose(cont["simulatedDuration"], 0.002, rel_tol=1e-12)
+    assert cont["remainingDuration"] == 0
+    assert submitted(lib) == 5
+
+
+# ------------------------------------------- the loop's remaining exits --
+
+def test_a_request_beyond_the_microstep_budget_is_refused_before_submitting(fake):
+    lib = fake([])
+    solver = create_mpm_mls_gpu_solver([PARTICLE], CONFIG, BOUNDS)
+    plan = plan_for(solver, 1, 8)
+    with pytest.raises(RangeError, match="adaptive CFL retry requires 3 microsteps with 2 remaining"):
+        solver.step_cfl_batch_adaptive(3, 0.001, plan, 1, 2, GRAVITY)
+    assert lib.batches == []
+
+
+def test_a_non_recoverable_status_is_raised(fake):
+    # a non-finite grid state (8) is not a CFL rejection: no retry
+    lib = fake([snapshot(1.0, 0, {0: 8, 1: 0xFFFFFFFF})])
+    solver = create_mpm_mls_gpu_solver([PARTICLE], CONFIG, BOUNDS)
+    with pytest.raises(MpmMlsGpuNumericalError, match="non-finite grid state"):
+        solver.step_cfl_batch_adaptive(1, 0.001, plan_for(solver, 1, 8), 1, 8, GRAVITY)
+    assert lib.clears == 0 and len(lib.batches) == 1
+
+
+def test_a_deformation_failure_with_a_finite_speed_is_retried(fake):
+    lib = fake([snapshot(2.0, 0, {0: 2, 1: 0, 6: 1}), snapshot(2.0, 2)])
+    solver = create_mpm_mls_gpu_solver([PARTICLE], CONFIG, BOUNDS)
+    m = solver.step_cfl_batch_adaptive(1, 0.001, plan_for(solver, 1, 8), 1, 8, GRAVITY)
+    assert m["retryCount"] == 1 and m["remainingDuration"] == 0
+    # the wave-speed bound only moves for CFL rejections
+    assert solver.cfl_bounds["waveSpeedBound"] == 25
+
+
+def test_a_cfl_retry_raises_the_wave_speed_bound(fake):
+    fake([cfl_violation(50.0, 0, wave=30.0), snapshot(50.0, 2)])
+    solver = create_mpm_mls_gpu_solver([PARTICLE], CONFIG, BOUNDS)
+    solver.step_cfl_batch_adaptive(1, 0.001, plan_for(solver, 1, 8), 1, 8, GRAVITY)
+    assert solver.cfl_bounds["waveSpeedBound"] == 30.0 * 1.25
+
+
+def test_an_impossible_completed_count_stops_recovery(fake):
+    # a failed batch of one microstep cannot have completed that microstep
+    fake([cfl_violation(50.0, 1)])
+    solver = create_mpm_mls_gpu_solver([PARTICLE], CONFIG, BOUNDS)
+    with pytest.raises(RuntimeError, match="could not determine completed microsteps"):
+        solver.step_cfl_batch_adaptive(1, 0.001, plan_for(solver, 1, 8), 1, 8, GRAVITY)
+
+
+def test_a_completed_count_beyond_the_batch_is_rejected(fake):
+    fake([snapshot(0.5, 9)])
+    solver = create_mpm_mls_gpu_solver([PARTICLE], CONFIG, BOUNDS)
+    with pytest.raises(RangeError, match="GPU reported 9 completed microsteps for a batch of 1"):
+        solver.step_cfl_batch_adaptive(1, 0.001, plan_for(solver, 1, 8), 1, 8, GRAVITY)
+
+
+def test_a_non_finite_observed_speed_stops_recovery(fake):
+    inf_speed = struct.unpack("<f", struct.pack("<I", 0x7F800000))[0]
+    fake([cfl_violation(inf_speed, 0, particle_speed=50.0)])
+    solver = create_mpm_mls_gpu_solver([PARTICLE], CONFIG, BOUNDS)
+    with pytest.raises(RuntimeError, match="non-finite velocity bound"):
+        solver.step_cfl_batch_adaptive(1, 0.001, plan_for(solver, 1, 8), 1, 8, GRAVITY)
+
+
+def test_an_exhausted_retry_budget_returns_partial_progress(fake):
+    # the failed batch of 3 leaves 1 microstep of a budget of 4: < 2 for a retry
+    lib = fake([cfl_violation(50.0, 2)])
+    solver = create_mpm_mls_gpu_solver([PARTICLE], CONFIG, BOUNDS)
+    m = solver.step_cfl_batch_adaptive(3, 0.001, plan_for(solver, 1, 4), 1, 4, GRAVITY)
+    assert m["attemptedMicroStepCount"] == 3 and m["retryCount"] == 0
+    assert math.isclose(m["remainingDuration"], 0.001, rel_tol=1e-9)
+    assert m["recommendedVelocityBound"] == 62.5
+    assert lib.clears == 1
+    # the solver stays usable for the continuation
+    assert solver._cfl_state_usable
+
+
+def test_a_retry_that_cannot_fit_a_finer_plan_returns_partial_progress(fake):
+    # 2 microsteps remain, but the failed interval needs more than 2 at the raised speed
+    lib = fake([cfl_violation(5_000.0, 0)])
+    solver = create_mpm_mls_gpu_solver([PARTICLE], CONFIG, BOUNDS)
+    m = solver.step_cfl_batch_adaptive(2, 0.001, plan_for(solver, 1, 4), 1, 4, GRAVITY)
+    assert m["retryCount"] == 0 and m["recommendedVelocityBound"] == 6_250.0
+    assert math.isclose(m["remainingDuration"], 0.002, rel_tol=1e-9)
+    assert len(lib.batches) == 1
+
+
+def test_a_continuation_without_budget_returns(fake):
+    # after a retry consumed the budget, a successful attempt that leaves
+    # duration behind returns with the rest to the caller
+    lib = fake([cfl_violation(50.0, 0), snapshot(50.0, 2)])
+    solver = create_mpm_mls_gpu_solver([PARTICLE], CONFIG, BOUNDS)
+    m = solver.step_cfl_batch_adaptive(3, 0.001, plan_for(solver, 1, 6), 1, 6, GRAVITY)
+    assert m["attemptedMicroStepCount"] == 5 and m["retryCount"] == 1
+    assert math.isclose(m["remainingDuration"], 0.002, rel_tol=1e-9)
+    assert m["recommendedVelocityBound"] == 62.5
+    assert len(lib.batches) == 2
+
+
+def test_a_continuation_limited_by_the_budget_keeps_a_partial_plan(fake):
+    # success after a retry, then the remainder needs more microsteps than the
+    # budget leaves: the continuation covers only what fits, and the rest
+    # returns to the caller
+    lib = fake([cfl_violation(200.0, 0), snapshot(200.0, 2), snapshot(200.0, 2)])
+    solver = create_mpm_mls_gpu_solver([PARTICLE], CONFIG, BOUNDS)
+    m = solver.step_cfl_batch_adaptive(3, 0.001, plan_for(solver, 1, 8), 1, 8, GRAVITY)
+    steps = [s[0] for s, _, _ in lib.batches]
+    assert steps == [3, 2, 2]
+    assert m["attemptedMicroStepCount"] == 7 and m["retryCount"] == 1
+    assert 0 < m["remainingDuration"] < 0.002
+    assert math.isclose(m["simulatedDuration"] + m["remainingDuration"], 0.003, rel_tol=1e-12)
+
+
+# ---------------------------------------------------- batched scene loop --
+
+def _batched(fake, script, scenes=2):
+    lib = fake(script, scene_counts=(1,) * scenes)
+    solver = create_mpm_batched_gpu_solver([([PARTICLE], CONFIG)] * scenes, [dict(BOUNDS) for _ in range(scenes)])
+    return lib, solver
+
+
+def test_batched_scenes_retry_alone_and_the_others_sit_out(fake):
+    script = [[snapshot(0.5, 1), cfl_violation(50.0, 0)],  # scene 1 fails its first microstep
+              [snapshot(0.0, 0), snapshot(50.0, 2)]]       # scene 1 retries at 2 microsteps
+    lib, solver = _batched(fake, script)
+    out = solver.step_cfl_batch_adaptive(0.001, [1, 1], 8, GRAVITY)
+    assert lib.batches[0][0] == [1, 1]
+    assert lib.batches[1][0] == [0, 2]  # the finished scene sits the retry out
+    assert out[0]["retryCount"] == 0 and out[0]["committedMicroStepCount"] == 1
+    assert out[1]["retryCount"] == 1 and out[1]["committedMicroStepCount"] == 2
+    assert out[1]["recommendedVelocityBound"] == 62.5
+    assert all(o["remainingDuration"] == 0 for o in out)
+    assert solver.cfl_bounds[1]["waveSpeedBound"] == 25 * 1.25 and solver.cfl_bounds[0]["waveSpeedBound"] == 25
+
+
+def test_batched_non_recoverable_status_is_raised(fake):
+    _, solver = _batched(fake, [[snapshot(0.0, 1), snapshot(0.0, 0, {0: 8, 1: 0xFFFFFFFF})]])
+    with pytest.raises(MpmMlsGpuNumericalError, match="non-finite grid state"):
+        solver.step_cfl_batch_adaptive(0.001, [1, 1], 8, GRAVITY)
+
+
+def test_batched_impossible_completed_count_is_raised(fake):
+    _, solver = _batched(fake, [[snapshot(0.0, 1), cfl_violation(50.0, 1)]])
+    with pytest.raises(RuntimeError, match="scene 1: adaptive CFL recovery could not determine completed"):
+        solver.step_cfl_batch_adaptive(0.001, [1, 1], 8, GRAVITY)
+
+
+def test_batched_exhausted_budget_ends_the_scene(fake):
+    # budget 2: the failed first microstep leaves 1, too few for a retry
+    lib, solver = _batched(fake, [[snapshot(0.0, 1), cfl_violation(50.0, 0)]])
+    out = solver.step_cfl_batch_adaptive(0.001, [1, 1], 2, GRAVITY)
+    assert len(lib.batches) == 1
+    assert out[1]["remainingDuration"] == pytest.approx(0.001) and out[1]["recommendedVelocityBound"] == 62.5
+    assert out[0]["remainingDuration"] == 0
+
+
+def test_batched_plan_beyond_budget_is_refused(fake):
+    _, solver = _batched(fake, [])
+    with pytest.raises(RangeError, match="maxMicrosteps"):
+        solver.step_cfl_batch_adaptive(0.001, [1, 1], 0, GRAVITY)
+
+
+def test_batched_continuation_after_a_retry(fake):
+    # scene 0 (3 microsteps at its velocity bound) fails after 1, retries the
+    # failed microstep's interval at 2, then continues with the remainder in a
+    # third submit while scene 1, done after the first, sits out
+    script = [[cfl_violation(50.0, 1), snapshot(0.0, 1)],
+              [snapshot(50.0, 2), snapshot(0.0, 0)],
+              [snapshot(50.0, 2), snapshot(0.0, 0)]]
+    lib, solver = _batched(fake, script)
+    out = solver.step_cfl_batch_adaptive(0.002, [300, 1], 16, GRAVITY)
+    steps = [s for s, _, _ in lib.batches]
+    assert len(steps) == 3
+    assert steps[0] == [3, 1] and steps[1] == [2, 0] and steps[2][1] == 0 and steps[2][0] >= 2
+    assert out[0]["retryCount"] == 1 and out[0]["remainingDuration"] == 0
+    assert out[0]["committedMicroStepCount"] == 1 + 2 + steps[2][0]
+    assert out[0]["attemptedMicroStepCount"] == 3 + 2 + steps[2][0]
+    assert solver.cfl_bounds[0]["waveSpeedBound"] == 25 * 1.25
+    assert out[1]["committedMicroStepCount"] == 1 and out[1]["retryCount"] == 0
