@@ -433,10 +433,9 @@ def plain_per_scene(scenes, gravity, macro_dt, device):
     return work / (device_ms * 1e-3)
 
 
-def run_b200_batched(args):
-    """The batched form: 512 independent SI Tait water tanks in one solver, one
-    step = one 1/240 s macrostep of every scene through the per-scene
-    adaptive CFL loop (MpmBatchedGpuSolver.step_cfl_batch_adaptive)."""
+def _init_ranks():
+    """(dist or None, rank, local_rank, world): the NCCL process group of a
+    multi-rank run (short timeout), the rank's device made current."""
     rank, local_rank, world = _rank_info()
     import torch
     dist = None
@@ -444,6 +443,30 @@ def run_b200_batched(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     torch.cuda.set_device(local_rank)
+    return dist, rank, local_rank, world
+
+
+def _finish_ranks(dist):
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_b200_batched(args):
+    dist, rank, local_rank, world = _init_ranks()
+    line = measure_batched(args.steps, args.warmup, args.cfl_recovery_factor, args.cfl_plan_margin, dist, rank,
+                           local_rank, world)
+    _finish_ranks(dist)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def measure_batched(steps, warmup, recovery_factor, plan_margin, dist, rank, local_rank, world):
+    """The batched form: 512 independent SI Tait water tanks in one solver, one
+    step = one 1/240 s macrostep of every scene through the per-scene
+    adaptive CFL loop (MpmBatchedGpuSolver.step_cfl_batch_adaptive).  Returns
+    the bench line of the form (`steps` timed after `warmup`)."""
+    import torch
     from mpm_b200 import create_mpm_batched_gpu_solver
     from mpm_b200.scenes import BATCHED_TANK_GRAVITY, create_batched_tank_scenes
     scenes = create_batched_tank_scenes(first=rank * 512)  # each rank its own shard of scenes
@@ -453,18 +476,18 @@ def run_b200_batched(args):
     n_total = int(batch.particle_counts.sum())
     velocity = [b["velocityBound"] for b in batch.cfl_bounds]
 
-    batch.recovery_bound_factor = args.cfl_recovery_factor
+    batch.recovery_bound_factor = recovery_factor
 
     def one_step():
         nonlocal velocity
-        bounds = [_batched_bound(v, macro_dt, gravity) * args.cfl_plan_margin for v in velocity]
+        bounds = [_batched_bound(v, macro_dt, gravity) * plan_margin for v in velocity]
         results = batch.step_cfl_batch_adaptive(macro_dt, bounds, BATCHED_MAX_MICROSTEPS, gravity)
         velocity = [r["recommendedVelocityBound"] for r in results]
         return results
 
     one_step()
     shape = batch.autotune(substeps=4)  # the project's launch-shape tuner, state restored
-    for _ in range(args.warmup - 1):
+    for _ in range(warmup - 1):
         one_step()
     torch.cuda.synchronize()
     if dist:
@@ -475,7 +498,7 @@ def run_b200_batched(args):
     batch.committed_particle_substeps = 0
     wall = 0.0
     submits = retries = 0
-    for _ in range(args.steps):
+    for _ in range(steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         results = one_step()
@@ -511,8 +534,8 @@ def run_b200_batched(args):
     counts = batch.particle_counts
     sides = [c["grid"]["cellsX"] for _, c in scenes]
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": device_s * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": warmup,
+        "ms_per_step": device_s * 1e3 / steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes, no dataset)",
         "config": {"workload": "batched: 512 independent SI Tait water tanks (0.2 m box, rho 1000, gamma 7, "
                                "c 20 m/s), N log-uniform in 1k-64k, S x S grids with S uniform in 64-512, "
@@ -524,13 +547,13 @@ def run_b200_batched(args):
                    "l2": "inputs larger than L2 (every scene's state, about 0.8 GB)",
                    "committed_particle_substeps": work, "submits": submits, "retries": retries,
                    "launch_shape": shape,
-                   "cfl_policy": {"recovery_factor": args.cfl_recovery_factor, "plan_margin": args.cfl_plan_margin,
-                                  "scene_macrosteps_per_device_s": world * len(scenes) * args.steps / device_s},
+                   "cfl_policy": {"recovery_factor": recovery_factor, "plan_margin": plan_margin,
+                                  "scene_macrosteps_per_device_s": world * len(scenes) * steps / device_s},
                    "plain_per_scene": {"value": plain, "unit": UNIT,
                                        "sample": f"the first {PLAIN_SAMPLE_SCENES} scenes, each alone in its own "
                                                  "solver, one timed macrostep each"}},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": submits * len(scenes) * 160 // args.steps,
-                "d2h_bytes_per_step": submits * len(scenes) * 256 // args.steps,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": submits * len(scenes) * 160 // steps,
+                "d2h_bytes_per_step": submits * len(scenes) * 256 // steps,
                 "path": "Python host MpmBatchedGpuSolver.step_cfl_batch_adaptive -> C ABI"},
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": dram_traffic(dominant + "@batched"),
@@ -545,11 +568,7 @@ def run_b200_batched(args):
         "gpu_launches": int(round(launches_per_substep * (work / max(1, n_total)))) if n_total else 0,
     }
     batch.dispose()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line
 
 
 ADJOINT_SUBSTEPS = 200
@@ -563,18 +582,20 @@ ADJOINT_BYTES_PER_PARTICLE = 48 + 24 + 48 + 72 + 24 + 72 + 48
 
 
 def run_b200_adjoint(args):
+    dist, rank, local_rank, world = _init_ranks()
+    line = measure_adjoint(args.steps, args.warmup, dist, rank, local_rank, world)
+    _finish_ranks(dist)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def measure_adjoint(steps_timed, warmup, dist, rank, local_rank, world, full_tape=True):
     """The differentiable form: 64 scenes of 12,288 Tait water + 4,096
     fixed-corotated particles on 256x256 grids, 200 substeps at each scene's
     fixed CFL dt, checkpoints every 20; one step = one forward pass (loss)
     and one backward pass (gradients wrt initial velocities and the scenes'
-    Tait coefficient, lambda, mu)."""
-    rank, local_rank, world = _rank_info()
+    Tait coefficient, lambda, mu).  Returns the bench line of the form."""
     import torch
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    torch.cuda.set_device(local_rank)
     from mpm_b200 import create_mpm_batched_gpu_solver
     from mpm_b200.adjoint import create_mpm_adjoint_engine, fixed_cfl_dt
     from mpm_b200.scenes import ADJOINT_GRAVITY, create_adjoint_scenes
@@ -594,7 +615,7 @@ def run_b200_adjoint(args):
         gv, gp = engine.backward()
         return loss, gv, gp
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         one_step()
     torch.cuda.synchronize()
     if dist:
@@ -602,7 +623,7 @@ def run_b200_adjoint(args):
     clocks = ClockSampler(local_rank)
     clocks.start()
     fwd = bwd = wall = 0.0
-    for _ in range(args.steps):
+    for _ in range(steps_timed):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         loss, gv, gp = one_step()
@@ -616,7 +637,7 @@ def run_b200_adjoint(args):
     # 200 substeps: every substep's state and node sums stay in HBM, the
     # backward pass recomputes nothing); after the timed region
     tape_fwd = tape_bwd = 0.0
-    for k in range(2):
+    for k in range(2 if full_tape else 0):
         engine.forward(steps, dts, targets, steps)
         engine.backward()
         if k == 1:
@@ -633,13 +654,13 @@ def run_b200_adjoint(args):
     batch.step_batch([steps] * len(scenes), dts, gravity)
     plain_ms = batch.last_batch_device_ms()
     batch.dispose()
-    work = world * n * steps * args.steps
+    work = world * n * steps * steps_timed
     value = work / bwd_s
     peak, peak_kind = _peaks()
-    achieved = ADJOINT_BYTES_PER_PARTICLE * n * steps * args.steps / bwd_s / 1e9
+    achieved = ADJOINT_BYTES_PER_PARTICLE * n * steps * steps_timed / bwd_s / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": "particle-substeps/s (adjoint)", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": (fwd_s + bwd_s) * 1e3 / args.steps,
+        "steps": steps_timed, "warmup": warmup, "ms_per_step": (fwd_s + bwd_s) * 1e3 / steps_timed,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded scenes, no dataset)",
         "config": {"workload": "differentiable form: 64 scenes of 12,288 Tait water + 4,096 fixed-corotated "
@@ -651,10 +672,11 @@ def run_b200_adjoint(args):
                    "parallelism": f"scene shards x{world} (64 different scenes per GPU)",
                    "l2": "inputs larger than L2 (1M particles' state and 64 grids of 67,081 nodes)",
                    "adjoint_forward_ratio": bwd_s / fwd_s,
-                   "adjoint_over_default_forward": (bwd_s / args.steps) / (plain_ms * 1e-3),
-                   "forward_ms": fwd_s * 1e3 / args.steps, "backward_ms": bwd_s * 1e3 / args.steps,
+                   "adjoint_over_default_forward": (bwd_s / steps_timed) / (plain_ms * 1e-3),
+                   "forward_ms": fwd_s * 1e3 / steps_timed, "backward_ms": bwd_s * 1e3 / steps_timed,
                    "default_solver_forward_ms": plain_ms,
-                   "full_tape": {"adjoint_forward_ratio": tape_bwd / tape_fwd, "forward_ms": tape_fwd,
+                   "full_tape": None if not full_tape else {
+                                 "adjoint_forward_ratio": tape_bwd / tape_fwd, "forward_ms": tape_fwd,
                                  "backward_ms": tape_bwd, "tape_gb": tape_gb,
                                  "note": "every substep's state and node sums kept in HBM (checkpoint_every = "
                                          "substeps): no recompute; measured once after the timed region"}},
@@ -667,23 +689,14 @@ def run_b200_adjoint(args):
                      "peak_source": peak_kind, "traffic": None,
                      "algorithmic_bytes_per_particle_substep": ADJOINT_BYTES_PER_PARTICLE},
         "clocks": clock_info,
-        "gpu_launches": int(args.steps * (2 * steps + 4 * steps + 1)),
+        "gpu_launches": int(steps_timed * (2 * steps + 4 * steps + 1)),
     }
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line
 
 
 def run_b200(args):
-    rank, local_rank, world = _rank_info()
+    dist, rank, local_rank, world = _init_ranks()
     import torch
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    torch.cuda.set_device(local_rank)
     from mpm_b200 import create_experimental_mpm_mls_atomic_gpu_solver, create_mpm_mls_gpu_solver
 
     particles, config, gravity, meta = build_workload(args.workload)
@@ -708,33 +721,46 @@ def run_b200(args):
     shape = solver.autotune(substeps=4) if args.p2g == "gather" else None
     for _ in range(args.warmup - 1):
         one_step()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
     clocks = ClockSampler(local_rank)
     clocks.start()
-    solver.device_ms_total = 0.0
-    solver.committed_microsteps_total = 0
-    wall = 0.0
-    retries = 0
-    h2d = d2h = 0
-    for _ in range(args.steps):
-        flush.zero_()  # L2 flush between timed steps (outside the timed batches)
+    # the timed region (K steps between barriers and synchronizes) is taken
+    # args.repeats times back to back; the line reports the repeat with the
+    # median device throughput and lists them all
+    repeats = []
+    for _ in range(args.repeats):
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        m = one_step()
-        wall += time.perf_counter() - t0
-        retries += m["retryCount"]
-        batches = 1 + m["retryCount"]
-        h2d += batches * 160  # StepParams upload per batch
-        d2h += batches * 40   # compact speed / progress / status readback
-    torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        solver.device_ms_total = 0.0
+        solver.committed_microsteps_total = 0
+        wall = 0.0
+        retries = 0
+        h2d = d2h = 0
+        for _ in range(args.steps):
+            flush.zero_()  # L2 flush between timed steps (outside the timed batches)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            m = one_step()
+            wall += time.perf_counter() - t0
+            retries += m["retryCount"]
+            batches = 1 + m["retryCount"]
+            h2d += batches * 160  # StepParams upload per batch
+            d2h += batches * 40   # compact speed / progress / status readback
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        (r_device_s, r_wall), (r_substeps,) = reduce_over_ranks(
+            dist, f"cuda:{local_rank}", [solver.device_ms_total / 1e3, wall], [solver.committed_microsteps_total])
+        repeats.append({"device_s": r_device_s, "wall_s": r_wall, "substeps": int(r_substeps), "retries": retries,
+                        "h2d": h2d, "d2h": d2h,
+                        "value": n * r_substeps / r_device_s, "e2e": n * r_substeps / r_wall})
     clock_info = clocks.stop()
-    device_s = solver.device_ms_total / 1e3
-    substeps = solver.committed_microsteps_total
-    (device_s, wall), _ = reduce_over_ranks(dist, f"cuda:{local_rank}", [device_s, wall], [])
-    value = world * n * substeps / device_s
-    e2e_value = world * n * substeps / wall
+    chosen = sorted(repeats, key=lambda r: r["value"])[len(repeats) // 2]
+    device_s, wall, retries, h2d, d2h = (chosen["device_s"], chosen["wall_s"], chosen["retries"], chosen["h2d"],
+                                         chosen["d2h"])
+    substeps = chosen["substeps"]  # summed over ranks
+    value = n * substeps / device_s
+    e2e_value = n * substeps / wall
 
     # roofline: kernel-by-kernel timing of real substeps right after the timed region
     plan, bound = plan_macrostep(solver, config, velocity, macro_dt, gravity)
@@ -754,14 +780,17 @@ def run_b200(args):
     gpu_launches = 0
     launches_per_substep = sum(l for _, l in prof.values()) / plan["stepCount"]
     gpu_launches = int(round(launches_per_substep * substeps / world)) if substeps else 0
+    substeps_rank = substeps // world
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": device_s * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene, no dataset)",
         "config": dict(meta, p2g=args.p2g, parallelism=f"replicas x{world}", l2="flushed (512 MiB write) "
-                       "between timed steps", committed_substeps=substeps, retries=retries, launch_shape=shape,
-                       substeps_per_step=substeps / args.steps / world),
+                       "between timed steps", committed_substeps=substeps_rank, retries=retries, launch_shape=shape,
+                       substeps_per_step=substeps_rank / args.steps,
+                       repeats={"count": args.repeats, "reported": "median by value",
+                                "values": [r["value"] for r in repeats], "e2e": [r["e2e"] for r in repeats]}),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps,
                 "path": "Python host mirror of MpmMlsGpuSolver.stepCflBatchAdaptive -> C ABI"},
@@ -792,9 +821,32 @@ def run_b200(args):
         line["cpu_baseline"] = cpu_baseline(particles, config, gravity, float(np.float32(plan["microDt"])),
                                             args.cpu_substeps)
     solver.dispose()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    del flush
+    torch.cuda.empty_cache()
+    if args.workload == "dam-break-1m" and args.p2g == "gather" and not args.no_legs:
+        # the metric's other two numbers, after the headline's timed region:
+        # the batched form (and the same scenes one solver each) and the
+        # differentiable form's adjoint/forward time ratio, each with fewer
+        # steps than the headline (stated in the leg)
+        b = measure_batched(args.leg_steps, 3, 1.25, 1.0, dist, rank, local_rank, world)
+        plain = b["config"]["plain_per_scene"]["value"]
+        line["batched"] = {"value": b["value"], "unit": UNIT, "plain_per_scene": plain,
+                           "batched_over_plain": None if not plain else b["value"] / plain,
+                           "steps": b["steps"], "warmup": b["warmup"], "e2e": b["e2e"]["value"],
+                           "workload": b["config"]["workload"], "scenes": b["config"]["scenes"],
+                           "particles": b["config"]["particles"], "retries": b["config"]["retries"],
+                           "roofline": {k: b["roofline"][k] for k in ("kernel", "achieved", "frac", "substep")},
+                           "clocks": b["clocks"]}
+        a = measure_adjoint(1, 1, dist, rank, local_rank, world, full_tape=False)
+        cfg = a["config"]
+        line["adjoint"] = {"forward_ms": cfg["forward_ms"], "backward_ms": cfg["backward_ms"],
+                           "adjoint_forward_ratio": cfg["adjoint_forward_ratio"],
+                           "checkpoint_every": cfg["checkpoint_every"], "substeps": cfg["substeps"],
+                           "default_solver_forward_ms": cfg["default_solver_forward_ms"],
+                           "adjoint_over_default_forward": cfg["adjoint_over_default_forward"],
+                           "value": a["value"], "unit": a["unit"], "steps": 1, "warmup": 1,
+                           "workload": cfg["workload"], "clocks": a["clocks"]}
+    _finish_ranks(dist)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -812,6 +864,9 @@ def main():
     ap.add_argument("--cpu-substeps", type=int, default=12)
     ap.add_argument("--reference-substeps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--repeats", type=int, default=5, help="timed regions of K steps; the median is reported")
+    ap.add_argument("--no-legs", action="store_true", help="skip the batched and adjoint legs of the default line")
+    ap.add_argument("--leg-steps", type=int, default=3, help="timed macrosteps of the batched leg")
     # the batched workload's adaptive CFL policy (the reference's: 1.25 and no margin)
     ap.add_argument("--cfl-recovery-factor", type=float, default=1.25)
     ap.add_argument("--cfl-plan-margin", type=float, default=1.0)

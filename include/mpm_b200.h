@@ -360,8 +360,11 @@ void mpma_destroy(mpm_adjoint *engine);
  * `count` and (cells_x+3)*(cells_y+3)+1 words.  Limits: count <= 65536 and
  * (cells_x+3)*(cells_y+3) <= 262144, else MPM_ERR_INVALID_ARGUMENT with the
  * reason written to `error_out` (may be NULL).  The first call on a device
- * resolves the array's address (make it before any stream capture); calls
- * share the array, so calls that overlap on one GPU race.  Blocks until done. */
+ * resolves the array's address and keeps it (make that call before any stream
+ * capture; after a cudaDeviceReset of that device the kept address is stale,
+ * so do not call it there again); calls share the array, so calls that
+ * overlap on one GPU race.  The caller's current device is restored on
+ * return.  Blocks until done. */
 int mpm_cell_sort_static(int32_t device, uint32_t cells_x, uint32_t cells_y, float cell_size,
                          const float *positions, uint32_t count, uint32_t *keys_out, uint32_t *perm_out,
                          uint32_t *cell_start_out, char *error_out, uint32_t error_capacity);

@@ -19,7 +19,10 @@
 // left in it; each call clears the parts that must start at zero.  Calls that
 // overlap on the same GPU (from two host threads) race on it: serialise them.
 // The first call on a device resolves the array's device address with
-// cudaGetSymbolAddress; make that first call before any stream capture.
+// cudaGetSymbolAddress and keeps it; make that first call before any stream
+// capture.  A cudaDeviceReset (or any teardown of the device's primary
+// context) invalidates the kept address: do not call this entry point on that
+// device afterwards.  The caller's current device is restored on return.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -52,6 +55,13 @@ constexpr size_t OFF_START = align256(OFF_COUNT + STATIC_SORT_MAX_NODES * sizeof
 constexpr size_t OFF_BLOCKS = align256(OFF_START + (STATIC_SORT_MAX_NODES + 1) * sizeof(uint32_t));
 constexpr size_t STATIC_SORT_BYTES =
     align256(OFF_BLOCKS + (STATIC_SORT_MAX_NODES / SCAN_CHUNK + 1) * sizeof(uint32_t));
+// k_scan_apply writes cell starts over the whole padded scan range (a
+// multiple of SCAN_CHUNK) plus one word: with the maximum a multiple of the
+// chunk, that range ends inside the start region
+static_assert(STATIC_SORT_MAX_NODES % SCAN_CHUNK == 0, "the node maximum must be a multiple of the scan chunk");
+static_assert(OFF_BLOCKS >= OFF_START + (STATIC_SORT_MAX_NODES + 1) * sizeof(uint32_t),
+              "the start region must hold the padded scan range and its end word");
+static_assert(OFF_START >= OFF_COUNT + STATIC_SORT_MAX_NODES * sizeof(uint32_t), "the count region is too small");
 
 // The scratch.  In host code this name is only a stand-in for the symbol:
 // kernels get the address that cudaGetSymbolAddress returns for the current
@@ -87,6 +97,10 @@ __global__ void k_static_stable_rank(Ctx c)
     c.perm[lo + rank] = i;
 }
 
+int sort_on_current_device(int32_t device, uint32_t cells_x, uint32_t cells_y, float cell_size,
+                           const float *positions, uint32_t count, uint64_t nodes, uint32_t *keys_out,
+                           uint32_t *perm_out, uint32_t *cell_start_out, char *error_out, uint32_t error_capacity);
+
 }  // namespace
 
 extern "C" int mpm_cell_sort_static(int32_t device, uint32_t cells_x, uint32_t cells_y, float cell_size,
@@ -107,7 +121,21 @@ extern "C" int mpm_cell_sort_static(int32_t device, uint32_t cells_x, uint32_t c
         return fail(error_out, error_capacity, MPM_ERR_INVALID_ARGUMENT, "the particle count exceeds the static sort maximum of 65536");
     if (device < 0 || device >= STATIC_SORT_MAX_DEVICES)
         return fail(error_out, error_capacity, MPM_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    int previous = -1;
+    if (cudaGetDevice(&previous) != cudaSuccess) previous = -1;
     if (cudaSetDevice(device) != cudaSuccess) return fail(error_out, error_capacity, MPM_ERR_CUDA, "cudaSetDevice failed");
+    const int rc = sort_on_current_device(device, cells_x, cells_y, cell_size, positions, count, nodes, keys_out,
+                                          perm_out, cell_start_out, error_out, error_capacity);
+    if (previous >= 0 && previous != device) cudaSetDevice(previous);
+    return rc;
+}
+
+namespace {
+
+int sort_on_current_device(int32_t device, uint32_t cells_x, uint32_t cells_y, float cell_size,
+                           const float *positions, uint32_t count, uint64_t nodes, uint32_t *keys_out,
+                           uint32_t *perm_out, uint32_t *cell_start_out, char *error_out, uint32_t error_capacity)
+{
 
     // one-time set-up on this device (must precede any stream capture)
     if (!g_scratch_address[device]) {
@@ -178,6 +206,9 @@ extern "C" int mpm_cell_sort_static(int32_t device, uint32_t cells_x, uint32_t c
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return fail(error_out, error_capacity, MPM_ERR_CUDA, cudaGetErrorString(e));
     if (status[0] != 0u)
-        return fail(error_out, error_capacity, MPM_ERR_INVALID_ARGUMENT, "a position lies outside the grid domain (status 1)");
+        return fail(error_out, error_capacity, MPM_ERR_INVALID_ARGUMENT,
+                    "a position is non-finite or its stencil leaves the grid halo (status 1)");
     return MPM_OK;
 }
+
+}  // namespace

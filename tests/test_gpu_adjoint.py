@@ -153,3 +153,47 @@ def test_checkpoint_interval_changes_gradients_by_rounding_only():
     for gv, gp in results[1:]:
         assert np.allclose(gp, gp0, rtol=1e-3, atol=1e-6 * np.abs(gp0).max())
         assert np.linalg.norm(gv - gv0) <= 1e-3 * np.linalg.norm(gv0)
+
+
+def test_adjoint_at_the_full_horizon_with_checkpoints():
+    # the differentiable workload's horizon: 200 substeps, a checkpoint every
+    # 20, on the 1,024-particle subset; against the FP64 adjoint and a
+    # directional central difference of the FP64 forward (relative step 1e-3)
+    steps = 200
+    scenes, dts = _scenes(1, steps=steps)
+    (p, c, t), = scenes
+    engine = _engine(scenes)
+    try:
+        loss = engine.forward(steps, dts, t, checkpoint_every=20)
+        gv, gp = engine.backward()
+    finally:
+        engine.dispose()
+    ref_loss, ref_gv, ref_gp, _ = _fp64(p, c, t, dts[0], steps)
+    assert abs(loss[0] - ref_loss) <= 1e-3 * ref_loss
+    for k in range(3):
+        assert abs(gp[0, k] - ref_gp[k]) <= 5e-2 * abs(ref_gp[k]) + 1e-6 * np.abs(ref_gp).max(), (k, gp[0], ref_gp)
+    a, b = gv.astype(np.float64).ravel(), ref_gv.ravel()
+    cosine = a @ b / (np.linalg.norm(a) * np.linalg.norm(b))
+    assert cosine > 0.995, cosine
+    assert np.linalg.norm(a - b) <= 1e-1 * np.linalg.norm(b)
+    state = validate_mpm_mls_gpu_input(p, c)
+    pk = state.packed_particles
+    liquid = pk[:, 13].view(np.uint32) == 2
+    pk64 = pk.astype(np.float64)
+    water, solid = pk64[liquid][0], pk64[~liquid][0]
+    scene = {"cells_x": 64, "cells_y": 64, "dx": 10.0, "dt": dts[0], "gx": ADJOINT_GRAVITY["x"],
+             "gy": ADJOINT_GRAVITY["y"], "solid_mass": float(np.float32(c["particleMass"])), "wall_friction": 0.0,
+             "rho": float(water[16]), "gamma": float(water[18]), "tait": float(water[14]),
+             "lambda_s": float(solid[14]), "mu_s": float(solid[15])}
+    target = np.asarray(t, np.float32).astype(np.float64)
+    v0 = pk64[:, 2:4]
+    d = np.random.default_rng(2).normal(size=v0.shape)
+    h = 1e-3 * np.abs(v0).mean()
+
+    def fp64_loss(v):
+        return adjoint_fp64(scene, pk64[:, 0:2], v, pk64[:, 4:8], pk64[:, 8:12], pk64[:, 17],
+                            liquid.astype(np.int32), target, steps)[0]
+
+    fd = (fp64_loss(v0 + h * d) - fp64_loss(v0 - h * d)) / (2 * h)
+    directional = float(np.sum(gv.astype(np.float64) * d))
+    assert abs(fd - directional) <= 5e-2 * abs(fd), (fd, directional)

@@ -4,9 +4,11 @@ Callers that cannot call cudaMalloc (an embedding host that owns the GPU
 memory budget, a frame loop that must not stall on an allocation, a thin
 foreign-function host without an allocator) use mpm_cell_sort_static, whose
 scratch is a static array inside the library.  Its keys, permutation and cell
-starts must equal those of the solver's own sort (mpm_probe_sort) bit for
-bit, on two calls in a row (the second call reuses the array the first call
-left behind), and sizes beyond its fixed maximum must be refused.
+starts must equal those of the solver's own sort (mpm_probe_sort) and the
+stable argsort of the keys bit for bit, on two calls in a row (the second call
+reuses the array the first call left behind); the calls must not take device
+memory (free memory, read with cudaMemGetInfo, stays within one allocation
+granule), and sizes beyond its fixed maximum must be refused.
 
 This file is collected last so that a run that stops at the first failure has
 already run every other test.
@@ -35,6 +37,13 @@ def _static_sort(lib, cells_x, cells_y, cell_size, positions):
     return rc, keys, perm, starts, error.value.decode()
 
 
+def _free_device_bytes():
+    runtime = ctypes.CDLL("libcudart.so.12")
+    free, total = ctypes.c_size_t(), ctypes.c_size_t()
+    assert runtime.cudaMemGetInfo(ctypes.byref(free), ctypes.byref(total)) == 0
+    return free.value
+
+
 def _library():
     lib = _lib.load_library()
     fn = lib.mpm_cell_sort_static
@@ -56,13 +65,24 @@ def test_static_sort_matches_the_solver_sort_on_two_calls(seed):
         solver.dispose()
     positions = validate_mpm_mls_gpu_input(particles, config).packed_particles[:, 0:2]
     grid = config["grid"]
-    for _ in range(2):
-        rc, keys, perm, starts, message = _static_sort(lib, grid["cellsX"], grid["cellsY"],
-                                                       np.float32(grid["cellSize"]), positions)
+    # the stable counting sort, stated directly: keys of the base cells, the
+    # stable argsort, the cell starts
+    dx = np.float32(grid["cellSize"])
+    base = np.floor((positions / dx).astype(np.float32) - np.float32(0.5)).astype(np.int64)
+    keys_np = (base[:, 1] + 1) * (grid["cellsX"] + 3) + (base[:, 0] + 1)
+    perm_np = np.argsort(keys_np, kind="stable")
+    counts = np.bincount(keys_np, minlength=(grid["cellsX"] + 3) * (grid["cellsY"] + 3))
+    starts_np = np.concatenate(([0], np.cumsum(counts)))
+    free_before = None
+    for call in range(3):
+        rc, keys, perm, starts, message = _static_sort(lib, grid["cellsX"], grid["cellsY"], dx, positions)
         assert rc == 0, message
-        assert np.array_equal(keys, keys_ref)
-        assert np.array_equal(perm, perm_ref)
-        assert np.array_equal(starts, starts_ref)
+        assert np.array_equal(keys, keys_ref) and np.array_equal(keys.astype(np.int64), keys_np)
+        assert np.array_equal(perm, perm_ref) and np.array_equal(perm.astype(np.int64), perm_np)
+        assert np.array_equal(starts, starts_ref) and np.array_equal(starts.astype(np.int64), starts_np)
+        if call == 0:
+            free_before = _free_device_bytes()  # after the first call's one-time set-up
+    assert free_before - _free_device_bytes() < 2 * 1024 * 1024
 
 
 def test_static_sort_refuses_sizes_beyond_its_maximum():
