@@ -257,13 +257,24 @@ def _reference_plan(workload: str):
     raise SystemExit(f"unknown workload {workload}")
 
 
+def _job_cost(kind, payload) -> int:
+    particles, config = payload[0], payload[1]
+    from mpm_b200.sharding import scene_cost
+    return scene_cost(len(particles), config["grid"]["cellsX"], config["grid"]["cellsY"])
+
+
 def _reference_share(workload: str, worker: int, workers: int):
     """The jobs of process `worker`: the whole scene for the plain form (a
-    replica), every workers-th scene otherwise."""
+    replica), its cost-balanced share of the scenes otherwise."""
     jobs, _ = _reference_plan(workload)
     from oracle import OracleState
+    from mpm_b200.sharding import shard_by_cost
     mine = []
-    picked = jobs if len(jobs) == 1 else jobs[worker::workers]
+    if len(jobs) == 1:
+        picked = jobs
+    else:
+        share = shard_by_cost([_job_cost(kind, payload) for kind, payload in jobs], workers)[worker]
+        picked = [jobs[k] for k in share]
     for kind, payload in picked:
         if kind == "step":
             particles, cfg = payload
@@ -468,8 +479,13 @@ def measure_batched(steps, warmup, recovery_factor, plan_margin, dist, rank, loc
     the bench line of the form (`steps` timed after `warmup`)."""
     import torch
     from mpm_b200 import create_mpm_batched_gpu_solver
-    from mpm_b200.scenes import BATCHED_TANK_GRAVITY, create_batched_tank_scenes
-    scenes = create_batched_tank_scenes(first=rank * 512)  # each rank its own shard of scenes
+    from mpm_b200.scenes import BATCHED_TANK_GRAVITY, batched_tank_scene_specs, create_batched_tank_scenes
+    from mpm_b200.sharding import scene_cost, shard_by_cost
+    # 512 scenes per GPU: the world's 512 x N seeded scenes bin-packed over the
+    # ranks by cost (particles + halo nodes), every rank computing the same split
+    specs = batched_tank_scene_specs(count=512 * world)
+    share = shard_by_cost([scene_cost(n, side, side) for n, side in specs], world)[rank]
+    scenes = create_batched_tank_scenes(indices=share)
     gravity = BATCHED_TANK_GRAVITY
     macro_dt = MACRO_DT
     batch = create_mpm_batched_gpu_solver(scenes, device=local_rank)
@@ -543,7 +559,7 @@ def measure_batched(steps, warmup, recovery_factor, plan_margin, dist, rank, loc
                    "scenes": len(scenes), "particles": n_total, "particles_range": [int(counts.min()),
                                                                                    int(counts.max())],
                    "grid_sides_range": [min(sides), max(sides)], "macro_dt": macro_dt, "courant": 0.3,
-                   "p2g": "gather", "parallelism": f"scene shards x{world} (512 different scenes per GPU)",
+                   "p2g": "gather", "parallelism": f"scene shards x{world} (512 x {world} scenes bin-packed by cost over the GPUs)",
                    "l2": "inputs larger than L2 (every scene's state, about 0.8 GB)",
                    "committed_particle_substeps": work, "submits": submits, "retries": retries,
                    "launch_shape": shape,
@@ -851,6 +867,49 @@ def run_b200(args):
         print(json.dumps(line), flush=True)
 
 
+PROFILE_CASES = ("batched", "dense", "adjoint")
+
+
+def run_profile_case(name: str):
+    """Small fixed cases for kernel profiling (ncu launch lists, a few hundred
+    launches each); prints the device milliseconds of the last pass.
+
+    batched: the 512 batched tanks, 2 x 4 substeps at the smallest CFL dt;
+    dense:   the 64 of those tanks with the most particles per cell, likewise;
+    adjoint: the 64 differentiable-form scenes, 2 x (40 forward + 40 backward).
+    """
+    from mpm_b200 import calculate_mpm_cfl_microsteps, create_mpm_batched_gpu_solver
+    from mpm_b200.adjoint import create_mpm_adjoint_engine, fixed_cfl_dt
+    from mpm_b200.scenes import (ADJOINT_GRAVITY, BATCHED_TANK_GRAVITY, create_adjoint_scenes,
+                                  create_batched_tank_scenes)
+    if name in ("batched", "dense"):
+        scenes = create_batched_tank_scenes()
+        if name == "dense":
+            per_cell = np.array([len(p.px) / c["grid"]["cellsX"] ** 2 for p, c in scenes])
+            scenes = [scenes[i] for i in np.argsort(per_cell)[-64:]]
+        b = create_mpm_batched_gpu_solver(scenes)
+        try:
+            dt = min(calculate_mpm_cfl_microsteps(1 / 240, c["grid"]["cellSize"], bounds["waveSpeedBound"], 1.0,
+                                                  4096)["microDt"] for (_, c), bounds in zip(scenes, b.cfl_bounds))
+            for _ in range(2):
+                b.step_batch([4] * len(scenes), [dt] * len(scenes), BATCHED_TANK_GRAVITY)
+            print(f"{name}: 4 substeps of {len(scenes)} scenes", b.last_batch_device_ms(), "ms")
+        finally:
+            b.dispose()
+        return
+    scenes = create_adjoint_scenes()
+    dts = [float(np.float32(fixed_cfl_dt(p, c, 90.0, 0.2))) for p, c, _ in scenes]
+    targets = np.concatenate([t for _, _, t in scenes]).astype(np.float32)
+    e = create_mpm_adjoint_engine([(p, c) for p, c, _ in scenes], ADJOINT_GRAVITY)
+    try:
+        for _ in range(2):
+            e.forward(40, dts, targets, 20)
+            e.backward()
+        print("adjoint: 40 substeps of 64 scenes, forward / backward", e.last_ms(), "ms")
+    finally:
+        e.dispose()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -867,10 +926,14 @@ def main():
     ap.add_argument("--repeats", type=int, default=5, help="timed regions of K steps; the median is reported")
     ap.add_argument("--no-legs", action="store_true", help="skip the batched and adjoint legs of the default line")
     ap.add_argument("--leg-steps", type=int, default=3, help="timed macrosteps of the batched leg")
+    ap.add_argument("--profile-case", choices=PROFILE_CASES, help="run a small fixed case for kernel profiling")
     # the batched workload's adaptive CFL policy (the reference's: 1.25 and no margin)
     ap.add_argument("--cfl-recovery-factor", type=float, default=1.25)
     ap.add_argument("--cfl-plan-margin", type=float, default=1.0)
     args = ap.parse_args()
+    if args.profile_case:
+        run_profile_case(args.profile_case)
+        return
     if args.warmup < 3:
         raise SystemExit("--warmup must be at least 3")
     if args.impl == "reference":

@@ -350,8 +350,23 @@ BATCHED_TANK_GRAVITY = {"x": 0.0, "y": -9.81}
 BATCHED_TANK_MAX_FILL_HEIGHT = 0.6  # of the box
 
 
+def batched_tank_scene_specs(count: int = 512, seed: int = 0x4D504D42, particles=(1_000, 64_000), sides=(64, 512),
+                             first: int = 0) -> list:
+    """(particle count N, grid side S) of scenes first .. first + count - 1
+    of create_batched_tank_scenes, without building their particles (the
+    first two draws of each scene's LCG)."""
+    out = []
+    for k in range(first, first + count):
+        rnd = SeededRandom((seed + k * 0x9E3779B9) % UINT32_RANGE)
+        log_lo, log_hi = math.log(particles[0]), math.log(particles[1])
+        n = int(round(math.exp(log_lo + rnd() * (log_hi - log_lo))))
+        side = min(int(sides[0] + math.floor(rnd() * (sides[1] - sides[0] + 1))), sides[1])
+        out.append((n, side))
+    return out
+
+
 def create_batched_tank_scenes(count: int = 512, seed: int = 0x4D504D42, particles=(1_000, 64_000),
-                               sides=(64, 512), first: int = 0):
+                               sides=(64, 512), first: int = 0, indices=None):
     """`count` independent SI Tait water tanks (rho 1000 kg/m^3, gamma 7,
     c = 20 m/s, 0.02 m extrusion, no-slip walls, at rest under y-up gravity
     9.81 m/s^2), each a 0.2 m square box.  Scene k (k = first, ..., first +
@@ -361,8 +376,9 @@ def create_batched_tank_scenes(count: int = 512, seed: int = 0x4D504D42, particl
     S), the width of its block (a quarter to 0.6 of the box) and the block's
     place.  The block is a lattice at dx / 2 (2 x 2 particles per cell) where
     N of them fit under 0.6 of the box height, else at the finer spacing that
-    fits; each particle is jittered by U(+-0.1) spacing.  Returns
-    [(particles, config), ...]."""
+    fits; each particle is jittered by U(+-0.1) spacing.  `indices`, when
+    given, replaces first .. first + count - 1 by those scene numbers.
+    Returns [(particles, config), ...]."""
     depth = MPM_SI_BOX_DOMAIN["extrusionDepthM"]
     tait = {"referenceDensityKgPerM3": 1000.0, "exponent": 7.0,
             "pressureCoefficientPa": derive_tait_pressure_coefficient_pa(1000.0, 7.0, 20.0)}
@@ -370,7 +386,7 @@ def create_batched_tank_scenes(count: int = 512, seed: int = 0x4D504D42, particl
     size = BATCHED_TANK_DOMAIN_M
     top = BATCHED_TANK_MAX_FILL_HEIGHT * size
     out = []
-    for k in range(first, first + count):
+    for k in (range(first, first + count) if indices is None else indices):
         rnd = SeededRandom((seed + k * 0x9E3779B9) % UINT32_RANGE)
         log_lo, log_hi = math.log(particles[0]), math.log(particles[1])
         n = int(round(math.exp(log_lo + rnd() * (log_hi - log_lo))))
