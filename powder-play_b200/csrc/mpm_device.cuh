@@ -77,7 +77,8 @@ struct Material {
     float mu;
     float density;
     float param;  // Tait exponent (liquids, 0 = linear EOS) or powder friction
-    float pad0, pad1, pad2;
+    float c2;     // liquids: lambda / density (the rest wave speed squared), rounded once
+    float pad1, pad2;
 };
 
 // Per-batch parameters, written by the host before each batch launch.  The

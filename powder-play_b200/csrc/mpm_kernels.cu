@@ -710,21 +710,35 @@ __global__ void k_tile_count(Ctx c0)
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const Ctx c = scene_ctx(c0, c0.n_scenes == 1u || i >= c0.n ? 0u : scene_of_slot(c0, i));
     const StepParams &P = *c.P;
-    bool valid = i < c0.n && takes_part(c);
+    bool valid;
+    if (c0.n_scenes == 1u) {
+        // one scene: whether it takes part, read once per CTA
+        __shared__ int s_part;
+        if (threadIdx.x == 0) s_part = takes_part(c) ? 1 : 0;
+        __syncthreads();
+        valid = i < c0.n && s_part != 0;
+    } else {
+        valid = i < c0.n && takes_part(c);
+    }
     uint32_t key = 0;
     if (valid) {
+        // every load of the slot at once (damage and plastic volume exist for
+        // every slot; only Neo-Hookean and snow particles use them)
+        const float2 pos = c.in.pos[i], vel = c.in.vel[i];
+        const float4 F = c.in.F[i], C = c.in.C[i];
+        const float vol = c.in.vol[i], damage_in = c.in.damage[i], pvol_in = c.in.pvol[i];
+        const uint32_t mat = c.in.mat[i], orig = c.in.orig[i];
         Stencil s;
-        if (!make_stencil_fast(P, c.in.pos[i], s) || !stencil_fits(P, s.bx, s.by)) {
+        if (!make_stencil_fast(P, pos, s) || !stencil_fits(P, s.bx, s.by)) {
             fail(c.status, ERROR_STENCIL);
             valid = false;
         } else {
             key = particle_tile(P, s.bx, s.by);
-            const uint32_t orig = c.in.orig[i];
             if (is_tracked(c, orig)) c.slot_in[orig] = i;
-            const Material m = c.mats[c.in.mat[i]];
-            const float damage = m.model == MODEL_NEO_HOOKEAN ? c.in.damage[i] : 0.0f;
-            const float pvol = m.model == MODEL_SNOW ? c.in.pvol[i] : 1.0f;
-            write_record(c, i, m, s, c.in.vel[i], c.in.F[i], c.in.vol[i], damage, pvol, c.in.C[i]);
+            const Material m = c.mats[mat];
+            const float damage = m.model == MODEL_NEO_HOOKEAN ? damage_in : 0.0f;
+            const float pvol = m.model == MODEL_SNOW ? pvol_in : 1.0f;
+            write_record(c, i, m, s, vel, F, vol, damage, pvol, C);
         }
     }
     const unsigned active = __ballot_sync(0xffffffffu, valid);
@@ -1273,34 +1287,42 @@ __device__ __forceinline__ NodeSources node_sources(const StepParams &P, const u
     return ns;
 }
 
-// Adds the ring records of a node into sum[] in source order: every word
-// when `all`, else only the water and oil volumes (words 6 and 10).
-__device__ __forceinline__ void add_sources(const Ctx &c, const NodeSources &ns, bool all, float (&sum)[ACC_WORDS])
+// Adds words W0 .. W0 + NW - 1 of a node's (up to four) ring records into
+// sum[] in source order.  All the loads are issued before the first add (one
+// L2 round trip, not one per source); a source without the channel adds +0,
+// which leaves the sum's bits unchanged (a sum that starts at +0 is never -0).
+template <int W0, int NW>
+__device__ __forceinline__ void add_channel(const float *part, const NodeSources &ns, uint32_t bit,
+                                            float (&sum)[ACC_WORDS])
 {
+    float v[4][NW];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const uint32_t mask = ns.mask[k];
-        if (!mask) continue;
-        const float *src = c.part + ns.base[k];
-        if (all) {
-            if (mask & 1u) {
-                sum[0] += src[0];
-                sum[1] += src[RING_NODES];
-                sum[2] += src[2 * RING_NODES];
-            }
-            if (mask & 2u) {
-                sum[3] += src[3 * RING_NODES];
-                sum[4] += src[4 * RING_NODES];
-                sum[5] += src[5 * RING_NODES];
-            }
-            if (mask & 4u) {
-                sum[7] += src[7 * RING_NODES];
-                sum[8] += src[8 * RING_NODES];
-                sum[9] += src[9 * RING_NODES];
-            }
-        }
-        if (mask & 2u) sum[6] += src[6 * RING_NODES];
-        if (mask & 4u) sum[10] += src[10 * RING_NODES];
+        const bool has = (ns.mask[k] & bit) != 0u;
+        const float *src = part + ns.base[k];
+#pragma unroll
+        for (int w = 0; w < NW; ++w) v[k][w] = has ? __ldcg(src + (W0 + w) * RING_NODES) : 0.0f;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int w = 0; w < NW; ++w) sum[W0 + w] += v[k][w];
+}
+
+// Adds the ring records of a node into sum[] in source order: every word of
+// the channels in `channels` when `all`, else only the water and oil volumes
+// (words 6 and 10).  `channels` (the union of the neighbour records' masks)
+// is the same for the whole CTA, so its branches do not diverge.
+__device__ __forceinline__ void add_sources(const Ctx &c, const NodeSources &ns, bool all, uint32_t channels,
+                                            float (&sum)[ACC_WORDS])
+{
+    if (all) {
+        if (channels & 1u) add_channel<0, 3>(c.part, ns, 1u, sum);
+        if (channels & 2u) add_channel<3, 4>(c.part, ns, 2u, sum);
+        if (channels & 4u) add_channel<7, 4>(c.part, ns, 4u, sum);
+    } else {
+        if (channels & 2u) add_channel<6, 1>(c.part, ns, 2u, sum);
+        if (channels & 4u) add_channel<10, 1>(c.part, ns, 4u, sum);
     }
 }
 
@@ -1449,7 +1471,7 @@ __device__ float wave_speed_bound(const Ctx &c, const Material &m, float4 F, flo
 {
     if (m.model == MODEL_WATER || m.model == MODEL_OIL) {
         if (!finite_f(m.lambda) || !finite_f(m.density) || m.lambda <= 0.f || m.density <= 0.f) return FLOAT_MAX;
-        float c2 = m.lambda / m.density;
+        float c2 = m.c2;  // lambda / density, divided once on the host
         if (m.param > 0.0f) {
             const float det = det2(F);
             if (!finite_f(m.param) || m.param <= 0.f || !finite_f(det) || det <= 0.f) return FLOAT_MAX;
@@ -1890,15 +1912,17 @@ __device__ __forceinline__ void stage_particle(const Ctx &c, uint32_t s, uint32_
     cp_async<4>(&orig[i], &c.in.orig[s]);
 }
 
-// Copies the G2P inputs of bucket entries [base, base + count) to shared
-// indices 0..count-1; count <= G2P_STAGE = 2 * G2P_THREADS, and both bucket
-// entries of a thread are read before either copy is issued.
-__device__ __forceinline__ void stage_chunk(const Ctx &c, uint32_t base, uint32_t count, float2 *pos, float4 *F,
-                                            float *vol, float *pvol, float *damage, uint32_t *mat, uint32_t *orig)
+// Copies the G2P inputs of the slots entries[0 .. count) (bucket entries, in
+// global or shared memory) to shared indices 0..count-1; count <= G2P_STAGE =
+// 2 * G2P_THREADS, and both entries of a thread are read before either copy
+// is issued.
+__device__ __forceinline__ void stage_chunk(const Ctx &c, const uint32_t *entries, uint32_t count, float2 *pos,
+                                            float4 *F, float *vol, float *pvol, float *damage, uint32_t *mat,
+                                            uint32_t *orig)
 {
     const uint32_t i0 = threadIdx.x, i1 = threadIdx.x + G2P_THREADS;
-    const uint32_t s0 = i0 < count ? c.perm[base + i0] : 0u;
-    const uint32_t s1 = i1 < count ? c.perm[base + i1] : 0u;
+    const uint32_t s0 = i0 < count ? entries[i0] : 0u;
+    const uint32_t s1 = i1 < count ? entries[i1] : 0u;
     if (i0 < count) stage_particle(c, s0, i0, pos, F, vol, pvol, damage, mat, orig);
     if (i1 < count) stage_particle(c, s1, i1, pos, F, vol, pvol, damage, mat, orig);
 }
@@ -1938,6 +1962,10 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
     __shared__ uint32_t s_tile[2];
     __shared__ uint2 s_range[2];
     __shared__ uint2 s_infos[2][9];
+    // with one scene: the next tile's first G2P_STAGE bucket entries and the
+    // scene's status words, copied in while this tile's particles move
+    __shared__ uint32_t s_perm[2][G2P_STAGE];
+    __shared__ __align__(16) uint32_t s_status[2][4];
     __shared__ float2 s_vol[VOL_X * VOL_Y];
     __shared__ float2 s_vs[RING_NODES];
     __shared__ float4 s_vw[RING_NODES];
@@ -1963,9 +1991,23 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
         // (the copies read here landed, and were made visible by a barrier,
         // during the previous tile)
         const uint32_t tile = fetched ? s_tile[buf] : c0.active_tiles[item];
+        const uint32_t nb = buf ^ 1u;
         const Ctx c = tile_ctx<SCENES>(c0, tile);
         const StepParams &P = *c.P;
         const uint32_t stamp = c.counters[COUNTER_STAMP];
+        // the next tile's first bucket entries and the status words, copied in
+        // during this tile (it has no particle phase when its scene failed)
+        auto prefetch_next = [&]() {
+            if constexpr (!SCENES) {
+                if (item + gridDim.x < n_active) {
+                    const uint2 nr = s_range[nb];
+                    const uint32_t count = min(nr.y, (uint32_t)G2P_STAGE);
+                    for (uint32_t i = threadIdx.x; i < count; i += G2P_THREADS)
+                        cp_async<4>(&s_perm[nb][i], &c.perm[nr.x + i]);
+                    if (threadIdx.x == G2P_THREADS - 1) cp_async<16>(&s_status[nb][0], c.status);
+                }
+            }
+        };
         const int tiles_x = (int)P.tiles_x, tiles_y = (int)P.tiles_y;
         const int node_w = (int)P.node_w, node_h = (int)P.node_h;
         const uint32_t local = tile - P.tile_base;
@@ -1973,6 +2015,7 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
         const int x0 = tx * TILE_X, y0 = ty * TILE_Y;
         const uint2 range = fetched ? s_range[buf] : c.tile_range[tile];
         const uint32_t begin = range.x, end = range.x + range.y;
+        if (fetched) cp_async_wait_all();  // this tile's entries and status words (visible after the barrier)
         __syncthreads();  // readers of the previous tile's shared data are done
         if (!fetched && threadIdx.x < 9) {
             const int sx = tx + (int)(threadIdx.x % 3) - 1, sy = ty + (int)(threadIdx.x / 3) - 1;
@@ -1980,16 +2023,18 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
                                     ? c.tile_info[P.tile_base + (uint32_t)(sy * tiles_x + sx)]
                                     : make_uint2(0xffffffffu, 0u);
         }
-        if (threadIdx.x == 0) s_fail = *(volatile uint32_t *)c.status != 0u ? 2 : 0;
+        // the status as the previous tile copied it in (a scene that failed
+        // since then has this tile computed for nothing: its substep is
+        // rolled back either way)
+        if (threadIdx.x == 0) s_fail = (fetched ? s_status[buf][0] : *(volatile uint32_t *)c.status) != 0u ? 2 : 0;
         // the first chunk of particles, copied in while the node phase runs
-        stage_chunk(c, begin, min(end - begin, (uint32_t)G2P_STAGE), p_pos, p_F, p_vol, p_pvol, p_damage, p_mat,
-                    p_orig);
+        stage_chunk(c, fetched ? s_perm[buf] : c.perm + begin, min(end - begin, (uint32_t)G2P_STAGE), p_pos, p_F,
+                    p_vol, p_pvol, p_damage, p_mat, p_orig);
         __syncthreads();
         if constexpr (!SCENES) {
             // the next tile's range and neighbour records (its index came in
             // during the previous tile) and the index of the tile after it;
             // every copy has landed by this tile's cp.async waits
-            const uint32_t nb = buf ^ 1u;
             if (item + gridDim.x < n_active && threadIdx.x < 10) {
                 const uint32_t tn = s_tile[nb];
                 if (threadIdx.x == 9) {
@@ -2010,6 +2055,7 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
         if (s_fail) {
             cp_async_wait_all();  // no copy may land after this tile's shared data is reused
             __syncthreads();      // and the copies are visible to the next tile
+            prefetch_next();
             continue;             // the scene's substep is rolled back
         }
         // node phase: thread t takes node (x0 - 1 + t % VOL_X, y0 - 1 + t / VOL_X)
@@ -2024,9 +2070,12 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
         float sum[ACC_WORDS];
 #pragma unroll
         for (int k = 0; k < ACC_WORDS; ++k) sum[k] = 0.f;
+        uint32_t channels = 0u;  // the channels any neighbour record of this substep holds
+#pragma unroll
+        for (int k = 0; k < 9; ++k) channels |= info[k].x == stamp ? info[k].y : 0u;
         if (in_grid) {
             const NodeSources ns = node_sources(P, info, tx, ty, hx, hy, stamp);
-            add_sources(c, ns, ring_node, sum);
+            add_sources(c, ns, ring_node, channels, sum);
         }
         if (in_region) s_vol[t] = make_float2(sum[6], sum[10]);
         __syncthreads();
@@ -2073,6 +2122,7 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
         }
         cp_async_wait_all();
         __syncthreads();
+        prefetch_next();
         if (s_fail) continue;
         for (uint32_t base = begin; base < end; base += G2P_THREADS) {
             const uint32_t p = base + threadIdx.x;
@@ -2080,8 +2130,8 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
             if (base != begin && chunk == 0u) {
                 // next chunk of a crowded tile
                 __syncthreads();
-                stage_chunk(c, base, min(end - base, (uint32_t)G2P_STAGE), p_pos, p_F, p_vol, p_pvol, p_damage,
-                            p_mat, p_orig);
+                stage_chunk(c, c.perm + base, min(end - base, (uint32_t)G2P_STAGE), p_pos, p_F, p_vol, p_pvol,
+                            p_damage, p_mat, p_orig);
                 cp_async_wait_all();
                 __syncthreads();
             }
@@ -2158,20 +2208,47 @@ __global__ void k_end_batch(Ctx c0, uint32_t total, uint32_t measure_speed)
             c0.slot_out[c0.tracked[k]] = c0.slot_in[c0.tracked[k]];
     }
     const bool one_scene = c0.n_scenes == 1u;
-    const bool restore_one = one_scene && ((batch_stop(c0, total) ^ total) & 1u) != 0u;
     if (one_scene) {
+        // the batch's outcome, read once per CTA
+        __shared__ int s_restore;
+        if (threadIdx.x == 0) s_restore = ((batch_stop(c0, total) ^ total) & 1u) != 0u ? 1 : 0;
+        __syncthreads();
+        const bool restore_one = s_restore != 0;
         float best = 0.0f;
-        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c0.n; i += gridDim.x * blockDim.x) {
-            if (restore_one) copy_particle(c0, i, i);
+        // END_BATCH_ITEMS particles per thread and pass, their loads in flight together
+        const uint32_t stride = gridDim.x * blockDim.x;
+        for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < c0.n; i0 += END_BATCH_ITEMS * stride) {
+            float2 v[END_BATCH_ITEMS];
+#pragma unroll
+            for (int u = 0; u < END_BATCH_ITEMS; ++u) {
+                const uint32_t i = i0 + (uint32_t)u * stride;
+                v[u] = make_float2(0.f, 0.f);
+                if (i < c0.n) {
+                    if (restore_one) copy_particle(c0, i, i);
+                    if (measure_speed) v[u] = restore_one ? c0.in.vel[i] : c0.out.vel[i];
+                }
+            }
             if (measure_speed) {
-                const float sp = length2(restore_one ? c0.in.vel[i] : c0.out.vel[i]);
-                best = fmaxf(best, finite_f(sp) ? sp : FLOAT_MAX);
+#pragma unroll
+                for (int u = 0; u < END_BATCH_ITEMS; ++u) {
+                    const float sp = length2(v[u]);
+                    best = fmaxf(best, finite_f(sp) ? sp : FLOAT_MAX);
+                }
             }
         }
         if (!measure_speed) return;
+        // one atomic per CTA: every warp of the grid on one word serialises in L2
+        __shared__ float s_best[32];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
-        if ((threadIdx.x & 31) == 0) atomicMax(c0.counters + COUNTER_MAX_SPEED, __float_as_uint(best));
+        if ((threadIdx.x & 31) == 0) s_best[threadIdx.x >> 5] = best;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            best = threadIdx.x < (blockDim.x >> 5) ? s_best[threadIdx.x] : 0.0f;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
+            if (threadIdx.x == 0) atomicMax(c0.counters + COUNTER_MAX_SPEED, __float_as_uint(best));
+        }
         return;
     }
     for (uint32_t base = blockIdx.x * blockDim.x; base < c0.n; base += gridDim.x * blockDim.x) {

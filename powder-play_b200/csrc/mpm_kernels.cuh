@@ -143,6 +143,8 @@ constexpr int BODY_THREADS = 64;              // k_body_impulses: one CTA per bo
 constexpr uint32_t PAIR_CACHE_BODIES = 2048;  // bodies up to which pair contacts are cached
 constexpr int BONDED_TRIANGLE_SOLVER_ITERATIONS = 2;
 constexpr int G2P_STAGE = 2 * G2P_THREADS;  // particles of a tile staged at once
+constexpr int END_BATCH_THREADS = 256;      // k_end_batch: threads per CTA and
+constexpr int END_BATCH_ITEMS = 4;          // particles per thread and pass
 static_assert(VOL_X * VOL_Y <= G2P_THREADS && RING_NODES <= G2P_THREADS, "one node per thread");
 
 // device counters beyond the three of mpm_device.cuh

@@ -355,8 +355,9 @@ void enqueue_substep(mpm_solver *s, int parity)
 void enqueue_end_batch(mpm_solver *s, int parity, uint32_t total, bool measure_speed)
 {
     const Ctx c = make_ctx(s, 1 - parity);  // out: the buffer the batch ends in
-    k_end_batch<<<std::min(blocks_for(s->n, PARTICLE_THREADS), 1184u), PARTICLE_THREADS, 0, s->stream>>>(
-        c, total, measure_speed ? 1u : 0u);
+    const unsigned ctas = s->n_scenes == 1 ? blocks_for(s->n, END_BATCH_THREADS * END_BATCH_ITEMS)
+                                           : std::min(blocks_for(s->n, END_BATCH_THREADS), 1184u);
+    k_end_batch<<<ctas, END_BATCH_THREADS, 0, s->stream>>>(c, total, measure_speed ? 1u : 0u);
     mark(K_END_BATCH);
 }
 
@@ -484,6 +485,12 @@ uint32_t intern_material(std::vector<Material> &table, const float *w)
     m.mu = w[15];
     m.density = w[16];
     m.param = m.model == MODEL_NEO_HOOKEAN ? 0.0f : w[18];
+    // the quotient the CFL wave-speed bound would divide out per particle
+    // (both IEEE float32 divisions: the same bits)
+    const bool liquid = m.model == MODEL_WATER || m.model == MODEL_OIL;
+    m.c2 = liquid && std::isfinite(m.lambda) && std::isfinite(m.density) && m.lambda > 0.0f && m.density > 0.0f
+               ? m.lambda / m.density
+               : 0.0f;
     for (size_t k = 0; k < table.size(); ++k) {
         const Material &t = table[k];
         if (t.model == m.model && f2u(t.lambda) == f2u(m.lambda) && f2u(t.mu) == f2u(m.mu) &&
