@@ -142,6 +142,8 @@ GATE4_DEFAULT_GRAVITY = {"x": 0.0, "y": 90.0}
 GATE4_LIQUID_PARTICLE_SPACING = 18
 GATE4_PARTICLE_AREA = 100
 GATE4_LIQUID_PARTICLE_DIAMETER = 20
+GATE4_LIQUID_PARTICLE_AREA = GATE4_LIQUID_PARTICLE_DIAMETER ** 2
+GATE4_LIQUID_BULK_MODULUS_SCALE = 4
 GATE4_SOLID_PARTICLE_MASS = 4
 GATE4_PEBBLE_COUNT = 50
 GATE4_PEBBLE_COLUMNS = 8
@@ -150,8 +152,8 @@ GATE4_PEBBLE_SPACING = 150
 GATE4_FRACTURE_COLUMNS, GATE4_FRACTURE_ROWS, GATE4_FRACTURE_SPACING = 6, 4, 20
 GATE4_FRACTURE_FAILURE_STRAIN = 0.12
 GATE4_PEBBLE_EDGE_LENGTH = GATE4_GRID["cellsX"] * GATE4_GRID["cellSize"] * 0.005 * 12
-GATE4_WATER_MATERIAL = {"lambda": 40_000 * 4, "mu": 0.0, "model": "water", "density": 0.02}
-GATE4_OIL_MATERIAL = {"lambda": 30_000 * 4, "mu": 0.0, "model": "oil", "density": 0.016}
+GATE4_WATER_MATERIAL = {"lambda": 40_000 * GATE4_LIQUID_BULK_MODULUS_SCALE, "mu": 0.0, "model": "water", "density": 0.02}
+GATE4_OIL_MATERIAL = {"lambda": 30_000 * GATE4_LIQUID_BULK_MODULUS_SCALE, "mu": 0.0, "model": "oil", "density": 0.016}
 GATE4_PEBBLE_MATERIAL = {"lambda": 20.0, "mu": 10.0, "model": "neo-hookean"}
 
 
@@ -499,8 +501,8 @@ def create_adjoint_scenes(count: int = 64, seed: int = 0x4D504D41, water_columns
 MAX_MPM_EMITTER_PARTICLES = 100_000
 _GOLDEN_ANGLE = math.pi * (3 - math.sqrt(5))
 _EMITTER_MATERIALS = {
-    "water": {"lambda": 40_000 * 4, "mu": 0.0, "model": "water", "density": 0.02},
-    "oil": {"lambda": 30_000 * 4, "mu": 0.0, "model": "oil", "density": 0.016},
+    "water": dict(GATE4_WATER_MATERIAL),
+    "oil": dict(GATE4_OIL_MATERIAL),
     "neo-hookean": {"lambda": 20.0, "mu": 10.0, "model": "neo-hookean"},
 }
 

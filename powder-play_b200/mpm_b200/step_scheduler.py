@@ -11,6 +11,9 @@ from .cfl_bounds import calculate_mpm_cfl_velocity_bound
 from .errors import RangeError
 from .layout import _is_safe_integer, fround
 
+DEFAULT_HORIZONTAL_OSCILLATION_AMPLITUDE = 240
+INITIAL_HORIZONTAL_OSCILLATION_AMPLITUDE = DEFAULT_HORIZONTAL_OSCILLATION_AMPLITUDE
+MAX_HORIZONTAL_OSCILLATION_AMPLITUDE = 360
 HORIZONTAL_OSCILLATION_FREQUENCY_HZ = 0.16
 
 

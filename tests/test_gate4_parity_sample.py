@@ -11,8 +11,9 @@ import numpy as np
 import pytest
 
 from mpm_b200 import RangeError, create_mpm_mls_gpu_solver
-from mpm_b200.scenes import (GATE4_GRID, GATE4_PARTICLE_AREA, GATE4_PEBBLE_EDGE_LENGTH, GATE4_SOLID_PARTICLE_MASS,
-                             create_mpm_cpu_parity_sample, create_mpm_gate4_scene)
+from mpm_b200.scenes import (GATE4_FIXED_STEP_SECONDS, GATE4_GRID, GATE4_LIQUID_PARTICLE_AREA, GATE4_PARTICLE_AREA,
+                             GATE4_PEBBLE_EDGE_LENGTH, GATE4_SOLID_PARTICLE_MASS, create_mpm_cpu_parity_sample,
+                             create_mpm_gate4_scene, create_mpm_gate4_step_config)
 from oracle import OracleState
 
 
@@ -32,6 +33,43 @@ def _values(state, index):
 @pytest.fixture(scope="module")
 def scene():
     return create_mpm_gate4_scene()
+
+
+def test_the_scene_is_the_shared_workload(scene):
+    """src/lib/mpm/reference/cpu-simulation.spec.ts:20-34: 50x40 water,
+    50x30 oil, 50 three-particle pebbles and a 6x4 fractured solid with its
+    horizontal, vertical and diagonal bonds; every liquid particle carries
+    the liquid area."""
+    particles, bonds, _ = scene
+    assert len(particles) == 50 * 40 + 50 * 30 + 50 * 3 + 6 * 4 == 3_674
+    assert np.count_nonzero(particles.material == 0) == 2_000  # water
+    assert np.count_nonzero(particles.material == 1) == 1_500  # oil
+    assert np.count_nonzero(particles.bonded_vertex >= 0) == 150
+    assert len(np.unique(particles.object_id[particles.bonded_vertex >= 0])) == 50
+    assert len(bonds) == 5 * 4 + 3 * 6 + 5 * 3
+    liquid = particles.material <= 1
+    assert np.all(particles.volume[liquid] == GATE4_LIQUID_PARTICLE_AREA)
+
+
+def test_stepping_carries_the_fracture_state(scene):
+    """src/lib/mpm/reference/cpu-simulation.spec.ts:93-116: a second step from
+    the first step's particles and bonds equals two steps in one run.  The
+    scene's bonds stay intact over the first steps, so one enters broken and
+    one partly damaged, and both must come out the same way."""
+    particles, bonds, _ = scene
+    bonds = [dict(bonds[0], broken=True, damage=1.0), dict(bonds[1], damage=0.3)] + list(bonds[2:])
+    config = dict(create_mpm_gate4_step_config(fracture_bonds=bonds), dt=GATE4_FIXED_STEP_SECONDS / 8)
+    stepped = OracleState(particles, config)
+    stepped.step(config)
+    stepped.step(config)
+    ran = OracleState(particles, config)
+    ran.run(config, 2)
+    assert np.array_equal(stepped.particles, ran.particles)
+    assert np.array_equal(stepped.bonds, ran.bonds)
+    assert len(stepped.bonds) == len(bonds)
+    assert stepped.bonds["broken"][0] == 1 and stepped.bonds["damage"][1] == 0.3
+    ends = [bonds[0]["firstParticle"], bonds[0]["secondParticle"]]
+    assert np.all(stepped.particles["damage"][ends] == 1.0)
 
 
 def test_sample_is_local_and_keeps_whole_triangles(scene):
