@@ -152,11 +152,32 @@ struct mpm_solver {
 
     // graphs of 2^k substeps starting from buffer parity p
     std::map<std::tuple<int, int>, cudaGraphExec_t> graphs;
+    // graphs of whole short batches: (substeps, start parity, guarded)
+    std::map<std::tuple<uint32_t, int, int>, cudaGraphExec_t> batch_graphs;
+    // the last batch's graph copied the compact readback (counters and
+    // status) to h_readback, and no call since could have changed them
+    bool readback_ready = false;
 
     bool gather() const { return cfg.p2g_mode == MPM_P2G_GATHER; }
 };
 
 namespace {
+
+// A call that may change the counters or status words: the next
+// mpm_read_compact copies them again instead of using the batch graph's copy.
+void forget_readback(mpm_solver *s)
+{
+    if (s) s->readback_ready = false;
+}
+
+// Drops every captured graph (they hold launch sizes and buffer pointers).
+void drop_graphs(mpm_solver *s)
+{
+    for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    s->graphs.clear();
+    for (auto &kv : s->batch_graphs) cudaGraphExecDestroy(kv.second);
+    s->batch_graphs.clear();
+}
 
 Ctx make_ctx(mpm_solver *s, int parity)
 {
@@ -449,29 +470,34 @@ void fill_params(mpm_solver *s, uint32_t scene, StepParams &p, float dt, float g
     }
 }
 
-// The same step for every scene.
-int upload_params(mpm_solver *s, float dt, float gx, float gy, const mpm_cfl_guard *guard, float bond_reference_dt,
-                  uint32_t steps)
+// Copies the pinned parameters to the device (a batch graph holds this copy
+// itself) and marks when the host may write them again.
+int copy_params(mpm_solver *s)
 {
-    CUDA_TRY(cudaEventSynchronize(s->params_copied));
-    for (uint32_t k = 0; k < s->n_scenes; ++k)
-        fill_params(s, k, s->h_params[k], dt, gx, gy, guard, bond_reference_dt, steps);
     CUDA_TRY(cudaMemcpyAsync(s->d_params, s->h_params, s->n_scenes * sizeof(StepParams), cudaMemcpyHostToDevice,
                              s->stream));
     CUDA_TRY(cudaEventRecord(s->params_copied, s->stream));
     return MPM_OK;
 }
 
-// A step of its own for each scene (steps[k] 0: the scene sits the batch out).
+// The same step for every scene; `copy` false leaves the copy to run_batch.
+int upload_params(mpm_solver *s, float dt, float gx, float gy, const mpm_cfl_guard *guard, float bond_reference_dt,
+                  uint32_t steps, bool copy = true)
+{
+    CUDA_TRY(cudaEventSynchronize(s->params_copied));
+    for (uint32_t k = 0; k < s->n_scenes; ++k)
+        fill_params(s, k, s->h_params[k], dt, gx, gy, guard, bond_reference_dt, steps);
+    return copy ? copy_params(s) : MPM_OK;
+}
+
+// A step of its own for each scene (steps[k] 0: the scene sits the batch
+// out); the copy is left to run_batch.
 int upload_scene_params(mpm_solver *s, const uint32_t *steps, const float *dt, const float *gx, const float *gy,
                         const mpm_cfl_guard *guards)
 {
     CUDA_TRY(cudaEventSynchronize(s->params_copied));
     for (uint32_t k = 0; k < s->n_scenes; ++k)
         fill_params(s, k, s->h_params[k], dt[k], gx[k], gy[k], guards ? guards + k : nullptr, 0.0f, steps[k]);
-    CUDA_TRY(cudaMemcpyAsync(s->d_params, s->h_params, s->n_scenes * sizeof(StepParams), cudaMemcpyHostToDevice,
-                             s->stream));
-    CUDA_TRY(cudaEventRecord(s->params_copied, s->stream));
     return MPM_OK;
 }
 
@@ -538,8 +564,7 @@ int unpack_and_upload(mpm_solver *s, const float *packed, uint32_t count, int ta
         CUDA_TRY(cudaMemcpyAsync(s->d_mats, s->mats.data(), s->mats.size() * sizeof(Material), cudaMemcpyHostToDevice,
                                  s->stream));
         // captured graphs hold the old table pointer
-        for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
-        s->graphs.clear();
+        drop_graphs(s);
     }
     ParticleBuffers &b = s->buf[target];
     const size_t d = slot_base;
@@ -608,8 +633,7 @@ void free_solver(mpm_solver *s)
     if (!s) return;
     if (s->device >= 0) cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
-    for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
-    s->graphs.clear();
+    drop_graphs(s);
     void *ptrs[] = {s->d_params, s->dyn, s->work, s->tile_scene, s->scene_p_base, s->bonded, s->obj, s->d_mats, s->keys, s->ranks,
                     s->tmp, s->perm, s->cell_count, s->cell_start, s->block_sums, s->p2g_solid, s->p2g_water,
                     s->p2g_oil, s->g_solid, s->g_water, s->g_oil, s->fixed, s->tile_stamp, s->d_active,
@@ -1020,8 +1044,7 @@ int refresh_count(mpm_solver *s)
     s->scenes[0].n = s->n;
     const uint32_t bounds[2] = {0u, s->n};
     CUDA_TRY(cudaMemcpy(s->scene_p_base, bounds, sizeof bounds, cudaMemcpyHostToDevice));
-    for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
-    s->graphs.clear();
+    drop_graphs(s);
     return MPM_OK;
 }
 
@@ -1061,7 +1084,7 @@ int mpm_step_batch(mpm_solver *s, uint32_t step_count, float dt, float gx, float
     if (!(dt > 0.0f) || !std::isfinite(dt)) return set_error(MPM_ERR_INVALID_ARGUMENT, "dt must be greater than zero");
     if (!std::isfinite(gx) || !std::isfinite(gy)) return set_error(MPM_ERR_INVALID_ARGUMENT, "gravity must be finite");
     CUDA_TRY(cudaSetDevice(s->device));
-    int rc = upload_params(s, dt, gx, gy, guard, bond_reference_dt, step_count);
+    int rc = upload_params(s, dt, gx, gy, guard, bond_reference_dt, step_count, false);
     if (rc != MPM_OK) return rc;
     return run_batch(s, step_count, guard != nullptr);
 }
@@ -1127,11 +1150,84 @@ uint32_t mpmb_scene_count(const mpm_solver *s) { return s ? s->n_scenes : 0u; }
 
 namespace {
 
+// Batches of at most this many substeps of a single scene run as one graph
+// (see capture_batch); longer ones launch graphs of 2^k substeps.
+constexpr uint32_t MAX_BATCH_GRAPH_STEPS = 16;
+
+// The whole batch on the stream being captured: the parameter copy from
+// pinned memory, the batch events, the prologue, the substeps, the epilogue
+// and the compact readback (counters and status words) to pinned memory.
+// Returns the first error; the caller ends the capture either way.
+cudaError_t capture_batch(mpm_solver *s, uint32_t step_count, int parity, bool guarded)
+{
+    cudaError_t e = cudaMemcpyAsync(s->d_params, s->h_params, s->n_scenes * sizeof(StepParams),
+                                    cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(s->batch_start, s->stream, cudaEventRecordExternal);
+    if (e != cudaSuccess) return e;
+    const Ctx c0 = make_ctx(s, parity);
+    k_begin_batch<<<blocks_for(s->n_scenes, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c0, guarded ? 1u : 0u);
+    if (s->gather()) enqueue_tile_count(s, c0);
+    int p = parity;
+    for (uint32_t k = 0; k < step_count; ++k) {
+        enqueue_substep(s, p);
+        p = 1 - p;
+    }
+    enqueue_end_batch(s, p, step_count, guarded);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(s->batch_stop, s->stream, cudaEventRecordExternal);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->h_readback, s->d_counters + COUNTER_PROGRESS, 2 * sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->h_readback + 2, s->d_status, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream);
+    return e;
+}
+
+int get_batch_graph(mpm_solver *s, uint32_t step_count, int parity, bool guarded, cudaGraphExec_t *out)
+{
+    const auto key = std::make_tuple(step_count, parity, guarded ? 1 : 0);
+    auto it = s->batch_graphs.find(key);
+    if (it != s->batch_graphs.end()) {
+        *out = it->second;
+        return MPM_OK;
+    }
+    CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    const cudaError_t body = capture_batch(s, step_count, parity, guarded);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t end = cudaStreamEndCapture(s->stream, &graph);
+    cudaError_t err = body != cudaSuccess ? body : end;
+    cudaGraphExec_t exec = nullptr;
+    if (err == cudaSuccess) err = cudaGraphInstantiate(&exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (err != cudaSuccess) return set_error(MPM_ERR_CUDA, "batch graph capture failed: %s", cudaGetErrorString(err));
+    s->batch_graphs[key] = exec;
+    *out = exec;
+    return MPM_OK;
+}
+
 // Submits one batch of `step_count` substeps (the most any scene takes) with
-// the parameters already uploaded; `guarded`: a CFL guard is on.
+// the parameters filled in h_params; `guarded`: a CFL guard is on.  A short
+// batch of one scene is a single graph launch (the host call is then one
+// launch and one event record); otherwise the parameters are copied, then
+// the prologue, graphs of 2^k substeps and the epilogue are launched.
 int run_batch(mpm_solver *s, uint32_t step_count, bool guarded)
 {
     int rc = MPM_OK;
+    s->readback_ready = false;
+    if (s->n_scenes == 1 && s->n > 0 && step_count <= MAX_BATCH_GRAPH_STEPS) {
+        cudaGraphExec_t exec;
+        rc = get_batch_graph(s, step_count, s->cur, guarded, &exec);
+        if (rc != MPM_OK) return rc;
+        CUDA_TRY(cudaGraphLaunch(exec, s->stream));
+        CUDA_TRY(cudaEventRecord(s->params_copied, s->stream));
+        if (step_count & 1u) s->cur = 1 - s->cur;
+        s->substeps_since_begin = step_count;
+        s->batch_timed = true;
+        s->readback_ready = true;
+        return MPM_OK;
+    }
+    rc = copy_params(s);
+    if (rc != MPM_OK) return rc;
     const Ctx c0 = make_ctx(s, s->cur);
     CUDA_TRY(cudaEventRecord(s->batch_start, s->stream));
     k_begin_batch<<<blocks_for(s->n_scenes, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c0, guarded ? 1u : 0u);
@@ -1182,6 +1278,7 @@ int mpm_profile_substeps(mpm_solver *s, uint32_t step_count, float dt, float gx,
                          const mpm_cfl_guard *guard, double *kernel_ms, uint32_t *kernel_launches)
 {
     g_last_error.clear();
+    forget_readback(s);
     if (!s || !kernel_ms || !kernel_launches)
         return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and outputs must not be NULL");
     if (step_count < 1) return set_error(MPM_ERR_INVALID_ARGUMENT, "stepCount must be a positive safe integer.");
@@ -1194,12 +1291,12 @@ int mpm_profile_substeps(mpm_solver *s, uint32_t step_count, float dt, float gx,
 int mpm_set_launch_shape(mpm_solver *s, uint32_t p2g_ctas, uint32_t g2p_ctas)
 {
     g_last_error.clear();
+    forget_readback(s);
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
     if (!s->gather()) return set_error(MPM_ERR_STATE, "launch shapes apply to the default P2G path");
     if (p2g_ctas) s->p2g_ctas = p2g_ctas;
     if (g2p_ctas) s->g2p_ctas = g2p_ctas;
-    for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
-    s->graphs.clear();
+    drop_graphs(s);
     return MPM_OK;
 }
 
@@ -1218,6 +1315,7 @@ int mpm_get_launch_shape(mpm_solver *s, uint32_t *p2g_ctas, uint32_t *g2p_ctas, 
 int mpm_autotune(mpm_solver *s, uint32_t substeps, uint32_t *p2g_ctas, uint32_t *g2p_ctas, double *best_ms)
 {
     g_last_error.clear();
+    forget_readback(s);
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
     if (!s->gather()) return set_error(MPM_ERR_STATE, "launch shapes apply to the default P2G path");
     if (!s->batch_timed) return set_error(MPM_ERR_STATE, "tune after a first batch (its parameters are reused)");
@@ -1323,8 +1421,7 @@ int mpm_autotune(mpm_solver *s, uint32_t substeps, uint32_t *p2g_ctas, uint32_t 
         if (p) cudaFree(p);
     s->p2g_ctas = rc == MPM_OK ? best_p : p0;
     s->g2p_ctas = rc == MPM_OK ? best_g : g0;
-    for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
-    s->graphs.clear();
+    drop_graphs(s);
     s->batch_timed = false;  // the batch events now time the trials
     if (rc != MPM_OK) return rc;
     if (p2g_ctas) *p2g_ctas = best_p;
@@ -1340,6 +1437,7 @@ uint32_t mpm_profile_kernel_slots(void) { return K_SLOTS; }
 int mpm_count_active_nodes(mpm_solver *s, uint32_t counts[3])
 {
     g_last_error.clear();
+    forget_readback(s);
     if (!s || !counts) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and counts must not be NULL");
     CUDA_TRY(cudaSetDevice(s->device));
     if (s->gather()) {
@@ -1374,9 +1472,12 @@ int mpm_read_compact(mpm_solver *s, float *maximum_speed, uint32_t *completed, u
     g_last_error.clear();
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
     CUDA_TRY(cudaSetDevice(s->device));
-    CUDA_TRY(cudaMemcpyAsync(s->h_readback, s->d_counters + COUNTER_PROGRESS, 2 * sizeof(uint32_t),
-                             cudaMemcpyDeviceToHost, s->stream));
-    CUDA_TRY(cudaMemcpyAsync(s->h_readback + 2, s->d_status, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    if (!s->readback_ready) {
+        CUDA_TRY(cudaMemcpyAsync(s->h_readback, s->d_counters + COUNTER_PROGRESS, 2 * sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(s->h_readback + 2, s->d_status, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                 s->stream));
+    }
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     if (completed) *completed = s->h_readback[0];
     if (maximum_speed) *maximum_speed = u2f(s->h_readback[1]);
@@ -1392,6 +1493,7 @@ int mpm_read_status(mpm_solver *s, uint32_t status[8])
 int mpm_clear_status(mpm_solver *s)
 {
     g_last_error.clear();
+    forget_readback(s);
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
     CUDA_TRY(cudaSetDevice(s->device));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
@@ -1468,6 +1570,7 @@ int mpm_read_particles(mpm_solver *s, const uint32_t *indices, uint32_t count, f
 int mpm_write_particles(mpm_solver *s, const float *packed, uint32_t count)
 {
     g_last_error.clear();
+    forget_readback(s);
     if (!s || !packed) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and packed_particles must not be NULL");
     if (count != s->n) return set_error(MPM_ERR_INVALID_ARGUMENT, "count must equal the particle count");
     if (s->allocated != s->n) return set_error(MPM_ERR_STATE, "particles were removed; the state cannot be overwritten");
@@ -1478,6 +1581,7 @@ int mpm_write_particles(mpm_solver *s, const float *packed, uint32_t count)
 int mpm_set_drag(mpm_solver *s, const mpm_drag *drag)
 {
     g_last_error.clear();
+    forget_readback(s);
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
     if (drag) {
         if (!(drag->radius > 0.0f) || !std::isfinite(drag->radius))
@@ -1493,6 +1597,7 @@ int mpm_set_drag(mpm_solver *s, const mpm_drag *drag)
 int mpm_queue_completion_ms(mpm_solver *s, double *ms)
 {
     g_last_error.clear();
+    forget_readback(s);
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
     CUDA_TRY(cudaSetDevice(s->device));
     cudaEvent_t a, b;
@@ -1513,6 +1618,7 @@ int mpm_append_particles(mpm_solver *s, const float *packed, const uint32_t *obj
                          uint32_t *first_index)
 {
     g_last_error.clear();
+    forget_readback(s);
     if (!s || (count > 0 && (!packed || !object_ids)))
         return set_error(MPM_ERR_INVALID_ARGUMENT, "solver, packed_particles and object_ids must not be NULL");
     if (s->n_scenes > 1) return set_error(MPM_ERR_STATE, "particles are appended to a single-scene solver");
@@ -1538,6 +1644,7 @@ int mpm_remove_particles_in_outlet(mpm_solver *s, float min_x, float min_y, floa
                                    uint32_t *removed_count)
 {
     g_last_error.clear();
+    forget_readback(s);
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
     if (s->n_scenes > 1) return set_error(MPM_ERR_STATE, "outlets act on a single-scene solver");
     if (!(min_x <= max_x) || !(min_y <= max_y))
@@ -1617,6 +1724,7 @@ int mpm_pick(mpm_solver *s, float x, float y, float radius, uint32_t *particle_i
              uint32_t *object_id)
 {
     g_last_error.clear();
+    forget_readback(s);
     if (!s || !particle_index) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and particle_index must not be NULL");
     if (s->n_scenes > 1) return set_error(MPM_ERR_STATE, "picking acts on a single-scene solver");
     if (!(radius >= 0.0f) || !std::isfinite(radius))
@@ -1654,6 +1762,7 @@ int mpm_pick(mpm_solver *s, float x, float y, float radius, uint32_t *particle_i
 int mpm_gather_surface_occupancy(mpm_solver *s, float *field_out, uint32_t *surface_flags_out)
 {
     g_last_error.clear();
+    forget_readback(s);
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
     if (s->n_scenes > 1) return set_error(MPM_ERR_STATE, "the surface field belongs to a single-scene solver");
     CUDA_TRY(cudaSetDevice(s->device));
@@ -1685,6 +1794,7 @@ int mpm_gather_surface_occupancy(mpm_solver *s, float *field_out, uint32_t *surf
 int mpm_surface_field_device(mpm_solver *s, const float **device_field, uint32_t *node_w, uint32_t *node_h)
 {
     g_last_error.clear();
+    forget_readback(s);
     if (!s || !device_field) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and device_field must not be NULL");
     if (!s->surface_field) return set_error(MPM_ERR_STATE, "no surface field has been gathered");
     *device_field = reinterpret_cast<const float *>(s->surface_field);
@@ -1697,6 +1807,7 @@ int mpm_clone_range(mpm_solver *s, uint32_t start, uint32_t count, float offset_
                     uint32_t object_id, uint32_t *first_index)
 {
     g_last_error.clear();
+    forget_readback(s);
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
     if (s->n_scenes > 1) return set_error(MPM_ERR_STATE, "cloning acts on a single-scene solver");
     if (!std::isfinite(offset_x) || !std::isfinite(offset_y))
@@ -1736,6 +1847,7 @@ const char *mpm_last_error(void) { return g_last_error.c_str(); }
 int mpm_probe_sort(mpm_solver *s, float dt, uint32_t *keys_out, uint32_t *perm_out, uint32_t *cell_start_out)
 {
     g_last_error.clear();
+    forget_readback(s);
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
     if (!s->gather()) return set_error(MPM_ERR_STATE, "the cell sort runs in gather mode only");
     if (s->n_scenes > 1) return set_error(MPM_ERR_STATE, "the sort probe takes a single-scene solver");
@@ -1768,6 +1880,7 @@ int mpm_probe_sort(mpm_solver *s, float dt, uint32_t *keys_out, uint32_t *perm_o
 int mpm_probe_triangle_field(mpm_solver *s, float dt, float *field_out)
 {
     g_last_error.clear();
+    forget_readback(s);
     if (!s || !field_out) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and field_out must not be NULL");
     if (!s->field) return set_error(MPM_ERR_STATE, "the scene has no bonded triangle bodies");
     CUDA_TRY(cudaSetDevice(s->device));
@@ -1832,6 +1945,7 @@ int mpm_probe_deformation(int device, const float *F, const float *C, uint32_t c
 int mpm_probe_fixed_point(mpm_solver *s, float dt, int32_t *words_out, float *affine_out)
 {
     g_last_error.clear();
+    forget_readback(s);
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
     if (s->cfg.p2g_mode != MPM_P2G_FIXED_POINT) return set_error(MPM_ERR_STATE, "the solver was not created in fixed-point mode");
     CUDA_TRY(cudaSetDevice(s->device));
