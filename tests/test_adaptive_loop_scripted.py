@@ -402,3 +402,43 @@ def test_batched_continuation_after_a_retry(fake):
     assert out[0]["attemptedMicroStepCount"] == 3 + 2 + steps[2][0]
     assert solver.cfl_bounds[0]["waveSpeedBound"] == 25 * 1.25
     assert out[1]["committedMicroStepCount"] == 1 and out[1]["retryCount"] == 0
+
+
+# ------------------------------------------ recovery policy (non-default) --
+
+def test_a_larger_recovery_factor_raises_the_retry_bounds_by_it(fake):
+    # the reference fixes the factor at 1.25 (solver.ts:73); the host mirror
+    # lets a caller study others: a CFL rejection at speed 50 and wave speed
+    # 30 retries at 2x both
+    lib = fake([cfl_violation(50.0, 0, wave=30.0), snapshot(50.0, 2)])
+    solver = create_mpm_mls_gpu_solver([PARTICLE], CONFIG, BOUNDS)
+    solver.recovery_bound_factor = 2.0
+    m = solver.step_cfl_batch_adaptive(1, 0.001, plan_for(solver, 1, 8), 1, 8, GRAVITY)
+    assert solver.cfl_bounds["waveSpeedBound"] == 60.0
+    assert m["recommendedVelocityBound"] == 100.0 and m["retryCount"] == 1
+    # the retry's guard certifies the raised velocity bound
+    assert lib.batches[1][2][0] >= 100.0
+
+
+def test_batched_recovery_factor_applies_to_the_failed_scene_only(fake):
+    script = [[snapshot(0.5, 1), cfl_violation(50.0, 0)],
+              [snapshot(0.0, 0), snapshot(50.0, 2)]]
+    lib, solver = _batched(fake, script)
+    solver.recovery_bound_factor = 1.5
+    out = solver.step_cfl_batch_adaptive(0.001, [1, 1], 8, GRAVITY)
+    assert out[1]["recommendedVelocityBound"] == 75.0
+    assert solver.cfl_bounds[1]["waveSpeedBound"] == 25 * 1.5 and solver.cfl_bounds[0]["waveSpeedBound"] == 25
+    assert lib.batches[1][0] == [0, 2]
+
+
+def test_a_planning_margin_plans_more_microsteps():
+    # bench.py's batched policy: each scene's planned velocity bound times
+    # the margin (1.0 is the reference's policy)
+    import bench
+    base = bench._batched_bound(3.0, 1 / 240, {"x": 0.0, "y": -9.81})
+    for margin in (1.0, 1.1, 1.25):
+        plans = [calculate_mpm_cfl_microsteps(1 / 240, 0.2 / 256, 3.0, base * m, 4096)["stepCount"]
+                 for m in (1.0, margin)]
+        assert plans[1] >= plans[0]
+    assert (calculate_mpm_cfl_microsteps(1 / 240, 0.2 / 256, 3.0, base * 1.25, 4096)["stepCount"]
+            > calculate_mpm_cfl_microsteps(1 / 240, 0.2 / 256, 3.0, base, 4096)["stepCount"])

@@ -166,6 +166,46 @@ def test_adaptive_macrosteps_commit_each_scene_its_own_plan():
         batch.dispose()
 
 
+def _run_policy(scenes, factor, margin, macrosteps=3):
+    """The adaptive loop under a recovery factor and a planning margin (the
+    bench's policy study): returns the results of each macrostep and the
+    final particles of each scene."""
+    from bench import _batched_bound
+    batch = create_mpm_batched_gpu_solver(scenes)
+    try:
+        batch.recovery_bound_factor = factor
+        velocity = [batch.cfl_bounds[k]["velocityBound"] for k in range(batch.scene_count)]
+        history = []
+        for _ in range(macrosteps):
+            bounds = [_batched_bound(v, 1 / 240, BATCHED_TANK_GRAVITY) * margin for v in velocity]
+            results = batch.step_cfl_batch_adaptive(1 / 240, bounds, 4096, BATCHED_TANK_GRAVITY)
+            velocity = [r["recommendedVelocityBound"] for r in results]
+            history.append(results)
+        return history, [batch.read_particles_packed(k)[0] for k in range(batch.scene_count)]
+    finally:
+        batch.dispose()
+
+
+@pytest.mark.parametrize("factor,margin", [(1.5, 1.0), (2.0, 1.0), (1.25, 1.25)])
+def test_a_recovery_policy_commits_every_macrostep(factor, margin):
+    scenes = _small_scenes(8, seed=3)
+    history, finals = _run_policy(scenes, factor, margin)
+    reference_history, _ = _run_policy(scenes, 1.25, 1.0)
+    for results in history:
+        assert all(r["remainingDuration"] == 0.0 and r["committedMicroStepCount"] >= 1 for r in results)
+    for (particles, config), got in zip(scenes, finals):
+        size = config["grid"]["cellsX"] * config["grid"]["cellSize"]
+        assert np.isfinite(got[:, STATE_WORDS]).all()
+        assert (got[:, 0:2] >= 0).all() and (got[:, 0:2] <= size).all()
+        assert got[:, 1].mean() < particles.py.mean()
+    # the first macrostep starts from the same state: a scene without a retry
+    # in either run plans at least as many microsteps under a margin
+    for r, q in zip(history[0], reference_history[0]):
+        if r["retryCount"] == 0 and q["retryCount"] == 0:
+            assert (r["committedMicroStepCount"] >= q["committedMicroStepCount"]) if margin > 1.0 else \
+                (r["committedMicroStepCount"] == q["committedMicroStepCount"])
+
+
 def test_a_batch_of_one_scene_matches_the_plain_solver():
     (particles, config), = _small_scenes(1, seed=5)
     batch = create_mpm_batched_gpu_solver([(particles, config)])
