@@ -148,6 +148,9 @@ struct mpm_solver {
 
     cudaEvent_t batch_start = nullptr, batch_stop = nullptr;
     bool batch_timed = false;
+    // the last batch's device milliseconds, once a readback waited for it
+    float batch_ms = 0.0f;
+    bool batch_ms_known = false;
     uint32_t *d_active = nullptr;
 
     // graphs of 2^k substeps starting from buffer parity p
@@ -1214,6 +1217,7 @@ int run_batch(mpm_solver *s, uint32_t step_count, bool guarded)
 {
     int rc = MPM_OK;
     s->readback_ready = false;
+    s->batch_ms_known = false;
     if (s->n_scenes == 1 && s->n > 0 && step_count <= MAX_BATCH_GRAPH_STEPS) {
         cudaGraphExec_t exec;
         rc = get_batch_graph(s, step_count, s->cur, guarded, &exec);
@@ -1266,11 +1270,13 @@ int mpm_last_batch_device_ms(mpm_solver *s, double *milliseconds)
     g_last_error.clear();
     if (!s || !milliseconds) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and milliseconds must not be NULL");
     if (!s->batch_timed) return set_error(MPM_ERR_STATE, "no batch has been submitted");
-    CUDA_TRY(cudaSetDevice(s->device));
-    CUDA_TRY(cudaEventSynchronize(s->batch_stop));
-    float ms = 0.0f;
-    CUDA_TRY(cudaEventElapsedTime(&ms, s->batch_start, s->batch_stop));
-    *milliseconds = ms;
+    if (!s->batch_ms_known) {
+        CUDA_TRY(cudaSetDevice(s->device));
+        CUDA_TRY(cudaEventSynchronize(s->batch_stop));
+        CUDA_TRY(cudaEventElapsedTime(&s->batch_ms, s->batch_start, s->batch_stop));
+        s->batch_ms_known = true;
+    }
+    *milliseconds = s->batch_ms;
     return MPM_OK;
 }
 
@@ -1479,6 +1485,11 @@ int mpm_read_compact(mpm_solver *s, float *maximum_speed, uint32_t *completed, u
                                  s->stream));
     }
     CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (s->batch_timed && !s->batch_ms_known) {
+        // the batch has ended: its time is read now, for mpm_last_batch_device_ms
+        CUDA_TRY(cudaEventElapsedTime(&s->batch_ms, s->batch_start, s->batch_stop));
+        s->batch_ms_known = true;
+    }
     if (completed) *completed = s->h_readback[0];
     if (maximum_speed) *maximum_speed = u2f(s->h_readback[1]);
     if (status) std::memcpy(status, s->h_readback + 2, 8 * sizeof(uint32_t));

@@ -211,8 +211,29 @@ def round_up_float32(value: float) -> float:
     return rounded
 
 
+_LIMIT_CACHE: dict = {}
+
+
 def calculate_mpm_cfl_velocity_limit(cellSize, waveSpeedBound, microDt, courantLimit=DEFAULT_MPM_COURANT_LIMIT):
-    """calculateMpmCflVelocityLimit, cfl.ts:234-273."""
+    """calculateMpmCflVelocityLimit, cfl.ts:234-273.  A pure function of its
+    arguments, remembered like the microstep plans (the solver certifies
+    every submitted plan with it)."""
+    args = (cellSize, waveSpeedBound, microDt, courantLimit)
+    try:
+        key = tuple((type(a), a) for a in args)
+        limit = _LIMIT_CACHE.get(key)
+    except TypeError:  # an unhashable argument: no caching
+        key, limit = None, None
+    if limit is None:
+        limit = _calculate_mpm_cfl_velocity_limit(*args)
+        if key is not None:
+            if len(_LIMIT_CACHE) >= _PLAN_CACHE_LIMIT:
+                _LIMIT_CACHE.clear()
+            _LIMIT_CACHE[key] = limit
+    return limit
+
+
+def _calculate_mpm_cfl_velocity_limit(cellSize, waveSpeedBound, microDt, courantLimit=DEFAULT_MPM_COURANT_LIMIT):
     if courantLimit is None:
         courantLimit = DEFAULT_MPM_COURANT_LIMIT
     cell, wave, micro, courant = map(_num, (cellSize, waveSpeedBound, microDt, courantLimit))

@@ -232,7 +232,12 @@ class MpmMlsGpuSolver:
         expected = calculate_mpm_cfl_microsteps(macro_dt, cell, b["waveSpeedBound"], velocity_bound, max_microsteps,
                                                 courantLimit=b.get("courantLimit"))
         certified = None
-        if (isinstance(microstep_plan, dict) and _is_safe_integer(microstep_plan.get("stepCount"))
+        if isinstance(microstep_plan, dict) and microstep_plan.get("stepCount") == expected["stepCount"] \
+                and _is_safe_integer(microstep_plan["stepCount"]):
+            # the plan at the required count: the refinement with that minimum
+            # is the required plan itself
+            certified = expected
+        elif (isinstance(microstep_plan, dict) and _is_safe_integer(microstep_plan.get("stepCount"))
                 and microstep_plan["stepCount"] >= expected["stepCount"]):
             certified = calculate_mpm_cfl_microsteps(macro_dt, cell, b["waveSpeedBound"], velocity_bound,
                                                      max_microsteps, minimumStepCount=microstep_plan["stepCount"],
