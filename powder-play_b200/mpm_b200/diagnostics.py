@@ -32,3 +32,23 @@ def summarize_si_water(packed: np.ndarray, reference_area: float) -> dict:
     return {"areaRatio": area / reference_area, "areaDriftPercent": 100.0 * (area / reference_area - 1.0),
             "determinantMin": float(det.min()), "determinantMax": float(det.max()),
             "densityErrorPercentP95": p95, "maximumSpeed": float(np.max(np.hypot(vel[:, 0], vel[:, 1])))}
+
+
+def summarize_dam_break_phase(packed: np.ndarray) -> dict:
+    """Bulk state of one liquid of the two-phase dam break from its packed
+    records: centre of mass and spread, mean specific kinetic energy, maximum
+    speed, the runout front (99.9th percentile of x), the free surface (0.1st
+    percentile of y, gravity +y) and the 5th / 95th percentiles of det F."""
+    if packed.shape[0] == 0:
+        raise RangeError("Dam-break diagnostics require particles.")
+    p = packed.astype(np.float64)
+    x, y, vx, vy = p[:, 0], p[:, 1], p[:, 2], p[:, 3]
+    F = p[:, 8:12]
+    det = F[:, 0] * F[:, 3] - F[:, 1] * F[:, 2]
+    if not np.all(np.isfinite(p[:, 0:12])):
+        raise RuntimeError("Non-finite state in dam-break diagnostics.")
+    speed2 = vx * vx + vy * vy
+    return {"cx": float(x.mean()), "cy": float(y.mean()), "sx": float(x.std()), "sy": float(y.std()),
+            "ke": float(0.5 * speed2.mean()), "vmax": float(np.sqrt(speed2.max())),
+            "front": float(np.quantile(x, 0.999)), "surface": float(np.quantile(y, 0.001)),
+            "detP05": float(np.quantile(det, 0.05)), "detP95": float(np.quantile(det, 0.95))}
