@@ -193,6 +193,10 @@ def kernel_bytes(name: str, n: int, active: tuple) -> float:
         # key + rank and writes the permutation (12 B)
         "k_tile_count": n * 16.0,
         "k_tile_scatter": n * 12.0,
+        # the whole substep in one launch (allocation, bucketing, P2G, grid
+        # update + G2P): the substep's 104 B per particle + 64 B per active
+        # channel-node
+        "k_substep": n * 104.0 + channel_nodes * 64.0,
     }
     return table.get(name, 0.0)
 

@@ -253,11 +253,39 @@ int mpm_set_launch_shape(mpm_solver *solver, uint32_t p2g_ctas, uint32_t g2p_cta
 int mpm_get_launch_shape(mpm_solver *solver, uint32_t *p2g_ctas, uint32_t *g2p_ctas, uint32_t *sm_count);
 
 /* The autotuner: times `substeps` real substeps of the last submit's
- * parameters for each candidate persistent grid (1 .. occupancy-limit CTAs
- * per SM), P2G first, then G2P with the best P2G, keeps the
- * fastest, and restores the particle state and counters it started from.
- * Needs one submitted batch.  Blocks. */
+ * parameters (the whole graph, device time) for each candidate variant and
+ * keeps the fastest: for each P2G stage capacity (640, 384), the one-launch
+ * substep over persistent grids of 1 .. co-resident CTAs per SM, and the
+ * four-launch substep over its P2G grids, then its G2P grids with the best
+ * P2G.  Restores the particle state and counters it started from.  Returns
+ * the chosen four-launch grids (mpm_get_substep_variant gives the rest) and
+ * the best milliseconds per substep.  Needs one submitted batch.  Blocks. */
 int mpm_autotune(mpm_solver *solver, uint32_t substeps, uint32_t *p2g_ctas, uint32_t *g2p_ctas, double *best_ms);
+
+/* The default path's substep variant (no counterpart in the reference,
+ * whose substep is a sequence of WebGPU compute passes).  `fused` 1 runs each
+ * substep as ONE cooperative launch of persistent CTAs (tile allocation,
+ * bucketing, P2G, grid update + G2P, with grid barriers between them), 0 as
+ * four launches; `stage_capacity` is the P2G stage (640 or 384 particles;
+ * 0 keeps it); `substep_ctas` the one-launch form's persistent grid (0 keeps
+ * it; at most the CTAs that fit on the GPU at once).  Solvers with bonded
+ * bodies or fracture bonds always take four launches.  Results do not depend
+ * on `fused` or the grids (the phases are the same device code); the stage
+ * capacity changes only the rounding of tiles holding more particles than it.
+ * mpm_get_substep_variant reports whether substeps run as one launch, the
+ * capacity, the grid and its co-resident limit. */
+int mpm_set_substep_variant(mpm_solver *solver, uint32_t fused, uint32_t stage_capacity, uint32_t substep_ctas);
+int mpm_get_substep_variant(mpm_solver *solver, uint32_t *fused, uint32_t *stage_capacity, uint32_t *substep_ctas,
+                            uint32_t *max_substep_ctas);
+
+/* The one-launch substep's grid-barrier waits give up after `limit_ns`
+ * nanoseconds (default 1 s; 1 us .. 60 s): the CTA that gave up raises status
+ * flag 1 << 20 in every scene, the others leave at their next barrier, and the
+ * batch's particle state is undefined (write the particles again).
+ * `skip_cta` below the grid makes that CTA leave before the first barrier
+ * without arriving, so that the others' waits run out: a test of the limit
+ * (0xffffffff: none).  No counterpart in the reference. */
+int mpm_set_barrier_limit(mpm_solver *solver, uint64_t limit_ns, uint32_t skip_cta);
 
 /* Nodes of the last substep with positive solid / water / oil mass. */
 int mpm_count_active_nodes(mpm_solver *solver, uint32_t counts[3]);

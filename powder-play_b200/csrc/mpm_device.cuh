@@ -28,6 +28,9 @@ constexpr uint32_t ERROR_TRIANGLE_BOND = 8192u;
 constexpr uint32_t ERROR_CFL_BOUND = 16384u;
 constexpr uint32_t ERROR_FRACTURE_BOND = 32768u;
 constexpr uint32_t ERROR_FIXED_POINT_RANGE = 65536u;
+// no counterpart in the reference: a grid barrier wait of the fused substep
+// kernel ran out (every scene of the launch gets it; the state is undefined)
+constexpr uint32_t ERROR_BARRIER = 1u << 20;
 
 // Constitutive model codes: src/lib/mpm/materials.ts:8-16, plus 5 =
 // fixed-corotated (no reference counterpart).

@@ -4,7 +4,9 @@
 // src/lib/mpm/kernels/solver.ts:1465-1570):
 //   k_tile_alloc (starts the substep) -> k_tile_scatter -> k_p2g_gather
 //   -> k_g2p_tile (grid update + G2P + next substep's tile counts)
-//   (k_begin_batch and k_tile_count run once at the start of a batch)
+//   (k_begin_batch and k_tile_count run once at the start of a batch);
+//   or the same four phases in one cooperative launch, k_substep, with grid
+//   barriers between them
 // The cell sort (k_count, k_scan_*, k_scatter, k_stable_rank) backs the sort
 // probe and the allocation-free cell sort.
 // Substep, fixed-point atomic P2G (createExperimentalMpmMlsAtomicGpuSolver):
@@ -391,6 +393,8 @@ __global__ void k_begin_batch(Ctx c, uint32_t reset_progress)
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         c.work[WORK_ACTIVE] = 0u;
         c.work[WORK_ACTIVE + 1] = 0u;
+        c.work[WORK_BARRIER] = 0u;  // an abandoned launch may have left arrivals
+        c.work[WORK_ABORT] = 0u;
     }
 }
 
@@ -782,20 +786,22 @@ __device__ __forceinline__ bool runs_flag(const Ctx &c, uint32_t scene)
 // 0 empties the tile list of the next substep (the other buffer parity).
 // Neither the order of the bucket ranges nor that of the list changes any
 // sum: P2G orders each tile's particles by cell, channel and original index.
-__global__ void __launch_bounds__(ALLOC_THREADS) k_tile_alloc(Ctx c0)
+// Allocation chunk b (1024 tiles of one scene) with ALLOC_THREADS threads.
+__device__ __forceinline__ void alloc_chunk(const Ctx &c0, uint32_t b)
 {
     __shared__ uint32_t s_base[2];
     __shared__ bool s_runs;
     const bool one_scene = c0.n_scenes == 1u;
-    const uint32_t scene = one_scene ? 0u : scene_of_chunk(c0, blockIdx.x);
-    const uint32_t chunk = one_scene ? blockIdx.x : blockIdx.x - c0.scene_chunk[scene];
+    const uint32_t scene = one_scene ? 0u : scene_of_chunk(c0, b);
+    const uint32_t chunk = one_scene ? b : b - c0.scene_chunk[scene];
     const Ctx c = scene_ctx(c0, scene);
     const StepParams &P = *c.P;
+    __syncthreads();  // the previous chunk's readers of s_base and s_runs are done
     if (threadIdx.x == 0) {
         const bool runs = substep_runs(c);
         s_runs = runs;
         c.counters[COUNTER_RUNS] = runs ? 1u : 0u;  // the same value from every CTA of the scene
-        if (blockIdx.x == 0) c0.work[WORK_ACTIVE + (c0.parity ^ 1u)] = 0u;
+        if (b == 0) c0.work[WORK_ACTIVE + (c0.parity ^ 1u)] = 0u;
     }
     // the counts are read before the answer is known (they exist either way)
     uint32_t *count = c.tile_count + P.tile_base;  // 32-byte aligned: scenes start on 8-tile boundaries
@@ -858,13 +864,12 @@ __global__ void __launch_bounds__(ALLOC_THREADS) k_tile_alloc(Ctx c0)
     }
 }
 
-// Bucket the slots by tile: perm[first entry of the tile + rank] = slot,
-// four slots per thread, for the scenes taking part in the substep (the
-// answer k_tile_alloc stored).  The first threads of CTA 0 start the substep
-// of every scene (begin_substep) and reset the scenes' bucket cursors.  With
-// several scenes, a warp whose slots lie in one scene asks once whether that
-// scene takes part.
-__global__ void k_tile_scatter(Ctx c)
+__global__ void __launch_bounds__(ALLOC_THREADS) k_tile_alloc(Ctx c0) { alloc_chunk(c0, blockIdx.x); }
+
+// Starts the substep of every scene (the first threads of CTA 0) and buckets
+// the slots 4q .. 4q + 3 of every quad q = q0 + lane for q0 from `first`
+// (a warp's first quad) in steps of `stride` quads (a multiple of 32).
+__device__ __forceinline__ void scatter_quads(const Ctx &c, uint32_t first, uint32_t stride)
 {
     if (blockIdx.x == 0) {
         for (uint32_t s = threadIdx.x; s < c.n_scenes; s += blockDim.x) {
@@ -873,38 +878,54 @@ __global__ void k_tile_scatter(Ctx c)
             cs.counters[COUNTER_CURSOR] = cs.P->p_base;
         }
     }
-    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) * 4u;
+    const uint32_t lane = threadIdx.x & 31u;
     if (c.n_scenes > 1u) {
-        const uint32_t first = min(i, c.n - 1u);
-        const uint32_t scene = scene_of_slot(c, first);
-        const uint32_t lead = __shfl_sync(0xffffffffu, scene, 0);
-        const uint32_t end = c.scene_p_base[lead + 1u];
-        const uint32_t warp_last = min(((blockIdx.x * blockDim.x + (threadIdx.x | 31u)) * 4u) + 3u, c.n - 1u);
-        const bool one = __shfl_sync(0xffffffffu, warp_last, 31) < end;
-        if (one && !runs_flag(c, lead)) return;
-        if (i >= c.n) return;
-        for (uint32_t j = i; j < min(i + 4u, c.n); ++j) {
-            if (!one && !runs_flag(c, scene_of_slot(c, j))) continue;
-            c.perm[c.tile_range[c.keys[j]].x + c.ranks[j]] = j;
+        for (uint32_t q0 = first; q0 * 4u < c.n; q0 += stride) {
+            const uint32_t i = (q0 + lane) * 4u;
+            const uint32_t first_slot = min(i, c.n - 1u);
+            const uint32_t scene = scene_of_slot(c, first_slot);
+            const uint32_t lead = __shfl_sync(0xffffffffu, scene, 0);
+            const uint32_t end = c.scene_p_base[lead + 1u];
+            const uint32_t warp_last = min((q0 + 31u) * 4u + 3u, c.n - 1u);
+            const bool one = warp_last < end;
+            if (one && !runs_flag(c, lead)) continue;
+            if (i >= c.n) continue;
+            for (uint32_t j = i; j < min(i + 4u, c.n); ++j) {
+                if (!one && !runs_flag(c, scene_of_slot(c, j))) continue;
+                c.perm[__ldcg(c.tile_range + __ldcg(c.keys + j)).x + __ldcg(c.ranks + j)] = j;
+            }
         }
         return;
     }
-    if (i >= c.n) return;
     const bool runs = runs_flag(c, 0u);
-    if (i + 4u <= c.n) {
-        const uint4 key = __ldcs(reinterpret_cast<const uint4 *>(c.keys + i));
-        const uint4 rank = __ldcs(reinterpret_cast<const uint4 *>(c.ranks + i));
-        if (!runs) return;
-        const uint32_t s0 = c.tile_range[key.x].x, s1 = c.tile_range[key.y].x, s2 = c.tile_range[key.z].x,
-                       s3 = c.tile_range[key.w].x;
-        c.perm[s0 + rank.x] = i;
-        c.perm[s1 + rank.y] = i + 1u;
-        c.perm[s2 + rank.z] = i + 2u;
-        c.perm[s3 + rank.w] = i + 3u;
-    } else {
-        if (!runs) return;
-        for (uint32_t j = i; j < c.n; ++j) c.perm[c.tile_range[c.keys[j]].x + c.ranks[j]] = j;
+    if (!runs) return;
+    for (uint32_t q0 = first; q0 * 4u < c.n; q0 += stride) {
+        const uint32_t i = (q0 + lane) * 4u;
+        if (i >= c.n) break;
+        if (i + 4u <= c.n) {
+            const uint4 key = __ldcs(reinterpret_cast<const uint4 *>(c.keys + i));
+            const uint4 rank = __ldcs(reinterpret_cast<const uint4 *>(c.ranks + i));
+            const uint32_t s0 = __ldcg(c.tile_range + key.x).x, s1 = __ldcg(c.tile_range + key.y).x,
+                           s2 = __ldcg(c.tile_range + key.z).x, s3 = __ldcg(c.tile_range + key.w).x;
+            c.perm[s0 + rank.x] = i;
+            c.perm[s1 + rank.y] = i + 1u;
+            c.perm[s2 + rank.z] = i + 2u;
+            c.perm[s3 + rank.w] = i + 3u;
+        } else {
+            for (uint32_t j = i; j < c.n; ++j) c.perm[__ldcg(c.tile_range + c.keys[j]).x + c.ranks[j]] = j;
+        }
     }
+}
+
+// Bucket the slots by tile: perm[first entry of the tile + rank] = slot,
+// four slots per thread, for the scenes taking part in the substep (the
+// answer k_tile_alloc stored).  The first threads of CTA 0 start the substep
+// of every scene (begin_substep) and reset the scenes' bucket cursors.  With
+// several scenes, a warp whose slots lie in one scene asks once whether that
+// scene takes part.
+__global__ void k_tile_scatter(Ctx c)
+{
+    scatter_quads(c, blockIdx.x * blockDim.x + (threadIdx.x & ~31u), gridDim.x * blockDim.x);
 }
 
 namespace {
@@ -912,14 +933,15 @@ namespace {
 // Shared-memory staging of the particles of one tile (or of one chunk of a
 // crowded tile): their P2G records, their grouping by base cell (in the
 // order channel, original index within a cell) and the ring accumulator.
+template <int CAP>
 struct Stage {
-    float4 state[STAGE_CAP];     // fx, fy, mass, liquid volume
-    float4 affine[STAGE_CAP];    // A = m C + (-dt V 4/dx^2) P F^T
-    float2 momentum[STAGE_CAP];  // m v
-    uint32_t orig[STAGE_CAP];    // original index; after the count pass channel << 30 | original index
-    uint32_t cell[STAGE_CAP];    // local cell | channel << 8 | REC_FAILED
-    uint16_t order[STAGE_CAP];   // arrival rank within the cell, then rank by (channel, original index)
-    uint16_t sorted[STAGE_CAP];  // staged indices grouped by cell
+    float4 state[CAP];     // fx, fy, mass, liquid volume
+    float4 affine[CAP];    // A = m C + (-dt V 4/dx^2) P F^T
+    float2 momentum[CAP];  // m v
+    uint32_t orig[CAP];    // original index; after the count pass channel << 30 | original index
+    uint32_t cell[CAP];    // local cell | channel << 8 | REC_FAILED
+    uint16_t order[CAP];   // arrival rank within the cell, then rank by (channel, original index)
+    uint16_t sorted[CAP];  // staged indices grouped by cell
     uint32_t count[TILE_CELLS];
     uint32_t start[TILE_CELLS + 1];
     float acc[ACC_WORDS][RING_NODES];
@@ -930,9 +952,52 @@ struct Stage {
     int failed;
 };
 
+// A P2G tile is taken by a group of TILE_CELLS threads (one per cell of the
+// tile in the count and scan passes): the whole CTA of k_p2g_gather, or one
+// of the GROUPS halves of a k_substep CTA, which then synchronise on named
+// barriers 1 and 2 (barrier 0 stays the CTA's).
+template <int GROUPS>
+__device__ __forceinline__ uint32_t p2g_group() { return GROUPS == 1 ? 0u : threadIdx.x / TILE_CELLS; }
+
+template <int GROUPS>
+__device__ __forceinline__ void group_sync()
+{
+    if constexpr (GROUPS == 1) {
+        __syncthreads();
+    } else {
+        // barrier ids as immediates (the group is uniform per warp)
+        if (p2g_group<GROUPS>() == 0u)
+            asm volatile("bar.sync 1, %0;" ::"n"(TILE_CELLS) : "memory");
+        else
+            asm volatile("bar.sync 2, %0;" ::"n"(TILE_CELLS) : "memory");
+    }
+}
+
+template <int GROUPS>
+__device__ __forceinline__ uint32_t group_sync_count(bool pred)
+{
+    if constexpr (GROUPS == 1) {
+        return (uint32_t)__syncthreads_count(pred);
+    } else {
+        uint32_t r;
+        if (p2g_group<GROUPS>() == 0u)
+            asm volatile("{\n .reg .pred p;\n setp.ne.u32 p, %1, 0;\n bar.red.popc.u32 %0, 1, %2, p;\n}\n"
+                         : "=r"(r)
+                         : "r"(pred ? 1u : 0u), "n"(TILE_CELLS)
+                         : "memory");
+        else
+            asm volatile("{\n .reg .pred p;\n setp.ne.u32 p, %1, 0;\n bar.red.popc.u32 %0, 2, %2, p;\n}\n"
+                         : "=r"(r)
+                         : "r"(pred ? 1u : 0u), "n"(TILE_CELLS)
+                         : "memory");
+        return r;
+    }
+}
+
 // First sorted entry of channel >= ch in the cell's entries [lo, hi) (they
 // are ordered by channel, then original index).
-__device__ __forceinline__ uint32_t channel_start(const Stage &sm, uint32_t lo, uint32_t hi, uint32_t ch)
+template <int CAP>
+__device__ __forceinline__ uint32_t channel_start(const Stage<CAP> &sm, uint32_t lo, uint32_t hi, uint32_t ch)
 {
     while (lo < hi) {
         const uint32_t mid = (lo + hi) / 2u;
@@ -944,9 +1009,37 @@ __device__ __forceinline__ uint32_t channel_start(const Stage &sm, uint32_t lo, 
     return lo;
 }
 
-__device__ __forceinline__ uint32_t sort_key(const Stage &sm, uint32_t k)
+template <int CAP>
+__device__ __forceinline__ uint32_t sort_key(const Stage<CAP> &sm, uint32_t k)
 {
     return sm.orig[k];  // channel << 30 | original index, set by p2g_chunk's count pass
+}
+
+// Exclusive scan of the 128 cell counts by the group's first warp (4 cells
+// per lane, `lane` its lane) into out[0 .. TILE_CELLS] (and into out2 when
+// given).
+__device__ __forceinline__ void scan_cell_counts(uint32_t lane, const uint32_t *count, uint32_t *out, uint32_t *out2)
+{
+    const uint32_t a = count[4 * lane], b = count[4 * lane + 1], d = count[4 * lane + 2], e = count[4 * lane + 3];
+    const uint32_t t = a + b + d + e;
+    uint32_t inc = t;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t up = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= (uint32_t)o) inc += up;
+    }
+    const uint32_t ex = inc - t;
+    out[4 * lane] = ex;
+    out[4 * lane + 1] = ex + a;
+    out[4 * lane + 2] = ex + a + b;
+    out[4 * lane + 3] = ex + a + b + d;
+    if (lane == 31) out[TILE_CELLS] = inc;
+    if (out2) {
+        out2[4 * lane] = ex;
+        out2[4 * lane + 1] = ex + a;
+        out2[4 * lane + 2] = ex + a + b;
+        out2[4 * lane + 3] = ex + a + b + d;
+    }
 }
 
 // Stages the records of the slots src[i0 .. i1) with asynchronous copies,
@@ -957,12 +1050,13 @@ __device__ __forceinline__ uint32_t sort_key(const Stage &sm, uint32_t k)
 // phases, one stencil offset per phase (no two cells of a phase share a
 // node), so every sum has a fixed order.  Returns false once a record had
 // failed.
-__device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, const uint32_t *src, uint32_t i0, uint32_t i1)
+template <int CAP, int GROUPS>
+__device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage<CAP> &sm, const uint32_t *src, uint32_t i0, uint32_t i1)
 {
     const StepParams &P = *c.P;
-    const uint32_t me = threadIdx.x;  // this thread's cell
+    const uint32_t me = threadIdx.x % TILE_CELLS;  // this thread's cell
     sm.count[me] = 0u;
-    __syncthreads();
+    group_sync<GROUPS>();
     for (uint32_t i = i0 + me; i < i1; i += TILE_CELLS) {
         const uint32_t s = src[i];
         const uint32_t k = i - i0;
@@ -973,7 +1067,7 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, const uint32_
         cp_async<4>(&sm.cell[k], &c.rec_cell[s]);
     }
     cp_async_wait_all();
-    __syncthreads();
+    group_sync<GROUPS>();
     const uint32_t n = i1 - i0;
     uint32_t mask = 0;
     for (uint32_t k = me; k < n; k += TILE_CELLS) {
@@ -995,29 +1089,12 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, const uint32_
         sm.orig[k] |= ((cell >> 8) & 3u) << 30;
     }
     if (mask) atomicOr(&sm.mask, mask);
-    __syncthreads();
+    group_sync<GROUPS>();
     if (sm.failed) return false;
-    // exclusive scan of the 128 cell counts (one warp, 4 cells per lane)
-    if (me < 32) {
-        const uint32_t a = sm.count[4 * me], b = sm.count[4 * me + 1], d = sm.count[4 * me + 2],
-                       e = sm.count[4 * me + 3];
-        const uint32_t t = a + b + d + e;
-        uint32_t inc = t;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t up = __shfl_up_sync(0xffffffffu, inc, o);
-            if (me >= (uint32_t)o) inc += up;
-        }
-        const uint32_t ex = inc - t;
-        sm.start[4 * me] = ex;
-        sm.start[4 * me + 1] = ex + a;
-        sm.start[4 * me + 2] = ex + a + b;
-        sm.start[4 * me + 3] = ex + a + b + d;
-        if (me == 31) sm.start[TILE_CELLS] = inc;
-    }
-    __syncthreads();
+    if (me < 32) scan_cell_counts(me, sm.count, sm.start, nullptr);
+    group_sync<GROUPS>();
     for (uint32_t k = me; k < n; k += TILE_CELLS) sm.sorted[sm.start[sm.cell[k] & 0xffu] + sm.order[k]] = (uint16_t)k;
-    __syncthreads();
+    group_sync<GROUPS>();
     // order each cell's entries by (channel, original index): every entry
     // counts the entries of its cell with a smaller key (keys are distinct),
     // so crowded cells spread over all threads
@@ -1027,27 +1104,27 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, const uint32_
         for (uint32_t j = sm.start[cell]; j < sm.start[cell + 1]; ++j) rank += sort_key(sm, sm.sorted[j]) < key;
         sm.order[k] = (uint16_t)rank;
     }
-    __syncthreads();
+    group_sync<GROUPS>();
     for (uint32_t k = me; k < n; k += TILE_CELLS) sm.sorted[sm.start[sm.cell[k] & 0xffu] + sm.order[k]] = (uint16_t)k;
-    __syncthreads();
+    group_sync<GROUPS>();
     // the cells holding entries, compacted; each gets a group of `share`
     // consecutive threads of one warp (a power of two up to 32, so that the
-    // groups fill the CTA): a crowded chunk of few cells spreads each cell's
-    // particles over its group, which adds their sums in a fixed tree order
-    // (with more than 64 such cells every thread takes its own cell)
+    // groups fill the 128 threads): a crowded chunk of few cells spreads each
+    // cell's particles over its group, which adds their sums in a fixed tree
+    // order (with more than 64 such cells every thread takes its own cell)
     const bool has = sm.start[me + 1] > sm.start[me];
-    const uint32_t n_cells = (uint32_t)__syncthreads_count(has);
+    const uint32_t n_cells = group_sync_count<GROUPS>(has);
     uint32_t share = 1;
     while (share < 32u && n_cells * share * 2u <= (uint32_t)TILE_CELLS) share *= 2u;
     if (share > 1u) {
         const unsigned ballot = __ballot_sync(0xffffffffu, has);
         const uint32_t lane = me & 31u, warp = me >> 5;
         if (lane == 0u) sm.warp_active[warp] = __popc(ballot);
-        __syncthreads();
+        group_sync<GROUPS>();
         uint32_t before = 0;
         for (uint32_t w = 0; w < warp; ++w) before += sm.warp_active[w];
         if (has) sm.active[before + __popc(ballot & ((1u << lane) - 1u))] = (uint8_t)me;
-        __syncthreads();
+        group_sync<GROUPS>();
     }
     const uint32_t group = me / share, part = me % share;
     const bool mine = share == 1u || group < n_cells;
@@ -1114,7 +1191,7 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, const uint32_
 #pragma unroll
             for (int ox = 0; ox < 3; ++ox) {
                 const int o = oy * 3 + ox;
-                __syncthreads();  // the previous phase's adds are done
+                group_sync<GROUPS>();  // the previous phase's adds are done
                 if (adds) {
                     const int r = (cy + oy) * RING_X + cx + ox;
                     sm.acc[word][r] += m[o];
@@ -1125,52 +1202,53 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage &sm, const uint32_
             }
         }
     }
-    __syncthreads();
+    group_sync<GROUPS>();
     return true;
 }
 
-}  // namespace
-
 // P2G (prepareParticle + the p2g of shaders.ts:808-963, :1072-1211; the
 // records carry prepareParticle's result from the previous G2P) for the
-// tiles holding particles, one tile per CTA iteration, one thread per cell.
+// tiles holding particles, one tile per group iteration, one thread per cell.
 // The sums of a tile's particles over its 18x10-node ring have a fixed
-// order (cell-major phases, original particle index within a cell), so
-// they do not depend on the order of the tile buckets and every run is
-// bit-identical.  A tile with more than STAGE_CAP particles is taken in
-// chunks of consecutive whole cells (a cell holding more than STAGE_CAP
-// particles in chunks of the bucket, whose order then decides the rounding
-// of its sums).  The sums go to the tile's own ring record; k_g2p_tile adds
-// the up to four records that cover a node.
-template <bool SCENES>
-__global__ void __launch_bounds__(TILE_CELLS) k_p2g_gather(Ctx c0)
+// order (cell-major phases, original particle index within a cell), so they
+// do not depend on the order of the tile buckets and every run is
+// bit-identical.  A tile with more than CAP particles is taken in chunks of
+// consecutive whole cells (a cell holding more than CAP particles in chunks
+// of the bucket, whose order then decides the rounding of its sums).  The
+// sums go to the tile's own ring record; the G2P adds the up to four
+// records that cover a node.  The GROUPS groups of a CTA take interleaved
+// tiles of the list, each with its own stage.
+template <bool SCENES, int CAP, int GROUPS>
+__device__ __forceinline__ void p2g_tiles(const Ctx &c0, Stage<CAP> *stages)
 {
-    __shared__ Stage sm;
-    const uint32_t n_active = c0.work[WORK_ACTIVE + c0.parity];
-    for (uint32_t item = blockIdx.x; item < n_active; item += gridDim.x) {
-        const uint32_t tile = c0.active_tiles[item];
+    const uint32_t g = p2g_group<GROUPS>();
+    const uint32_t me = threadIdx.x % TILE_CELLS;
+    Stage<CAP> &sm = stages[g];
+    const uint32_t n_active = __ldcg(c0.work + WORK_ACTIVE + c0.parity);
+    for (uint32_t item = blockIdx.x * GROUPS + g; item < n_active; item += gridDim.x * GROUPS) {
+        const uint32_t tile = __ldcg(c0.active_tiles + item);
         const Ctx c = tile_ctx<SCENES>(c0, tile);
-        const uint32_t stamp = c.counters[COUNTER_STAMP];
-        const uint2 range = c.tile_range[tile];
+        const uint32_t stamp = __ldcg(c.counters + COUNTER_STAMP);
+        const uint2 range = __ldcg(c.tile_range + tile);
         const uint32_t begin = range.x, n_tile = range.y;
-        __syncthreads();  // the previous tile's readers of sm are done
-        for (int k = threadIdx.x; k < ACC_WORDS * RING_NODES; k += TILE_CELLS) (&sm.acc[0][0])[k] = 0.f;
-        if (threadIdx.x == 0) {
-            sm.failed = *(volatile uint32_t *)c.status != 0u ? 1 : 0;  // one read for the whole CTA
+        group_sync<GROUPS>();  // the previous tile's readers of sm are done
+        for (int k = me; k < ACC_WORDS * RING_NODES; k += TILE_CELLS) (&sm.acc[0][0])[k] = 0.f;
+        if (me == 0) {
+            sm.failed = *(volatile uint32_t *)c.status != 0u ? 1 : 0;  // one read for the whole group
             sm.mask = 0u;
         }
-        __syncthreads();
+        group_sync<GROUPS>();
         if (sm.failed) continue;  // the scene's substep is rolled back
         // a tile above one stage: its entries are first ordered by cell into
         // the scratch list tmp[begin .. begin + n_tile) (arrival order within
         // a cell), then taken in chunks of consecutive whole cells holding at
-        // most STAGE_CAP particles in all; a cell holding more is taken in
-        // chunks of its list, whose arrival order then decides the rounding
+        // most CAP particles in all; a cell holding more is taken in chunks of
+        // its list, whose arrival order then decides the rounding
         const uint32_t *src = c.perm + begin;
-        if (n_tile > (uint32_t)STAGE_CAP) {
-            sm.count[threadIdx.x] = 0u;  // one thread per cell
-            __syncthreads();
-            for (uint32_t i = threadIdx.x; i < n_tile; i += 4 * TILE_CELLS) {
+        if (n_tile > (uint32_t)CAP) {
+            sm.count[me] = 0u;  // one thread per cell
+            group_sync<GROUPS>();
+            for (uint32_t i = me; i < n_tile; i += 4 * TILE_CELLS) {
                 uint32_t s[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) s[u] = i + u * TILE_CELLS < n_tile ? src[i + u * TILE_CELLS] : 0xffffffffu;
@@ -1178,33 +1256,12 @@ __global__ void __launch_bounds__(TILE_CELLS) k_p2g_gather(Ctx c0)
                 for (int u = 0; u < 4; ++u)
                     if (s[u] != 0xffffffffu) atomicAdd(&sm.count[c.rec_cell[s[u]] & 0xffu], 1u);
             }
-            __syncthreads();
-            if (threadIdx.x < 32) {
-                const uint32_t me = threadIdx.x;
-                const uint32_t a = sm.count[4 * me], b = sm.count[4 * me + 1], d = sm.count[4 * me + 2],
-                               e = sm.count[4 * me + 3];
-                const uint32_t t = a + b + d + e;
-                uint32_t inc = t;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t up = __shfl_up_sync(0xffffffffu, inc, o);
-                    if (me >= (uint32_t)o) inc += up;
-                }
-                const uint32_t ex = inc - t;
-                sm.cells[4 * me] = ex;
-                sm.cells[4 * me + 1] = ex + a;
-                sm.cells[4 * me + 2] = ex + a + b;
-                sm.cells[4 * me + 3] = ex + a + b + d;
-                if (me == 31) sm.cells[TILE_CELLS] = inc;
-                // cursors for the placement below
-                sm.start[4 * me] = ex;
-                sm.start[4 * me + 1] = ex + a;
-                sm.start[4 * me + 2] = ex + a + b;
-                sm.start[4 * me + 3] = ex + a + b + d;
-            }
-            __syncthreads();
+            group_sync<GROUPS>();
+            // the cells' first entries, and cursors for the placement below
+            if (me < 32) scan_cell_counts(me, sm.count, sm.cells, sm.start);
+            group_sync<GROUPS>();
             uint32_t *list = c.tmp + begin;
-            for (uint32_t i = threadIdx.x; i < n_tile; i += 4 * TILE_CELLS) {
+            for (uint32_t i = me; i < n_tile; i += 4 * TILE_CELLS) {
                 uint32_t s[4], cell[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) s[u] = i + u * TILE_CELLS < n_tile ? src[i + u * TILE_CELLS] : 0xffffffffu;
@@ -1214,28 +1271,30 @@ __global__ void __launch_bounds__(TILE_CELLS) k_p2g_gather(Ctx c0)
                 for (int u = 0; u < 4; ++u)
                     if (s[u] != 0xffffffffu) list[atomicAdd(&sm.start[cell[u]], 1u)] = s[u];
             }
-            __syncthreads();  // the list is written (global, read back by this CTA)
+            // the list is written (global, read back by this group)
+            if constexpr (GROUPS > 1) __threadfence_block();
+            group_sync<GROUPS>();
             src = list;
         }
         bool ok = true;
         uint32_t q = 0, i0 = 0;
         while (ok && q < (uint32_t)TILE_CELLS) {
             uint32_t q1 = TILE_CELLS, lo = 0, hi = n_tile;
-            if (n_tile > (uint32_t)STAGE_CAP) {
-                if (sm.cells[q + 1] - sm.cells[q] > (uint32_t)STAGE_CAP) {
+            if (n_tile > (uint32_t)CAP) {
+                if (sm.cells[q + 1] - sm.cells[q] > (uint32_t)CAP) {
                     q1 = q + 1;
                     lo = sm.cells[q] + i0;
-                    hi = min(lo + (uint32_t)STAGE_CAP, sm.cells[q + 1]);
+                    hi = min(lo + (uint32_t)CAP, sm.cells[q + 1]);
                 } else {
                     q1 = q;
-                    while (q1 < (uint32_t)TILE_CELLS && sm.cells[q1 + 1] - sm.cells[q] <= (uint32_t)STAGE_CAP) ++q1;
+                    while (q1 < (uint32_t)TILE_CELLS && sm.cells[q1 + 1] - sm.cells[q] <= (uint32_t)CAP) ++q1;
                     lo = sm.cells[q];
                     hi = sm.cells[q1];
                 }
             }
-            ok = p2g_chunk(c, sm, src, lo, hi);
-            if (n_tile > (uint32_t)STAGE_CAP && q1 == q + 1 && hi < sm.cells[q + 1]) {
-                i0 += (uint32_t)STAGE_CAP;  // next chunk of the same crowded cell
+            ok = p2g_chunk<CAP, GROUPS>(c, sm, src, lo, hi);
+            if (n_tile > (uint32_t)CAP && q1 == q + 1 && hi < sm.cells[q + 1]) {
+                i0 += (uint32_t)CAP;  // next chunk of the same crowded cell
             } else {
                 q = q1;
                 i0 = 0;
@@ -1243,14 +1302,23 @@ __global__ void __launch_bounds__(TILE_CELLS) k_p2g_gather(Ctx c0)
         }
         if (!ok) continue;
         const uint32_t mask = sm.mask;
-        if (threadIdx.x == 0) c.tile_info[tile] = make_uint2(stamp, mask);
+        if (me == 0) c.tile_info[tile] = make_uint2(stamp, mask);
         float *out = c.part + (size_t)tile * (ACC_WORDS * RING_NODES);
-        for (int k = threadIdx.x; k < ACC_WORDS * RING_NODES; k += TILE_CELLS) {
+        for (int k = me; k < ACC_WORDS * RING_NODES; k += TILE_CELLS) {
             const int word = k / RING_NODES;
             const uint32_t bit = word < 3 ? 1u : (word < 7 ? 2u : 4u);
             if (mask & bit) out[k] = (&sm.acc[0][0])[k];
         }
     }
+}
+
+}  // namespace
+
+template <bool SCENES, int CAP>
+__global__ void __launch_bounds__(TILE_CELLS) k_p2g_gather(Ctx c0)
+{
+    extern __shared__ __align__(16) unsigned char dsm[];
+    p2g_tiles<SCENES, CAP, 1>(c0, reinterpret_cast<Stage<CAP> *>(dsm));
 }
 
 namespace {
@@ -1953,31 +2021,49 @@ __device__ __forceinline__ void flush_active_nodes(uint32_t *counters, uint32_t 
 // whose ring holds a failing node raises the grid status and moves none of
 // its particles (the substep is rolled back); tiles elsewhere still move
 // theirs, so their G2P flags can join the status of that substep.
-template <bool SCENES, bool BODIES>
-__global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
-{
+// Shared memory of the G2P phase.
+struct G2PShared {
     // per buffer parity: the tile, its bucket range and its 3x3 neighbours'
     // (stamp, mask); with one scene the next tile's are copied in while this
     // one's particles move, and the index of the one after it
-    __shared__ uint32_t s_tile[2];
-    __shared__ uint2 s_range[2];
-    __shared__ uint2 s_infos[2][9];
+    uint32_t tile[2];
+    uint2 range[2];
+    uint2 infos[2][9];
     // with one scene: the next tile's first G2P_STAGE bucket entries and the
     // scene's status words, copied in while this tile's particles move
-    __shared__ uint32_t s_perm[2][G2P_STAGE];
-    __shared__ __align__(16) uint32_t s_status[2][4];
-    __shared__ float2 s_vol[VOL_X * VOL_Y];
-    __shared__ float2 s_vs[RING_NODES];
-    __shared__ float4 s_vw[RING_NODES];
-    __shared__ float4 s_vo[RING_NODES];
-    __shared__ int s_fail;
+    uint32_t perm[2][G2P_STAGE];
+    __align__(16) uint32_t status[2][4];
+    float2 vol[VOL_X * VOL_Y];
+    float2 vs[RING_NODES];
+    float4 vw[RING_NODES];
+    float4 vo[RING_NODES];
+    int fail;
     // the particles of the tile (or of one chunk of a crowded tile), copied
     // in while the node phase runs
-    __shared__ float4 p_F[G2P_STAGE];
-    __shared__ float2 p_pos[G2P_STAGE];
-    __shared__ float p_vol[G2P_STAGE], p_pvol[G2P_STAGE], p_damage[G2P_STAGE];
-    __shared__ uint32_t p_mat[G2P_STAGE], p_orig[G2P_STAGE];
-    const uint32_t n_active = c0.work[WORK_ACTIVE + c0.parity];
+    float4 F[G2P_STAGE];
+    float2 pos[G2P_STAGE];
+    float pvol_in[G2P_STAGE], vol_in[G2P_STAGE], damage[G2P_STAGE];
+    uint32_t mat[G2P_STAGE], orig[G2P_STAGE];
+};
+
+template <bool SCENES, bool BODIES>
+__device__ __forceinline__ void g2p_tiles(const Ctx &c0, G2PShared &sh)
+{
+    uint32_t *const s_tile = sh.tile;
+    uint2 *const s_range = sh.range;
+    uint2(*const s_infos)[9] = sh.infos;
+    uint32_t(*const s_perm)[G2P_STAGE] = sh.perm;
+    uint32_t(*const s_status)[4] = sh.status;
+    float2 *const s_vol = sh.vol;
+    float2 *const s_vs = sh.vs;
+    float4 *const s_vw = sh.vw;
+    float4 *const s_vo = sh.vo;
+    int &s_fail = sh.fail;
+    float4 *const p_F = sh.F;
+    float2 *const p_pos = sh.pos;
+    float *const p_vol = sh.vol_in, *const p_pvol = sh.pvol_in, *const p_damage = sh.damage;
+    uint32_t *const p_mat = sh.mat, *const p_orig = sh.orig;
+    const uint32_t n_active = __ldcg(c0.work + WORK_ACTIVE + c0.parity);
     uint32_t ws = 0, ww = 0, wo = 0;
     if constexpr (!SCENES) {
         // visible after the first iteration's barrier
@@ -2171,6 +2257,129 @@ __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
     }
     if constexpr (!SCENES) flush_active_nodes(c0.counters, ws, ww, wo);
 }
+
+template <bool SCENES, bool BODIES>
+__global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
+{
+    __shared__ G2PShared sh;
+    g2p_tiles<SCENES, BODIES>(c0, sh);
+}
+
+// ------------------------------------------------- one launch per substep --
+
+namespace {
+
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t *p)
+{
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_gpu(uint32_t *p, uint32_t v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Marks the launch abandoned and raises ERROR_BARRIER in every scene.
+__device__ void abandon_launch(const Ctx &c)
+{
+    atomicExch(c.work + WORK_ABORT, 1u);
+    for (uint32_t s = 0; s < c.n_scenes; ++s) fail(c.dyn + (size_t)s * SCENE_WORDS, ERROR_BARRIER);
+}
+
+// Grid-wide barrier of k_substep: every CTA of the cooperative launch calls
+// it the same number of times.  Thread 0 of each CTA arrives on
+// work[WORK_BARRIER]; the last arrival resets the count and advances the
+// generation work[WORK_BARRIER + 1], which the others wait for (the
+// release / acquire pair makes every CTA's writes before the barrier visible
+// to every CTA after it).  A wait gives up after c.barrier_limit_ns: that CTA
+// marks the launch abandoned, raises ERROR_BARRIER in every scene and
+// returns false; a CTA that finds the launch abandoned, before arriving or
+// while waiting, returns false too, so no CTA outlasts the limit by more than
+// one phase.  With `index` 0, CTA c.barrier_skip leaves without arriving (the
+// others' waits then run out: the test of the limit).
+__device__ bool grid_barrier(const Ctx &c, uint32_t index)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t *count = c.work + WORK_BARRIER, *gen = c.work + WORK_BARRIER + 1;
+        const uint32_t *abandoned = c.work + WORK_ABORT;
+        int ok = ld_acquire_gpu(abandoned) == 0u;
+        if (ok && index == 0u && blockIdx.x == c.barrier_skip) ok = 0;
+        if (ok) {
+            // the generation cannot move before this CTA arrives
+            const uint32_t g = ld_acquire_gpu(gen);
+            __threadfence();
+            if (atomicAdd(count, 1u) == gridDim.x - 1u) {
+                atomicExch(count, 0u);
+                __threadfence();
+                st_release_gpu(gen, g + 1u);
+            } else {
+                const unsigned long long t0 = global_ns();
+                while (ld_acquire_gpu(gen) == g) {
+                    if (ld_acquire_gpu(abandoned) != 0u) {
+                        ok = 0;
+                        break;
+                    }
+                    if (global_ns() - t0 > c.barrier_limit_ns) {
+                        abandon_launch(c);
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+            }
+            __threadfence();
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+}  // namespace
+
+static_assert(SUBSTEP_THREADS == ALLOC_THREADS && SUBSTEP_THREADS == 2 * TILE_CELLS && SUBSTEP_THREADS == G2P_THREADS,
+              "the substep kernel runs every phase with one CTA shape");
+
+// One substep of the default path in one cooperative launch of persistent
+// CTAs (at most as many as fit on the GPU at once, so every CTA runs to each
+// barrier): the tile allocation chunks over the CTAs (k_tile_alloc), then the
+// bucketing of every slot with the start of the substep (k_tile_scatter),
+// then P2G over the listed tiles with two tiles at a time per CTA, one per
+// 128-thread group (k_p2g_gather), then the grid update and G2P over the
+// same list (k_g2p_tile), with a grid barrier between phases.  The phases
+// run the four kernels' device functions, so the two forms are
+// bit-identical.  Shared memory is one dynamic buffer: the two P2G stages in
+// that phase, the G2P arrays in the next.
+template <bool SCENES, int CAP>
+__global__ void __launch_bounds__(SUBSTEP_THREADS, CAP == STAGE_CAP ? 2 : 3) k_substep(Ctx c0)
+{
+    extern __shared__ __align__(16) unsigned char dsm[];
+    for (uint32_t b = blockIdx.x; b < c0.alloc_chunks; b += gridDim.x) alloc_chunk(c0, b);
+    if (!grid_barrier(c0, 0u)) return;
+    scatter_quads(c0, blockIdx.x * SUBSTEP_THREADS + (threadIdx.x & ~31u), gridDim.x * SUBSTEP_THREADS);
+    if (!grid_barrier(c0, 1u)) return;
+    p2g_tiles<SCENES, CAP, 2>(c0, reinterpret_cast<Stage<CAP> *>(dsm));
+    if (!grid_barrier(c0, 2u)) return;
+    g2p_tiles<SCENES, false>(c0, *reinterpret_cast<G2PShared *>(dsm));
+}
+
+size_t p2g_shared_bytes(int cap)
+{
+    return cap == STAGE_CAP_NARROW ? sizeof(Stage<STAGE_CAP_NARROW>) : sizeof(Stage<STAGE_CAP>);
+}
+
+size_t substep_shared_bytes(int cap) { return std::max(2 * p2g_shared_bytes(cap), sizeof(G2PShared)); }
 
 // The start of a substep of the fixed-point path (k_tile_alloc starts those
 // of the default path): begin_substep for every scene.
@@ -3104,8 +3313,14 @@ __global__ void k_probe_deformation(const float4 *F, const float4 *C, float dt, 
     substeps[i] = t.substeps;
 }
 
-template __global__ void k_p2g_gather<false>(Ctx);
-template __global__ void k_p2g_gather<true>(Ctx);
+template __global__ void k_p2g_gather<false, STAGE_CAP>(Ctx);
+template __global__ void k_p2g_gather<true, STAGE_CAP>(Ctx);
+template __global__ void k_p2g_gather<false, STAGE_CAP_NARROW>(Ctx);
+template __global__ void k_p2g_gather<true, STAGE_CAP_NARROW>(Ctx);
+template __global__ void k_substep<false, STAGE_CAP>(Ctx);
+template __global__ void k_substep<true, STAGE_CAP>(Ctx);
+template __global__ void k_substep<false, STAGE_CAP_NARROW>(Ctx);
+template __global__ void k_substep<true, STAGE_CAP_NARROW>(Ctx);
 template __global__ void k_g2p_tile<false, false>(Ctx);
 template __global__ void k_g2p_tile<false, true>(Ctx);
 template __global__ void k_g2p_tile<true, false>(Ctx);

@@ -116,6 +116,12 @@ struct Ctx {
     const uint32_t *topology;     // fracture CSR: offsets[n + 1], then bond indices
     const uint32_t *endpoints;    // original indices with at least one fracture bond
     uint32_t n_endpoints;
+    // k_substep's grid barriers: how long a CTA waits for the others, and a
+    // CTA that leaves before the first barrier without arriving (0xffffffff:
+    // none; set only to exercise the wait limit)
+    unsigned long long barrier_limit_ns;
+    uint32_t barrier_skip;
+    uint32_t alloc_chunks;  // allocation chunks of 1024 tiles over all scenes
 };
 
 constexpr int SCAN_THREADS = 512;
@@ -132,7 +138,8 @@ constexpr int RING_X = TILE_X + 2;
 constexpr int RING_Y = TILE_Y + 2;
 constexpr int RING_NODES = RING_X * RING_Y;
 constexpr int TILE_CELLS = TILE_X * TILE_Y;
-constexpr int STAGE_CAP = 640;  // particles staged in shared memory at once
+constexpr int STAGE_CAP = 640;         // particles of a tile staged in shared memory at once (default variant)
+constexpr int STAGE_CAP_NARROW = 384;  // the narrow-stage variant (smaller stages, more tiles in flight)
 constexpr int ACC_WORDS = 11;   // solid m,px,py | water m,px,py,V | oil m,px,py,V
 constexpr uint32_t REC_FAILED = 1u << 16;  // the record's prepareParticle failed
 constexpr int VOL_X = RING_X + 2;          // ring nodes and their neighbours
@@ -157,6 +164,10 @@ constexpr int COUNTER_RUNS = 12;         // the scene takes part in the substep 
 constexpr uint32_t STOP_NONE = 0xffffffffu;
 constexpr int SCENE_WORDS = 64;  // per scene: status [0, 32), counters [32, 64)
 constexpr int WORK_ACTIVE = 0;   // work[0], work[1]: tiles listed for the substeps from buffer 0 / 1
+constexpr int WORK_BARRIER = 2;  // work[2]: arrivals at the substep kernel's grid barrier, work[3]: its generation
+constexpr int WORK_ABORT = 4;    // work[4]: non-zero once a barrier wait of the substep kernel ran out
+constexpr int WORK_WORDS = 8;
+constexpr int SUBSTEP_THREADS = 256;  // k_substep: one CTA shape for all four phases
 
 __global__ void k_count(Ctx c);
 __global__ void k_scan_reduce(Ctx c, uint32_t n_chunks);
@@ -167,9 +178,18 @@ __global__ void k_stable_rank(Ctx c);
 __global__ void k_tile_count(Ctx c);
 __global__ void k_tile_alloc(Ctx c);
 __global__ void k_tile_scatter(Ctx c);
-// SCENES: the solver holds several scenes
-template <bool SCENES>
+// SCENES: the solver holds several scenes; CAP: particles staged at once
+template <bool SCENES, int CAP>
 __global__ void k_p2g_gather(Ctx c);
+// The whole substep of the default path in one cooperative launch: tile
+// allocation, bucketing, P2G and G2P, separated by grid barriers whose waits
+// give up after Ctx::barrier_limit_ns (then ERROR_BARRIER is raised in every
+// scene and the launch returns).
+template <bool SCENES, int CAP>
+__global__ void k_substep(Ctx c);
+// dynamic shared memory of k_p2g_gather and k_substep for stage capacity cap
+size_t p2g_shared_bytes(int cap);
+size_t substep_shared_bytes(int cap);
 // BODIES: the solver holds bonded-triangle bodies or fracture bonds
 template <bool SCENES, bool BODIES>
 __global__ void k_g2p_tile(Ctx c);

@@ -137,7 +137,17 @@ struct mpm_solver {
     float2 *body_vel = nullptr;
     uint32_t *bonds = nullptr, *topology = nullptr, *endpoints = nullptr;
     uint32_t n_endpoints = 0, fracture_particles = 0, fracture_incidence = 0;
-    unsigned p2g_ctas = 1, g2p_ctas = 1;  // persistent grids of the default path
+    unsigned p2g_ctas = 1, g2p_ctas = 1;  // persistent grids of the default path's P2G and G2P kernels
+    // the default path's substep variant: one cooperative launch (k_substep)
+    // or four launches, the P2G stage capacity, k_substep's persistent grid
+    // and the most CTAs of it that fit on the GPU at once
+    bool fused = true;
+    int stage_cap = STAGE_CAP;
+    unsigned substep_ctas = 1, substep_max_ctas = 1;
+    // k_substep's barrier waits: the limit, and a CTA that leaves without
+    // arriving (tests of the limit only)
+    unsigned long long barrier_limit_ns = 1000000000ull;
+    uint32_t barrier_skip = 0xffffffffu;
 
     mpm_drag drag{};
     bool drag_active = false;
@@ -244,6 +254,9 @@ Ctx make_ctx(mpm_solver *s, int parity)
     c.topology = s->topology;
     c.endpoints = s->endpoints;
     c.n_endpoints = s->n_endpoints;
+    c.barrier_limit_ns = s->barrier_limit_ns;
+    c.barrier_skip = s->barrier_skip;
+    c.alloc_chunks = s->alloc_ctas;
     return c;
 }
 
@@ -254,11 +267,11 @@ constexpr unsigned PARTICLE_THREADS = 256;
 // Kernel slots of the profiled substep (mpm_profile_substeps).
 enum KernelSlot {
     K_TILE_COUNT, K_TILE_ALLOC, K_TILE_SCATTER, K_P2G_GATHER, K_G2P_TILE, K_PREPARE_SCATTER,
-    K_FIXED_DECODE, K_GRID_UPDATE, K_G2P, K_SUBSTEP_BEGIN, K_END_BATCH, K_SLOTS
+    K_FIXED_DECODE, K_GRID_UPDATE, K_G2P, K_SUBSTEP_BEGIN, K_END_BATCH, K_SUBSTEP, K_SLOTS
 };
 const char *const KERNEL_NAMES[K_SLOTS] = {
     "k_tile_count", "k_tile_alloc", "k_tile_scatter", "k_p2g_gather", "k_g2p_tile", "k_prepare_scatter",
-    "k_fixed_decode", "k_grid_update", "k_g2p", "k_substep_begin", "k_end_batch"};
+    "k_fixed_decode", "k_grid_update", "k_g2p", "k_substep_begin", "k_end_batch", "k_substep"};
 
 // When set, an event is recorded after every kernel launch so that the
 // kernels of a substep can be timed one by one.  The profiled substeps are
@@ -335,21 +348,93 @@ void enqueue_bodies(mpm_solver *s, const Ctx &c)
     if (s->gather() && s->n_tracked) k_body_finish<<<blocks_for(s->n_tracked, 64), 64, 0, s->stream>>>(c);
 }
 
+// The k_substep instantiation for the scene count and stage capacity.
+const void *substep_kernel(bool scenes, int cap)
+{
+    if (cap == STAGE_CAP_NARROW)
+        return scenes ? (const void *)k_substep<true, STAGE_CAP_NARROW> : (const void *)k_substep<false, STAGE_CAP_NARROW>;
+    return scenes ? (const void *)k_substep<true, STAGE_CAP> : (const void *)k_substep<false, STAGE_CAP>;
+}
+
+const void *p2g_kernel(bool scenes, int cap)
+{
+    if (cap == STAGE_CAP_NARROW)
+        return scenes ? (const void *)k_p2g_gather<true, STAGE_CAP_NARROW> : (const void *)k_p2g_gather<false, STAGE_CAP_NARROW>;
+    return scenes ? (const void *)k_p2g_gather<true, STAGE_CAP> : (const void *)k_p2g_gather<false, STAGE_CAP>;
+}
+
+// Whether the substeps of this solver run as one k_substep launch each:
+// the default path without bonded bodies or fracture bonds (their passes
+// run between and after P2G and G2P), when that variant is chosen.
+bool runs_fused(const mpm_solver *s) { return s->gather() && s->fused && s->n_tracked == 0 && s->n_bodies == 0; }
+
+// Enqueues k_substep as a cooperative launch (every CTA resident at once).
+cudaError_t launch_substep(mpm_solver *s, const Ctx &c)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(s->substep_ctas);
+    cfg.blockDim = dim3(SUBSTEP_THREADS);
+    cfg.dynamicSmemBytes = substep_shared_bytes(s->stage_cap);
+    cfg.stream = s->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    void *args[] = {const_cast<Ctx *>(&c)};
+    return cudaLaunchKernelExC(&cfg, substep_kernel(s->n_scenes > 1, s->stage_cap), args);
+}
+
+// Shared-memory limits of the stage variants (set once per process and
+// device; the attributes are per function).
+cudaError_t configure_variant_kernels()
+{
+    const int caps[2] = {STAGE_CAP, STAGE_CAP_NARROW};
+    for (int cap : caps) {
+        for (int scenes = 0; scenes < 2; ++scenes) {
+            const void *fns[2] = {p2g_kernel(scenes != 0, cap), substep_kernel(scenes != 0, cap)};
+            const size_t bytes[2] = {p2g_shared_bytes(cap), substep_shared_bytes(cap)};
+            for (int k = 0; k < 2; ++k) {
+                cudaError_t e = cudaFuncSetAttribute(fns[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes[k]);
+                if (e == cudaSuccess) e = cudaFuncSetAttribute(fns[k], cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+                if (e != cudaSuccess) return e;
+            }
+        }
+    }
+    return cudaSuccess;
+}
+
+// CTAs per SM of the P2G kernel and of k_substep for stage capacity `cap`.
+cudaError_t variant_occupancy(int cap, int *per_sm_p2g, int *per_sm_substep)
+{
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm_p2g, p2g_kernel(false, cap), TILE_CELLS,
+                                                                  p2g_shared_bytes(cap));
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm_substep, substep_kernel(false, cap), SUBSTEP_THREADS,
+                                                          substep_shared_bytes(cap));
+    return e;
+}
+
 // One full substep from buffer `parity` into 1 - parity.
 void enqueue_substep(mpm_solver *s, int parity)
 {
     const Ctx c = make_ctx(s, parity);
     const unsigned pb = blocks_for(s->n, PARTICLE_THREADS);
     const dim3 tiles(s->tiles_x, s->tiles_y);
-    if (s->gather()) {
+    if (runs_fused(s)) {
+        const cudaError_t e = launch_substep(s, c);
+        if (e != cudaSuccess && g_recorder && g_recorder->error == cudaSuccess) g_recorder->error = e;
+        mark(K_SUBSTEP);
+    } else if (s->gather()) {
         k_tile_alloc<<<s->alloc_ctas, ALLOC_THREADS, 0, s->stream>>>(c);
         mark(K_TILE_ALLOC);
         k_tile_scatter<<<blocks_for((s->n + 3) / 4, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c);
         mark(K_TILE_SCATTER);
-        if (s->n_scenes > 1)
-            k_p2g_gather<true><<<s->p2g_ctas, TILE_CELLS, 0, s->stream>>>(c);
-        else
-            k_p2g_gather<false><<<s->p2g_ctas, TILE_CELLS, 0, s->stream>>>(c);
+        {
+            void *args[] = {const_cast<Ctx *>(&c)};
+            cudaLaunchKernel(p2g_kernel(s->n_scenes > 1, s->stage_cap), dim3(s->p2g_ctas), dim3(TILE_CELLS), args,
+                             p2g_shared_bytes(s->stage_cap), s->stream);
+        }
         mark(K_P2G_GATHER);
         if (s->n_bodies) k_triangle_field<<<tiles, TILE_NODES, 0, s->stream>>>(c);
         if (s->n_scenes > 1)
@@ -809,7 +894,7 @@ int create_impl(const mpm_config *configs, uint32_t n_scenes, const uint32_t *co
     const size_t cap = s->capacity;
     ALLOC(s->d_params, n_scenes);
     ALLOC(s->dyn, (size_t)n_scenes * SCENE_WORDS);
-    ALLOC(s->work, 4);
+    ALLOC(s->work, WORK_WORDS);
     ALLOC(s->scene_p_base, (size_t)n_scenes + 1);
     s->d_status = s->dyn;  // scene 0
     s->d_counters = s->dyn + 32;
@@ -879,19 +964,17 @@ int create_impl(const mpm_config *configs, uint32_t n_scenes, const uint32_t *co
         if (cudaMemsetAsync(s->tile_info, 0xff, n_tiles * sizeof(uint2), s->stream) != cudaSuccess ||
             cudaMemsetAsync(s->tile_count, 0, n_tiles * sizeof(uint32_t), s->stream) != cudaSuccess)
             return fail(set_error(MPM_ERR_CUDA, "cudaMemset failed"));
-        int sms = 0, per_sm_p2g = 0, per_sm_g2p = 0;
-        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device) != cudaSuccess ||
-            cudaFuncSetAttribute(k_p2g_gather<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100) !=
-                cudaSuccess ||
-            cudaFuncSetAttribute(k_p2g_gather<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100) !=
-                cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_p2g, k_p2g_gather<false>, TILE_CELLS, 0) !=
-                cudaSuccess ||
+        int sms = 0, per_sm_p2g = 0, per_sm_g2p = 0, per_sm_substep = 0;
+        if (configure_variant_kernels() != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device) != cudaSuccess ||
+            variant_occupancy(s->stage_cap, &per_sm_p2g, &per_sm_substep) != cudaSuccess ||
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_g2p, k_g2p_tile<false, false>, G2P_THREADS, 0) !=
                 cudaSuccess)
             return fail(set_error(MPM_ERR_CUDA, "occupancy query failed"));
         s->p2g_ctas = (unsigned)std::max<size_t>(1, std::min<size_t>(n_tiles, (size_t)sms * std::max(1, per_sm_p2g)));
         s->g2p_ctas = (unsigned)std::max<size_t>(1, std::min<size_t>(n_tiles, (size_t)sms * std::max(1, per_sm_g2p)));
+        s->substep_max_ctas = (unsigned)std::max(1, sms * per_sm_substep);
+        s->substep_ctas = s->substep_max_ctas;
     }
     if (c.p2g_mode == MPM_P2G_FIXED_POINT) {
         ALLOC(s->p2g_solid, s->node_count);
@@ -963,7 +1046,7 @@ int create_impl(const mpm_config *configs, uint32_t n_scenes, const uint32_t *co
             dyn[(size_t)k * SCENE_WORDS + 1] = 0xffffffffu;
             dyn[(size_t)k * SCENE_WORDS + 32 + COUNTER_STAMP] = 1u;
         }
-        const uint32_t zeros[4] = {0, 0, 0, 0};
+        const uint32_t zeros[WORK_WORDS] = {};
         if (cudaMemcpy(s->dyn, dyn.data(), dyn.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemcpy(s->work, zeros, sizeof zeros, cudaMemcpyHostToDevice) != cudaSuccess)
             return fail(set_error(MPM_ERR_CUDA, "status upload failed"));
@@ -1037,6 +1120,43 @@ int profile_run(mpm_solver *s, uint32_t step_count, bool guarded, double *kernel
     return MPM_OK;
 }
 
+// Runs `step_count` real substeps with the uploaded parameters as one graph
+// (prologue, substeps, epilogue; no events between kernels) and returns its
+// device milliseconds (events around the graph launch).
+int timed_run(mpm_solver *s, uint32_t step_count, bool guarded, double *ms)
+{
+    const Ctx c0 = make_ctx(s, s->cur);
+    CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    k_begin_batch<<<blocks_for(s->n_scenes, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c0, guarded ? 1u : 0u);
+    if (s->gather() && s->n > 0) enqueue_tile_count(s, c0);
+    int parity = s->cur;
+    for (uint32_t k = 0; k < step_count; ++k) {
+        enqueue_substep(s, parity);
+        parity = 1 - parity;
+    }
+    if (s->n > 0) enqueue_end_batch(s, parity, step_count, guarded);
+    cudaError_t e = cudaGetLastError();
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t end = cudaStreamEndCapture(s->stream, &graph);
+    if (e == cudaSuccess) e = end;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e == cudaSuccess) e = cudaEventRecord(s->batch_start, s->stream);
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, s->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(s->batch_stop, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    float t = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, s->batch_start, s->batch_stop);
+    if (e == cudaSuccess) {
+        s->cur = parity;
+        s->substeps_since_begin = step_count;
+        *ms = t;
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return set_error(MPM_ERR_CUDA, "timed substeps failed: %s", cudaGetErrorString(e));
+    return MPM_OK;
+}
 
 int run_batch(mpm_solver *s, uint32_t step_count, bool guarded);
 
@@ -1318,6 +1438,58 @@ int mpm_get_launch_shape(mpm_solver *s, uint32_t *p2g_ctas, uint32_t *g2p_ctas, 
     return MPM_OK;
 }
 
+int mpm_set_substep_variant(mpm_solver *s, uint32_t fused, uint32_t stage_capacity, uint32_t substep_ctas)
+{
+    g_last_error.clear();
+    forget_readback(s);
+    if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
+    if (!s->gather()) return set_error(MPM_ERR_STATE, "substep variants apply to the default P2G path");
+    if (fused > 1u) return set_error(MPM_ERR_INVALID_ARGUMENT, "fused must be 0 or 1");
+    if (stage_capacity != 0u && stage_capacity != (uint32_t)STAGE_CAP && stage_capacity != (uint32_t)STAGE_CAP_NARROW)
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "stage capacity must be %d or %d", STAGE_CAP, STAGE_CAP_NARROW);
+    CUDA_TRY(cudaSetDevice(s->device));
+    const int cap = stage_capacity ? (int)stage_capacity : s->stage_cap;
+    int sms = 0, per_sm_p2g = 1, per_sm_substep = 1;
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+    CUDA_TRY(variant_occupancy(cap, &per_sm_p2g, &per_sm_substep));
+    const unsigned most = (unsigned)std::max(1, sms * per_sm_substep);
+    if (substep_ctas > most)
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "substep_ctas %u exceeds the %u CTAs that fit on the GPU at once",
+                         substep_ctas, most);
+    s->fused = fused != 0u;
+    s->stage_cap = cap;
+    s->substep_max_ctas = most;
+    if (substep_ctas) s->substep_ctas = substep_ctas;
+    s->substep_ctas = std::min(s->substep_ctas, most);
+    drop_graphs(s);
+    return MPM_OK;
+}
+
+int mpm_get_substep_variant(mpm_solver *s, uint32_t *fused, uint32_t *stage_capacity, uint32_t *substep_ctas,
+                            uint32_t *max_substep_ctas)
+{
+    g_last_error.clear();
+    if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
+    if (fused) *fused = runs_fused(s) ? 1u : 0u;
+    if (stage_capacity) *stage_capacity = (uint32_t)s->stage_cap;
+    if (substep_ctas) *substep_ctas = s->substep_ctas;
+    if (max_substep_ctas) *max_substep_ctas = s->substep_max_ctas;
+    return MPM_OK;
+}
+
+int mpm_set_barrier_limit(mpm_solver *s, uint64_t limit_ns, uint32_t skip_cta)
+{
+    g_last_error.clear();
+    forget_readback(s);
+    if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
+    if (limit_ns < 1000u || limit_ns > 60000000000ull)
+        return set_error(MPM_ERR_INVALID_ARGUMENT, "the barrier limit must lie in [1 us, 60 s]");
+    s->barrier_limit_ns = limit_ns;
+    s->barrier_skip = skip_cta;
+    drop_graphs(s);
+    return MPM_OK;
+}
+
 int mpm_autotune(mpm_solver *s, uint32_t substeps, uint32_t *p2g_ctas, uint32_t *g2p_ctas, double *best_ms)
 {
     g_last_error.clear();
@@ -1381,58 +1553,93 @@ int mpm_autotune(mpm_solver *s, uint32_t substeps, uint32_t *p2g_ctas, uint32_t 
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(s->d_params, s->h_params, s->n_scenes * sizeof(StepParams), cudaMemcpyHostToDevice,
                             s->stream);
-    int sms = 0, per_sm_p2g = 1, per_sm_g2p = 1;
+    int sms = 0, per_sm_g2p = 1;
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
-    if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_p2g, k_p2g_gather<false>, TILE_CELLS, 0);
     if (e == cudaSuccess)
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_g2p, k_g2p_tile<false, false>, G2P_THREADS, 0);
     int rc = e == cudaSuccess ? MPM_OK : set_error(MPM_ERR_CUDA, "autotune set-up failed: %s", cudaGetErrorString(e));
     const bool guarded = s->h_params[0].cfl_enabled != 0u;
-    auto trial = [&](unsigned p, unsigned g, double &p_ms, double &g_ms) {
-        s->p2g_ctas = p;
-        s->g2p_ctas = g;
+    // one candidate: every setting of the variant, timed over `substeps`
+    // real substeps from the saved state (the whole graph, no events between
+    // kernels, so the four-launch and one-launch forms compare fairly)
+    struct Candidate {
+        bool fused;
+        int cap;
+        unsigned p2g, g2p, substep;
+    };
+    auto trial = [&](const Candidate &v, double &ms) {
+        s->fused = v.fused;
+        s->stage_cap = v.cap;
+        s->p2g_ctas = v.p2g;
+        s->g2p_ctas = v.g2p;
+        s->substep_ctas = v.substep;
         const cudaError_t r = restore();
         if (r != cudaSuccess) return set_error(MPM_ERR_CUDA, "autotune restore failed: %s", cudaGetErrorString(r));
-        double ms[K_SLOTS];
-        uint32_t launches[K_SLOTS];
-        const int prc = profile_run(s, substeps, guarded, ms, launches);
-        p_ms = ms[K_P2G_GATHER];
-        g_ms = ms[K_G2P_TILE];
-        return prc;
+        return timed_run(s, substeps, guarded, &ms);
     };
-    const unsigned p0 = s->p2g_ctas, g0 = s->g2p_ctas;
-    unsigned best_p = p0, best_g = g0;
-    double best_p_ms = 1e300, best_g_ms = 1e300;
-    // P2G and G2P are separate launches, tuned one after the other: persistent
-    // grids of 1 .. (occupancy limit) CTAs per SM (a grid of one CTA per tile
-    // would pay for every tile of every scene in substeps that list few)
+    const Candidate v0{s->fused, s->stage_cap, s->p2g_ctas, s->g2p_ctas, s->substep_ctas};
+    Candidate best = v0;
+    double best_ms_total = 1e300;
+    auto consider = [&](const Candidate &v) {
+        double ms = 0.0;
+        if (rc == MPM_OK) rc = trial(v, ms);
+        if (rc == MPM_OK && ms < best_ms_total) best_ms_total = ms, best = v;
+    };
+    // the stage variants; for each, the one-launch form over persistent grids
+    // of 1 .. (co-resident limit) CTAs per SM, and the four-launch form over
+    // its P2G grids, then its G2P grids with the best P2G (a grid of one CTA
+    // per tile is not a candidate: it pays for every tile of every scene in
+    // substeps that list few)
     const unsigned tiles = std::max(1u, s->n_tiles_total);
-    for (int k = 1; rc == MPM_OK && k <= std::max(1, per_sm_p2g); ++k) {
-        const unsigned p = std::min(tiles, (unsigned)(sms * k));
-        double pm = 0, gm = 0;
-        rc = trial(p, g0, pm, gm);
-        if (rc == MPM_OK && pm < best_p_ms) best_p_ms = pm, best_p = p;
+    const bool can_fuse = s->n_tracked == 0 && s->n_bodies == 0;
+    const int caps[2] = {STAGE_CAP, STAGE_CAP_NARROW};
+    for (int cap : caps) {
+        int per_sm_p2g = 1, per_sm_substep = 1;
+        if (rc == MPM_OK) {
+            const cudaError_t q = variant_occupancy(cap, &per_sm_p2g, &per_sm_substep);
+            if (q != cudaSuccess) rc = set_error(MPM_ERR_CUDA, "autotune occupancy failed: %s", cudaGetErrorString(q));
+        }
+        for (int k = 1; can_fuse && rc == MPM_OK && k <= per_sm_substep; ++k)
+            consider(Candidate{true, cap, v0.p2g, v0.g2p, (unsigned)(sms * k)});
+        Candidate four{false, cap, v0.p2g, v0.g2p, v0.substep};
+        double four_ms = 1e300;
+        for (int k = 1; rc == MPM_OK && k <= std::max(1, per_sm_p2g); ++k) {
+            const Candidate v{false, cap, std::min(tiles, (unsigned)(sms * k)), v0.g2p, v0.substep};
+            double ms = 0.0;
+            rc = trial(v, ms);
+            if (rc == MPM_OK && ms < four_ms) four_ms = ms, four = v;
+        }
+        for (int k = 1; rc == MPM_OK && k <= std::max(1, per_sm_g2p); ++k) {
+            const Candidate v{false, cap, four.p2g, std::min(tiles, (unsigned)(sms * k)), v0.substep};
+            double ms = 0.0;
+            rc = trial(v, ms);
+            if (rc == MPM_OK && ms < four_ms) four_ms = ms, four = v;
+        }
+        if (rc == MPM_OK && four_ms < best_ms_total) best_ms_total = four_ms, best = four;
     }
-    for (int k = 1; rc == MPM_OK && k <= std::max(1, per_sm_g2p); ++k) {
-        const unsigned g = std::min(tiles, (unsigned)(sms * k));
-        double pm = 0, gm = 0;
-        rc = trial(best_p, g, pm, gm);
-        if (rc == MPM_OK && gm < best_g_ms) best_g_ms = gm, best_g = g;
+    s->substep_max_ctas = 1;
+    {
+        int per_sm_p2g = 1, per_sm_substep = 1;
+        if (variant_occupancy(rc == MPM_OK ? best.cap : v0.cap, &per_sm_p2g, &per_sm_substep) == cudaSuccess)
+            s->substep_max_ctas = (unsigned)std::max(1, sms * per_sm_substep);
     }
     const cudaError_t r = restore();
     if (rc == MPM_OK && r != cudaSuccess) rc = set_error(MPM_ERR_CUDA, "autotune restore failed: %s", cudaGetErrorString(r));
     void *ptrs[] = {save.pos, save.vel, save.C, save.F, save.pvol, save.damage, save.vol, save.mat, save.orig, slots};
     for (void *p : ptrs)
         if (p) cudaFree(p);
-    s->p2g_ctas = rc == MPM_OK ? best_p : p0;
-    s->g2p_ctas = rc == MPM_OK ? best_g : g0;
+    const Candidate &chosen = rc == MPM_OK ? best : v0;
+    s->fused = chosen.fused;
+    s->stage_cap = chosen.cap;
+    s->p2g_ctas = chosen.p2g;
+    s->g2p_ctas = chosen.g2p;
+    s->substep_ctas = chosen.substep;
     drop_graphs(s);
     s->batch_timed = false;  // the batch events now time the trials
     if (rc != MPM_OK) return rc;
-    if (p2g_ctas) *p2g_ctas = best_p;
-    if (g2p_ctas) *g2p_ctas = best_g;
-    if (best_ms) *best_ms = (best_p_ms + best_g_ms) / substeps;
+    if (p2g_ctas) *p2g_ctas = best.p2g;
+    if (g2p_ctas) *g2p_ctas = best.g2p;
+    if (best_ms) *best_ms = best_ms_total / substeps;
     return MPM_OK;
 }
 

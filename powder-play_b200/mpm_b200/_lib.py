@@ -27,6 +27,7 @@ EXPORTED_SYMBOLS = (
     "mpmb_create", "mpmb_step_batch", "mpmb_read_compact", "mpmb_scene_count",
     "mpm_allocated_particle_count", "mpm_append_particles", "mpm_remove_particles_in_outlet", "mpm_pick",
     "mpm_clone_range", "mpm_set_launch_shape", "mpm_get_launch_shape", "mpm_autotune",
+    "mpm_set_substep_variant", "mpm_get_substep_variant", "mpm_set_barrier_limit",
     "mpm_gather_surface_occupancy", "mpm_surface_field_device",
     "mpma_create", "mpma_set_parameters", "mpma_get_parameters", "mpma_set_velocities", "mpma_forward",
     "mpma_backward", "mpma_read_positions", "mpma_last_ms", "mpma_destroy",
@@ -143,6 +144,12 @@ def load_library(path: str = LIBRARY_PATH) -> ctypes.CDLL:
     lib.mpm_get_launch_shape.restype = i32
     lib.mpm_autotune.argtypes = [vp, u32, P(u32), P(u32), P(ctypes.c_double)]
     lib.mpm_autotune.restype = i32
+    lib.mpm_set_substep_variant.argtypes = [vp, u32, u32, u32]
+    lib.mpm_set_substep_variant.restype = i32
+    lib.mpm_get_substep_variant.argtypes = [vp, P(u32), P(u32), P(u32), P(u32)]
+    lib.mpm_get_substep_variant.restype = i32
+    lib.mpm_set_barrier_limit.argtypes = [vp, ctypes.c_uint64, u32]
+    lib.mpm_set_barrier_limit.restype = i32
     lib.mpma_create.argtypes = [vp, u32, vp, vp, vp, P(vp)]
     lib.mpma_create.restype = i32
     for name in ("mpma_set_parameters", "mpma_get_parameters", "mpma_set_velocities", "mpma_read_positions"):

@@ -33,6 +33,7 @@ _FLAG_DETAILS = (
     (16384, "particle exceeded the enforced CFL wave-speed or velocity bound"),
     (32768, "invalid persistent solid-fracture bond state"),
     (65536, "experimental fixed-point P2G contribution or accumulator overflow"),
+    (1 << 20, "a grid barrier wait of the substep kernel ran out (launch abandoned; particle state undefined)"),
 )
 
 

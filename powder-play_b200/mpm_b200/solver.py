@@ -809,7 +809,33 @@ class MpmMlsGpuSolver:
         p, g, ms = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_double()
         _check(self._lib.mpm_autotune(self._handle, int(substeps), ctypes.byref(p), ctypes.byref(g), ctypes.byref(ms)),
                "autotune failed")
-        return {"p2gCtas": int(p.value), "g2pCtas": int(g.value), "transferMsPerSubstep": float(ms.value)}
+        return dict(self.substep_variant(), p2gCtas=int(p.value), g2pCtas=int(g.value),
+                    transferMsPerSubstep=float(ms.value))
+
+    def substep_variant(self) -> dict:
+        """How the default path runs a substep: `fused` (one cooperative launch
+        of persistent CTAs, else four launches), the P2G stage capacity, the
+        one-launch form's persistent grid and its co-resident limit."""
+        f, cap, n, most = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        _check(self._lib.mpm_get_substep_variant(self._handle, ctypes.byref(f), ctypes.byref(cap), ctypes.byref(n),
+                                                 ctypes.byref(most)), "substep variant read failed")
+        return {"fused": bool(f.value), "stageCapacity": int(cap.value), "substepCtas": int(n.value),
+                "maxSubstepCtas": int(most.value)}
+
+    def set_substep_variant(self, fused: bool = True, stage_capacity: int = 0, substep_ctas: int = 0) -> None:
+        """Chooses the substep variant (mpm_set_substep_variant; 0 keeps the
+        stage capacity or the grid).  Results do not depend on `fused` or the
+        grid."""
+        self._assert_active()
+        _check(self._lib.mpm_set_substep_variant(self._handle, 1 if fused else 0, int(stage_capacity),
+                                                 int(substep_ctas)), "substep variant change failed")
+
+    def set_barrier_limit(self, limit_ns: int, skip_cta: int = 0xFFFFFFFF) -> None:
+        """The one-launch substep's barrier wait limit in nanoseconds; `skip_cta`
+        makes one CTA leave without arriving (a test of the limit)."""
+        self._assert_active()
+        _check(self._lib.mpm_set_barrier_limit(self._handle, int(limit_ns), int(skip_cta)),
+               "barrier limit change failed")
 
     def dispose(self) -> None:
         if self._disposed:

@@ -1,0 +1,156 @@
+"""The default path's substep variants and the barrier wait limit.
+
+A substep runs either as ONE cooperative launch of persistent CTAs
+(k_substep: tile allocation, bucketing, P2G, grid update + G2P, with grid
+barriers between the phases) or as four launches of the same device code, so
+the two forms must agree bit for bit, whatever the persistent grid.  The
+narrow P2G stage (384 particles) changes only how a crowded tile is cut into
+chunks, so it must stay within the oracle tolerances.  A CTA that leaves
+before the first barrier without arriving makes the others' waits run out:
+the launch must then report status flag 1 << 20 and return instead of
+hanging, and the solver must step normally once its particles are written
+back.
+"""
+import numpy as np
+import pytest
+
+from mpm_b200 import create_mpm_batched_gpu_solver, create_mpm_mls_gpu_solver
+from mpm_b200.errors import decode_numerical_error, is_recoverable_cfl_error
+from mpm_b200.layout import ParticleArrays
+from mpm_b200.scenes import (BATCHED_TANK_GRAVITY, DAM_BREAK_GRAVITY, SI_TANK_GRAVITY, create_batched_tank_scenes,
+                             create_dam_break_scene, create_si_tank_scene)
+from oracle import OracleState
+
+pytestmark = pytest.mark.gpu
+
+STATE_WORDS = slice(0, 12)  # x, v, C, F of the packed 20-word record
+ERROR_BARRIER = 1 << 20
+SMALL_DAM = {"cellsX": 256, "cellsY": 512, "cellSize": 10}
+
+
+def _bits(packed):
+    return np.ascontiguousarray(packed[:, STATE_WORDS]).view(np.uint32)
+
+
+def _step(particles, config, variant, steps, dt, gravity):
+    solver = create_mpm_mls_gpu_solver(particles, config)
+    try:
+        solver.set_substep_variant(**variant)
+        chosen = solver.substep_variant()
+        solver.step_batch(steps, dt, gravity)
+        status = solver._read_compact()[2]
+        packed, _ = solver.read_particles_packed()
+    finally:
+        solver.dispose()
+    return packed, status, chosen
+
+
+def test_one_launch_and_four_launches_agree_bitwise_on_a_dam_break():
+    p, config = create_dam_break_scene(particles_per_phase=20_000, columns=200, grid=SMALL_DAM)
+    dt = 1.0 / 1200.0
+    runs = {}
+    for name, variant in {"one": dict(fused=True, stage_capacity=640),
+                          "one_148": dict(fused=True, stage_capacity=640, substep_ctas=148),
+                          "four": dict(fused=False, stage_capacity=640),
+                          "one_narrow": dict(fused=True, stage_capacity=384),
+                          "four_narrow": dict(fused=False, stage_capacity=384)}.items():
+        packed, status, chosen = _step(p, config, variant, 24, dt, DAM_BREAK_GRAVITY)
+        assert status[0] == 0, name
+        assert chosen["fused"] == variant["fused"] and chosen["stageCapacity"] == variant["stage_capacity"]
+        runs[name] = packed
+    assert np.array_equal(_bits(runs["one"]), _bits(runs["four"]))
+    assert np.array_equal(_bits(runs["one"]), _bits(runs["one_148"]))
+    assert np.array_equal(_bits(runs["one_narrow"]), _bits(runs["four_narrow"]))
+    # both stage capacities agree within the oracle tolerances (position 1e-3 dx)
+    dx = config["grid"]["cellSize"]
+    assert np.max(np.abs(runs["one"][:, 0:2].astype(np.float64) - runs["one_narrow"][:, 0:2])) <= 1e-3 * dx
+
+
+def _crowded_tank(per_side):
+    """The SI tank's water as a block of per_side^2 particles per cell over
+    12 x 12 cells: its tiles hold far more than one stage (the crowded path of
+    either capacity)."""
+    _, config = create_si_tank_scene(seed=1)
+    dx = config["grid"]["cellSize"]
+    spacing = dx / per_side
+    side = 12 * per_side
+    r, c = np.divmod(np.arange(side * side), side)
+    p = ParticleArrays.empty(side * side)
+    p.px[:] = 12 * dx + (c + 0.5) * spacing
+    p.py[:] = 12 * dx + (r + 0.5) * spacing
+    p.volume[:] = spacing * spacing
+    config = dict(config, particleMass=config["material"]["density"] * spacing * spacing,
+                  particleVolume=spacing * spacing)
+    return p, config
+
+
+@pytest.mark.parametrize("per_side", [6, 10])
+def test_crowded_tiles_match_the_oracle_in_every_variant(per_side):
+    p, config = _crowded_tank(per_side)
+    dt = 2e-5
+    steps = 6
+    dt32 = float(np.float32(dt))
+    ref = OracleState(p, dict(config, dt=dt32, gravity=SI_TANK_GRAVITY))
+    ref.run(dict(config, dt=dt32, gravity=SI_TANK_GRAVITY), steps)
+    dx = config["grid"]["cellSize"]
+    results = {}
+    for fused in (True, False):
+        for cap in (640, 384):
+            packed, status, _ = _step(p, config, dict(fused=fused, stage_capacity=cap), steps, dt, SI_TANK_GRAVITY)
+            assert status[0] == 0
+            assert np.max(np.abs(packed[:, 0:2].astype(np.float64) - ref.positions())) <= 1e-3 * dx
+            vel_err = np.abs(packed[:, 2:4].astype(np.float64) - ref.velocities()) / (1 + np.abs(ref.velocities()))
+            assert np.max(vel_err) <= 1e-3
+            results[(fused, cap)] = packed
+    for cap in (640, 384):
+        assert np.array_equal(_bits(results[(True, cap)]), _bits(results[(False, cap)]))
+
+
+def test_batched_scenes_agree_bitwise_in_one_launch_and_four():
+    scenes = create_batched_tank_scenes(7, seed=5, particles=(200, 4000), sides=(20, 128))
+    out = {}
+    for fused in (True, False):
+        batch = create_mpm_batched_gpu_solver(scenes)
+        try:
+            batch.set_substep_variant(fused=fused, stage_capacity=640)
+            assert batch.substep_variant()["fused"] == fused
+            dts = [2e-4 * (1 + 0.1 * k) for k in range(batch.scene_count)]
+            batch.step_batch([4 + (k % 3) for k in range(batch.scene_count)], dts, BATCHED_TANK_GRAVITY)
+            batch.step_batch([0 if k % 2 else 3 for k in range(batch.scene_count)], dts, BATCHED_TANK_GRAVITY)
+            assert all(e is None for e in batch.check_numerical_status())
+            out[fused] = [batch.read_particles_packed(k)[0] for k in range(batch.scene_count)]
+        finally:
+            batch.dispose()
+    for k, (a, b) in enumerate(zip(out[True], out[False])):
+        assert np.array_equal(_bits(a), _bits(b)), f"scene {k}"
+
+
+def test_a_barrier_wait_that_runs_out_reports_the_status_and_the_solver_recovers():
+    particles, config = create_si_tank_scene(seed=1)
+    dt = 2e-4
+    solver = create_mpm_mls_gpu_solver(particles, config)
+    try:
+        solver.set_substep_variant(fused=True)
+        assert solver.substep_variant()["fused"]
+        start, _ = solver.read_particles_packed()
+        # CTA 1 leaves before the first barrier: every other CTA's wait runs
+        # out after 2 ms, and the launch (and the batch's next one) returns
+        solver.set_barrier_limit(2_000_000, skip_cta=1)
+        solver.step_batch(3, dt, SI_TANK_GRAVITY)
+        _, _, status = solver._read_compact()
+        assert status[0] & ERROR_BARRIER
+        error = decode_numerical_error(status)
+        assert "grid barrier" in str(error) and not is_recoverable_cfl_error(error)
+        # the default limit, the status cleared and the particles written
+        # back: the solver steps exactly like a fresh one
+        solver.set_barrier_limit(1_000_000_000)
+        solver._clear_status()
+        solver.write_particles_packed(start)
+        solver.step_batch(5, dt, SI_TANK_GRAVITY)
+        assert solver._read_compact()[2][0] == 0
+        got, _ = solver.read_particles_packed()
+    finally:
+        solver.dispose()
+    fresh, status, _ = _step(particles, config, dict(fused=True), 5, dt, SI_TANK_GRAVITY)
+    assert status[0] == 0
+    assert np.array_equal(_bits(got), _bits(fresh))
