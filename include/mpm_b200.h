@@ -268,15 +268,20 @@ int mpm_autotune(mpm_solver *solver, uint32_t substeps, uint32_t *p2g_ctas, uint
  * bucketing, P2G, grid update + G2P, with grid barriers between them), 0 as
  * four launches; `stage_capacity` is the P2G stage (640 or 384 particles;
  * 0 keeps it); `substep_ctas` the one-launch form's persistent grid (0 keeps
- * it; at most the CTAs that fit on the GPU at once).  Solvers with bonded
- * bodies or fracture bonds always take four launches.  Results do not depend
- * on `fused` or the grids (the phases are the same device code); the stage
- * capacity changes only the rounding of tiles holding more particles than it.
+ * it; at most the CTAs that fit on the GPU at once); `liquid_kernels` 1 lets
+ * G2P run its instantiation compiled for water and oil only whenever every
+ * material of the solver is one of them (the default), 0 keeps the general
+ * one.  Solvers with bonded bodies or fracture bonds always take four
+ * launches and the general G2P.  Results do not depend on `fused`, the grids
+ * or `liquid_kernels` (the same arithmetic); the stage capacity changes only
+ * the rounding of tiles holding more particles than it.
  * mpm_get_substep_variant reports whether substeps run as one launch, the
- * capacity, the grid and its co-resident limit. */
-int mpm_set_substep_variant(mpm_solver *solver, uint32_t fused, uint32_t stage_capacity, uint32_t substep_ctas);
+ * capacity, the grid, its co-resident limit and whether the water-and-oil
+ * G2P runs. */
+int mpm_set_substep_variant(mpm_solver *solver, uint32_t fused, uint32_t stage_capacity, uint32_t substep_ctas,
+                            uint32_t liquid_kernels);
 int mpm_get_substep_variant(mpm_solver *solver, uint32_t *fused, uint32_t *stage_capacity, uint32_t *substep_ctas,
-                            uint32_t *max_substep_ctas);
+                            uint32_t *max_substep_ctas, uint32_t *liquid_kernels);
 
 /* The one-launch substep's grid-barrier waits give up after `limit_ns`
  * nanoseconds (default 1 s; 1 us .. 60 s): the CTA that gave up raises status

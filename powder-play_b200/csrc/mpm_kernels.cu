@@ -86,11 +86,33 @@ __device__ __forceinline__ bool make_stencil_fast(const StepParams &P, float2 po
 }
 
 
+// The liquid branch of prepareParticle's stress (shaders.ts:808-963): the
+// Tait pressure, or the legacy linear EOS when the exponent is 0.  Returns
+// false for invalid material parameters.
+__device__ __forceinline__ bool liquid_stress(const Material &m, float det, float tait_pow, float4 &s)
+{
+    if (!finite_f(m.density) || m.density <= 0.0f || !finite_f(m.lambda) || m.lambda <= 0.0f || !finite_f(m.param) ||
+        m.param < 0.0f)
+        return false;
+    if (m.param > 0.0f) {
+        const float pw = tait_pow >= 0.0f ? tait_pow : pow_wgsl(__fdiv_rn(1.0f, det), m.param);
+        const float pressure = m.lambda * (pw - 1.0f);
+        const float stress = -det * pressure;
+        s = make_float4(stress, 0.f, 0.f, stress);
+    } else {
+        const float pressure = m.lambda * fminf(det - 1.0f, 0.0f);
+        s = make_float4(pressure, 0.f, 0.f, pressure);
+    }
+    return true;
+}
+
 // prepareParticle: shaders.ts:808-963.  Computes the per-particle stress
 // cache (affine momentum A = m C + (-dt V 4/dx^2) P F^T), mass and current
 // liquid area from the particle's state.  Returns 0, or the reference's
 // status flags for the failure with `indexed` telling whether the reference
-// also reports the particle index.
+// also reports the particle index.  LIQ: every material of the solver is
+// water or oil, so the other models' branches are compiled out.
+template <bool LIQ = false>
 __device__ __forceinline__ uint32_t prepare_core(const StepParams &P, const Material &m, float4 F, float volume,
                                                  float damage, float pvol, float4 C, float4 &affine, float &mass,
                                                  float &vliq, bool &indexed, float tait_pow = -1.0f)
@@ -103,66 +125,59 @@ __device__ __forceinline__ uint32_t prepare_core(const StepParams &P, const Mate
     }
     float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
     const uint32_t bad = ERROR_P2G | ERROR_P2G_INVALID_MATERIAL;
-    if (m.model == MODEL_NEO_HOOKEAN) {
-        if (!finite_f(damage) || damage < 0.0f || damage > 1.0f) return bad;
-        const float4 it = make_float4(F.w / det, -F.z / det, -F.y / det, F.x / det);
-        const float pressure = m.lambda * logf(det);
-        const float4 pk = make_float4(m.mu * (F.x - it.x) + pressure * it.x, m.mu * (F.y - it.y) + pressure * it.y,
-                                      m.mu * (F.z - it.z) + pressure * it.z, m.mu * (F.w - it.w) + pressure * it.w);
-        const float keep = 1.0f - fminf(fmaxf(damage, 0.0f), 1.0f);
-        s = make_float4((pk.x * F.x + pk.y * F.y) * keep, (pk.x * F.z + pk.y * F.w) * keep,
-                        (pk.z * F.x + pk.w * F.y) * keep, (pk.z * F.z + pk.w * F.w) * keep);
-    } else if (m.model == MODEL_SNOW || m.model == MODEL_FIXED_COROTATED) {
-        float hardening = 1.0f;
-        if (m.model == MODEL_SNOW) {
-            if (!finite_f(pvol) || pvol < SNOW_MIN_PLASTIC_VOLUME || pvol > SNOW_MAX_PLASTIC_VOLUME) return bad;
-            const float e = fminf(fmaxf(SNOW_HARDENING * (1.0f - pvol), -SNOW_MAX_HARDENING_EXPONENT),
-                                  SNOW_MAX_HARDENING_EXPONENT);
-            hardening = expf(e);
-        }
-        const Decomp d = decompose(F);
-        if (!finite_f(d.s0) || !finite_f(d.s1) || d.s0 <= 0.0f || d.s1 <= 0.0f) return bad;
-        const float4 R = polar_rotation(d);
-        const float mu = m.mu * hardening, lambda = m.lambda * hardening;
-        const float4 diff = make_float4(F.x - R.x, F.y - R.y, F.z - R.z, F.w - R.w);
-        const float shear = 2.0f * mu;
-        const float volumetric = lambda * det * (det - 1.0f);
-        s = make_float4(shear * (diff.x * F.x + diff.y * F.y) + volumetric, shear * (diff.x * F.z + diff.y * F.w),
-                        shear * (diff.z * F.x + diff.w * F.y), shear * (diff.z * F.z + diff.w * F.w) + volumetric);
-    } else if (m.model == MODEL_WATER || m.model == MODEL_OIL) {
-        if (!finite_f(m.density) || m.density <= 0.0f || !finite_f(m.lambda) || m.lambda <= 0.0f ||
-            !finite_f(m.param) || m.param < 0.0f)
-            return bad;
-        if (m.param > 0.0f) {
-            const float pw = tait_pow >= 0.0f ? tait_pow : pow_wgsl(__fdiv_rn(1.0f, det), m.param);
-            const float pressure = m.lambda * (pw - 1.0f);
-            const float stress = -det * pressure;
-            s = make_float4(stress, 0.f, 0.f, stress);
-        } else {
-            const float pressure = m.lambda * fminf(det - 1.0f, 0.0f);
-            s = make_float4(pressure, 0.f, 0.f, pressure);
-        }
-    } else if (m.model == MODEL_POWDER) {
-        if (!finite_f(m.lambda) || !finite_f(m.mu) || m.mu <= 0.0f || !finite_f(m.param) || m.param < 0.0f)
-            return bad;
-        // granularStressTimesFt: shaders.ts:408-441
-        const Decomp d = decompose(F);
-        const float l0 = logf(d.s0), l1 = logf(d.s1);
-        const float lv = l0 + l1;
-        const float blv = fmaxf(logf(MIN_POWDER_DETERMINANT), lv);
-        const float pressure = fmaxf(0.0f, -(m.lambda + m.mu) * blv);
-        const float dev = 0.5f * (l0 - l1);
-        const float maxdev = m.param * pressure / (2.0f * m.mu);
-        const float pdev = fminf(dev, maxdev);
-        const float mean = 0.5f * lv;
-        const float p0 = 2.0f * m.mu * (mean + pdev) + m.lambda * lv;
-        const float p1 = 2.0f * m.mu * (mean - pdev) + m.lambda * lv;
-        s = make_float4(p0 * d.u0.x * d.u0.x + p1 * d.u1.x * d.u1.x, p0 * d.u0.x * d.u0.y + p1 * d.u1.x * d.u1.y,
-                        p0 * d.u0.y * d.u0.x + p1 * d.u1.y * d.u1.x, p0 * d.u0.y * d.u0.y + p1 * d.u1.y * d.u1.y);
+    if constexpr (LIQ) {
+        if (!liquid_stress(m, det, tait_pow, s)) return bad;
     } else {
-        return bad;
+        if (m.model == MODEL_NEO_HOOKEAN) {
+            if (!finite_f(damage) || damage < 0.0f || damage > 1.0f) return bad;
+            const float4 it = make_float4(F.w / det, -F.z / det, -F.y / det, F.x / det);
+            const float pressure = m.lambda * logf(det);
+            const float4 pk = make_float4(m.mu * (F.x - it.x) + pressure * it.x, m.mu * (F.y - it.y) + pressure * it.y,
+                                          m.mu * (F.z - it.z) + pressure * it.z, m.mu * (F.w - it.w) + pressure * it.w);
+            const float keep = 1.0f - fminf(fmaxf(damage, 0.0f), 1.0f);
+            s = make_float4((pk.x * F.x + pk.y * F.y) * keep, (pk.x * F.z + pk.y * F.w) * keep,
+                            (pk.z * F.x + pk.w * F.y) * keep, (pk.z * F.z + pk.w * F.w) * keep);
+        } else if (m.model == MODEL_SNOW || m.model == MODEL_FIXED_COROTATED) {
+            float hardening = 1.0f;
+            if (m.model == MODEL_SNOW) {
+                if (!finite_f(pvol) || pvol < SNOW_MIN_PLASTIC_VOLUME || pvol > SNOW_MAX_PLASTIC_VOLUME) return bad;
+                const float e = fminf(fmaxf(SNOW_HARDENING * (1.0f - pvol), -SNOW_MAX_HARDENING_EXPONENT),
+                                      SNOW_MAX_HARDENING_EXPONENT);
+                hardening = expf(e);
+            }
+            const Decomp d = decompose(F);
+            if (!finite_f(d.s0) || !finite_f(d.s1) || d.s0 <= 0.0f || d.s1 <= 0.0f) return bad;
+            const float4 R = polar_rotation(d);
+            const float mu = m.mu * hardening, lambda = m.lambda * hardening;
+            const float4 diff = make_float4(F.x - R.x, F.y - R.y, F.z - R.z, F.w - R.w);
+            const float shear = 2.0f * mu;
+            const float volumetric = lambda * det * (det - 1.0f);
+            s = make_float4(shear * (diff.x * F.x + diff.y * F.y) + volumetric, shear * (diff.x * F.z + diff.y * F.w),
+                            shear * (diff.z * F.x + diff.w * F.y), shear * (diff.z * F.z + diff.w * F.w) + volumetric);
+        } else if (m.model == MODEL_WATER || m.model == MODEL_OIL) {
+            if (!liquid_stress(m, det, tait_pow, s)) return bad;
+        } else if (m.model == MODEL_POWDER) {
+            if (!finite_f(m.lambda) || !finite_f(m.mu) || m.mu <= 0.0f || !finite_f(m.param) || m.param < 0.0f)
+                return bad;
+            // granularStressTimesFt: shaders.ts:408-441
+            const Decomp d = decompose(F);
+            const float l0 = logf(d.s0), l1 = logf(d.s1);
+            const float lv = l0 + l1;
+            const float blv = fmaxf(logf(MIN_POWDER_DETERMINANT), lv);
+            const float pressure = fmaxf(0.0f, -(m.lambda + m.mu) * blv);
+            const float dev = 0.5f * (l0 - l1);
+            const float maxdev = m.param * pressure / (2.0f * m.mu);
+            const float pdev = fminf(dev, maxdev);
+            const float mean = 0.5f * lv;
+            const float p0 = 2.0f * m.mu * (mean + pdev) + m.lambda * lv;
+            const float p1 = 2.0f * m.mu * (mean - pdev) + m.lambda * lv;
+            s = make_float4(p0 * d.u0.x * d.u0.x + p1 * d.u1.x * d.u1.x, p0 * d.u0.x * d.u0.y + p1 * d.u1.x * d.u1.y,
+                            p0 * d.u0.y * d.u0.x + p1 * d.u1.y * d.u1.x, p0 * d.u0.y * d.u0.y + p1 * d.u1.y * d.u1.y);
+        } else {
+            return bad;
+        }
     }
-    const bool liquid = m.model == MODEL_WATER || m.model == MODEL_OIL;
+    const bool liquid = LIQ || m.model == MODEL_WATER || m.model == MODEL_OIL;
     mass = liquid ? __fmul_rn(m.density, volume) : P.particle_mass;
     vliq = liquid ? __fmul_rn(volume, det) : 0.0f;
     const float scale = -P.dt * volume * P.gradient_scale;
@@ -283,6 +298,7 @@ __device__ __forceinline__ bool is_tracked(const Ctx &c, uint32_t orig)
 // base stencil (the next substep's prepareParticle, evaluated early).  A
 // failure is kept in the record and raised by the P2G that reads it, so the
 // status appears in the same substep as in the reference.
+template <bool LIQ = false>
 __device__ __forceinline__ void write_record(const Ctx &c, uint32_t d, const Material &m, const Stencil &st,
                                              float2 vel, float4 F, float volume, float damage, float pvol, float4 C,
                                              float tait_pow = -1.0f)
@@ -290,9 +306,9 @@ __device__ __forceinline__ void write_record(const Ctx &c, uint32_t d, const Mat
     float4 A;
     float mass, vliq;
     bool indexed;
-    const uint32_t flags = prepare_core(*c.P, m, F, volume, damage, pvol, C, A, mass, vliq, indexed, tait_pow);
+    const uint32_t flags = prepare_core<LIQ>(*c.P, m, F, volume, damage, pvol, C, A, mass, vliq, indexed, tait_pow);
     const uint32_t lx = (uint32_t)(st.bx + 1) % TILE_X, ly = (uint32_t)(st.by + 1) % TILE_Y;
-    const uint32_t ch = m.model == MODEL_WATER ? 1u : (m.model == MODEL_OIL ? 2u : 0u);
+    const uint32_t ch = m.model == MODEL_WATER ? 1u : (LIQ || m.model == MODEL_OIL ? 2u : 0u);
     uint32_t cell = (ly * TILE_X + lx) | (ch << 8);
     if (flags != 0u) {
         c.rec_state[d] = make_float4(__uint_as_float(flags), __uint_as_float(indexed ? 1u : 0u), 0.f, 0.f);
@@ -554,19 +570,20 @@ struct NodeVel {
 // The node update of updateGrid (shaders.ts:1485-1746) for one node given its
 // P2G sums and the water/oil volumes of its four neighbours (xp, xm, yp, ym;
 // zero outside the halo or where no particle deposited).  Returns false
-// after raising a status.
-template <bool BODIES>
+// after raising a status.  LIQ: the solver holds no solid particle, so the
+// solid channel (its sums are zero) is not evaluated and its velocity is 0.
+template <bool BODIES, bool LIQ = false>
 __device__ __forceinline__ bool node_velocity(const Ctx &c, uint32_t n, int x, int y, float4 S, float4 W, float4 O,
                                               float2 xp, float2 xm, float2 yp, float2 ym, NodeVel &out)
 {
     const StepParams &P = *c.P;
-    if (!finite_f(S.x) || S.x < 0.f || !finite_f(S.y) || !finite_f(S.z) || !finite_f(W.x) || W.x < 0.f ||
+    if ((!LIQ && (!finite_f(S.x) || S.x < 0.f || !finite_f(S.y) || !finite_f(S.z))) || !finite_f(W.x) || W.x < 0.f ||
         !finite_f(W.y) || !finite_f(W.z) || !finite_f(W.w) || W.w < 0.f || !finite_f(O.x) || O.x < 0.f ||
         !finite_f(O.y) || !finite_f(O.z) || !finite_f(O.w) || O.w < 0.f) {
         fail(c.status, ERROR_GRID);
         return false;
     }
-    float2 vs = finish_velocity(P, S.x, S.y, S.z, x, y);
+    float2 vs = LIQ ? make_float2(0.f, 0.f) : finish_velocity(P, S.x, S.y, S.z, x, y);
     float2 vw = finish_velocity(P, W.x, W.y, W.z, x, y);
     float2 vo = finish_velocity(P, O.x, O.y, O.z, x, y);
     if (x >= 0 && y >= 0 && x <= (int)P.cells_x && y <= (int)P.cells_y && W.x > 0.f && O.x > 0.f && W.w > 0.f &&
@@ -654,20 +671,24 @@ __device__ __forceinline__ bool node_velocity(const Ctx &c, uint32_t n, int x, i
             }
         }
     }
-    if (!finite2(vs) || !finite2(vw) || !finite2(vo) || !finite2(impulse)) {
+    if ((!LIQ && !finite2(vs)) || !finite2(vw) || !finite2(vo) || !finite2(impulse)) {
         fail(c.status, ERROR_GRID | ERROR_TRIANGLE_CONTACT);
         return false;
     }
     const int cx = (int)P.cells_x, cy = (int)P.cells_y;
     const float fr = P.wall_friction;
-    vs.x = wall_cushion(vs.x, x, cx);
-    vs.y = wall_cushion(vs.y, y, cy);
+    if (!LIQ) {
+        vs.x = wall_cushion(vs.x, x, cx);
+        vs.y = wall_cushion(vs.y, y, cy);
+    }
     vw.x = wall_cushion(vw.x, x, cx);
     vw.y = wall_cushion(vw.y, y, cy);
     vo.x = wall_cushion(vo.x, x, cx);
     vo.y = wall_cushion(vo.y, y, cy);
-    vs.x = wall_friction(vs.x, y, cy, fr);
-    vs.y = wall_friction(vs.y, x, cx, fr);
+    if (!LIQ) {
+        vs.x = wall_friction(vs.x, y, cy, fr);
+        vs.y = wall_friction(vs.y, x, cx, fr);
+    }
     vw.x = wall_friction(vw.x, y, cy, fr);
     vw.y = wall_friction(vw.y, x, cx, fr);
     vo.x = wall_friction(vo.x, y, cy, fr);
@@ -1377,13 +1398,48 @@ __device__ __forceinline__ void add_channel(const float *part, const NodeSources
         for (int w = 0; w < NW; ++w) sum[W0 + w] += v[k][w];
 }
 
+// add_channel for two channels at once: every load of both is issued before
+// the first add (one L2 round trip for the water and oil sums together); each
+// word's sum keeps its source order, so the result is add_channel's.
+template <int W0, int NW, int W1, int NW1>
+__device__ __forceinline__ void add_two_channels(const float *part, const NodeSources &ns, uint32_t bit0,
+                                                 uint32_t bit1, float (&sum)[ACC_WORDS])
+{
+    float v[4][NW], u[4][NW1];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const bool has0 = (ns.mask[k] & bit0) != 0u, has1 = (ns.mask[k] & bit1) != 0u;
+        const float *src = part + ns.base[k];
+#pragma unroll
+        for (int w = 0; w < NW; ++w) v[k][w] = has0 ? __ldcg(src + (W0 + w) * RING_NODES) : 0.0f;
+#pragma unroll
+        for (int w = 0; w < NW1; ++w) u[k][w] = has1 ? __ldcg(src + (W1 + w) * RING_NODES) : 0.0f;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+#pragma unroll
+        for (int w = 0; w < NW; ++w) sum[W0 + w] += v[k][w];
+#pragma unroll
+        for (int w = 0; w < NW1; ++w) sum[W1 + w] += u[k][w];
+    }
+}
+
 // Adds the ring records of a node into sum[] in source order: every word of
 // the channels in `channels` when `all`, else only the water and oil volumes
 // (words 6 and 10).  `channels` (the union of the neighbour records' masks)
-// is the same for the whole CTA, so its branches do not diverge.
+// is the same for the whole CTA, so its branches do not diverge.  With LIQ
+// (no solid channel) the water and oil words are loaded together.
+template <bool LIQ = false>
 __device__ __forceinline__ void add_sources(const Ctx &c, const NodeSources &ns, bool all, uint32_t channels,
                                             float (&sum)[ACC_WORDS])
 {
+    if (LIQ && channels == 6u) {
+        if (all)
+            add_two_channels<3, 4, 7, 4>(c.part, ns, 2u, 4u, sum);
+        else
+            add_two_channels<6, 1, 10, 1>(c.part, ns, 2u, 4u, sum);
+        return;
+    }
     if (all) {
         if (channels & 1u) add_channel<0, 3>(c.part, ns, 1u, sum);
         if (channels & 2u) add_channel<3, 4>(c.part, ns, 2u, sum);
@@ -1534,10 +1590,11 @@ namespace {
 // particleWaveSpeedBound: shaders.ts:268-353
 // `tait_pow` is (1 / det F)^gamma of a Tait liquid when the caller has it
 // (negative: not computed); (1 / det)^(gamma - 1) is then tait_pow * det.
+template <bool LIQ = false>
 __device__ float wave_speed_bound(const Ctx &c, const Material &m, float4 F, float damage, float volume,
                                   float tait_pow)
 {
-    if (m.model == MODEL_WATER || m.model == MODEL_OIL) {
+    if (LIQ || m.model == MODEL_WATER || m.model == MODEL_OIL) {
         if (!finite_f(m.lambda) || !finite_f(m.density) || m.lambda <= 0.f || m.density <= 0.f) return FLOAT_MAX;
         float c2 = m.c2;  // lambda / density, divided once on the host
         if (m.param > 0.0f) {
@@ -1581,13 +1638,14 @@ __device__ __forceinline__ void copy_particle(const Ctx &c, uint32_t from, uint3
 }
 
 // validateCflParticle: shaders.ts:2423-2454
+template <bool LIQ = false>
 __device__ void validate_cfl(const Ctx &c, uint32_t id, const Material &m, float2 vel, float4 F, float damage,
                              float volume, float tait_pow)
 {
     const StepParams &P = *c.P;
     if (!P.cfl_enabled) return;
     const float speed = length2(vel);
-    const float wave = wave_speed_bound(c, m, F, damage, volume, tait_pow);
+    const float wave = wave_speed_bound<LIQ>(c, m, F, damage, volume, tait_pow);
     if (!finite2(vel) || !finite_f(speed) || !finite_f(wave) || speed > P.cfl_velocity_limit ||
         wave > P.cfl_wave_bound) {
         // the reference reads the status word before the bounds; a particle
@@ -1670,6 +1728,22 @@ __device__ float2 project_from_triangles(const Ctx &c, float2 pos, float radius)
     return make_float2(pos.x + (radius - sd) * nrm.x, pos.y + (radius - sd) * nrm.y);
 }
 
+// projectLiquidDeformation (shaders.ts:474-488): the rotation of the trial F
+// scaled by the square root of its clamped determinant.
+__device__ __forceinline__ float4 project_liquid(float4 trial)
+{
+    const float2 rn = make_float2(trial.x + trial.w, trial.z - trial.y);
+    const float rs = fmaxf(fabsf(rn.x), fabsf(rn.y));
+    const float irs = __frcp_rn(rs);
+    const float2 nr = make_float2(rn.x * irs, rn.y * irs);
+    const float irl = rsqrtf(nr.x * nr.x + nr.y * nr.y);
+    const float2 rot = make_float2(nr.x * irl, nr.y * irl);
+    const float vol = det2(trial);
+    const float bv = fminf(fmaxf(vol, MIN_LIQUID_DETERMINANT), MAX_LIQUID_DETERMINANT);
+    const float sc = sqrtf(bv);
+    return make_float4(sc * rot.x, sc * -rot.y, sc * rot.y, sc * rot.x);
+}
+
 // The input state G2P reads for one particle.
 struct ParticleIn {
     float2 pos;
@@ -1695,8 +1769,9 @@ __device__ __forceinline__ ParticleIn load_particle(const Ctx &c, uint32_t s)
 // Returns false when the particle raised a status (the substep is then
 // rolled back).  When the next substep's tiles are counted, `next` receives
 // the stencil of the new position and the slot's P2G record is written.
-// BODIES: the solver may hold bonded-triangle bodies or fracture bonds.
-template <bool BODIES, class Grid>
+// BODIES: the solver may hold bonded-triangle bodies or fracture bonds; LIQ:
+// every material is water or oil (the other models' code is compiled out).
+template <bool BODIES, bool LIQ, class Grid>
 __device__ __forceinline__ bool g2p_particle(const Ctx &c, const ParticleIn &in, uint32_t d, const Stencil &st,
                                              const Grid &grid, Stencil &next, bool &count_next)
 {
@@ -1705,7 +1780,7 @@ __device__ __forceinline__ bool g2p_particle(const Ctx &c, const ParticleIn &in,
     const float2 pos = in.pos;
     const uint32_t id = in.orig;
     const Material m = c.mats[in.mat];
-    const bool water = m.model == MODEL_WATER, oil = m.model == MODEL_OIL, liquid = water || oil;
+    const bool water = m.model == MODEL_WATER, oil = !water && (LIQ || m.model == MODEL_OIL), liquid = water || oil;
     float wx[3], wy[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -1804,61 +1879,55 @@ __device__ __forceinline__ bool g2p_particle(const Ctx &c, const ParticleIn &in,
         fail(c.status, ERROR_DEFORMATION);
         return false;
     }
-    if (m.model == MODEL_SNOW) {
-        const Decomp dd = decompose(trial);
-        if (!finite_f(dd.s0) || !finite_f(dd.s1) || dd.s0 <= 0.f || dd.s1 <= 0.f) {
-            fail(c.status, ERROR_G2P);
-            return false;
-        }
-        const float lo = 1.0f - SNOW_COMPRESSION_YIELD, hi = 1.0f + SNOW_STRETCH_YIELD;
-        const float a = fminf(fmaxf(dd.s0, lo), hi), b = fminf(fmaxf(dd.s1, lo), hi);
-        pv = fminf(fmaxf(pv * tdet / (a * b), SNOW_MIN_PLASTIC_VOLUME), SNOW_MAX_PLASTIC_VOLUME);
-        Fn = reconstruct(dd, a, b);
-    } else if (m.model == MODEL_POWDER) {
-        if (!finite_f(m.lambda) || !finite_f(m.mu) || m.mu <= 0.f || !finite_f(m.param) || m.param < 0.f) {
-            fail(c.status, ERROR_G2P);
-            return false;
-        }
-        // projectGranularDeformation: shaders.ts:443-472
-        const Decomp dd = decompose(trial);
-        const float l0 = logf(dd.s0), l1 = logf(dd.s1);
-        const float lv = l0 + l1;
-        const float minlv = logf(MIN_POWDER_DETERMINANT);
-        const float blv = fmaxf(minlv, lv);
-        const float pressure = fmaxf(0.f, -(m.lambda + m.mu) * blv);
-        const float dev = 0.5f * (l0 - l1);
-        const float maxdev = m.param * pressure / (2.0f * m.mu);
-        if (!(dev <= maxdev && lv >= minlv)) {
-            const float pdev = fminf(dev, maxdev);
-            const float mean = 0.5f * blv;
-            Fn = reconstruct(dd, expf(mean + pdev), expf(mean - pdev));
-        }
-    } else if (liquid) {
-        // projectLiquidDeformation: shaders.ts:474-488
-        const float2 rn = make_float2(trial.x + trial.w, trial.z - trial.y);
-        const float rs = fmaxf(fabsf(rn.x), fabsf(rn.y));
-        const float irs = __frcp_rn(rs);
-        const float2 nr = make_float2(rn.x * irs, rn.y * irs);
-        const float irl = rsqrtf(nr.x * nr.x + nr.y * nr.y);
-        const float2 rot = make_float2(nr.x * irl, nr.y * irl);
-        const float vol = det2(trial);
-        const float bv = fminf(fmaxf(vol, MIN_LIQUID_DETERMINANT), MAX_LIQUID_DETERMINANT);
-        const float sc = sqrtf(bv);
-        Fn = make_float4(sc * rot.x, sc * -rot.y, sc * rot.y, sc * rot.x);
-    } else if (m.model == MODEL_NEO_HOOKEAN) {
-        const float tr = trial.x * trial.x + trial.y * trial.y + trial.z * trial.z + trial.w * trial.w;
-        if (!finite_f(tr)) {
-            fail(c.status, ERROR_G2P);
-            return false;
-        }
-        if (tdet < MIN_NEO_HOOKEAN_STRETCH * sqrtf(tr) || tr > MAX_NEO_HOOKEAN_STRETCH * MAX_NEO_HOOKEAN_STRETCH) {
+    if constexpr (LIQ) {
+        Fn = project_liquid(trial);
+    } else {
+        if (m.model == MODEL_SNOW) {
             const Decomp dd = decompose(trial);
-            Fn = reconstruct(dd, fminf(fmaxf(dd.s0, MIN_NEO_HOOKEAN_STRETCH), MAX_NEO_HOOKEAN_STRETCH),
-                             fminf(fmaxf(dd.s1, MIN_NEO_HOOKEAN_STRETCH), MAX_NEO_HOOKEAN_STRETCH));
+            if (!finite_f(dd.s0) || !finite_f(dd.s1) || dd.s0 <= 0.f || dd.s1 <= 0.f) {
+                fail(c.status, ERROR_G2P);
+                return false;
+            }
+            const float lo = 1.0f - SNOW_COMPRESSION_YIELD, hi = 1.0f + SNOW_STRETCH_YIELD;
+            const float a = fminf(fmaxf(dd.s0, lo), hi), b = fminf(fmaxf(dd.s1, lo), hi);
+            pv = fminf(fmaxf(pv * tdet / (a * b), SNOW_MIN_PLASTIC_VOLUME), SNOW_MAX_PLASTIC_VOLUME);
+            Fn = reconstruct(dd, a, b);
+        } else if (m.model == MODEL_POWDER) {
+            if (!finite_f(m.lambda) || !finite_f(m.mu) || m.mu <= 0.f || !finite_f(m.param) || m.param < 0.f) {
+                fail(c.status, ERROR_G2P);
+                return false;
+            }
+            // projectGranularDeformation: shaders.ts:443-472
+            const Decomp dd = decompose(trial);
+            const float l0 = logf(dd.s0), l1 = logf(dd.s1);
+            const float lv = l0 + l1;
+            const float minlv = logf(MIN_POWDER_DETERMINANT);
+            const float blv = fmaxf(minlv, lv);
+            const float pressure = fmaxf(0.f, -(m.lambda + m.mu) * blv);
+            const float dev = 0.5f * (l0 - l1);
+            const float maxdev = m.param * pressure / (2.0f * m.mu);
+            if (!(dev <= maxdev && lv >= minlv)) {
+                const float pdev = fminf(dev, maxdev);
+                const float mean = 0.5f * blv;
+                Fn = reconstruct(dd, expf(mean + pdev), expf(mean - pdev));
+            }
+        } else if (liquid) {
+            Fn = project_liquid(trial);
+        } else if (m.model == MODEL_NEO_HOOKEAN) {
+            const float tr = trial.x * trial.x + trial.y * trial.y + trial.z * trial.z + trial.w * trial.w;
+            if (!finite_f(tr)) {
+                fail(c.status, ERROR_G2P);
+                return false;
+            }
+            if (tdet < MIN_NEO_HOOKEAN_STRETCH * sqrtf(tr) || tr > MAX_NEO_HOOKEAN_STRETCH * MAX_NEO_HOOKEAN_STRETCH) {
+                const Decomp dd = decompose(trial);
+                Fn = reconstruct(dd, fminf(fmaxf(dd.s0, MIN_NEO_HOOKEAN_STRETCH), MAX_NEO_HOOKEAN_STRETCH),
+                                 fminf(fmaxf(dd.s1, MIN_NEO_HOOKEAN_STRETCH), MAX_NEO_HOOKEAN_STRETCH));
+            }
+        } else if (m.model != MODEL_FIXED_COROTATED) {
+            fail(c.status, ERROR_G2P);
+            return false;
         }
-    } else if (m.model != MODEL_FIXED_COROTATED) {
-        fail(c.status, ERROR_G2P);
-        return false;
     }
     const float udet = det2(Fn);
     if (!finite4(Fn) || !finite_f(pv) || pv < SNOW_MIN_PLASTIC_VOLUME || pv > SNOW_MAX_PLASTIC_VOLUME) {
@@ -1908,7 +1977,7 @@ __device__ __forceinline__ bool g2p_particle(const Ctx &c, const ParticleIn &in,
     // next substep's pressure (both evaluate it at the new F)
     float tait_pow = -1.0f;
     if (liquid && m.param > 0.0f && finite_f(m.param)) tait_pow = pow_wgsl(__fdiv_rn(1.0f, udet), m.param);
-    if (!BODIES || P.n_bodies == 0u) validate_cfl(c, id, m, outv, Fn, damage, volume, tait_pow);
+    if (!BODIES || P.n_bodies == 0u) validate_cfl<LIQ>(c, id, m, outv, Fn, damage, volume, tait_pow);
     if (BODIES && is_tracked(c, id)) {
         // a body vertex or fracture particle: its final state comes after the
         // body kernels, which then count its tile and write its record
@@ -1918,7 +1987,7 @@ __device__ __forceinline__ bool g2p_particle(const Ctx &c, const ParticleIn &in,
             fail(c.status, ERROR_STENCIL);
             return false;
         }
-        write_record(c, d, m, next, outv, Fn, volume, damage, pv, Cn, tait_pow);
+        write_record<LIQ>(c, d, m, next, outv, Fn, volume, damage, pv, Cn, tait_pow);
         count_next = true;
     }
     return true;
@@ -1951,7 +2020,7 @@ __global__ void k_g2p(Ctx c)
             } else {
                 const GlobalGrid grid{c.g_solid, c.g_water, c.g_oil, node_index(P, st.bx, st.by), P.node_w};
                 bool count_it;
-                if (g2p_particle<true>(c, in, d, st, grid, next, count_it) && count_it) {
+                if (g2p_particle<true, false>(c, in, d, st, grid, next, count_it) && count_it) {
                     key = particle_tile(P, next.bx, next.by);
                     counted = true;
                 }
@@ -2046,7 +2115,7 @@ struct G2PShared {
     uint32_t mat[G2P_STAGE], orig[G2P_STAGE];
 };
 
-template <bool SCENES, bool BODIES>
+template <bool SCENES, bool BODIES, bool LIQ>
 __device__ __forceinline__ void g2p_tiles(const Ctx &c0, G2PShared &sh)
 {
     uint32_t *const s_tile = sh.tile;
@@ -2161,7 +2230,7 @@ __device__ __forceinline__ void g2p_tiles(const Ctx &c0, G2PShared &sh)
         for (int k = 0; k < 9; ++k) channels |= info[k].x == stamp ? info[k].y : 0u;
         if (in_grid) {
             const NodeSources ns = node_sources(P, info, tx, ty, hx, hy, stamp);
-            add_sources(c, ns, ring_node, channels, sum);
+            add_sources<LIQ>(c, ns, ring_node, channels, sum);
         }
         if (in_region) s_vol[t] = make_float2(sum[6], sum[10]);
         __syncthreads();
@@ -2175,7 +2244,7 @@ __device__ __forceinline__ void g2p_tiles(const Ctx &c0, G2PShared &sh)
                 const float4 W = make_float4(sum[3], sum[4], sum[5], sum[6]);
                 const float4 O = make_float4(sum[7], sum[8], sum[9], sum[10]);
                 const uint32_t n = (uint32_t)hy * (uint32_t)node_w + (uint32_t)hx;
-                if (!node_velocity<BODIES>(c, n, hx - 1, hy - 1, S, W, O, s_vol[t + 1], s_vol[t - 1], s_vol[t + VOL_X],
+                if (!node_velocity<BODIES, LIQ>(c, n, hx - 1, hy - 1, S, W, O, s_vol[t + 1], s_vol[t - 1], s_vol[t + VOL_X],
                                    s_vol[t - VOL_X], v)) {
                     s_fail = 1;
                 } else {
@@ -2241,7 +2310,7 @@ __device__ __forceinline__ void g2p_tiles(const Ctx &c0, G2PShared &sh)
                 } else {
                     const RingGrid grid{s_vs, s_vw, s_vo, (uint32_t)(ly * RING_X + lx), RING_X};
                     bool count_it;
-                    if (g2p_particle<BODIES>(c, in, p, st, grid, next, count_it) && count_it) {
+                    if (g2p_particle<BODIES, LIQ>(c, in, p, st, grid, next, count_it) && count_it) {
                         key = particle_tile(P, next.bx, next.by);
                         counted = true;
                     }
@@ -2258,11 +2327,11 @@ __device__ __forceinline__ void g2p_tiles(const Ctx &c0, G2PShared &sh)
     if constexpr (!SCENES) flush_active_nodes(c0.counters, ws, ww, wo);
 }
 
-template <bool SCENES, bool BODIES>
+template <bool SCENES, bool BODIES, bool LIQ>
 __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
 {
     __shared__ G2PShared sh;
-    g2p_tiles<SCENES, BODIES>(c0, sh);
+    g2p_tiles<SCENES, BODIES, LIQ>(c0, sh);
 }
 
 // ------------------------------------------------- one launch per substep --
@@ -2361,7 +2430,7 @@ static_assert(SUBSTEP_THREADS == ALLOC_THREADS && SUBSTEP_THREADS == 2 * TILE_CE
 // run the four kernels' device functions, so the two forms are
 // bit-identical.  Shared memory is one dynamic buffer: the two P2G stages in
 // that phase, the G2P arrays in the next.
-template <bool SCENES, int CAP>
+template <bool SCENES, int CAP, bool LIQ>
 __global__ void __launch_bounds__(SUBSTEP_THREADS, CAP == STAGE_CAP ? 2 : 3) k_substep(Ctx c0)
 {
     extern __shared__ __align__(16) unsigned char dsm[];
@@ -2371,7 +2440,7 @@ __global__ void __launch_bounds__(SUBSTEP_THREADS, CAP == STAGE_CAP ? 2 : 3) k_s
     if (!grid_barrier(c0, 1u)) return;
     p2g_tiles<SCENES, CAP, 2>(c0, reinterpret_cast<Stage<CAP> *>(dsm));
     if (!grid_barrier(c0, 2u)) return;
-    g2p_tiles<SCENES, false>(c0, *reinterpret_cast<G2PShared *>(dsm));
+    g2p_tiles<SCENES, false, LIQ>(c0, *reinterpret_cast<G2PShared *>(dsm));
 }
 
 size_t p2g_shared_bytes(int cap)
@@ -3317,12 +3386,18 @@ template __global__ void k_p2g_gather<false, STAGE_CAP>(Ctx);
 template __global__ void k_p2g_gather<true, STAGE_CAP>(Ctx);
 template __global__ void k_p2g_gather<false, STAGE_CAP_NARROW>(Ctx);
 template __global__ void k_p2g_gather<true, STAGE_CAP_NARROW>(Ctx);
-template __global__ void k_substep<false, STAGE_CAP>(Ctx);
-template __global__ void k_substep<true, STAGE_CAP>(Ctx);
-template __global__ void k_substep<false, STAGE_CAP_NARROW>(Ctx);
-template __global__ void k_substep<true, STAGE_CAP_NARROW>(Ctx);
-template __global__ void k_g2p_tile<false, false>(Ctx);
-template __global__ void k_g2p_tile<false, true>(Ctx);
-template __global__ void k_g2p_tile<true, false>(Ctx);
+template __global__ void k_substep<false, STAGE_CAP, false>(Ctx);
+template __global__ void k_substep<true, STAGE_CAP, false>(Ctx);
+template __global__ void k_substep<false, STAGE_CAP_NARROW, false>(Ctx);
+template __global__ void k_substep<true, STAGE_CAP_NARROW, false>(Ctx);
+template __global__ void k_substep<false, STAGE_CAP, true>(Ctx);
+template __global__ void k_substep<true, STAGE_CAP, true>(Ctx);
+template __global__ void k_substep<false, STAGE_CAP_NARROW, true>(Ctx);
+template __global__ void k_substep<true, STAGE_CAP_NARROW, true>(Ctx);
+template __global__ void k_g2p_tile<false, false, false>(Ctx);
+template __global__ void k_g2p_tile<false, true, false>(Ctx);
+template __global__ void k_g2p_tile<true, false, false>(Ctx);
+template __global__ void k_g2p_tile<false, false, true>(Ctx);
+template __global__ void k_g2p_tile<true, false, true>(Ctx);
 
 }  // namespace mpm

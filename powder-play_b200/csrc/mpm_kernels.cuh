@@ -185,13 +185,14 @@ __global__ void k_p2g_gather(Ctx c);
 // allocation, bucketing, P2G and G2P, separated by grid barriers whose waits
 // give up after Ctx::barrier_limit_ns (then ERROR_BARRIER is raised in every
 // scene and the launch returns).
-template <bool SCENES, int CAP>
+template <bool SCENES, int CAP, bool LIQ>
 __global__ void k_substep(Ctx c);
 // dynamic shared memory of k_p2g_gather and k_substep for stage capacity cap
 size_t p2g_shared_bytes(int cap);
 size_t substep_shared_bytes(int cap);
-// BODIES: the solver holds bonded-triangle bodies or fracture bonds
-template <bool SCENES, bool BODIES>
+// BODIES: the solver holds bonded-triangle bodies or fracture bonds; LIQ:
+// every material is water or oil (the other models' code compiled out)
+template <bool SCENES, bool BODIES, bool LIQ>
 __global__ void k_g2p_tile(Ctx c);
 __global__ void k_prepare_scatter(Ctx c);
 __global__ void k_fixed_decode(Ctx c);

@@ -143,6 +143,8 @@ struct mpm_solver {
     // and the most CTAs of it that fit on the GPU at once
     bool fused = true;
     int stage_cap = STAGE_CAP;
+    // G2P compiled for water and oil only, used when every material is one
+    bool liquid_kernels = true;
     unsigned substep_ctas = 1, substep_max_ctas = 1;
     // k_substep's barrier waits: the limit, and a CTA that leaves without
     // arriving (tests of the limit only)
@@ -348,12 +350,20 @@ void enqueue_bodies(mpm_solver *s, const Ctx &c)
     if (s->gather() && s->n_tracked) k_body_finish<<<blocks_for(s->n_tracked, 64), 64, 0, s->stream>>>(c);
 }
 
-// The k_substep instantiation for the scene count and stage capacity.
-const void *substep_kernel(bool scenes, int cap)
+// The k_substep instantiation for the scene count, stage capacity and
+// material set.
+const void *substep_kernel(bool scenes, int cap, bool liq)
 {
+    if (liq) {
+        if (cap == STAGE_CAP_NARROW)
+            return scenes ? (const void *)k_substep<true, STAGE_CAP_NARROW, true>
+                          : (const void *)k_substep<false, STAGE_CAP_NARROW, true>;
+        return scenes ? (const void *)k_substep<true, STAGE_CAP, true> : (const void *)k_substep<false, STAGE_CAP, true>;
+    }
     if (cap == STAGE_CAP_NARROW)
-        return scenes ? (const void *)k_substep<true, STAGE_CAP_NARROW> : (const void *)k_substep<false, STAGE_CAP_NARROW>;
-    return scenes ? (const void *)k_substep<true, STAGE_CAP> : (const void *)k_substep<false, STAGE_CAP>;
+        return scenes ? (const void *)k_substep<true, STAGE_CAP_NARROW, false>
+                      : (const void *)k_substep<false, STAGE_CAP_NARROW, false>;
+    return scenes ? (const void *)k_substep<true, STAGE_CAP, false> : (const void *)k_substep<false, STAGE_CAP, false>;
 }
 
 const void *p2g_kernel(bool scenes, int cap)
@@ -367,6 +377,16 @@ const void *p2g_kernel(bool scenes, int cap)
 // the default path without bonded bodies or fracture bonds (their passes
 // run between and after P2G and G2P), when that variant is chosen.
 bool runs_fused(const mpm_solver *s) { return s->gather() && s->fused && s->n_tracked == 0 && s->n_bodies == 0; }
+
+// Whether G2P runs its water-and-oil instantiation: every material of the
+// solver is water or oil and it holds no bodies or fracture bonds.
+bool runs_liquid(const mpm_solver *s)
+{
+    if (!s->liquid_kernels || s->n_tracked != 0 || s->n_bodies != 0 || s->mats.empty()) return false;
+    for (const Material &m : s->mats)
+        if (m.model != MODEL_WATER && m.model != MODEL_OIL) return false;
+    return true;
+}
 
 // Enqueues k_substep as a cooperative launch (every CTA resident at once).
 cudaError_t launch_substep(mpm_solver *s, const Ctx &c)
@@ -382,7 +402,7 @@ cudaError_t launch_substep(mpm_solver *s, const Ctx &c)
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     void *args[] = {const_cast<Ctx *>(&c)};
-    return cudaLaunchKernelExC(&cfg, substep_kernel(s->n_scenes > 1, s->stage_cap), args);
+    return cudaLaunchKernelExC(&cfg, substep_kernel(s->n_scenes > 1, s->stage_cap, runs_liquid(s)), args);
 }
 
 // Shared-memory limits of the stage variants (set once per process and
@@ -392,9 +412,10 @@ cudaError_t configure_variant_kernels()
     const int caps[2] = {STAGE_CAP, STAGE_CAP_NARROW};
     for (int cap : caps) {
         for (int scenes = 0; scenes < 2; ++scenes) {
-            const void *fns[2] = {p2g_kernel(scenes != 0, cap), substep_kernel(scenes != 0, cap)};
-            const size_t bytes[2] = {p2g_shared_bytes(cap), substep_shared_bytes(cap)};
-            for (int k = 0; k < 2; ++k) {
+            const void *fns[3] = {p2g_kernel(scenes != 0, cap), substep_kernel(scenes != 0, cap, false),
+                                  substep_kernel(scenes != 0, cap, true)};
+            const size_t bytes[3] = {p2g_shared_bytes(cap), substep_shared_bytes(cap), substep_shared_bytes(cap)};
+            for (int k = 0; k < 3; ++k) {
                 cudaError_t e = cudaFuncSetAttribute(fns[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes[k]);
                 if (e == cudaSuccess) e = cudaFuncSetAttribute(fns[k], cudaFuncAttributePreferredSharedMemoryCarveout, 100);
                 if (e != cudaSuccess) return e;
@@ -410,7 +431,7 @@ cudaError_t variant_occupancy(int cap, int *per_sm_p2g, int *per_sm_substep)
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm_p2g, p2g_kernel(false, cap), TILE_CELLS,
                                                                   p2g_shared_bytes(cap));
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm_substep, substep_kernel(false, cap), SUBSTEP_THREADS,
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm_substep, substep_kernel(false, cap, false), SUBSTEP_THREADS,
                                                           substep_shared_bytes(cap));
     return e;
 }
@@ -437,12 +458,17 @@ void enqueue_substep(mpm_solver *s, int parity)
         }
         mark(K_P2G_GATHER);
         if (s->n_bodies) k_triangle_field<<<tiles, TILE_NODES, 0, s->stream>>>(c);
-        if (s->n_scenes > 1)
-            k_g2p_tile<true, false><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
+        const bool liq = runs_liquid(s);
+        if (s->n_scenes > 1 && liq)
+            k_g2p_tile<true, false, true><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
+        else if (s->n_scenes > 1)
+            k_g2p_tile<true, false, false><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
         else if (s->n_tracked > 0)
-            k_g2p_tile<false, true><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
+            k_g2p_tile<false, true, false><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
+        else if (liq)
+            k_g2p_tile<false, false, true><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
         else
-            k_g2p_tile<false, false><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
+            k_g2p_tile<false, false, false><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
         mark(K_G2P_TILE);
     } else {
         k_substep_begin<<<blocks_for(s->n_scenes, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c);
@@ -968,7 +994,7 @@ int create_impl(const mpm_config *configs, uint32_t n_scenes, const uint32_t *co
         if (configure_variant_kernels() != cudaSuccess ||
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device) != cudaSuccess ||
             variant_occupancy(s->stage_cap, &per_sm_p2g, &per_sm_substep) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_g2p, k_g2p_tile<false, false>, G2P_THREADS, 0) !=
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_g2p, k_g2p_tile<false, false, false>, G2P_THREADS, 0) !=
                 cudaSuccess)
             return fail(set_error(MPM_ERR_CUDA, "occupancy query failed"));
         s->p2g_ctas = (unsigned)std::max<size_t>(1, std::min<size_t>(n_tiles, (size_t)sms * std::max(1, per_sm_p2g)));
@@ -1438,13 +1464,14 @@ int mpm_get_launch_shape(mpm_solver *s, uint32_t *p2g_ctas, uint32_t *g2p_ctas, 
     return MPM_OK;
 }
 
-int mpm_set_substep_variant(mpm_solver *s, uint32_t fused, uint32_t stage_capacity, uint32_t substep_ctas)
+int mpm_set_substep_variant(mpm_solver *s, uint32_t fused, uint32_t stage_capacity, uint32_t substep_ctas,
+                            uint32_t liquid_kernels)
 {
     g_last_error.clear();
     forget_readback(s);
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
     if (!s->gather()) return set_error(MPM_ERR_STATE, "substep variants apply to the default P2G path");
-    if (fused > 1u) return set_error(MPM_ERR_INVALID_ARGUMENT, "fused must be 0 or 1");
+    if (fused > 1u || liquid_kernels > 1u) return set_error(MPM_ERR_INVALID_ARGUMENT, "fused and liquid_kernels must be 0 or 1");
     if (stage_capacity != 0u && stage_capacity != (uint32_t)STAGE_CAP && stage_capacity != (uint32_t)STAGE_CAP_NARROW)
         return set_error(MPM_ERR_INVALID_ARGUMENT, "stage capacity must be %d or %d", STAGE_CAP, STAGE_CAP_NARROW);
     CUDA_TRY(cudaSetDevice(s->device));
@@ -1457,6 +1484,7 @@ int mpm_set_substep_variant(mpm_solver *s, uint32_t fused, uint32_t stage_capaci
         return set_error(MPM_ERR_INVALID_ARGUMENT, "substep_ctas %u exceeds the %u CTAs that fit on the GPU at once",
                          substep_ctas, most);
     s->fused = fused != 0u;
+    s->liquid_kernels = liquid_kernels != 0u;
     s->stage_cap = cap;
     s->substep_max_ctas = most;
     if (substep_ctas) s->substep_ctas = substep_ctas;
@@ -1466,7 +1494,7 @@ int mpm_set_substep_variant(mpm_solver *s, uint32_t fused, uint32_t stage_capaci
 }
 
 int mpm_get_substep_variant(mpm_solver *s, uint32_t *fused, uint32_t *stage_capacity, uint32_t *substep_ctas,
-                            uint32_t *max_substep_ctas)
+                            uint32_t *max_substep_ctas, uint32_t *liquid_kernels)
 {
     g_last_error.clear();
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
@@ -1474,6 +1502,7 @@ int mpm_get_substep_variant(mpm_solver *s, uint32_t *fused, uint32_t *stage_capa
     if (stage_capacity) *stage_capacity = (uint32_t)s->stage_cap;
     if (substep_ctas) *substep_ctas = s->substep_ctas;
     if (max_substep_ctas) *max_substep_ctas = s->substep_max_ctas;
+    if (liquid_kernels) *liquid_kernels = s->gather() && runs_liquid(s) ? 1u : 0u;
     return MPM_OK;
 }
 
@@ -1556,7 +1585,7 @@ int mpm_autotune(mpm_solver *s, uint32_t substeps, uint32_t *p2g_ctas, uint32_t 
     int sms = 0, per_sm_g2p = 1;
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_g2p, k_g2p_tile<false, false>, G2P_THREADS, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_g2p, k_g2p_tile<false, false, false>, G2P_THREADS, 0);
     int rc = e == cudaSuccess ? MPM_OK : set_error(MPM_ERR_CUDA, "autotune set-up failed: %s", cudaGetErrorString(e));
     const bool guarded = s->h_params[0].cfl_enabled != 0u;
     // one candidate: every setting of the variant, timed over `substeps`

@@ -327,20 +327,24 @@ class MpmBatchedGpuSolver:
     def substep_variant(self) -> dict:
         """How the default path runs a substep: `fused` (one cooperative launch
         of persistent CTAs, else four launches), the P2G stage capacity, the
-        one-launch form's persistent grid and its co-resident limit."""
-        f, cap, n, most = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        one-launch form's persistent grid and its co-resident limit, and
+        whether G2P runs its water-and-oil instantiation."""
+        f, cap, n, most, liq = (ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32(),
+                                ctypes.c_uint32())
         _check(self._lib.mpm_get_substep_variant(self._handle, ctypes.byref(f), ctypes.byref(cap), ctypes.byref(n),
-                                                 ctypes.byref(most)), "substep variant read failed")
+                                                 ctypes.byref(most), ctypes.byref(liq)), "substep variant read failed")
         return {"fused": bool(f.value), "stageCapacity": int(cap.value), "substepCtas": int(n.value),
-                "maxSubstepCtas": int(most.value)}
+                "maxSubstepCtas": int(most.value), "liquidKernels": bool(liq.value)}
 
-    def set_substep_variant(self, fused: bool = True, stage_capacity: int = 0, substep_ctas: int = 0) -> None:
+    def set_substep_variant(self, fused: bool = True, stage_capacity: int = 0, substep_ctas: int = 0,
+                            liquid_kernels: bool = True) -> None:
         """Chooses the substep variant (mpm_set_substep_variant; 0 keeps the
-        stage capacity or the grid).  Results do not depend on `fused` or the
-        grid."""
+        stage capacity or the grid).  Results do not depend on `fused`, the
+        grid or `liquid_kernels`."""
         self._assert_active()
         _check(self._lib.mpm_set_substep_variant(self._handle, 1 if fused else 0, int(stage_capacity),
-                                                 int(substep_ctas)), "substep variant change failed")
+                                                 int(substep_ctas), 1 if liquid_kernels else 0),
+               "substep variant change failed")
 
     def set_barrier_limit(self, limit_ns: int, skip_cta: int = 0xFFFFFFFF) -> None:
         """The one-launch substep's barrier wait limit in nanoseconds; `skip_cta`

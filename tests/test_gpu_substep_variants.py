@@ -3,7 +3,9 @@
 A substep runs either as ONE cooperative launch of persistent CTAs
 (k_substep: tile allocation, bucketing, P2G, grid update + G2P, with grid
 barriers between the phases) or as four launches of the same device code, so
-the two forms must agree bit for bit, whatever the persistent grid.  The
+the two forms must agree bit for bit, whatever the persistent grid; so must
+G2P's water-and-oil instantiation and its general one on a scene of water
+and oil.  The
 narrow P2G stage (384 particles) changes only how a crowded tile is cut into
 chunks, so it must stay within the oracle tolerances.  A CTA that leaves
 before the first barrier without arriving makes the others' waits run out:
@@ -52,13 +54,19 @@ def test_one_launch_and_four_launches_agree_bitwise_on_a_dam_break():
     for name, variant in {"one": dict(fused=True, stage_capacity=640),
                           "one_148": dict(fused=True, stage_capacity=640, substep_ctas=148),
                           "four": dict(fused=False, stage_capacity=640),
+                          "four_general": dict(fused=False, stage_capacity=640, liquid_kernels=False),
+                          "one_general": dict(fused=True, stage_capacity=640, liquid_kernels=False),
                           "one_narrow": dict(fused=True, stage_capacity=384),
                           "four_narrow": dict(fused=False, stage_capacity=384)}.items():
         packed, status, chosen = _step(p, config, variant, 24, dt, DAM_BREAK_GRAVITY)
         assert status[0] == 0, name
         assert chosen["fused"] == variant["fused"] and chosen["stageCapacity"] == variant["stage_capacity"]
+        # water and oil only: G2P runs its water-and-oil instantiation unless told not to
+        assert chosen["liquidKernels"] == variant.get("liquid_kernels", True)
         runs[name] = packed
     assert np.array_equal(_bits(runs["one"]), _bits(runs["four"]))
+    assert np.array_equal(_bits(runs["four"]), _bits(runs["four_general"]))
+    assert np.array_equal(_bits(runs["one"]), _bits(runs["one_general"]))
     assert np.array_equal(_bits(runs["one"]), _bits(runs["one_148"]))
     assert np.array_equal(_bits(runs["one_narrow"]), _bits(runs["four_narrow"]))
     # both stage capacities agree within the oracle tolerances (position 1e-3 dx)
@@ -109,20 +117,22 @@ def test_crowded_tiles_match_the_oracle_in_every_variant(per_side):
 def test_batched_scenes_agree_bitwise_in_one_launch_and_four():
     scenes = create_batched_tank_scenes(7, seed=5, particles=(200, 4000), sides=(20, 128))
     out = {}
-    for fused in (True, False):
+    for fused, liquid in ((True, True), (False, True), (False, False)):
         batch = create_mpm_batched_gpu_solver(scenes)
         try:
-            batch.set_substep_variant(fused=fused, stage_capacity=640)
-            assert batch.substep_variant()["fused"] == fused
+            batch.set_substep_variant(fused=fused, stage_capacity=640, liquid_kernels=liquid)
+            chosen = batch.substep_variant()
+            assert chosen["fused"] == fused and chosen["liquidKernels"] == liquid
             dts = [2e-4 * (1 + 0.1 * k) for k in range(batch.scene_count)]
             batch.step_batch([4 + (k % 3) for k in range(batch.scene_count)], dts, BATCHED_TANK_GRAVITY)
             batch.step_batch([0 if k % 2 else 3 for k in range(batch.scene_count)], dts, BATCHED_TANK_GRAVITY)
             assert all(e is None for e in batch.check_numerical_status())
-            out[fused] = [batch.read_particles_packed(k)[0] for k in range(batch.scene_count)]
+            out[(fused, liquid)] = [batch.read_particles_packed(k)[0] for k in range(batch.scene_count)]
         finally:
             batch.dispose()
-    for k, (a, b) in enumerate(zip(out[True], out[False])):
-        assert np.array_equal(_bits(a), _bits(b)), f"scene {k}"
+    for other in ((False, True), (False, False)):
+        for k, (a, b) in enumerate(zip(out[(True, True)], out[other])):
+            assert np.array_equal(_bits(a), _bits(b)), f"scene {k}, variant {other}"
 
 
 def test_a_barrier_wait_that_runs_out_reports_the_status_and_the_solver_recovers():
