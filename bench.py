@@ -118,6 +118,10 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
+# the launch-shape tuner runs after the first warm-up step unless --no-autotune
+AUTOTUNE = True
+
+
 def _peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -506,7 +510,8 @@ def measure_batched(steps, warmup, recovery_factor, plan_margin, dist, rank, loc
         return results
 
     one_step()
-    shape = batch.autotune(substeps=4)  # the project's launch-shape tuner, state restored
+    # the project's launch-shape tuner, state restored (skipped for profiling runs)
+    shape = batch.autotune(substeps=4) if AUTOTUNE else dict(batch.substep_variant(), **batch.launch_shape())
     for _ in range(warmup - 1):
         one_step()
     torch.cuda.synchronize()
@@ -738,7 +743,9 @@ def run_b200(args):
         return m
 
     one_step()
-    shape = solver.autotune(substeps=4) if args.p2g == "gather" else None
+    shape = None
+    if args.p2g == "gather":
+        shape = solver.autotune(substeps=4) if AUTOTUNE else dict(solver.substep_variant(), **solver.launch_shape())
     for _ in range(args.warmup - 1):
         one_step()
     clocks = ClockSampler(local_rank)
@@ -931,10 +938,14 @@ def main():
     ap.add_argument("--no-legs", action="store_true", help="skip the batched and adjoint legs of the default line")
     ap.add_argument("--leg-steps", type=int, default=3, help="timed macrosteps of the batched leg")
     ap.add_argument("--profile-case", choices=PROFILE_CASES, help="run a small fixed case for kernel profiling")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch variant (profiling runs: the tuner's trials distort under a profiler)")
     # the batched workload's adaptive CFL policy (the reference's: 1.25 and no margin)
     ap.add_argument("--cfl-recovery-factor", type=float, default=1.25)
     ap.add_argument("--cfl-plan-margin", type=float, default=1.0)
     args = ap.parse_args()
+    global AUTOTUNE
+    AUTOTUNE = not args.no_autotune
     if args.profile_case:
         run_profile_case(args.profile_case)
         return

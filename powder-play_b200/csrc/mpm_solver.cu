@@ -141,7 +141,7 @@ struct mpm_solver {
     // the default path's substep variant: one cooperative launch (k_substep)
     // or four launches, the P2G stage capacity, k_substep's persistent grid
     // and the most CTAs of it that fit on the GPU at once
-    bool fused = true;
+    bool fused = false;
     int stage_cap = STAGE_CAP;
     // G2P compiled for water and oil only, used when every material is one
     bool liquid_kernels = true;
