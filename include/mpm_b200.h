@@ -257,7 +257,7 @@ int mpm_get_launch_shape(mpm_solver *solver, uint32_t *p2g_ctas, uint32_t *g2p_c
  * keeps the fastest: for each P2G stage capacity (640, 384), the one-launch
  * substep over persistent grids of 1 .. co-resident CTAs per SM, and the
  * four-launch substep over its P2G grids, then its G2P grids with the best
- * P2G.  Restores the particle state and counters it started from.  Returns
+ * P2G, then both ways of handing prepareParticle's results to P2G.  Restores the particle state and counters it started from.  Returns
  * the chosen four-launch grids (mpm_get_substep_variant gives the rest) and
  * the best milliseconds per substep.  Needs one submitted batch.  Blocks. */
 int mpm_autotune(mpm_solver *solver, uint32_t substeps, uint32_t *p2g_ctas, uint32_t *g2p_ctas, double *best_ms);
@@ -271,17 +271,21 @@ int mpm_autotune(mpm_solver *solver, uint32_t substeps, uint32_t *p2g_ctas, uint
  * it; at most the CTAs that fit on the GPU at once); `liquid_kernels` 1 lets
  * G2P run its instantiation compiled for water and oil only whenever every
  * material of the solver is one of them (the default), 0 keeps the general
- * one.  Solvers with bonded bodies or fracture bonds always take four
- * launches and the general G2P.  Results do not depend on `fused`, the grids
- * or `liquid_kernels` (the same arithmetic); the stage capacity changes only
- * the rounding of tiles holding more particles than it.
- * mpm_get_substep_variant reports whether substeps run as one launch, the
- * capacity, the grid, its co-resident limit and whether the water-and-oil
- * G2P runs. */
+ * one; `p2g_records` 1 has G2P write each particle's prepared P2G record
+ * (prepareParticle, evaluated where G2P has F and C in registers) for the
+ * next P2G, 0 has P2G prepare each particle from its state, 2 picks by the
+ * materials (records unless every material is a liquid with the linear EOS;
+ * the one-launch form always prepares in P2G).  Solvers with bonded bodies or
+ * fracture bonds always take four launches and the general G2P.  Results do
+ * not depend on `fused`, the grids, `liquid_kernels` or `p2g_records` (the
+ * same arithmetic); the stage capacity changes only the rounding of tiles
+ * holding more particles than it.  mpm_get_substep_variant reports whether
+ * substeps run as one launch, the capacity, the grid, its co-resident limit,
+ * whether the water-and-oil G2P runs and whether records are used. */
 int mpm_set_substep_variant(mpm_solver *solver, uint32_t fused, uint32_t stage_capacity, uint32_t substep_ctas,
-                            uint32_t liquid_kernels);
+                            uint32_t liquid_kernels, uint32_t p2g_records);
 int mpm_get_substep_variant(mpm_solver *solver, uint32_t *fused, uint32_t *stage_capacity, uint32_t *substep_ctas,
-                            uint32_t *max_substep_ctas, uint32_t *liquid_kernels);
+                            uint32_t *max_substep_ctas, uint32_t *liquid_kernels, uint32_t *p2g_records);
 
 /* The one-launch substep's grid-barrier waits give up after `limit_ns`
  * nanoseconds (default 1 s; 1 us .. 60 s): the CTA that gave up raises status

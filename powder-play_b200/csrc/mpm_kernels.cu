@@ -295,9 +295,10 @@ __device__ __forceinline__ bool is_tracked(const Ctx &c, uint32_t orig)
 }
 
 // Writes the P2G record of slot d for a particle with the given state and
-// base stencil (the next substep's prepareParticle, evaluated early).  A
-// failure is kept in the record and raised by the P2G that reads it, so the
-// status appears in the same substep as in the reference.
+// base stencil (the next substep's prepareParticle, evaluated early; the
+// records variant).  A failure is kept in the record and raised by the P2G
+// that reads it, so the status appears in the same substep as in the
+// reference.
 template <bool LIQ = false>
 __device__ __forceinline__ void write_record(const Ctx &c, uint32_t d, const Material &m, const Stencil &st,
                                              float2 vel, float4 F, float volume, float damage, float pvol, float4 C,
@@ -728,8 +729,18 @@ __device__ __forceinline__ uint32_t particle_tile(const StepParams &P, int bx, i
     return P.tile_base + tile_of_node(P, (uint32_t)(bx + 1), (uint32_t)(by + 1));
 }
 
-// Batch prologue of the default path: tile key, rank within the tile and
-// P2G record of the particle in each slot (later substeps get them from G2P).
+// The bucket key stored per slot: the particle's tile in the low 24 bits and
+// its base node's cell within the tile in the top 8 (P2G's crowded path
+// orders a tile's entries by that cell without recomputing the stencil).
+__device__ __forceinline__ uint32_t bucket_key(uint32_t tile, int bx, int by)
+{
+    const uint32_t cell = ((uint32_t)(by + 1) % TILE_Y) * TILE_X + (uint32_t)(bx + 1) % TILE_X;
+    return tile | (cell << KEY_CELL_SHIFT);
+}
+
+// Batch prologue of the default path: tile key and rank within the tile of
+// the particle in each slot, and with the records variant its P2G record
+// (later substeps get them from G2P).
 __global__ void k_tile_count(Ctx c0)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -745,30 +756,33 @@ __global__ void k_tile_count(Ctx c0)
     } else {
         valid = i < c0.n && takes_part(c);
     }
-    uint32_t key = 0;
+    uint32_t tile = 0, key = 0;
     if (valid) {
-        // every load of the slot at once (damage and plastic volume exist for
-        // every slot; only Neo-Hookean and snow particles use them)
-        const float2 pos = c.in.pos[i], vel = c.in.vel[i];
-        const float4 F = c.in.F[i], C = c.in.C[i];
-        const float vol = c.in.vol[i], damage_in = c.in.damage[i], pvol_in = c.in.pvol[i];
-        const uint32_t mat = c.in.mat[i], orig = c.in.orig[i];
+        const float2 pos = c.in.pos[i];
+        const uint32_t orig = c.in.orig[i];
         Stencil s;
         if (!make_stencil_fast(P, pos, s) || !stencil_fits(P, s.bx, s.by)) {
             fail(c.status, ERROR_STENCIL);
             valid = false;
         } else {
-            key = particle_tile(P, s.bx, s.by);
+            tile = particle_tile(P, s.bx, s.by);
+            key = bucket_key(tile, s.bx, s.by);
             if (is_tracked(c, orig)) c.slot_in[orig] = i;
-            const Material m = c.mats[mat];
-            const float damage = m.model == MODEL_NEO_HOOKEAN ? damage_in : 0.0f;
-            const float pvol = m.model == MODEL_SNOW ? pvol_in : 1.0f;
-            write_record(c, i, m, s, vel, F, vol, damage, pvol, C);
+            if (c.rec_state) {
+                // the records variant: the first substep's P2G records
+                const float2 vel = c.in.vel[i];
+                const float4 F = c.in.F[i], C = c.in.C[i];
+                const float vol = c.in.vol[i], damage_in = c.in.damage[i], pvol_in = c.in.pvol[i];
+                const Material m = c.mats[c.in.mat[i]];
+                const float damage = m.model == MODEL_NEO_HOOKEAN ? damage_in : 0.0f;
+                const float pvol = m.model == MODEL_SNOW ? pvol_in : 1.0f;
+                write_record(c, i, m, s, vel, F, vol, damage, pvol, C);
+            }
         }
     }
     const unsigned active = __ballot_sync(0xffffffffu, valid);
     if (!valid) return;
-    c.ranks[i] = warp_count(c.tile_count, key, active);
+    c.ranks[i] = warp_count(c.tile_count, tile, active);
     c.keys[i] = key;
 }
 
@@ -913,7 +927,7 @@ __device__ __forceinline__ void scatter_quads(const Ctx &c, uint32_t first, uint
             if (i >= c.n) continue;
             for (uint32_t j = i; j < min(i + 4u, c.n); ++j) {
                 if (!one && !runs_flag(c, scene_of_slot(c, j))) continue;
-                c.perm[__ldcg(c.tile_range + __ldcg(c.keys + j)).x + __ldcg(c.ranks + j)] = j;
+                c.perm[__ldcg(c.tile_range + (__ldcg(c.keys + j) & KEY_TILE_MASK)).x + __ldcg(c.ranks + j)] = j;
             }
         }
         return;
@@ -926,14 +940,16 @@ __device__ __forceinline__ void scatter_quads(const Ctx &c, uint32_t first, uint
         if (i + 4u <= c.n) {
             const uint4 key = __ldcs(reinterpret_cast<const uint4 *>(c.keys + i));
             const uint4 rank = __ldcs(reinterpret_cast<const uint4 *>(c.ranks + i));
-            const uint32_t s0 = __ldcg(c.tile_range + key.x).x, s1 = __ldcg(c.tile_range + key.y).x,
-                           s2 = __ldcg(c.tile_range + key.z).x, s3 = __ldcg(c.tile_range + key.w).x;
+            const uint32_t s0 = __ldcg(c.tile_range + (key.x & KEY_TILE_MASK)).x,
+                           s1 = __ldcg(c.tile_range + (key.y & KEY_TILE_MASK)).x,
+                           s2 = __ldcg(c.tile_range + (key.z & KEY_TILE_MASK)).x,
+                           s3 = __ldcg(c.tile_range + (key.w & KEY_TILE_MASK)).x;
             c.perm[s0 + rank.x] = i;
             c.perm[s1 + rank.y] = i + 1u;
             c.perm[s2 + rank.z] = i + 2u;
             c.perm[s3 + rank.w] = i + 3u;
         } else {
-            for (uint32_t j = i; j < c.n; ++j) c.perm[__ldcg(c.tile_range + c.keys[j]).x + c.ranks[j]] = j;
+            for (uint32_t j = i; j < c.n; ++j) c.perm[__ldcg(c.tile_range + (c.keys[j] & KEY_TILE_MASK)).x + c.ranks[j]] = j;
         }
     }
 }
@@ -952,8 +968,9 @@ __global__ void k_tile_scatter(Ctx c)
 namespace {
 
 // Shared-memory staging of the particles of one tile (or of one chunk of a
-// crowded tile): their P2G records, their grouping by base cell (in the
-// order channel, original index within a cell) and the ring accumulator.
+// crowded tile): their P2G records (prepared in place from the staged
+// state), their grouping by base cell (in the order channel, original index
+// within a cell) and the ring accumulator.
 template <int CAP>
 struct Stage {
     float4 state[CAP];     // fx, fy, mass, liquid volume
@@ -1071,34 +1088,112 @@ __device__ __forceinline__ void scan_cell_counts(uint32_t lane, const uint32_t *
 // phases, one stencil offset per phase (no two cells of a phase share a
 // node), so every sum has a fixed order.  Returns false once a record had
 // failed.
-template <int CAP, int GROUPS>
+template <int CAP, int GROUPS, bool LIQ, bool REC>
 __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage<CAP> &sm, const uint32_t *src, uint32_t i0, uint32_t i1)
 {
     const StepParams &P = *c.P;
     const uint32_t me = threadIdx.x % TILE_CELLS;  // this thread's cell
     sm.count[me] = 0u;
     group_sync<GROUPS>();
-    for (uint32_t i = i0 + me; i < i1; i += TILE_CELLS) {
-        const uint32_t s = src[i];
-        const uint32_t k = i - i0;
-        cp_async<16>(&sm.state[k], &c.rec_state[s]);
-        cp_async<16>(&sm.affine[k], &c.rec_affine[s]);
-        cp_async<8>(&sm.momentum[k], &c.rec_mom[s]);
-        cp_async<4>(&sm.orig[k], &c.in.orig[s]);
-        cp_async<4>(&sm.cell[k], &c.rec_cell[s]);
-    }
-    cp_async_wait_all();
-    group_sync<GROUPS>();
     const uint32_t n = i1 - i0;
+    if constexpr (REC) {
+        // the records variant: the P2G records the previous G2P (or the
+        // batch prologue) wrote
+        for (uint32_t i = i0 + me; i < i1; i += TILE_CELLS) {
+            const uint32_t s = src[i];
+            const uint32_t k = i - i0;
+            cp_async<16>(&sm.state[k], &c.rec_state[s]);
+            cp_async<16>(&sm.affine[k], &c.rec_affine[s]);
+            cp_async<8>(&sm.momentum[k], &c.rec_mom[s]);
+            cp_async<4>(&sm.orig[k], &c.in.orig[s]);
+            cp_async<4>(&sm.cell[k], &c.rec_cell[s]);
+        }
+        cp_async_wait_all();
+        group_sync<GROUPS>();
+        for (uint32_t k = me; k < n; k += TILE_CELLS) {
+            const uint32_t cell = sm.cell[k];
+            if (cell & REC_FAILED) {  // the record carries prepareParticle's flags
+                const float4 f = sm.state[k];
+                if (__float_as_uint(f.y) != 0u)
+                    fail_at(c.status, sm.orig[k], __float_as_uint(f.x));
+                else
+                    fail(c.status, __float_as_uint(f.x));
+            }
+        }
+    } else {
+        // the state prepareParticle reads: F, C, v and the material index copied
+        // into the slots their results replace (state, affine, momentum, cell);
+        // position, volume (and damage and plastic volume for the general
+        // models) loaded into this thread's registers while the copies fly
+        constexpr int PER = (CAP + TILE_CELLS - 1) / TILE_CELLS;  // entries per thread
+        float2 pos[PER];
+        float vol[PER], dmg[PER], pvl[PER];
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+            const uint32_t i = i0 + me + (uint32_t)u * TILE_CELLS;
+            if (i < i1) {
+                const uint32_t s = src[i];
+                const uint32_t k = i - i0;
+                cp_async<16>(&sm.state[k], &c.in.F[s]);
+                cp_async<16>(&sm.affine[k], &c.in.C[s]);
+                cp_async<8>(&sm.momentum[k], &c.in.vel[s]);
+                cp_async<4>(&sm.orig[k], &c.in.orig[s]);
+                cp_async<4>(&sm.cell[k], &c.in.mat[s]);
+                pos[u] = c.in.pos[s];
+                vol[u] = c.in.vol[s];
+                if constexpr (!LIQ) {
+                    dmg[u] = c.in.damage[s];
+                    pvl[u] = c.in.pvol[s];
+                }
+            }
+        }
+        cp_async_wait_all();
+        group_sync<GROUPS>();
+        // prepareParticle (shaders.ts:808-963) of this thread's entries, in place:
+        // (fx, fy, mass, liquid volume), the affine momentum, m v and the entry's
+        // local cell | channel << 8 (| REC_FAILED after raising its status)
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+            const uint32_t k = me + (uint32_t)u * TILE_CELLS;
+            if (k < n) {
+                const Material m = c.mats[sm.cell[k]];
+                const float4 F = sm.state[k], C = sm.affine[k];
+                const float2 v = sm.momentum[k];
+                const float damage = (!LIQ && m.model == MODEL_NEO_HOOKEAN) ? dmg[u] : 0.0f;
+                const float pvol = (!LIQ && m.model == MODEL_SNOW) ? pvl[u] : 1.0f;
+                Stencil st;
+                uint32_t cell = REC_FAILED;
+                if (!make_stencil_fast(P, pos[u], st) || !stencil_fits(P, st.bx, st.by)) {
+                    fail(c.status, ERROR_STENCIL);
+                } else {
+                    float4 A;
+                    float mass, vliq;
+                    bool indexed;
+                    const uint32_t flags = prepare_core<LIQ>(P, m, F, vol[u], damage, pvol, C, A, mass, vliq, indexed);
+                    const uint32_t lx = (uint32_t)(st.bx + 1) % TILE_X, ly = (uint32_t)(st.by + 1) % TILE_Y;
+                    const uint32_t ch = m.model == MODEL_WATER ? 1u : (LIQ || m.model == MODEL_OIL ? 2u : 0u);
+                    cell = (ly * TILE_X + lx) | (ch << 8);
+                    if (flags != 0u) {
+                        if (indexed)
+                            fail_at(c.status, sm.orig[k], flags);
+                        else
+                            fail(c.status, flags);
+                        cell |= REC_FAILED;
+                    } else {
+                        sm.state[k] = make_float4(st.fx, st.fy, mass, vliq);
+                        sm.affine[k] = A;
+                        sm.momentum[k] = make_float2(mass * v.x, mass * v.y);
+                    }
+                }
+                sm.cell[k] = cell;
+            }
+        }
+        group_sync<GROUPS>();
+    }
     uint32_t mask = 0;
     for (uint32_t k = me; k < n; k += TILE_CELLS) {
         const uint32_t cell = sm.cell[k];
-        if (cell & REC_FAILED) {
-            const float4 f = sm.state[k];
-            if (__float_as_uint(f.y) != 0u)
-                fail_at(c.status, sm.orig[k], __float_as_uint(f.x));
-            else
-                fail(c.status, __float_as_uint(f.x));
+        if (cell & REC_FAILED) {  // its status is raised
             sm.failed = 1;
             continue;
         }
@@ -1227,9 +1322,9 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage<CAP> &sm, const ui
     return true;
 }
 
-// P2G (prepareParticle + the p2g of shaders.ts:808-963, :1072-1211; the
-// records carry prepareParticle's result from the previous G2P) for the
-// tiles holding particles, one tile per group iteration, one thread per cell.
+// P2G (prepareParticle + the p2g of shaders.ts:808-963, :1072-1211; each
+// staged particle is prepared in shared memory from its state) for the tiles
+// holding particles, one tile per group iteration, one thread per cell.
 // The sums of a tile's particles over its 18x10-node ring have a fixed
 // order (cell-major phases, original particle index within a cell), so they
 // do not depend on the order of the tile buckets and every run is
@@ -1239,7 +1334,7 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage<CAP> &sm, const ui
 // sums go to the tile's own ring record; the G2P adds the up to four
 // records that cover a node.  The GROUPS groups of a CTA take interleaved
 // tiles of the list, each with its own stage.
-template <bool SCENES, int CAP, int GROUPS>
+template <bool SCENES, int CAP, int GROUPS, bool LIQ, bool REC>
 __device__ __forceinline__ void p2g_tiles(const Ctx &c0, Stage<CAP> *stages)
 {
     const uint32_t g = p2g_group<GROUPS>();
@@ -1275,7 +1370,7 @@ __device__ __forceinline__ void p2g_tiles(const Ctx &c0, Stage<CAP> *stages)
                 for (int u = 0; u < 4; ++u) s[u] = i + u * TILE_CELLS < n_tile ? src[i + u * TILE_CELLS] : 0xffffffffu;
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
-                    if (s[u] != 0xffffffffu) atomicAdd(&sm.count[c.rec_cell[s[u]] & 0xffu], 1u);
+                    if (s[u] != 0xffffffffu) atomicAdd(&sm.count[c.keys[s[u]] >> KEY_CELL_SHIFT], 1u);
             }
             group_sync<GROUPS>();
             // the cells' first entries, and cursors for the placement below
@@ -1287,7 +1382,7 @@ __device__ __forceinline__ void p2g_tiles(const Ctx &c0, Stage<CAP> *stages)
 #pragma unroll
                 for (int u = 0; u < 4; ++u) s[u] = i + u * TILE_CELLS < n_tile ? src[i + u * TILE_CELLS] : 0xffffffffu;
 #pragma unroll
-                for (int u = 0; u < 4; ++u) cell[u] = s[u] != 0xffffffffu ? c.rec_cell[s[u]] & 0xffu : 0u;
+                for (int u = 0; u < 4; ++u) cell[u] = s[u] != 0xffffffffu ? c.keys[s[u]] >> KEY_CELL_SHIFT : 0u;
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
                     if (s[u] != 0xffffffffu) list[atomicAdd(&sm.start[cell[u]], 1u)] = s[u];
@@ -1313,7 +1408,7 @@ __device__ __forceinline__ void p2g_tiles(const Ctx &c0, Stage<CAP> *stages)
                     hi = sm.cells[q1];
                 }
             }
-            ok = p2g_chunk<CAP, GROUPS>(c, sm, src, lo, hi);
+            ok = p2g_chunk<CAP, GROUPS, LIQ, REC>(c, sm, src, lo, hi);
             if (n_tile > (uint32_t)CAP && q1 == q + 1 && hi < sm.cells[q + 1]) {
                 i0 += (uint32_t)CAP;  // next chunk of the same crowded cell
             } else {
@@ -1335,11 +1430,11 @@ __device__ __forceinline__ void p2g_tiles(const Ctx &c0, Stage<CAP> *stages)
 
 }  // namespace
 
-template <bool SCENES, int CAP>
-__global__ void __launch_bounds__(TILE_CELLS) k_p2g_gather(Ctx c0)
+template <bool SCENES, int CAP, bool LIQ, bool REC>
+__global__ void __launch_bounds__(TILE_CELLS, 5) k_p2g_gather(Ctx c0)
 {
     extern __shared__ __align__(16) unsigned char dsm[];
-    p2g_tiles<SCENES, CAP, 1>(c0, reinterpret_cast<Stage<CAP> *>(dsm));
+    p2g_tiles<SCENES, CAP, 1, LIQ, REC>(c0, reinterpret_cast<Stage<CAP> *>(dsm));
 }
 
 namespace {
@@ -1768,10 +1863,11 @@ __device__ __forceinline__ ParticleIn load_particle(const Ctx &c, uint32_t s)
 // The G2P of one particle with base stencil st: reads `in`, writes slot d.
 // Returns false when the particle raised a status (the substep is then
 // rolled back).  When the next substep's tiles are counted, `next` receives
-// the stencil of the new position and the slot's P2G record is written.
+// the stencil of the new position.
 // BODIES: the solver may hold bonded-triangle bodies or fracture bonds; LIQ:
-// every material is water or oil (the other models' code is compiled out).
-template <bool BODIES, bool LIQ, class Grid>
+// every material is water or oil (the other models' code is compiled out);
+// REC: the records variant, which also writes the slot's P2G record.
+template <bool BODIES, bool LIQ, bool REC, class Grid>
 __device__ __forceinline__ bool g2p_particle(const Ctx &c, const ParticleIn &in, uint32_t d, const Stencil &st,
                                              const Grid &grid, Stencil &next, bool &count_next)
 {
@@ -1973,10 +2069,12 @@ __device__ __forceinline__ bool g2p_particle(const Ctx &c, const ParticleIn &in,
     c.out.vol[d] = volume;
     c.out.mat[d] = in.mat;
     c.out.orig[d] = id;
-    // (1 / det F)^gamma of a Tait liquid, shared by the CFL wave speed and the
-    // next substep's pressure (both evaluate it at the new F)
+    // (1 / det F)^gamma of a Tait liquid at the new F, for the CFL wave speed
+    // and the next substep's pressure (the record here, or the next P2G, which
+    // evaluates the same expression)
     float tait_pow = -1.0f;
-    if (liquid && m.param > 0.0f && finite_f(m.param)) tait_pow = pow_wgsl(__fdiv_rn(1.0f, udet), m.param);
+    if ((REC || P.cfl_enabled) && liquid && m.param > 0.0f && finite_f(m.param))
+        tait_pow = pow_wgsl(__fdiv_rn(1.0f, udet), m.param);
     if (!BODIES || P.n_bodies == 0u) validate_cfl<LIQ>(c, id, m, outv, Fn, damage, volume, tait_pow);
     if (BODIES && is_tracked(c, id)) {
         // a body vertex or fracture particle: its final state comes after the
@@ -1987,7 +2085,7 @@ __device__ __forceinline__ bool g2p_particle(const Ctx &c, const ParticleIn &in,
             fail(c.status, ERROR_STENCIL);
             return false;
         }
-        write_record<LIQ>(c, d, m, next, outv, Fn, volume, damage, pv, Cn, tait_pow);
+        if constexpr (REC) write_record<LIQ>(c, d, m, next, outv, Fn, volume, damage, pv, Cn, tait_pow);
         count_next = true;
     }
     return true;
@@ -2020,7 +2118,7 @@ __global__ void k_g2p(Ctx c)
             } else {
                 const GlobalGrid grid{c.g_solid, c.g_water, c.g_oil, node_index(P, st.bx, st.by), P.node_w};
                 bool count_it;
-                if (g2p_particle<true, false>(c, in, d, st, grid, next, count_it) && count_it) {
+                if (g2p_particle<true, false, false>(c, in, d, st, grid, next, count_it) && count_it) {
                     key = particle_tile(P, next.bx, next.by);
                     counted = true;
                 }
@@ -2115,7 +2213,7 @@ struct G2PShared {
     uint32_t mat[G2P_STAGE], orig[G2P_STAGE];
 };
 
-template <bool SCENES, bool BODIES, bool LIQ>
+template <bool SCENES, bool BODIES, bool LIQ, bool REC>
 __device__ __forceinline__ void g2p_tiles(const Ctx &c0, G2PShared &sh)
 {
     uint32_t *const s_tile = sh.tile;
@@ -2291,7 +2389,7 @@ __device__ __forceinline__ void g2p_tiles(const Ctx &c0, G2PShared &sh)
                 __syncthreads();
             }
             bool counted = false;
-            uint32_t key = 0;
+            uint32_t key = 0, packed_key = 0;
             if (p < end) {
                 const uint32_t k = chunk + threadIdx.x;
                 ParticleIn in;
@@ -2310,8 +2408,9 @@ __device__ __forceinline__ void g2p_tiles(const Ctx &c0, G2PShared &sh)
                 } else {
                     const RingGrid grid{s_vs, s_vw, s_vo, (uint32_t)(ly * RING_X + lx), RING_X};
                     bool count_it;
-                    if (g2p_particle<BODIES, LIQ>(c, in, p, st, grid, next, count_it) && count_it) {
+                    if (g2p_particle<BODIES, LIQ, REC>(c, in, p, st, grid, next, count_it) && count_it) {
                         key = particle_tile(P, next.bx, next.by);
+                        packed_key = bucket_key(key, next.bx, next.by);
                         counted = true;
                     }
                 }
@@ -2319,7 +2418,7 @@ __device__ __forceinline__ void g2p_tiles(const Ctx &c0, G2PShared &sh)
             const unsigned active = __ballot_sync(0xffffffffu, counted);
             if (counted) {
                 c.ranks[p] = warp_count(c.tile_count, key, active);
-                c.keys[p] = key;
+                c.keys[p] = packed_key;
             }
         }
         if constexpr (SCENES) flush_active_nodes(c.counters, ws, ww, wo);  // the tile's scene
@@ -2327,11 +2426,11 @@ __device__ __forceinline__ void g2p_tiles(const Ctx &c0, G2PShared &sh)
     if constexpr (!SCENES) flush_active_nodes(c0.counters, ws, ww, wo);
 }
 
-template <bool SCENES, bool BODIES, bool LIQ>
+template <bool SCENES, bool BODIES, bool LIQ, bool REC>
 __global__ void __launch_bounds__(G2P_THREADS, 4) k_g2p_tile(Ctx c0)
 {
     __shared__ G2PShared sh;
-    g2p_tiles<SCENES, BODIES, LIQ>(c0, sh);
+    g2p_tiles<SCENES, BODIES, LIQ, REC>(c0, sh);
 }
 
 // ------------------------------------------------- one launch per substep --
@@ -2438,9 +2537,9 @@ __global__ void __launch_bounds__(SUBSTEP_THREADS, CAP == STAGE_CAP ? 2 : 3) k_s
     if (!grid_barrier(c0, 0u)) return;
     scatter_quads(c0, blockIdx.x * SUBSTEP_THREADS + (threadIdx.x & ~31u), gridDim.x * SUBSTEP_THREADS);
     if (!grid_barrier(c0, 1u)) return;
-    p2g_tiles<SCENES, CAP, 2>(c0, reinterpret_cast<Stage<CAP> *>(dsm));
+    p2g_tiles<SCENES, CAP, 2, LIQ, false>(c0, reinterpret_cast<Stage<CAP> *>(dsm));
     if (!grid_barrier(c0, 2u)) return;
-    g2p_tiles<SCENES, false, LIQ>(c0, *reinterpret_cast<G2PShared *>(dsm));
+    g2p_tiles<SCENES, false, LIQ, false>(c0, *reinterpret_cast<G2PShared *>(dsm));
 }
 
 size_t p2g_shared_bytes(int cap)
@@ -3176,8 +3275,9 @@ __global__ void k_fracture_damage(Ctx c)
     c.out.damage[slot] = damage;
 }
 
-// The tile count and P2G record of each tracked particle, from its state
-// after the body and fracture passes (G2P left them out).
+// The tile count (and with the records variant the P2G record) of each
+// tracked particle, from its state after the body and fracture passes (G2P
+// left them out).
 __global__ void k_body_finish(Ctx c)
 {
     const StepParams &P = *c.P;
@@ -3192,9 +3292,11 @@ __global__ void k_body_finish(Ctx c)
     }
     const uint32_t key = particle_tile(P, st.bx, st.by);
     c.ranks[d] = atomicAdd(&c.tile_count[key], 1u);
-    c.keys[d] = key;
-    const Material m = c.mats[c.out.mat[d]];
-    write_record(c, d, m, st, c.out.vel[d], c.out.F[d], c.out.vol[d], c.out.damage[d], c.out.pvol[d], c.out.C[d]);
+    c.keys[d] = bucket_key(key, st.bx, st.by);
+    if (c.rec_state) {
+        const Material m = c.mats[c.out.mat[d]];
+        write_record(c, d, m, st, c.out.vel[d], c.out.F[d], c.out.vol[d], c.out.damage[d], c.out.pvol[d], c.out.C[d]);
+    }
 }
 
 // --------------------------------------------------------- interaction --
@@ -3382,10 +3484,22 @@ __global__ void k_probe_deformation(const float4 *F, const float4 *C, float dt, 
     substeps[i] = t.substeps;
 }
 
-template __global__ void k_p2g_gather<false, STAGE_CAP>(Ctx);
-template __global__ void k_p2g_gather<true, STAGE_CAP>(Ctx);
-template __global__ void k_p2g_gather<false, STAGE_CAP_NARROW>(Ctx);
-template __global__ void k_p2g_gather<true, STAGE_CAP_NARROW>(Ctx);
+template __global__ void k_p2g_gather<false, STAGE_CAP, false, false>(Ctx);
+template __global__ void k_p2g_gather<true, STAGE_CAP, false, false>(Ctx);
+template __global__ void k_p2g_gather<false, STAGE_CAP_NARROW, false, false>(Ctx);
+template __global__ void k_p2g_gather<true, STAGE_CAP_NARROW, false, false>(Ctx);
+template __global__ void k_p2g_gather<false, STAGE_CAP, true, false>(Ctx);
+template __global__ void k_p2g_gather<true, STAGE_CAP, true, false>(Ctx);
+template __global__ void k_p2g_gather<false, STAGE_CAP_NARROW, true, false>(Ctx);
+template __global__ void k_p2g_gather<true, STAGE_CAP_NARROW, true, false>(Ctx);
+template __global__ void k_p2g_gather<false, STAGE_CAP, false, true>(Ctx);
+template __global__ void k_p2g_gather<true, STAGE_CAP, false, true>(Ctx);
+template __global__ void k_p2g_gather<false, STAGE_CAP_NARROW, false, true>(Ctx);
+template __global__ void k_p2g_gather<true, STAGE_CAP_NARROW, false, true>(Ctx);
+template __global__ void k_p2g_gather<false, STAGE_CAP, true, true>(Ctx);
+template __global__ void k_p2g_gather<true, STAGE_CAP, true, true>(Ctx);
+template __global__ void k_p2g_gather<false, STAGE_CAP_NARROW, true, true>(Ctx);
+template __global__ void k_p2g_gather<true, STAGE_CAP_NARROW, true, true>(Ctx);
 template __global__ void k_substep<false, STAGE_CAP, false>(Ctx);
 template __global__ void k_substep<true, STAGE_CAP, false>(Ctx);
 template __global__ void k_substep<false, STAGE_CAP_NARROW, false>(Ctx);
@@ -3394,10 +3508,15 @@ template __global__ void k_substep<false, STAGE_CAP, true>(Ctx);
 template __global__ void k_substep<true, STAGE_CAP, true>(Ctx);
 template __global__ void k_substep<false, STAGE_CAP_NARROW, true>(Ctx);
 template __global__ void k_substep<true, STAGE_CAP_NARROW, true>(Ctx);
-template __global__ void k_g2p_tile<false, false, false>(Ctx);
-template __global__ void k_g2p_tile<false, true, false>(Ctx);
-template __global__ void k_g2p_tile<true, false, false>(Ctx);
-template __global__ void k_g2p_tile<false, false, true>(Ctx);
-template __global__ void k_g2p_tile<true, false, true>(Ctx);
+template __global__ void k_g2p_tile<false, false, false, false>(Ctx);
+template __global__ void k_g2p_tile<false, true, false, false>(Ctx);
+template __global__ void k_g2p_tile<true, false, false, false>(Ctx);
+template __global__ void k_g2p_tile<false, false, true, false>(Ctx);
+template __global__ void k_g2p_tile<true, false, true, false>(Ctx);
+template __global__ void k_g2p_tile<false, false, false, true>(Ctx);
+template __global__ void k_g2p_tile<false, true, false, true>(Ctx);
+template __global__ void k_g2p_tile<true, false, false, true>(Ctx);
+template __global__ void k_g2p_tile<false, false, true, true>(Ctx);
+template __global__ void k_g2p_tile<true, false, true, true>(Ctx);
 
 }  // namespace mpm

@@ -7,9 +7,10 @@
 //     are kept sorted by base cell: G2P of substep k reads slot perm[d] and
 //     writes slot d, so every particle kernel reads and writes coalesced.
 //   per original particle (constant): object id u32, bonded-vertex marker u32
-//   P2G records per slot (default path): float4 (fx, fy, mass, liquid
-//     volume), float4 affine momentum, float2 m v, u32 local cell | channel
-//   tile buckets: tile key u32 and rank u32 per slot, permutation u32
+//   with the records variant, P2G records per slot: float4 (fx, fy, mass,
+//     liquid volume), float4 affine momentum, float2 m v, u32 local cell |
+//     channel
+//   tile buckets: key u32 (tile | local cell << 24) and rank u32 per slot, permutation u32
 //     (bucketed position -> slot), per-tile count/start u32; the cell sort of
 //     the probes adds per-cell count/start u32 and a bucket scratch u32
 //   halo grid, (cellsX+3) x (cellsY+3) nodes, row-major by (y+1)*W + (x+1),
@@ -86,8 +87,9 @@ struct Ctx {
     const uint32_t *scene_chunk;  // per scene: its first CTA of k_tile_alloc, then the CTA total
     float *part;             // per tile: ACC_WORDS x RING_NODES sums, word-major
     uint2 *tile_info;        // per tile: (substep stamp of the sums, channel mask)
-    // P2G records of the particles in the input slots, written by the batch
-    // prologue and by each G2P for the next substep (default path only)
+    // the records variant: P2G records of the particles in the input slots,
+    // written by the batch prologue and by each G2P for the next substep
+    // (NULL: P2G prepares each particle from its state)
     float4 *rec_state;   // fx, fy, mass, liquid volume (failed: flags, indexed)
     float4 *rec_affine;  // A = m C + (-dt V 4/dx^2) P F^T
     float2 *rec_mom;     // m v
@@ -141,7 +143,9 @@ constexpr int TILE_CELLS = TILE_X * TILE_Y;
 constexpr int STAGE_CAP = 640;         // particles of a tile staged in shared memory at once (default variant)
 constexpr int STAGE_CAP_NARROW = 384;  // the narrow-stage variant (smaller stages, more tiles in flight)
 constexpr int ACC_WORDS = 11;   // solid m,px,py | water m,px,py,V | oil m,px,py,V
-constexpr uint32_t REC_FAILED = 1u << 16;  // the record's prepareParticle failed
+constexpr uint32_t REC_FAILED = 1u << 16;  // a P2G entry whose prepareParticle failed
+constexpr uint32_t KEY_CELL_SHIFT = 24;    // bucket key: tile in the low 24 bits, local cell above
+constexpr uint32_t KEY_TILE_MASK = (1u << KEY_CELL_SHIFT) - 1u;
 constexpr int VOL_X = RING_X + 2;          // ring nodes and their neighbours
 constexpr int VOL_Y = RING_Y + 2;
 constexpr int G2P_THREADS = 256;
@@ -178,8 +182,10 @@ __global__ void k_stable_rank(Ctx c);
 __global__ void k_tile_count(Ctx c);
 __global__ void k_tile_alloc(Ctx c);
 __global__ void k_tile_scatter(Ctx c);
-// SCENES: the solver holds several scenes; CAP: particles staged at once
-template <bool SCENES, int CAP>
+// SCENES: the solver holds several scenes; CAP: particles staged at once;
+// LIQ: every material is water or oil; REC: the records variant (P2G reads
+// the records G2P wrote instead of preparing each particle from its state)
+template <bool SCENES, int CAP, bool LIQ, bool REC>
 __global__ void k_p2g_gather(Ctx c);
 // The whole substep of the default path in one cooperative launch: tile
 // allocation, bucketing, P2G and G2P, separated by grid barriers whose waits
@@ -191,8 +197,9 @@ __global__ void k_substep(Ctx c);
 size_t p2g_shared_bytes(int cap);
 size_t substep_shared_bytes(int cap);
 // BODIES: the solver holds bonded-triangle bodies or fracture bonds; LIQ:
-// every material is water or oil (the other models' code compiled out)
-template <bool SCENES, bool BODIES, bool LIQ>
+// every material is water or oil (the other models' code compiled out);
+// REC: the records variant (G2P also writes the next P2G's records)
+template <bool SCENES, bool BODIES, bool LIQ, bool REC>
 __global__ void k_g2p_tile(Ctx c);
 __global__ void k_prepare_scatter(Ctx c);
 __global__ void k_fixed_decode(Ctx c);

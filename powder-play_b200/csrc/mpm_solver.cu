@@ -125,7 +125,7 @@ struct mpm_solver {
     uint32_t alloc_ctas = 1;
     float *part = nullptr;
     uint2 *tile_info = nullptr;
-    float4 *rec_state = nullptr, *rec_affine = nullptr;
+    float4 *rec_state = nullptr, *rec_affine = nullptr;  // the records variant's P2G records
     float2 *rec_mom = nullptr;
     uint32_t *rec_cell = nullptr;
     // bonded-triangle bodies and fracture bonds
@@ -145,6 +145,9 @@ struct mpm_solver {
     int stage_cap = STAGE_CAP;
     // G2P compiled for water and oil only, used when every material is one
     bool liquid_kernels = true;
+    // the records variant (G2P writes the next P2G's prepared records): 1 on,
+    // 0 off (P2G prepares each particle from its state), -1 by the materials
+    int records = -1;
     unsigned substep_ctas = 1, substep_max_ctas = 1;
     // k_substep's barrier waits: the limit, and a CTA that leaves without
     // arriving (tests of the limit only)
@@ -194,6 +197,20 @@ void drop_graphs(mpm_solver *s)
     s->batch_graphs.clear();
 }
 
+// Whether the records variant runs: as chosen, or by default when a material
+// is not a liquid with the linear EOS (preparing a Tait liquid or a solid
+// costs P2G more than reading a record; a linear-EOS liquid costs it less
+// than G2P writing one).
+bool uses_records(const mpm_solver *s)
+{
+    if (s->fused && s->n_tracked == 0 && s->n_bodies == 0) return false;  // the one-launch form prepares in P2G
+    if (s->records >= 0) return s->records != 0;
+    if (s->n_scenes > 1) return true;
+    for (const Material &m : s->mats)
+        if ((m.model != MODEL_WATER && m.model != MODEL_OIL) || m.param > 0.0f) return true;
+    return false;
+}
+
 Ctx make_ctx(mpm_solver *s, int parity)
 {
     Ctx c{};
@@ -237,10 +254,11 @@ Ctx make_ctx(mpm_solver *s, int parity)
     c.active_tiles = s->active_tiles;
     c.part = s->part;
     c.tile_info = s->tile_info;
-    c.rec_state = s->rec_state;
-    c.rec_affine = s->rec_affine;
-    c.rec_mom = s->rec_mom;
-    c.rec_cell = s->rec_cell;
+    const bool rec = s->gather() && uses_records(s);
+    c.rec_state = rec ? s->rec_state : nullptr;
+    c.rec_affine = rec ? s->rec_affine : nullptr;
+    c.rec_mom = rec ? s->rec_mom : nullptr;
+    c.rec_cell = rec ? s->rec_cell : nullptr;
     c.affine_out = nullptr;
     c.field = s->field;
     c.body_starts = s->body_starts;
@@ -366,11 +384,28 @@ const void *substep_kernel(bool scenes, int cap, bool liq)
     return scenes ? (const void *)k_substep<true, STAGE_CAP, false> : (const void *)k_substep<false, STAGE_CAP, false>;
 }
 
-const void *p2g_kernel(bool scenes, int cap)
+template <bool REC>
+const void *p2g_kernel_rec(bool scenes, int cap, bool liq)
 {
+    if (liq) {
+        if (cap == STAGE_CAP_NARROW)
+            return scenes ? (const void *)k_p2g_gather<true, STAGE_CAP_NARROW, true, REC>
+                          : (const void *)k_p2g_gather<false, STAGE_CAP_NARROW, true, REC>;
+        return scenes ? (const void *)k_p2g_gather<true, STAGE_CAP, true, REC>
+                      : (const void *)k_p2g_gather<false, STAGE_CAP, true, REC>;
+    }
     if (cap == STAGE_CAP_NARROW)
-        return scenes ? (const void *)k_p2g_gather<true, STAGE_CAP_NARROW> : (const void *)k_p2g_gather<false, STAGE_CAP_NARROW>;
-    return scenes ? (const void *)k_p2g_gather<true, STAGE_CAP> : (const void *)k_p2g_gather<false, STAGE_CAP>;
+        return scenes ? (const void *)k_p2g_gather<true, STAGE_CAP_NARROW, false, REC>
+                      : (const void *)k_p2g_gather<false, STAGE_CAP_NARROW, false, REC>;
+    return scenes ? (const void *)k_p2g_gather<true, STAGE_CAP, false, REC>
+                  : (const void *)k_p2g_gather<false, STAGE_CAP, false, REC>;
+}
+
+// The k_p2g_gather instantiation for the scene count, stage capacity,
+// material set and records variant.
+const void *p2g_kernel(bool scenes, int cap, bool liq, bool rec)
+{
+    return rec ? p2g_kernel_rec<true>(scenes, cap, liq) : p2g_kernel_rec<false>(scenes, cap, liq);
 }
 
 // Whether the substeps of this solver run as one k_substep launch each:
@@ -412,10 +447,12 @@ cudaError_t configure_variant_kernels()
     const int caps[2] = {STAGE_CAP, STAGE_CAP_NARROW};
     for (int cap : caps) {
         for (int scenes = 0; scenes < 2; ++scenes) {
-            const void *fns[3] = {p2g_kernel(scenes != 0, cap), substep_kernel(scenes != 0, cap, false),
-                                  substep_kernel(scenes != 0, cap, true)};
-            const size_t bytes[3] = {p2g_shared_bytes(cap), substep_shared_bytes(cap), substep_shared_bytes(cap)};
-            for (int k = 0; k < 3; ++k) {
+            const void *fns[6] = {p2g_kernel(scenes != 0, cap, false, false), p2g_kernel(scenes != 0, cap, true, false),
+                                  p2g_kernel(scenes != 0, cap, false, true),  p2g_kernel(scenes != 0, cap, true, true),
+                                  substep_kernel(scenes != 0, cap, false), substep_kernel(scenes != 0, cap, true)};
+            const size_t bytes[6] = {p2g_shared_bytes(cap), p2g_shared_bytes(cap), p2g_shared_bytes(cap),
+                                     p2g_shared_bytes(cap), substep_shared_bytes(cap), substep_shared_bytes(cap)};
+            for (int k = 0; k < 6; ++k) {
                 cudaError_t e = cudaFuncSetAttribute(fns[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes[k]);
                 if (e == cudaSuccess) e = cudaFuncSetAttribute(fns[k], cudaFuncAttributePreferredSharedMemoryCarveout, 100);
                 if (e != cudaSuccess) return e;
@@ -428,12 +465,29 @@ cudaError_t configure_variant_kernels()
 // CTAs per SM of the P2G kernel and of k_substep for stage capacity `cap`.
 cudaError_t variant_occupancy(int cap, int *per_sm_p2g, int *per_sm_substep)
 {
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm_p2g, p2g_kernel(false, cap), TILE_CELLS,
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm_p2g, p2g_kernel(false, cap, false, false), TILE_CELLS,
                                                                   p2g_shared_bytes(cap));
     if (e == cudaSuccess)
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm_substep, substep_kernel(false, cap, false), SUBSTEP_THREADS,
                                                           substep_shared_bytes(cap));
     return e;
+}
+
+// The k_g2p_tile instantiation for the solver's scenes, bodies, materials
+// and records variant.
+template <bool REC>
+void launch_g2p(mpm_solver *s, const Ctx &c, bool liq)
+{
+    if (s->n_scenes > 1 && liq)
+        k_g2p_tile<true, false, true, REC><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
+    else if (s->n_scenes > 1)
+        k_g2p_tile<true, false, false, REC><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
+    else if (s->n_tracked > 0)
+        k_g2p_tile<false, true, false, REC><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
+    else if (liq)
+        k_g2p_tile<false, false, true, REC><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
+    else
+        k_g2p_tile<false, false, false, REC><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
 }
 
 // One full substep from buffer `parity` into 1 - parity.
@@ -453,22 +507,17 @@ void enqueue_substep(mpm_solver *s, int parity)
         mark(K_TILE_SCATTER);
         {
             void *args[] = {const_cast<Ctx *>(&c)};
-            cudaLaunchKernel(p2g_kernel(s->n_scenes > 1, s->stage_cap), dim3(s->p2g_ctas), dim3(TILE_CELLS), args,
+            cudaLaunchKernel(p2g_kernel(s->n_scenes > 1, s->stage_cap, runs_liquid(s), uses_records(s)), dim3(s->p2g_ctas),
+                             dim3(TILE_CELLS), args,
                              p2g_shared_bytes(s->stage_cap), s->stream);
         }
         mark(K_P2G_GATHER);
         if (s->n_bodies) k_triangle_field<<<tiles, TILE_NODES, 0, s->stream>>>(c);
         const bool liq = runs_liquid(s);
-        if (s->n_scenes > 1 && liq)
-            k_g2p_tile<true, false, true><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
-        else if (s->n_scenes > 1)
-            k_g2p_tile<true, false, false><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
-        else if (s->n_tracked > 0)
-            k_g2p_tile<false, true, false><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
-        else if (liq)
-            k_g2p_tile<false, false, true><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
+        if (uses_records(s))
+            launch_g2p<true>(s, c, liq);
         else
-            k_g2p_tile<false, false, false><<<s->g2p_ctas, G2P_THREADS, 0, s->stream>>>(c);
+            launch_g2p<false>(s, c, liq);
         mark(K_G2P_TILE);
     } else {
         k_substep_begin<<<blocks_for(s->n_scenes, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c);
@@ -899,6 +948,8 @@ int create_impl(const mpm_config *configs, uint32_t n_scenes, const uint32_t *co
         free_solver(s);
         return code;
     };
+    // (this also keeps every tile index below 2^24, the tile field of a bucket key)
+    static_assert(0xffffffffull / (ACC_WORDS * RING_NODES) <= KEY_TILE_MASK, "tile indices must fit a bucket key");
     if ((uint64_t)s->n_tiles_total * (ACC_WORDS * RING_NODES) >= 0xffffffffull)
         return fail(set_error(MPM_ERR_INVALID_ARGUMENT, "the scenes' halo grids exceed the GPU index range"));
 #define ALLOC(ptr, n)                                                                                          \
@@ -994,7 +1045,7 @@ int create_impl(const mpm_config *configs, uint32_t n_scenes, const uint32_t *co
         if (configure_variant_kernels() != cudaSuccess ||
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device) != cudaSuccess ||
             variant_occupancy(s->stage_cap, &per_sm_p2g, &per_sm_substep) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_g2p, k_g2p_tile<false, false, false>, G2P_THREADS, 0) !=
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_g2p, k_g2p_tile<false, false, false, false>, G2P_THREADS, 0) !=
                 cudaSuccess)
             return fail(set_error(MPM_ERR_CUDA, "occupancy query failed"));
         s->p2g_ctas = (unsigned)std::max<size_t>(1, std::min<size_t>(n_tiles, (size_t)sms * std::max(1, per_sm_p2g)));
@@ -1465,13 +1516,14 @@ int mpm_get_launch_shape(mpm_solver *s, uint32_t *p2g_ctas, uint32_t *g2p_ctas, 
 }
 
 int mpm_set_substep_variant(mpm_solver *s, uint32_t fused, uint32_t stage_capacity, uint32_t substep_ctas,
-                            uint32_t liquid_kernels)
+                            uint32_t liquid_kernels, uint32_t p2g_records)
 {
     g_last_error.clear();
     forget_readback(s);
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
     if (!s->gather()) return set_error(MPM_ERR_STATE, "substep variants apply to the default P2G path");
     if (fused > 1u || liquid_kernels > 1u) return set_error(MPM_ERR_INVALID_ARGUMENT, "fused and liquid_kernels must be 0 or 1");
+    if (p2g_records > 2u) return set_error(MPM_ERR_INVALID_ARGUMENT, "p2g_records must be 0, 1 or 2");
     if (stage_capacity != 0u && stage_capacity != (uint32_t)STAGE_CAP && stage_capacity != (uint32_t)STAGE_CAP_NARROW)
         return set_error(MPM_ERR_INVALID_ARGUMENT, "stage capacity must be %d or %d", STAGE_CAP, STAGE_CAP_NARROW);
     CUDA_TRY(cudaSetDevice(s->device));
@@ -1485,6 +1537,7 @@ int mpm_set_substep_variant(mpm_solver *s, uint32_t fused, uint32_t stage_capaci
                          substep_ctas, most);
     s->fused = fused != 0u;
     s->liquid_kernels = liquid_kernels != 0u;
+    s->records = p2g_records == 2u ? -1 : (int)p2g_records;
     s->stage_cap = cap;
     s->substep_max_ctas = most;
     if (substep_ctas) s->substep_ctas = substep_ctas;
@@ -1494,7 +1547,7 @@ int mpm_set_substep_variant(mpm_solver *s, uint32_t fused, uint32_t stage_capaci
 }
 
 int mpm_get_substep_variant(mpm_solver *s, uint32_t *fused, uint32_t *stage_capacity, uint32_t *substep_ctas,
-                            uint32_t *max_substep_ctas, uint32_t *liquid_kernels)
+                            uint32_t *max_substep_ctas, uint32_t *liquid_kernels, uint32_t *p2g_records)
 {
     g_last_error.clear();
     if (!s) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver must not be NULL");
@@ -1503,6 +1556,7 @@ int mpm_get_substep_variant(mpm_solver *s, uint32_t *fused, uint32_t *stage_capa
     if (substep_ctas) *substep_ctas = s->substep_ctas;
     if (max_substep_ctas) *max_substep_ctas = s->substep_max_ctas;
     if (liquid_kernels) *liquid_kernels = s->gather() && runs_liquid(s) ? 1u : 0u;
+    if (p2g_records) *p2g_records = s->gather() && uses_records(s) ? 1u : 0u;
     return MPM_OK;
 }
 
@@ -1585,7 +1639,7 @@ int mpm_autotune(mpm_solver *s, uint32_t substeps, uint32_t *p2g_ctas, uint32_t 
     int sms = 0, per_sm_g2p = 1;
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_g2p, k_g2p_tile<false, false, false>, G2P_THREADS, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_g2p, k_g2p_tile<false, false, false, false>, G2P_THREADS, 0);
     int rc = e == cudaSuccess ? MPM_OK : set_error(MPM_ERR_CUDA, "autotune set-up failed: %s", cudaGetErrorString(e));
     const bool guarded = s->h_params[0].cfl_enabled != 0u;
     // one candidate: every setting of the variant, timed over `substeps`
@@ -1595,6 +1649,7 @@ int mpm_autotune(mpm_solver *s, uint32_t substeps, uint32_t *p2g_ctas, uint32_t 
         bool fused;
         int cap;
         unsigned p2g, g2p, substep;
+        int records;
     };
     auto trial = [&](const Candidate &v, double &ms) {
         s->fused = v.fused;
@@ -1602,11 +1657,12 @@ int mpm_autotune(mpm_solver *s, uint32_t substeps, uint32_t *p2g_ctas, uint32_t 
         s->p2g_ctas = v.p2g;
         s->g2p_ctas = v.g2p;
         s->substep_ctas = v.substep;
+        s->records = v.records;
         const cudaError_t r = restore();
         if (r != cudaSuccess) return set_error(MPM_ERR_CUDA, "autotune restore failed: %s", cudaGetErrorString(r));
         return timed_run(s, substeps, guarded, &ms);
     };
-    const Candidate v0{s->fused, s->stage_cap, s->p2g_ctas, s->g2p_ctas, s->substep_ctas};
+    const Candidate v0{s->fused, s->stage_cap, s->p2g_ctas, s->g2p_ctas, s->substep_ctas, s->records};
     Candidate best = v0;
     double best_ms_total = 1e300;
     auto consider = [&](const Candidate &v) {
@@ -1629,17 +1685,24 @@ int mpm_autotune(mpm_solver *s, uint32_t substeps, uint32_t *p2g_ctas, uint32_t 
             if (q != cudaSuccess) rc = set_error(MPM_ERR_CUDA, "autotune occupancy failed: %s", cudaGetErrorString(q));
         }
         for (int k = 1; can_fuse && rc == MPM_OK && k <= per_sm_substep; ++k)
-            consider(Candidate{true, cap, v0.p2g, v0.g2p, (unsigned)(sms * k)});
-        Candidate four{false, cap, v0.p2g, v0.g2p, v0.substep};
+            consider(Candidate{true, cap, v0.p2g, v0.g2p, (unsigned)(sms * k), v0.records});
+        Candidate four{false, cap, v0.p2g, v0.g2p, v0.substep, v0.records};
         double four_ms = 1e300;
         for (int k = 1; rc == MPM_OK && k <= std::max(1, per_sm_p2g); ++k) {
-            const Candidate v{false, cap, std::min(tiles, (unsigned)(sms * k)), v0.g2p, v0.substep};
+            const Candidate v{false, cap, std::min(tiles, (unsigned)(sms * k)), v0.g2p, v0.substep, v0.records};
             double ms = 0.0;
             rc = trial(v, ms);
             if (rc == MPM_OK && ms < four_ms) four_ms = ms, four = v;
         }
         for (int k = 1; rc == MPM_OK && k <= std::max(1, per_sm_g2p); ++k) {
-            const Candidate v{false, cap, four.p2g, std::min(tiles, (unsigned)(sms * k)), v0.substep};
+            const Candidate v{false, cap, four.p2g, std::min(tiles, (unsigned)(sms * k)), v0.substep, v0.records};
+            double ms = 0.0;
+            rc = trial(v, ms);
+            if (rc == MPM_OK && ms < four_ms) four_ms = ms, four = v;
+        }
+        // both ways of handing prepareParticle's results to P2G, with the best grids
+        for (int r = 0; can_fuse && rc == MPM_OK && r < 2; ++r) {
+            const Candidate v{false, cap, four.p2g, four.g2p, v0.substep, r};
             double ms = 0.0;
             rc = trial(v, ms);
             if (rc == MPM_OK && ms < four_ms) four_ms = ms, four = v;
@@ -1663,6 +1726,7 @@ int mpm_autotune(mpm_solver *s, uint32_t substeps, uint32_t *p2g_ctas, uint32_t 
     s->p2g_ctas = chosen.p2g;
     s->g2p_ctas = chosen.g2p;
     s->substep_ctas = chosen.substep;
+    s->records = chosen.records;
     drop_graphs(s);
     s->batch_timed = false;  // the batch events now time the trials
     if (rc != MPM_OK) return rc;

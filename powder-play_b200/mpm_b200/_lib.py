@@ -144,9 +144,9 @@ def load_library(path: str = LIBRARY_PATH) -> ctypes.CDLL:
     lib.mpm_get_launch_shape.restype = i32
     lib.mpm_autotune.argtypes = [vp, u32, P(u32), P(u32), P(ctypes.c_double)]
     lib.mpm_autotune.restype = i32
-    lib.mpm_set_substep_variant.argtypes = [vp, u32, u32, u32, u32]
+    lib.mpm_set_substep_variant.argtypes = [vp, u32, u32, u32, u32, u32]
     lib.mpm_set_substep_variant.restype = i32
-    lib.mpm_get_substep_variant.argtypes = [vp, P(u32), P(u32), P(u32), P(u32), P(u32)]
+    lib.mpm_get_substep_variant.argtypes = [vp, P(u32), P(u32), P(u32), P(u32), P(u32), P(u32)]
     lib.mpm_get_substep_variant.restype = i32
     lib.mpm_set_barrier_limit.argtypes = [vp, ctypes.c_uint64, u32]
     lib.mpm_set_barrier_limit.restype = i32

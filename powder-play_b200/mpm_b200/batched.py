@@ -327,23 +327,26 @@ class MpmBatchedGpuSolver:
     def substep_variant(self) -> dict:
         """How the default path runs a substep: `fused` (one cooperative launch
         of persistent CTAs, else four launches), the P2G stage capacity, the
-        one-launch form's persistent grid and its co-resident limit, and
-        whether G2P runs its water-and-oil instantiation."""
-        f, cap, n, most, liq = (ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32(),
-                                ctypes.c_uint32())
+        one-launch form's persistent grid and its co-resident limit, whether
+        G2P runs its water-and-oil instantiation and whether G2P writes the
+        next P2G's records."""
+        f, cap, n, most, liq, rec = (ctypes.c_uint32() for _ in range(6))
         _check(self._lib.mpm_get_substep_variant(self._handle, ctypes.byref(f), ctypes.byref(cap), ctypes.byref(n),
-                                                 ctypes.byref(most), ctypes.byref(liq)), "substep variant read failed")
+                                                 ctypes.byref(most), ctypes.byref(liq), ctypes.byref(rec)),
+               "substep variant read failed")
         return {"fused": bool(f.value), "stageCapacity": int(cap.value), "substepCtas": int(n.value),
-                "maxSubstepCtas": int(most.value), "liquidKernels": bool(liq.value)}
+                "maxSubstepCtas": int(most.value), "liquidKernels": bool(liq.value), "p2gRecords": bool(rec.value)}
 
     def set_substep_variant(self, fused: bool = True, stage_capacity: int = 0, substep_ctas: int = 0,
-                            liquid_kernels: bool = True) -> None:
+                            liquid_kernels: bool = True, p2g_records=None) -> None:
         """Chooses the substep variant (mpm_set_substep_variant; 0 keeps the
-        stage capacity or the grid).  Results do not depend on `fused`, the
-        grid or `liquid_kernels`."""
+        stage capacity or the grid; `p2g_records` None picks by the
+        materials).  Results do not depend on `fused`, the grid,
+        `liquid_kernels` or `p2g_records`."""
         self._assert_active()
+        records = 2 if p2g_records is None else (1 if p2g_records else 0)
         _check(self._lib.mpm_set_substep_variant(self._handle, 1 if fused else 0, int(stage_capacity),
-                                                 int(substep_ctas), 1 if liquid_kernels else 0),
+                                                 int(substep_ctas), 1 if liquid_kernels else 0, records),
                "substep variant change failed")
 
     def set_barrier_limit(self, limit_ns: int, skip_cta: int = 0xFFFFFFFF) -> None:

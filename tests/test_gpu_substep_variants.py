@@ -5,7 +5,8 @@ A substep runs either as ONE cooperative launch of persistent CTAs
 barriers between the phases) or as four launches of the same device code, so
 the two forms must agree bit for bit, whatever the persistent grid; so must
 G2P's water-and-oil instantiation and its general one on a scene of water
-and oil.  The
+and oil, and the two ways of handing prepareParticle's results to P2G
+(records written by G2P, or each particle prepared in P2G).  The
 narrow P2G stage (384 particles) changes only how a crowded tile is cut into
 chunks, so it must stay within the oracle tolerances.  A CTA that leaves
 before the first barrier without arriving makes the others' waits run out:
@@ -56,6 +57,9 @@ def test_one_launch_and_four_launches_agree_bitwise_on_a_dam_break():
                           "four": dict(fused=False, stage_capacity=640),
                           "four_general": dict(fused=False, stage_capacity=640, liquid_kernels=False),
                           "one_general": dict(fused=True, stage_capacity=640, liquid_kernels=False),
+                          "four_records": dict(fused=False, stage_capacity=640, p2g_records=True),
+                          "four_records_general": dict(fused=False, stage_capacity=640, p2g_records=True,
+                                                       liquid_kernels=False),
                           "one_narrow": dict(fused=True, stage_capacity=384),
                           "four_narrow": dict(fused=False, stage_capacity=384)}.items():
         packed, status, chosen = _step(p, config, variant, 24, dt, DAM_BREAK_GRAVITY)
@@ -63,10 +67,14 @@ def test_one_launch_and_four_launches_agree_bitwise_on_a_dam_break():
         assert chosen["fused"] == variant["fused"] and chosen["stageCapacity"] == variant["stage_capacity"]
         # water and oil only: G2P runs its water-and-oil instantiation unless told not to
         assert chosen["liquidKernels"] == variant.get("liquid_kernels", True)
+        # linear-EOS liquids: P2G prepares each particle unless records are asked for
+        assert chosen["p2gRecords"] == variant.get("p2g_records", False)
         runs[name] = packed
     assert np.array_equal(_bits(runs["one"]), _bits(runs["four"]))
     assert np.array_equal(_bits(runs["four"]), _bits(runs["four_general"]))
     assert np.array_equal(_bits(runs["one"]), _bits(runs["one_general"]))
+    assert np.array_equal(_bits(runs["four"]), _bits(runs["four_records"]))
+    assert np.array_equal(_bits(runs["four"]), _bits(runs["four_records_general"]))
     assert np.array_equal(_bits(runs["one"]), _bits(runs["one_148"]))
     assert np.array_equal(_bits(runs["one_narrow"]), _bits(runs["four_narrow"]))
     # both stage capacities agree within the oracle tolerances (position 1e-3 dx)
@@ -102,36 +110,41 @@ def test_crowded_tiles_match_the_oracle_in_every_variant(per_side):
     ref.run(dict(config, dt=dt32, gravity=SI_TANK_GRAVITY), steps)
     dx = config["grid"]["cellSize"]
     results = {}
-    for fused in (True, False):
+    for fused, records in ((True, None), (False, True), (False, False)):
         for cap in (640, 384):
-            packed, status, _ = _step(p, config, dict(fused=fused, stage_capacity=cap), steps, dt, SI_TANK_GRAVITY)
+            packed, status, _ = _step(p, config, dict(fused=fused, stage_capacity=cap, p2g_records=records), steps,
+                                      dt, SI_TANK_GRAVITY)
             assert status[0] == 0
             assert np.max(np.abs(packed[:, 0:2].astype(np.float64) - ref.positions())) <= 1e-3 * dx
             vel_err = np.abs(packed[:, 2:4].astype(np.float64) - ref.velocities()) / (1 + np.abs(ref.velocities()))
             assert np.max(vel_err) <= 1e-3
-            results[(fused, cap)] = packed
+            results[(fused, records, cap)] = packed
     for cap in (640, 384):
-        assert np.array_equal(_bits(results[(True, cap)]), _bits(results[(False, cap)]))
+        assert np.array_equal(_bits(results[(True, None, cap)]), _bits(results[(False, True, cap)]))
+        assert np.array_equal(_bits(results[(True, None, cap)]), _bits(results[(False, False, cap)]))
 
 
 def test_batched_scenes_agree_bitwise_in_one_launch_and_four():
     scenes = create_batched_tank_scenes(7, seed=5, particles=(200, 4000), sides=(20, 128))
     out = {}
-    for fused, liquid in ((True, True), (False, True), (False, False)):
+    for fused, liquid, records in ((True, True, None), (False, True, None), (False, False, None),
+                                   (False, True, False)):
         batch = create_mpm_batched_gpu_solver(scenes)
         try:
-            batch.set_substep_variant(fused=fused, stage_capacity=640, liquid_kernels=liquid)
+            batch.set_substep_variant(fused=fused, stage_capacity=640, liquid_kernels=liquid, p2g_records=records)
             chosen = batch.substep_variant()
             assert chosen["fused"] == fused and chosen["liquidKernels"] == liquid
+            # several scenes: records by default (the one-launch form prepares in P2G)
+            assert chosen["p2gRecords"] == (not fused and records is not False)
             dts = [2e-4 * (1 + 0.1 * k) for k in range(batch.scene_count)]
             batch.step_batch([4 + (k % 3) for k in range(batch.scene_count)], dts, BATCHED_TANK_GRAVITY)
             batch.step_batch([0 if k % 2 else 3 for k in range(batch.scene_count)], dts, BATCHED_TANK_GRAVITY)
             assert all(e is None for e in batch.check_numerical_status())
-            out[(fused, liquid)] = [batch.read_particles_packed(k)[0] for k in range(batch.scene_count)]
+            out[(fused, liquid, records)] = [batch.read_particles_packed(k)[0] for k in range(batch.scene_count)]
         finally:
             batch.dispose()
-    for other in ((False, True), (False, False)):
-        for k, (a, b) in enumerate(zip(out[(True, True)], out[other])):
+    for other in ((False, True, None), (False, False, None), (False, True, False)):
+        for k, (a, b) in enumerate(zip(out[(True, True, None)], out[other])):
             assert np.array_equal(_bits(a), _bits(b)), f"scene {k}, variant {other}"
 
 
