@@ -1096,6 +1096,18 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage<CAP> &sm, const ui
     sm.count[me] = 0u;
     group_sync<GROUPS>();
     const uint32_t n = i1 - i0;
+    // Up to the cell counts every thread works on the entries it copies in
+    // itself (k = me, me + TILE_CELLS, ...), which its own cp.async wait makes
+    // visible to it, so no group barrier is needed before the counts are read.
+    uint32_t mask = 0;
+    // the entry's arrival rank within its cell; from here on its word holds
+    // its sort key: channel in the top two bits over the original index
+    // (below 2^30: far more particles than the device memory holds)
+    auto count_entry = [&](uint32_t k, uint32_t cell) {
+        sm.order[k] = (uint16_t)atomicAdd(&sm.count[cell & 0xffu], 1u);
+        mask |= 1u << ((cell >> 8) & 3u);
+        sm.orig[k] |= ((cell >> 8) & 3u) << 30;
+    };
     if constexpr (REC) {
         // the records variant: the P2G records the previous G2P (or the
         // batch prologue) wrote
@@ -1109,7 +1121,6 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage<CAP> &sm, const ui
             cp_async<4>(&sm.cell[k], &c.rec_cell[s]);
         }
         cp_async_wait_all();
-        group_sync<GROUPS>();
         for (uint32_t k = me; k < n; k += TILE_CELLS) {
             const uint32_t cell = sm.cell[k];
             if (cell & REC_FAILED) {  // the record carries prepareParticle's flags
@@ -1118,7 +1129,10 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage<CAP> &sm, const ui
                     fail_at(c.status, sm.orig[k], __float_as_uint(f.x));
                 else
                     fail(c.status, __float_as_uint(f.x));
+                sm.failed = 1;
+                continue;
             }
+            count_entry(k, cell);
         }
     } else {
         // the state prepareParticle reads: F, C, v and the material index copied
@@ -1148,7 +1162,6 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage<CAP> &sm, const ui
             }
         }
         cp_async_wait_all();
-        group_sync<GROUPS>();
         // prepareParticle (shaders.ts:808-963) of this thread's entries, in place:
         // (fx, fy, mass, liquid volume), the affine momentum, m v and the entry's
         // local cell | channel << 8 (| REC_FAILED after raising its status)
@@ -1186,23 +1199,12 @@ __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage<CAP> &sm, const ui
                     }
                 }
                 sm.cell[k] = cell;
+                if (cell & REC_FAILED)  // its status is raised
+                    sm.failed = 1;
+                else
+                    count_entry(k, cell);
             }
         }
-        group_sync<GROUPS>();
-    }
-    uint32_t mask = 0;
-    for (uint32_t k = me; k < n; k += TILE_CELLS) {
-        const uint32_t cell = sm.cell[k];
-        if (cell & REC_FAILED) {  // its status is raised
-            sm.failed = 1;
-            continue;
-        }
-        sm.order[k] = (uint16_t)atomicAdd(&sm.count[cell & 0xffu], 1u);
-        mask |= 1u << ((cell >> 8) & 3u);
-        // from here on the entry's word holds its sort key: channel in the top
-        // two bits over the original index (below 2^30: far more particles
-        // than the device memory holds)
-        sm.orig[k] |= ((cell >> 8) & 3u) << 30;
     }
     if (mask) atomicOr(&sm.mask, mask);
     group_sync<GROUPS>();

@@ -20,8 +20,9 @@ import pytest
 from mpm_b200 import create_mpm_batched_gpu_solver, create_mpm_mls_gpu_solver
 from mpm_b200.errors import decode_numerical_error, is_recoverable_cfl_error
 from mpm_b200.layout import ParticleArrays
-from mpm_b200.scenes import (BATCHED_TANK_GRAVITY, DAM_BREAK_GRAVITY, SI_TANK_GRAVITY, create_batched_tank_scenes,
-                             create_dam_break_scene, create_si_tank_scene)
+from mpm_b200.scenes import (BATCHED_TANK_GRAVITY, DAM_BREAK_GRAVITY, GATE4_FIXED_STEP_SECONDS, SI_TANK_GRAVITY,
+                             create_batched_tank_scenes, create_dam_break_scene, create_mpm_gate4_scene,
+                             create_mpm_gate4_step_config, create_si_tank_scene)
 from oracle import OracleState
 
 pytestmark = pytest.mark.gpu
@@ -146,6 +147,25 @@ def test_batched_scenes_agree_bitwise_in_one_launch_and_four():
     for other in ((False, True, None), (False, False, None), (False, True, False)):
         for k, (a, b) in enumerate(zip(out[(True, True, None)], out[other])):
             assert np.array_equal(_bits(a), _bits(b)), f"scene {k}, variant {other}"
+
+
+def test_bonded_bodies_and_fracture_agree_bitwise_with_and_without_records():
+    # the multi-material scene: water, oil, bonded-triangle pebbles and a
+    # fractured Neo-Hookean block (bodies take four launches and the general
+    # G2P; their moved particles get their bucket keys, and records when
+    # used, from the body pass)
+    p, bonds, _ = create_mpm_gate4_scene()
+    config = create_mpm_gate4_step_config(fracture_bonds=bonds)
+    dt = GATE4_FIXED_STEP_SECONDS / 5
+    out = {}
+    for records in (True, False):
+        packed, status, chosen = _step(p, config, dict(fused=False, p2g_records=records), 6, dt, config["gravity"])
+        assert status[0] == 0 and not chosen["fused"] and not chosen["liquidKernels"]
+        assert chosen["p2gRecords"] == records
+        out[records] = packed
+    assert np.array_equal(_bits(out[True]), _bits(out[False]))
+    # and the damage word of the fractured block
+    assert np.array_equal(out[True][:, 18].view(np.uint32), out[False][:, 18].view(np.uint32))
 
 
 def test_a_barrier_wait_that_runs_out_reports_the_status_and_the_solver_recovers():
