@@ -19,11 +19,13 @@ import pytest
 
 from mpm_b200 import create_mpm_batched_gpu_solver, create_mpm_mls_gpu_solver
 from mpm_b200.errors import decode_numerical_error, is_recoverable_cfl_error
-from mpm_b200.layout import ParticleArrays
+from mpm_b200.layout import ParticleArrays, particles_from_dicts
 from mpm_b200.scenes import (BATCHED_TANK_GRAVITY, DAM_BREAK_GRAVITY, GATE4_FIXED_STEP_SECONDS, SI_TANK_GRAVITY,
                              create_batched_tank_scenes, create_dam_break_scene, create_mpm_gate4_scene,
                              create_mpm_gate4_step_config, create_si_tank_scene)
 from oracle import OracleState
+
+from helpers import transfer_regression_fixture
 
 pytestmark = pytest.mark.gpu
 
@@ -147,6 +149,21 @@ def test_batched_scenes_agree_bitwise_in_one_launch_and_four():
     for other in ((False, True, None), (False, False, None), (False, True, False)):
         for k, (a, b) in enumerate(zip(out[(True, True, None)], out[other])):
             assert np.array_equal(_bits(a), _bits(b)), f"scene {k}, variant {other}"
+
+
+def test_every_material_model_agrees_bitwise_with_and_without_records():
+    # the reference's 45-particle five-model fixture (Neo-Hookean, snow, water,
+    # oil, powder): P2G's general prepare path against the records G2P writes
+    particles, config = transfer_regression_fixture()
+    p = particles_from_dicts(particles)
+    out = {}
+    for records in (True, False):
+        packed, status, chosen = _step(p, config, dict(fused=False, p2g_records=records), 16, 0.01,
+                                       {"x": 0.0, "y": -0.5})
+        assert status[0] == 0 and chosen["p2gRecords"] == records and not chosen["liquidKernels"]
+        out[records] = packed
+    assert np.array_equal(np.ascontiguousarray(out[True]).view(np.uint32),
+                          np.ascontiguousarray(out[False]).view(np.uint32))
 
 
 def test_bonded_bodies_and_fracture_agree_bitwise_with_and_without_records():
