@@ -240,6 +240,20 @@ __device__ __forceinline__ Ctx tile_ctx(const Ctx &c0, uint32_t tile)
         return c0;
 }
 
+// The substep's listed tiles: the heavy ones (more particles than a stage)
+// first, from the end of the list array, then the light ones from its start.
+__device__ __forceinline__ uint32_t listed_count(const Ctx &c)
+{
+    return __ldcg(c.work + WORK_ACTIVE + c.parity) + __ldcg(c.work + WORK_HEAVY + c.parity);
+}
+
+__device__ __forceinline__ uint32_t heavy_count(const Ctx &c) { return __ldcg(c.work + WORK_HEAVY + c.parity); }
+
+__device__ __forceinline__ const uint32_t *listed_tile(const Ctx &c, uint32_t item, uint32_t heavy)
+{
+    return item < heavy ? c.active_tiles + (c.n_tiles - 1u - item) : c.active_tiles + (item - heavy);
+}
+
 // Whether the scene takes part in the current substep: no status raised and
 // substeps of this batch left.
 __device__ __forceinline__ bool takes_part(const Ctx &c)
@@ -410,6 +424,8 @@ __global__ void k_begin_batch(Ctx c, uint32_t reset_progress)
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         c.work[WORK_ACTIVE] = 0u;
         c.work[WORK_ACTIVE + 1] = 0u;
+        c.work[WORK_HEAVY] = 0u;
+        c.work[WORK_HEAVY + 1] = 0u;
         c.work[WORK_BARRIER] = 0u;  // an abandoned launch may have left arrivals
         c.work[WORK_ABORT] = 0u;
     }
@@ -824,7 +840,7 @@ __device__ __forceinline__ bool runs_flag(const Ctx &c, uint32_t scene)
 // Allocation chunk b (1024 tiles of one scene) with ALLOC_THREADS threads.
 __device__ __forceinline__ void alloc_chunk(const Ctx &c0, uint32_t b)
 {
-    __shared__ uint32_t s_base[2];
+    __shared__ uint32_t s_base[3];
     __shared__ bool s_runs;
     const bool one_scene = c0.n_scenes == 1u;
     const uint32_t scene = one_scene ? 0u : scene_of_chunk(c0, b);
@@ -836,7 +852,13 @@ __device__ __forceinline__ void alloc_chunk(const Ctx &c0, uint32_t b)
         const bool runs = substep_runs(c);
         s_runs = runs;
         c.counters[COUNTER_RUNS] = runs ? 1u : 0u;  // the same value from every CTA of the scene
-        if (b == 0) c0.work[WORK_ACTIVE + (c0.parity ^ 1u)] = 0u;
+        if (b == 0) {
+            // the next substep's lists start empty; this substep's tile claims start at 0
+            c0.work[WORK_ACTIVE + (c0.parity ^ 1u)] = 0u;
+            c0.work[WORK_HEAVY + (c0.parity ^ 1u)] = 0u;
+            c0.work[WORK_CLAIM] = 0u;
+            c0.work[WORK_CLAIM + 1] = 0u;
+        }
     }
     // the counts are read before the answer is known (they exist either way)
     uint32_t *count = c.tile_count + P.tile_base;  // 32-byte aligned: scenes start on 8-tile boundaries
@@ -854,24 +876,29 @@ __device__ __forceinline__ void alloc_chunk(const Ctx &c0, uint32_t b)
     __syncthreads();
     if (s_runs) {
         uint2 *range = c.tile_range + P.tile_base;
-        uint32_t sum = 0, nonempty = 0;
+        uint32_t sum = 0, light = 0, heavy = 0;
 #pragma unroll
         for (int k = 0; k < ALLOC_ITEMS; ++k) {
             sum += v[k];
-            nonempty += v[k] != 0u;
+            light += v[k] != 0u && v[k] <= HEAVY_TILE;
+            heavy += v[k] > HEAVY_TILE;
         }
-        // particles in the high word, listed tiles (at most 1024) in the low
+        // particles in the high word; listed light and heavy tiles (at most
+        // 1024 each) in the low and high halves of the low word
         unsigned long long total;
-        const unsigned long long offset =
-            block_exclusive_scan<ALLOC_THREADS, unsigned long long>(((unsigned long long)sum << 32) | nonempty, total);
+        const unsigned long long offset = block_exclusive_scan<ALLOC_THREADS, unsigned long long>(
+            ((unsigned long long)sum << 32) | (heavy << 16) | light, total);
         if (threadIdx.x == 0) {
-            const uint32_t particles = (uint32_t)(total >> 32), listed = (uint32_t)total;
+            const uint32_t particles = (uint32_t)(total >> 32), n_light = (uint32_t)total & 0xffffu,
+                           n_heavy = ((uint32_t)total >> 16) & 0xffffu;
             s_base[0] = particles ? atomicAdd(c.counters + COUNTER_CURSOR, particles) : 0u;
-            s_base[1] = listed ? atomicAdd(c0.work + WORK_ACTIVE + c0.parity, listed) : 0u;
+            s_base[1] = n_light ? atomicAdd(c0.work + WORK_ACTIVE + c0.parity, n_light) : 0u;
+            s_base[2] = n_heavy ? atomicAdd(c0.work + WORK_HEAVY + c0.parity, n_heavy) : 0u;
         }
         __syncthreads();
         uint32_t at = s_base[0] + (uint32_t)(offset >> 32);
-        uint32_t slot = s_base[1] + (uint32_t)offset;
+        uint32_t slot = s_base[1] + ((uint32_t)offset & 0xffffu);
+        uint32_t heavy_slot = s_base[2] + (((uint32_t)offset >> 16) & 0xffffu);
         uint2 r[ALLOC_ITEMS];
 #pragma unroll
         for (int k = 0; k < ALLOC_ITEMS; ++k) {
@@ -891,10 +918,15 @@ __device__ __forceinline__ void alloc_chunk(const Ctx &c0, uint32_t b)
                 }
             }
         }
-        if (nonempty) {
+        if (light | heavy) {
+            // light tiles from the front of the list, heavy ones from its end
 #pragma unroll
-            for (int k = 0; k < ALLOC_ITEMS; ++k)
-                if (v[k] != 0u) c.active_tiles[slot++] = P.tile_base + first + k;
+            for (int k = 0; k < ALLOC_ITEMS; ++k) {
+                if (v[k] > HEAVY_TILE)
+                    c.active_tiles[c0.n_tiles - 1u - heavy_slot++] = P.tile_base + first + k;
+                else if (v[k] != 0u)
+                    c.active_tiles[slot++] = P.tile_base + first + k;
+            }
         }
     }
 }
@@ -988,6 +1020,7 @@ struct Stage {
     uint32_t warp_active[TILE_CELLS / 32];
     uint32_t mask;
     int failed;
+    uint32_t item;  // the tile this group claimed (several scenes)
 };
 
 // A P2G tile is taken by a group of TILE_CELLS threads (one per cell of the
@@ -1342,9 +1375,22 @@ __device__ __forceinline__ void p2g_tiles(const Ctx &c0, Stage<CAP> *stages)
     const uint32_t g = p2g_group<GROUPS>();
     const uint32_t me = threadIdx.x % TILE_CELLS;
     Stage<CAP> &sm = stages[g];
-    const uint32_t n_active = __ldcg(c0.work + WORK_ACTIVE + c0.parity);
-    for (uint32_t item = blockIdx.x * GROUPS + g; item < n_active; item += gridDim.x * GROUPS) {
-        const uint32_t tile = __ldcg(c0.active_tiles + item);
+    const uint32_t n_active = listed_count(c0), n_heavy = heavy_count(c0);
+    // several scenes: each group claims its next tile (the heavy ones are
+    // listed first), which evens out tiles of very different sizes; one scene
+    // (tiles of similar size): a fixed stride
+    auto next = [&](uint32_t prev) -> uint32_t {
+        if constexpr (SCENES) {
+            group_sync<GROUPS>();  // the readers of the previous claim are done
+            if (me == 0) sm.item = atomicAdd(c0.work + WORK_CLAIM, 1u);
+            group_sync<GROUPS>();
+            return sm.item;
+        } else {
+            return prev + gridDim.x * GROUPS;
+        }
+    };
+    for (uint32_t item = SCENES ? next(0u) : blockIdx.x * GROUPS + g; item < n_active; item = next(item)) {
+        const uint32_t tile = __ldcg(listed_tile(c0, item, n_heavy));
         const Ctx c = tile_ctx<SCENES>(c0, tile);
         const uint32_t stamp = __ldcg(c.counters + COUNTER_STAMP);
         const uint2 range = __ldcg(c.tile_range + tile);
@@ -2207,6 +2253,7 @@ struct G2PShared {
     float4 vw[RING_NODES];
     float4 vo[RING_NODES];
     int fail;
+    uint32_t claim;  // the tile this CTA claimed (several scenes)
     // the particles of the tile (or of one chunk of a crowded tile), copied
     // in while the node phase runs
     float4 F[G2P_STAGE];
@@ -2232,20 +2279,33 @@ __device__ __forceinline__ void g2p_tiles(const Ctx &c0, G2PShared &sh)
     float2 *const p_pos = sh.pos;
     float *const p_vol = sh.vol_in, *const p_pvol = sh.pvol_in, *const p_damage = sh.damage;
     uint32_t *const p_mat = sh.mat, *const p_orig = sh.orig;
-    const uint32_t n_active = __ldcg(c0.work + WORK_ACTIVE + c0.parity);
+    const uint32_t n_active = listed_count(c0), n_heavy = heavy_count(c0);
     uint32_t ws = 0, ww = 0, wo = 0;
     if constexpr (!SCENES) {
         // visible after the first iteration's barrier
-        if (threadIdx.x == 0 && blockIdx.x + gridDim.x < n_active) s_tile[1] = c0.active_tiles[blockIdx.x + gridDim.x];
+        if (threadIdx.x == 0 && blockIdx.x + gridDim.x < n_active)
+            s_tile[1] = *listed_tile(c0, blockIdx.x + gridDim.x, n_heavy);
     }
+    // several scenes: each CTA claims its next tile (the heavy ones are listed
+    // first); one scene: a fixed stride, with the next tile's data copied in
+    auto next = [&](uint32_t prev) -> uint32_t {
+        if constexpr (SCENES) {
+            __syncthreads();  // the readers of the previous claim are done
+            if (threadIdx.x == 0) sh.claim = atomicAdd(c0.work + WORK_CLAIM + 1, 1u);
+            __syncthreads();
+            return sh.claim;
+        } else {
+            return prev + gridDim.x;
+        }
+    };
     uint32_t it = 0;
-    for (uint32_t item = blockIdx.x; item < n_active; item += gridDim.x, ++it) {
+    for (uint32_t item = SCENES ? next(0u) : blockIdx.x; item < n_active; item = next(item), ++it) {
         const uint32_t buf = it & 1u;
         const bool fetched = !SCENES && it > 0u;  // copied in during the previous tile
         uint2 *const info = s_infos[buf];
         // (the copies read here landed, and were made visible by a barrier,
         // during the previous tile)
-        const uint32_t tile = fetched ? s_tile[buf] : c0.active_tiles[item];
+        const uint32_t tile = fetched ? s_tile[buf] : *listed_tile(c0, item, n_heavy);
         const uint32_t nb = buf ^ 1u;
         const Ctx c = tile_ctx<SCENES>(c0, tile);
         const StepParams &P = *c.P;
@@ -2305,7 +2365,7 @@ __device__ __forceinline__ void g2p_tiles(const Ctx &c0, G2PShared &sh)
                 }
             }
             if (threadIdx.x == 10 && item + 2u * gridDim.x < n_active)
-                cp_async<4>(&s_tile[buf], &c0.active_tiles[item + 2u * gridDim.x]);
+                cp_async<4>(&s_tile[buf], listed_tile(c0, item + 2u * gridDim.x, n_heavy));
         }
         if (s_fail) {
             cp_async_wait_all();  // no copy may land after this tile's shared data is reused

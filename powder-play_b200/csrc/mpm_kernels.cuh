@@ -170,7 +170,10 @@ constexpr int SCENE_WORDS = 64;  // per scene: status [0, 32), counters [32, 64)
 constexpr int WORK_ACTIVE = 0;   // work[0], work[1]: tiles listed for the substeps from buffer 0 / 1
 constexpr int WORK_BARRIER = 2;  // work[2]: arrivals at the substep kernel's grid barrier, work[3]: its generation
 constexpr int WORK_ABORT = 4;    // work[4]: non-zero once a barrier wait of the substep kernel ran out
-constexpr int WORK_WORDS = 8;
+constexpr int WORK_HEAVY = 5;    // work[5], work[6]: heavy tiles listed for the substeps from buffer 0 / 1
+constexpr int WORK_CLAIM = 7;    // work[7], work[8]: tiles claimed so far by this substep's P2G / G2P (several scenes)
+constexpr int WORK_WORDS = 16;
+constexpr uint32_t HEAVY_TILE = 640;  // a tile holding more particles is listed first (it takes longest)
 constexpr int SUBSTEP_THREADS = 256;  // k_substep: one CTA shape for all four phases
 
 __global__ void k_count(Ctx c);
