@@ -1113,13 +1113,14 @@ __device__ __forceinline__ void scan_cell_counts(uint32_t lane, const uint32_t *
     }
 }
 
-// Stages the records of the slots src[i0 .. i1) with asynchronous copies,
-// raises the status of failed records and groups the entries by cell.  Then
-// the thread of each cell sums the P2G contributions of its particles of
-// one channel, in original-index order, over the 3x3 stencil nodes in
-// registers, and the cells add those sums into the ring accumulator in nine
-// phases, one stencil offset per phase (no two cells of a phase share a
-// node), so every sum has a fixed order.  Returns false once a record had
+// Stages the particles of the slots src[i0 .. i1) with asynchronous copies
+// and prepares each of them in shared memory (REC: stages the records G2P
+// wrote), raises the status of failed preparations and groups the entries by
+// cell.  Then the thread of each cell sums the P2G contributions of its
+// particles of one channel, in original-index order, over the 3x3 stencil
+// nodes in registers, and the cells add those sums into the ring accumulator
+// in nine phases, one stencil offset per phase (no two cells of a phase share
+// a node), so every sum has a fixed order.  Returns false once a particle
 // failed.
 template <int CAP, int GROUPS, bool LIQ, bool REC>
 __device__ __forceinline__ bool p2g_chunk(const Ctx &c, Stage<CAP> &sm, const uint32_t *src, uint32_t i0, uint32_t i1)
