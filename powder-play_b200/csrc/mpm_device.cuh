@@ -98,10 +98,15 @@ struct alignas(16) StepParams {
     float bond_rest_length, bond_stiffness, band, contact_reach;
     float cfl_wave_bound, cfl_velocity_limit, bond_reference_dt, wall_friction;
     float fixed_scale, drag_x, drag_y, drag_radius;
-    float drag_stiffness, drag_damping, inv_dx, pad1;
+    // cfl_speed2_bound / cfl_wave2_bound: the largest float whose correctly
+    // rounded square root is at most cfl_velocity_limit / cfl_wave_bound, so
+    // a speed or wave speed exceeds its bound exactly when its square exceeds
+    // this (NaN for a NaN bound, -1 for a negative one)
+    float drag_stiffness, drag_damping, inv_dx, cfl_speed2_bound;
     // the scene's place in a batch of scenes: its first slot and first tile
     // (its tiles are followed by one sentinel entry) and its tile count
-    uint32_t p_base, tile_base, scene_tiles, pad2;
+    uint32_t p_base, tile_base, scene_tiles;
+    float cfl_wave2_bound;
 };
 
 // Device counters (one 32-word line): stamp of the current substep, committed

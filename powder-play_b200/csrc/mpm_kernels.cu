@@ -1731,41 +1731,41 @@ __global__ void __launch_bounds__(TILE_NODES) k_grid_update(Ctx c)
 
 namespace {
 
-// particleWaveSpeedBound: shaders.ts:268-353
+// particleWaveSpeedBound: shaders.ts:268-353, squared: returns the square
+// whose square root the reference returns, or -1 where it returns FLOAT_MAX.
 // `tait_pow` is (1 / det F)^gamma of a Tait liquid when the caller has it
 // (negative: not computed); (1 / det)^(gamma - 1) is then tait_pow * det.
 template <bool LIQ = false>
-__device__ float wave_speed_bound(const Ctx &c, const Material &m, float4 F, float damage, float volume,
-                                  float tait_pow)
+__device__ float wave_speed_sq(const Ctx &c, const Material &m, float4 F, float damage, float volume, float tait_pow)
 {
     if (LIQ || m.model == MODEL_WATER || m.model == MODEL_OIL) {
-        if (!finite_f(m.lambda) || !finite_f(m.density) || m.lambda <= 0.f || m.density <= 0.f) return FLOAT_MAX;
+        if (!finite_f(m.lambda) || !finite_f(m.density) || m.lambda <= 0.f || m.density <= 0.f) return -1.0f;
         float c2 = m.c2;  // lambda / density, divided once on the host
         if (m.param > 0.0f) {
             const float det = det2(F);
-            if (!finite_f(m.param) || m.param <= 0.f || !finite_f(det) || det <= 0.f) return FLOAT_MAX;
+            if (!finite_f(m.param) || m.param <= 0.f || !finite_f(det) || det <= 0.f) return -1.0f;
             const float scale = tait_pow >= 0.0f ? tait_pow * det : pow_wgsl(1.0f / det, m.param - 1.0f);
             c2 = m.param * c2 * scale;
         }
-        if (!finite_f(c2) || c2 < 0.f) return FLOAT_MAX;
-        return sqrtf(c2);
+        if (!finite_f(c2) || c2 < 0.f) return -1.0f;
+        return c2;
     }
-    if (m.model != MODEL_NEO_HOOKEAN) return FLOAT_MAX;
-    if (!finite_f(damage)) return FLOAT_MAX;
+    if (m.model != MODEL_NEO_HOOKEAN) return -1.0f;
+    if (!finite_f(damage)) return -1.0f;
     const float remaining = 1.0f - fminf(fmaxf(damage, 0.f), 1.f);
     if (remaining <= 0.f) return 0.f;
     const float lambda = m.lambda * remaining, mu = m.mu * remaining;
     const float det = det2(F);
     const float tr = F.x * F.x + F.y * F.y + F.z * F.z + F.w * F.w;
     if (!finite_f(det) || det <= 0.f || !finite_f(tr) || !finite_f(lambda) || !finite_f(mu) || mu < 0.f)
-        return FLOAT_MAX;
+        return -1.0f;
     const float disc = sqrtf(fmaxf(0.f, tr * tr - 4.0f * det * det));
     const float maxs2 = 0.5f * (tr + disc);
     const float vt = fabsf(lambda + mu - lambda * logf(det));
     const float rho = c.P->particle_mass / volume;
     const float c2 = (mu * maxs2 + vt) / rho;
-    if (!finite_f(rho) || rho <= 0.f || !finite_f(c2) || c2 < 0.f) return FLOAT_MAX;
-    return sqrtf(c2);
+    if (!finite_f(rho) || rho <= 0.f || !finite_f(c2) || c2 < 0.f) return -1.0f;
+    return c2;
 }
 
 __device__ __forceinline__ void copy_particle(const Ctx &c, uint32_t from, uint32_t to)
@@ -1788,13 +1788,20 @@ __device__ void validate_cfl(const Ctx &c, uint32_t id, const Material &m, float
 {
     const StepParams &P = *c.P;
     if (!P.cfl_enabled) return;
-    const float speed = length2(vel);
-    const float wave = wave_speed_bound<LIQ>(c, m, F, damage, volume, tait_pow);
-    if (!finite2(vel) || !finite_f(speed) || !finite_f(wave) || speed > P.cfl_velocity_limit ||
-        wave > P.cfl_wave_bound) {
+    // The speed and the wave speed are compared through their squares: a
+    // correctly rounded square root exceeds a bound exactly when its argument
+    // exceeds the bound's square_bound (a non-finite square is a non-finite
+    // speed), and the wave speed is finite (FLOAT_MAX where the reference
+    // gives up), so the decisions are the reference's.
+    const float s2 = __fadd_rn(__fmul_rn(vel.x, vel.x), __fmul_rn(vel.y, vel.y));
+    const float c2 = wave_speed_sq<LIQ>(c, m, F, damage, volume, tait_pow);
+    const bool wave_out = c2 < 0.0f ? FLOAT_MAX > P.cfl_wave_bound : c2 > P.cfl_wave2_bound;
+    if (!finite2(vel) || !finite_f(s2) || s2 > P.cfl_speed2_bound || wave_out) {
         // the reference reads the status word before the bounds; a particle
         // within them records nothing either way, so only a violation reads it
         if (*(volatile uint32_t *)c.status != 0u) return;
+        const float speed = length2(vel);
+        const float wave = c2 < 0.0f ? FLOAT_MAX : sqrtf(c2);
         const uint32_t prev = atomicOr(c.status + 6, 3u);
         if (prev == 0u) {
             atomicExch(c.status + 1, id);

@@ -574,6 +574,25 @@ int get_graph(mpm_solver *s, int log2_steps, int parity, cudaGraphExec_t *out)
     return MPM_OK;
 }
 
+// The largest float t >= 0 with sqrt(t) <= bound (square roots correctly
+// rounded, as the device's are): a square root of s > bound exactly when
+// s > t, for every finite s >= 0.  sqrt is monotone, so t is found from
+// bound^2 by stepping one ulp at a time (a step or two).
+static float square_bound(float bound)
+{
+    if (std::isnan(bound)) return bound;
+    if (bound < 0.0f) return -1.0f;
+    if (std::isinf(bound)) return bound;
+    float t = (float)((double)bound * (double)bound);
+    while (t > 0.0f && std::sqrt(t) > bound) t = std::nextafter(t, 0.0f);
+    for (;;) {
+        const float up = std::nextafter(t, INFINITY);
+        if (!std::isfinite(up) || std::sqrt(up) > bound) break;
+        t = up;
+    }
+    return t;
+}
+
 void fill_params(mpm_solver *s, uint32_t scene, StepParams &p, float dt, float gx, float gy,
                  const mpm_cfl_guard *guard, float bond_reference_dt, uint32_t steps)
 {
@@ -620,6 +639,8 @@ void fill_params(mpm_solver *s, uint32_t scene, StepParams &p, float dt, float g
     p.contact_reach = (float)(std::sqrt((double)c.particle_volume / M_PI) + (double)c.cell_size * 0.75);
     p.cfl_wave_bound = guard ? guard->wave_speed_bound : 0.0f;
     p.cfl_velocity_limit = guard ? guard->velocity_limit : 0.0f;
+    p.cfl_wave2_bound = square_bound(p.cfl_wave_bound);
+    p.cfl_speed2_bound = square_bound(p.cfl_velocity_limit);
     p.bond_reference_dt = bond_reference_dt > 0.0f ? bond_reference_dt
                                                    : (c.bond_reference_dt > 0.0f ? c.bond_reference_dt : dt);
     p.wall_friction = c.wall_friction;

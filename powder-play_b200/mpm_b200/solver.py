@@ -801,6 +801,12 @@ class MpmMlsGpuSolver:
                "launch shape read failed")
         return {"p2gCtas": int(p.value), "g2pCtas": int(g.value), "smCount": int(sms.value)}
 
+    def set_launch_shape(self, p2g_ctas: int = 0, g2p_ctas: int = 0) -> None:
+        """Sets the persistent grids of the default path's P2G and G2P
+        kernels (0 keeps a value); results do not depend on them."""
+        self._assert_active()
+        _check(self._lib.mpm_set_launch_shape(self._handle, int(p2g_ctas), int(g2p_ctas)), "launch shape failed")
+
     def autotune(self, substeps: int = 8) -> dict:
         """Picks the fastest persistent grids for P2G and G2P on this
         workload (mpm_autotune: real substeps timed per candidate, the state

@@ -38,10 +38,12 @@ def _bits(packed):
     return np.ascontiguousarray(packed[:, STATE_WORDS]).view(np.uint32)
 
 
-def _step(particles, config, variant, steps, dt, gravity):
+def _step(particles, config, variant, steps, dt, gravity, g2p_ctas=0):
     solver = create_mpm_mls_gpu_solver(particles, config)
     try:
         solver.set_substep_variant(**variant)
+        if g2p_ctas:
+            solver.set_launch_shape(g2p_ctas=g2p_ctas)
         chosen = solver.substep_variant()
         solver.step_batch(steps, dt, gravity)
         status = solver._read_compact()[2]
@@ -83,6 +85,27 @@ def test_one_launch_and_four_launches_agree_bitwise_on_a_dam_break():
     # both stage capacities agree within the oracle tolerances (position 1e-3 dx)
     dx = config["grid"]["cellSize"]
     assert np.max(np.abs(runs["one"][:, 0:2].astype(np.float64) - runs["one_narrow"][:, 0:2])) <= 1e-3 * dx
+
+
+@pytest.mark.parametrize("g2p_ctas", [7, 64])
+def test_small_persistent_g2p_grids_agree_bitwise(g2p_ctas):
+    # With one scene each G2P CTA copies the next tile's bucket range,
+    # neighbour records, first bucket entries and status words in while the
+    # current tile's particles move; a small persistent grid gives every CTA
+    # many tiles, so most tiles run on prefetched data, among them tiles at
+    # the edge of the fluid whose neighbours hold no record or only one
+    # liquid's channel.  The water-and-oil and the general instantiation
+    # must agree bit for bit there too.
+    p, config = create_dam_break_scene(particles_per_phase=20_000, columns=200, grid=SMALL_DAM)
+    dt = 1.0 / 1200.0
+    liquid, status, chosen = _step(p, config, dict(fused=False), 24, dt, DAM_BREAK_GRAVITY, g2p_ctas=g2p_ctas)
+    assert status[0] == 0 and chosen["liquidKernels"]
+    general, status, chosen = _step(p, config, dict(fused=False, liquid_kernels=False), 24, dt, DAM_BREAK_GRAVITY,
+                                    g2p_ctas=g2p_ctas)
+    assert status[0] == 0 and not chosen["liquidKernels"]
+    assert np.array_equal(_bits(liquid), _bits(general))
+    default, status, _ = _step(p, config, dict(fused=False), 24, dt, DAM_BREAK_GRAVITY)
+    assert np.array_equal(_bits(liquid), _bits(default))
 
 
 def _crowded_tank(per_side):
