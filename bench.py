@@ -143,18 +143,19 @@ def build_workload(name: str):
         p, config = create_si_tank_scene(seed=1)
         return p, config, SI_TANK_GRAVITY, {
             "workload": "SI Tait water tank, 1,600 particles, 80x80 grid (dx 2.5 mm), macrostep 1/120 s",
-            "particles": len(p), "grid": "80x80", "macro_dt": 1 / 120, "courant": 0.3}
+            "particles": len(p), "grid": "80x80", "macro_dt": 1 / 120, "courant": 0.3,
+            "max_microsteps": 4096}  # its 20 m/s sound speed takes about 280 substeps per macrostep
     raise SystemExit(f"unknown workload {name}")
 
 
-def plan_macrostep(solver, config, velocity, macro_dt, gravity):
+def plan_macrostep(solver, config, velocity, macro_dt, gravity, max_microsteps=MAX_MICROSTEPS):
     from mpm_b200 import calculate_mpm_cfl_microsteps
     from mpm_b200.cfl_bounds import calculate_mpm_cfl_velocity_bound
     gmag = math.hypot(gravity["x"], gravity["y"])
     bound = calculate_mpm_cfl_velocity_bound(velocity, macro_dt, gmag, 0, 0, 0, 0)
     bound = max(bound, solver._last_scheduled_velocity_bound or 0.0)
     plan = calculate_mpm_cfl_microsteps(macro_dt, config["grid"]["cellSize"], solver.cfl_bounds["waveSpeedBound"],
-                                        bound, MAX_MICROSTEPS)
+                                        bound, max_microsteps)
     return plan, bound
 
 
@@ -732,13 +733,14 @@ def run_b200(args):
         solver = create_mpm_mls_gpu_solver(particles, config, device=local_rank)
     n = len(particles)
     macro_dt = meta["macro_dt"]
+    max_micro = meta.get("max_microsteps", MAX_MICROSTEPS)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
     velocity = solver.cfl_bounds["velocityBound"]
 
     def one_step():
         nonlocal velocity
-        plan, bound = plan_macrostep(solver, config, velocity, macro_dt, gravity)
-        m = solver.step_cfl_batch_adaptive(1, macro_dt, plan, bound, MAX_MICROSTEPS, gravity)
+        plan, bound = plan_macrostep(solver, config, velocity, macro_dt, gravity, max_micro)
+        m = solver.step_cfl_batch_adaptive(1, macro_dt, plan, bound, max_micro, gravity)
         velocity = m["recommendedVelocityBound"]
         return m
 
@@ -790,7 +792,7 @@ def run_b200(args):
     e2e_value = n * substeps / wall
 
     # roofline: kernel-by-kernel timing of real substeps right after the timed region
-    plan, bound = plan_macrostep(solver, config, velocity, macro_dt, gravity)
+    plan, bound = plan_macrostep(solver, config, velocity, macro_dt, gravity, max_micro)
     from mpm_b200.cfl import calculate_mpm_cfl_velocity_limit
     limit = calculate_mpm_cfl_velocity_limit(config["grid"]["cellSize"], solver.cfl_bounds["waveSpeedBound"],
                                              plan["microDt"])
