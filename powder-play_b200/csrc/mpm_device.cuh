@@ -255,6 +255,15 @@ __device__ __forceinline__ float wall_cushion(float vel, int coord, int extent)
     return vel * fminf(fmaxf(dist / cushion, 0.0f), 1.0f);
 }
 
+// Whether every coordinate in [lo, hi] lies at least the cushion from both
+// walls of an axis of `extent` cells: wall_cushion and wall_friction then
+// return the velocity they are given, for either sign.
+__device__ __forceinline__ bool beyond_wall_cushion(int lo, int hi, int extent)
+{
+    const float cushion = fminf(WALL_CUSHION_CELLS, (float)extent / 4.0f);
+    return (float)lo >= cushion && (float)(extent - hi) >= cushion;
+}
+
 __device__ __forceinline__ float wall_friction(float vel, int coord, int extent, float friction)
 {
     if (friction <= 0.0f) return vel;

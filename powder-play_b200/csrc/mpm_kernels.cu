@@ -95,7 +95,7 @@ __device__ __forceinline__ bool liquid_stress(const Material &m, float det, floa
         m.param < 0.0f)
         return false;
     if (m.param > 0.0f) {
-        const float pw = tait_pow >= 0.0f ? tait_pow : pow_wgsl(__fdiv_rn(1.0f, det), m.param);
+        const float pw = tait_pow >= 0.0f ? tait_pow : pow_wgsl(__frcp_rn(det), m.param);
         const float pressure = m.lambda * (pw - 1.0f);
         const float stress = -det * pressure;
         s = make_float4(stress, 0.f, 0.f, stress);
@@ -589,9 +589,13 @@ struct NodeVel {
 // zero outside the halo or where no particle deposited).  Returns false
 // after raising a status.  LIQ: the solver holds no solid particle, so the
 // solid channel (its sums are zero) is not evaluated and its velocity is 0.
+// near_wall false: the caller knows the node lies at least one wall cushion
+// from every wall, where the cushion and the friction leave velocities as
+// they are, so they are not evaluated.
 template <bool BODIES, bool LIQ = false>
 __device__ __forceinline__ bool node_velocity(const Ctx &c, uint32_t n, int x, int y, float4 S, float4 W, float4 O,
-                                              float2 xp, float2 xm, float2 yp, float2 ym, NodeVel &out)
+                                              float2 xp, float2 xm, float2 yp, float2 ym, NodeVel &out,
+                                              bool near_wall = true)
 {
     const StepParams &P = *c.P;
     if ((!LIQ && (!finite_f(S.x) || S.x < 0.f || !finite_f(S.y) || !finite_f(S.z))) || !finite_f(W.x) || W.x < 0.f ||
@@ -692,24 +696,26 @@ __device__ __forceinline__ bool node_velocity(const Ctx &c, uint32_t n, int x, i
         fail(c.status, ERROR_GRID | ERROR_TRIANGLE_CONTACT);
         return false;
     }
-    const int cx = (int)P.cells_x, cy = (int)P.cells_y;
-    const float fr = P.wall_friction;
-    if (!LIQ) {
-        vs.x = wall_cushion(vs.x, x, cx);
-        vs.y = wall_cushion(vs.y, y, cy);
+    if (near_wall) {
+        const int cx = (int)P.cells_x, cy = (int)P.cells_y;
+        const float fr = P.wall_friction;
+        if (!LIQ) {
+            vs.x = wall_cushion(vs.x, x, cx);
+            vs.y = wall_cushion(vs.y, y, cy);
+        }
+        vw.x = wall_cushion(vw.x, x, cx);
+        vw.y = wall_cushion(vw.y, y, cy);
+        vo.x = wall_cushion(vo.x, x, cx);
+        vo.y = wall_cushion(vo.y, y, cy);
+        if (!LIQ) {
+            vs.x = wall_friction(vs.x, y, cy, fr);
+            vs.y = wall_friction(vs.y, x, cx, fr);
+        }
+        vw.x = wall_friction(vw.x, y, cy, fr);
+        vw.y = wall_friction(vw.y, x, cx, fr);
+        vo.x = wall_friction(vo.x, y, cy, fr);
+        vo.y = wall_friction(vo.y, x, cx, fr);
     }
-    vw.x = wall_cushion(vw.x, x, cx);
-    vw.y = wall_cushion(vw.y, y, cy);
-    vo.x = wall_cushion(vo.x, x, cx);
-    vo.y = wall_cushion(vo.y, y, cy);
-    if (!LIQ) {
-        vs.x = wall_friction(vs.x, y, cy, fr);
-        vs.y = wall_friction(vs.y, x, cx, fr);
-    }
-    vw.x = wall_friction(vw.x, y, cy, fr);
-    vw.y = wall_friction(vw.y, x, cx, fr);
-    vo.x = wall_friction(vo.x, y, cy, fr);
-    vo.y = wall_friction(vo.y, x, cx, fr);
     const float lm = W.x + O.x, lv = W.w + O.w;
     out.vs = vs;
     out.vw = make_float4(vw.x, vw.y, lm, lv);
@@ -1496,13 +1502,15 @@ struct NodeSources {
     uint32_t mask[4];
 };
 
-// Sources of halo node (hx, hy), which lies in the 3x3 tiles around tile
-// (tx, ty); info[] holds those tiles' (stamp, mask), row-major from (-1, -1).
+// Sources of halo node (hx, hy) (both >= 0), which lies in the 3x3 tiles
+// around tile (tx, ty); info[] holds those tiles' (stamp, mask), row-major
+// from (-1, -1).
 __device__ __forceinline__ NodeSources node_sources(const StepParams &P, const uint2 *info, int tx, int ty, int hx,
                                                     int hy, uint32_t stamp)
 {
     NodeSources ns;
-    const int ntx = hx / TILE_X, nty = hy / TILE_Y, lx = hx % TILE_X, ly = hy % TILE_Y;
+    const int ntx = (int)((uint32_t)hx / TILE_X), nty = (int)((uint32_t)hy / TILE_Y);
+    const int lx = (int)((uint32_t)hx % TILE_X), ly = (int)((uint32_t)hy % TILE_Y);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const int sx = (k & 1) ? ntx - 1 : ntx, sy = (k & 2) ? nty - 1 : nty;
@@ -2130,7 +2138,7 @@ __device__ __forceinline__ bool g2p_particle(const Ctx &c, const ParticleIn &in,
     // evaluates the same expression)
     float tait_pow = -1.0f;
     if ((REC || P.cfl_enabled) && liquid && m.param > 0.0f && finite_f(m.param))
-        tait_pow = pow_wgsl(__fdiv_rn(1.0f, udet), m.param);
+        tait_pow = pow_wgsl(__frcp_rn(udet), m.param);
     if (!BODIES || P.n_bodies == 0u) validate_cfl<LIQ>(c, id, m, outv, Fn, damage, volume, tait_pow);
     if (BODIES && is_tracked(c, id)) {
         // a body vertex or fracture particle: its final state comes after the
@@ -2401,6 +2409,9 @@ __device__ __forceinline__ void g2p_tiles(const Ctx &c0, G2PShared &sh)
             add_sources<LIQ>(c, ns, ring_node, channels, sum);
         }
         if (in_region) s_vol[t] = make_float2(sum[6], sum[10]);
+        // ring nodes have coordinates x0 - 1 .. x0 + TILE_X, y0 - 1 .. y0 + TILE_Y
+        const bool near_wall = !(beyond_wall_cushion(x0 - 1, x0 + TILE_X, (int)P.cells_x) &&
+                                 beyond_wall_cushion(y0 - 1, y0 + TILE_Y, (int)P.cells_y));
         __syncthreads();
         if (ring_node) {
             const int rx = vx - 1, ry = vy - 1, r = ry * RING_X + rx;
@@ -2413,7 +2424,7 @@ __device__ __forceinline__ void g2p_tiles(const Ctx &c0, G2PShared &sh)
                 const float4 O = make_float4(sum[7], sum[8], sum[9], sum[10]);
                 const uint32_t n = (uint32_t)hy * (uint32_t)node_w + (uint32_t)hx;
                 if (!node_velocity<BODIES, LIQ>(c, n, hx - 1, hy - 1, S, W, O, s_vol[t + 1], s_vol[t - 1], s_vol[t + VOL_X],
-                                   s_vol[t - VOL_X], v)) {
+                                   s_vol[t - VOL_X], v, near_wall)) {
                     s_fail = 1;
                 } else {
                     // count the node once: in the first active tile of (its
