@@ -866,6 +866,7 @@ def run_b200(args):
                            "steps": b["steps"], "warmup": b["warmup"], "e2e": b["e2e"]["value"],
                            "workload": b["config"]["workload"], "scenes": b["config"]["scenes"],
                            "particles": b["config"]["particles"], "retries": b["config"]["retries"],
+                           "launch_shape": b["config"]["launch_shape"],
                            "roofline": {k: b["roofline"][k] for k in ("kernel", "achieved", "frac", "substep")},
                            "clocks": b["clocks"]}
         a = measure_adjoint(1, 1, dist, rank, local_rank, world, full_tape=False)

@@ -102,6 +102,7 @@ struct mpm_solver {
 
     StepParams *d_params = nullptr;  // per scene
     StepParams *h_params = nullptr;  // pinned staging, per scene
+    std::vector<StepParams> full_params;  // the last submit every scene took part in (several scenes)
     cudaEvent_t params_copied = nullptr;
     uint32_t *d_status = nullptr;    // scene 0's status words (in dyn)
     uint32_t *d_counters = nullptr;  // scene 0's counters (in dyn)
@@ -680,8 +681,14 @@ int upload_scene_params(mpm_solver *s, const uint32_t *steps, const float *dt, c
                         const mpm_cfl_guard *guards)
 {
     CUDA_TRY(cudaEventSynchronize(s->params_copied));
-    for (uint32_t k = 0; k < s->n_scenes; ++k)
+    bool every = true;
+    for (uint32_t k = 0; k < s->n_scenes; ++k) {
         fill_params(s, k, s->h_params[k], dt[k], gx[k], gy[k], guards ? guards + k : nullptr, 0.0f, steps[k]);
+        every = every && steps[k] > 0;
+    }
+    // the autotuner times the substeps of the last submit every scene took
+    // part in (a retry submit holds only the scenes that failed)
+    if (every) s->full_params.assign(s->h_params, s->h_params + s->n_scenes);
     return MPM_OK;
 }
 
@@ -1651,7 +1658,10 @@ int mpm_autotune(mpm_solver *s, uint32_t substeps, uint32_t *p2g_ctas, uint32_t 
         e = cudaMemcpyAsync(slots, s->slot_of[start], s->allocated * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
                             s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
-    // the last submit's parameters, `substeps` for every scene that took part
+    // the parameters of the last submit every scene took part in (else the
+    // last submit's), `substeps` for every scene that takes part
+    if (s->full_params.size() == s->n_scenes)
+        std::copy(s->full_params.begin(), s->full_params.end(), s->h_params);
     for (uint32_t k = 0; k < s->n_scenes; ++k)
         if (s->h_params[k].batch_steps > 0) s->h_params[k].batch_steps = substeps;
     if (e == cudaSuccess)
