@@ -415,7 +415,6 @@ __global__ void k_begin_batch(Ctx c, uint32_t reset_progress)
         uint32_t *counters = c.dyn + (size_t)s * SCENE_WORDS + 32;
         if (reset_progress) counters[COUNTER_PROGRESS] = 0u;
         counters[COUNTER_MAX_SPEED] = 0u;
-        for (int k = 0; k < 4; ++k) counters[COUNTER_ACTIVE + k] = 0u;
         counters[COUNTER_SUBSTEP] = 0u;
         counters[COUNTER_FRESH] = 1u;
         counters[COUNTER_STOP] = STOP_NONE;
@@ -2228,18 +2227,6 @@ __device__ __forceinline__ void stage_chunk(const Ctx &c, const uint32_t *entrie
 
 }  // namespace
 
-// Adds a warp's counts of active solid / water / oil nodes to the counters
-// and clears them.
-__device__ __forceinline__ void flush_active_nodes(uint32_t *counters, uint32_t &ws, uint32_t &ww, uint32_t &wo)
-{
-    const uint32_t a = warp_sum(ws), b = warp_sum(ww), d = warp_sum(wo);
-    if ((threadIdx.x & 31u) == 0u) {
-        if (a) atomicAdd(counters + COUNTER_ACTIVE, a);
-        if (b) atomicAdd(counters + COUNTER_ACTIVE + 1, b);
-        if (d) atomicAdd(counters + COUNTER_ACTIVE + 2, d);
-    }
-    ws = ww = wo = 0u;
-}
 
 // The grid update and G2P of one tile holding particles (updateGrid,
 // shaders.ts:1485-1746, then g2p as in k_g2p), one tile per CTA iteration.
@@ -2296,7 +2283,6 @@ __device__ __forceinline__ void g2p_tiles(const Ctx &c0, G2PShared &sh)
     float *const p_vol = sh.vol_in, *const p_pvol = sh.pvol_in, *const p_damage = sh.damage;
     uint32_t *const p_mat = sh.mat, *const p_orig = sh.orig;
     const uint32_t n_active = listed_count(c0), n_heavy = heavy_count(c0);
-    uint32_t ws = 0, ww = 0, wo = 0;
     if constexpr (!SCENES) {
         // visible after the first iteration's barrier
         if (threadIdx.x == 0 && blockIdx.x + gridDim.x < n_active)
@@ -2426,9 +2412,9 @@ __device__ __forceinline__ void g2p_tiles(const Ctx &c0, G2PShared &sh)
                 if (!node_velocity<BODIES, LIQ>(c, n, hx - 1, hy - 1, S, W, O, s_vol[t + 1], s_vol[t - 1], s_vol[t + VOL_X],
                                    s_vol[t - VOL_X], v, near_wall)) {
                     s_fail = 1;
-                } else {
-                    // count the node once: in the first active tile of (its
-                    // tile, left, below, below-left)
+                } else if (BODIES && c.field) {
+                    // the body impulse of a node is stored once: by the first
+                    // active tile of (its tile, left, below, below-left)
                     const int dx = rx >= TILE_X ? 1 : 0, dy = ry >= TILE_Y ? 1 : 0;
                     int ox = dx, oy = dy;
                     if (info[(dy + 1) * 3 + dx + 1].x != stamp) {
@@ -2440,13 +2426,8 @@ __device__ __forceinline__ void g2p_tiles(const Ctx &c0, G2PShared &sh)
                             ox = dx - 1, oy = dy - 1;
                     }
                     if (ox == 0 && oy == 0) {
-                        ws += S.x > 0.f;
-                        ww += W.x > 0.f;
-                        wo += O.x > 0.f;
-                        if (BODIES && c.field) {  // the body impulse of a node is stored once
-                            c.field[n].ix = v.impulse.x;
-                            c.field[n].iy = v.impulse.y;
-                        }
+                        c.field[n].ix = v.impulse.x;
+                        c.field[n].iy = v.impulse.y;
                     }
                 }
             }
@@ -2502,9 +2483,7 @@ __device__ __forceinline__ void g2p_tiles(const Ctx &c0, G2PShared &sh)
                 c.keys[p] = packed_key;
             }
         }
-        if constexpr (SCENES) flush_active_nodes(c.counters, ws, ww, wo);  // the tile's scene
     }
-    if constexpr (!SCENES) flush_active_nodes(c0.counters, ws, ww, wo);
 }
 
 template <bool SCENES, bool BODIES, bool LIQ, bool REC>
@@ -2761,6 +2740,49 @@ __global__ void __launch_bounds__(TILE_NODES) k_count_active_nodes(Ctx c, uint32
     }
 }
 
+// Nodes of the last substep with positive solid / water / oil mass on the
+// default path: CTA b takes tile b (of all scenes) and sums its own 16x8
+// nodes' ring records in node_sources' order, as G2P does.
+__global__ void __launch_bounds__(TILE_NODES) k_count_ring_nodes(Ctx c0, uint32_t *counts)
+{
+    const uint32_t tile = blockIdx.x;
+    const Ctx c = scene_ctx(c0, c0.tile_scene[tile]);
+    const StepParams &P = *c.P;
+    const uint32_t local = tile - P.tile_base;
+    if (local >= P.tiles_x * P.tiles_y) return;  // the scene's sentinel entry
+    const uint32_t stamp = c.counters[COUNTER_STAMP];
+    const int tx = (int)(local % P.tiles_x), ty = (int)(local / P.tiles_x);
+    __shared__ uint2 info[9];
+    if (threadIdx.x < 9) {
+        const int sx = tx + (int)(threadIdx.x % 3) - 1, sy = ty + (int)(threadIdx.x / 3) - 1;
+        info[threadIdx.x] = (sx >= 0 && sy >= 0 && sx < (int)P.tiles_x && sy < (int)P.tiles_y)
+                                ? c.tile_info[P.tile_base + (uint32_t)(sy * (int)P.tiles_x + sx)]
+                                : make_uint2(0xffffffffu, 0u);
+    }
+    __syncthreads();
+    const int hx = tx * TILE_X + (int)(threadIdx.x % TILE_X), hy = ty * TILE_Y + (int)(threadIdx.x / TILE_X);
+    uint32_t s = 0, w = 0, o = 0;
+    if (hx < (int)P.node_w && hy < (int)P.node_h) {
+        uint32_t channels = 0u;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) channels |= info[k].x == stamp ? info[k].y : 0u;
+        float sum[ACC_WORDS];
+#pragma unroll
+        for (int k = 0; k < ACC_WORDS; ++k) sum[k] = 0.f;
+        add_sources(c, node_sources(P, info, tx, ty, hx, hy, stamp), true, channels, sum);
+        s = sum[0] > 0.f;
+        w = sum[3] > 0.f;
+        o = sum[7] > 0.f;
+    }
+    s = __reduce_add_sync(0xffffffffu, s);
+    w = __reduce_add_sync(0xffffffffu, w);
+    o = __reduce_add_sync(0xffffffffu, o);
+    if ((threadIdx.x & 31) == 0) {
+        if (s) atomicAdd(counts, s);
+        if (w) atomicAdd(counts + 1, w);
+        if (o) atomicAdd(counts + 2, o);
+    }
+}
 
 // ------------------------------------------------------ bodies, fracture --
 // Bonded-triangle bodies ("pebbles") and fracture bonds of the multi-material

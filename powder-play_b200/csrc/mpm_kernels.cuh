@@ -159,7 +159,6 @@ constexpr int END_BATCH_ITEMS = 4;          // particles per thread and pass
 static_assert(VOL_X * VOL_Y <= G2P_THREADS && RING_NODES <= G2P_THREADS, "one node per thread");
 
 // device counters beyond the three of mpm_device.cuh
-constexpr int COUNTER_ACTIVE = 4;        // [4..6] active solid/water/oil nodes (summed over the batch), [7] free
 constexpr int COUNTER_SUBSTEP = 8;       // the substep of this batch under way (failed and skipped included)
 constexpr int COUNTER_FRESH = 9;         // 1 from the start of a batch until its first substep starts
 constexpr int COUNTER_STOP = 10;         // substeps completed in this batch (STOP_NONE while running)
@@ -223,6 +222,7 @@ __global__ void k_fracture_bonds(Ctx c);
 __global__ void k_fracture_damage(Ctx c);
 __global__ void k_body_finish(Ctx c);
 __global__ void k_count_active_nodes(Ctx c, uint32_t *counts);
+__global__ void k_count_ring_nodes(Ctx c0, uint32_t *counts);
 __global__ void k_probe_deformation(const float4 *F, const float4 *C, float dt, uint32_t n, float4 *trial,
                                     float2 *increment_det, uint32_t *substeps, uint32_t *flags);
 // surface occupancy (status word 7 flags: shaders.ts:187-189)

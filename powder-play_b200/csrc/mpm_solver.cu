@@ -91,7 +91,6 @@ struct mpm_solver {
     uint32_t cell_pad = 0, n_chunks = 0;
     uint32_t n_bodies = 0, n_bonds = 0;
     int cur = 0;  // buffer holding the current particle state
-    uint32_t substeps_since_begin = 0;
     // scenes: one for mpm_create, several for mpmb_create
     std::vector<SceneHost> scenes;
     uint32_t n_scenes = 1, n_tiles_total = 0;
@@ -1206,10 +1205,7 @@ int profile_run(mpm_solver *s, uint32_t step_count, bool guarded, double *kernel
     if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
     if (e == cudaSuccess) e = cudaGraphLaunch(exec, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
-    if (e == cudaSuccess) {
-        s->cur = parity;
-        s->substeps_since_begin = step_count;
-    }
+    if (e == cudaSuccess) s->cur = parity;
     for (size_t k = 1; e == cudaSuccess && k < rec.events.size(); ++k) {
         float ms = 0.0f;
         e = cudaEventElapsedTime(&ms, rec.events[k - 1], rec.events[k]);
@@ -1254,7 +1250,6 @@ int timed_run(mpm_solver *s, uint32_t step_count, bool guarded, double *ms)
     if (e == cudaSuccess) e = cudaEventElapsedTime(&t, s->batch_start, s->batch_stop);
     if (e == cudaSuccess) {
         s->cur = parity;
-        s->substeps_since_begin = step_count;
         *ms = t;
     }
     if (exec) cudaGraphExecDestroy(exec);
@@ -1450,7 +1445,6 @@ int run_batch(mpm_solver *s, uint32_t step_count, bool guarded)
         CUDA_TRY(cudaGraphLaunch(exec, s->stream));
         CUDA_TRY(cudaEventRecord(s->params_copied, s->stream));
         if (step_count & 1u) s->cur = 1 - s->cur;
-        s->substeps_since_begin = step_count;
         s->batch_timed = true;
         s->readback_ready = true;
         return MPM_OK;
@@ -1460,7 +1454,6 @@ int run_batch(mpm_solver *s, uint32_t step_count, bool guarded)
     const Ctx c0 = make_ctx(s, s->cur);
     CUDA_TRY(cudaEventRecord(s->batch_start, s->stream));
     k_begin_batch<<<blocks_for(s->n_scenes, PARTICLE_THREADS), PARTICLE_THREADS, 0, s->stream>>>(c0, guarded ? 1u : 0u);
-    s->substeps_since_begin = 0;
     if (s->gather() && s->n > 0) enqueue_tile_count(s, c0);
     CUDA_TRY(cudaGetLastError());
     if (s->n > 0) {
@@ -1477,7 +1470,6 @@ int run_batch(mpm_solver *s, uint32_t step_count, bool guarded)
                 if (k < MAX_GRAPH_LOG2) break;
             }
         }
-        s->substeps_since_begin = step_count;
         enqueue_end_batch(s, s->cur, step_count, guarded);
         CUDA_TRY(cudaGetLastError());
     }
@@ -1777,24 +1769,12 @@ int mpm_count_active_nodes(mpm_solver *s, uint32_t counts[3])
     forget_readback(s);
     if (!s || !counts) return set_error(MPM_ERR_INVALID_ARGUMENT, "solver and counts must not be NULL");
     CUDA_TRY(cudaSetDevice(s->device));
-    if (s->gather()) {
-        // accumulated by k_g2p_tile since the last batch began, summed over
-        // the scenes: average per substep of the batch
-        std::vector<uint32_t> dyn((size_t)s->n_scenes * SCENE_WORDS);
-        CUDA_TRY(cudaMemcpyAsync(dyn.data(), s->dyn, dyn.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                                 s->stream));
-        CUDA_TRY(cudaStreamSynchronize(s->stream));
-        const uint64_t steps = std::max(1u, s->substeps_since_begin);
-        for (int k = 0; k < 3; ++k) {
-            uint64_t sum = 0;
-            for (uint32_t sc = 0; sc < s->n_scenes; ++sc) sum += dyn[(size_t)sc * SCENE_WORDS + 32 + COUNTER_ACTIVE + k];
-            counts[k] = (uint32_t)(sum / steps);
-        }
-        return MPM_OK;
-    }
     CUDA_TRY(cudaMemsetAsync(s->d_active, 0, 4 * sizeof(uint32_t), s->stream));
     const Ctx c = make_ctx(s, s->cur);
-    k_count_active_nodes<<<dim3(s->tiles_x, s->tiles_y), TILE_NODES, 0, s->stream>>>(c, s->d_active);
+    if (s->gather())  // the ring records of the last substep, every scene
+        k_count_ring_nodes<<<s->n_tiles_total, TILE_NODES, 0, s->stream>>>(c, s->d_active);
+    else
+        k_count_active_nodes<<<dim3(s->tiles_x, s->tiles_y), TILE_NODES, 0, s->stream>>>(c, s->d_active);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(s->h_readback, s->d_active, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));

@@ -108,6 +108,48 @@ def test_small_persistent_g2p_grids_agree_bitwise(g2p_ctas):
     assert np.array_equal(_bits(liquid), _bits(default))
 
 
+def _touched_nodes(px, py, dx):
+    """Nodes with a positive quadratic weight from the particles at (px, py):
+    the base node's stencil as the kernels form it (position * (1 / dx),
+    base = floor(g - 0.5), f = g - base; float32), offsets 0 and 1 always
+    and 2 where f > 0.5 (the third weight is 0.5 (f - 0.5)^2)."""
+    inv = np.float32(1) / np.float32(dx)
+
+    def axis(x):
+        g = np.asarray(x, np.float32) * inv
+        base = np.floor(g - np.float32(0.5))
+        return base.astype(np.int64), (g - base) > np.float32(0.5)
+
+    (bx, third_x), (by, third_y) = axis(px), axis(py)
+    nodes = set()
+    for ox in range(3):
+        for oy in range(3):
+            keep = np.ones(len(bx), bool)
+            if ox == 2:
+                keep &= third_x
+            if oy == 2:
+                keep &= third_y
+            nodes.update(zip((bx[keep] + ox).tolist(), (by[keep] + oy).tolist()))
+    return len(nodes)
+
+
+def test_active_node_count_is_the_last_substeps_nodes_with_mass():
+    # the default path counts, from the ring records of the last substep, the
+    # nodes whose summed water / oil mass is positive: after one substep from
+    # the uploaded state those are the nodes the particles' stencils weigh
+    p, config = create_dam_break_scene(particles_per_phase=20_000, columns=200, grid=SMALL_DAM)
+    solver = create_mpm_mls_gpu_solver(p, config)
+    try:
+        solver.step_batch(1, 1.0 / 1200.0, DAM_BREAK_GRAVITY)
+        assert solver._read_compact()[2][0] == 0
+        counts = solver.count_active_nodes()
+    finally:
+        solver.dispose()
+    water, oil = p.material == 0, p.material == 1
+    dx = config["grid"]["cellSize"]
+    assert counts == (0, _touched_nodes(p.px[water], p.py[water], dx), _touched_nodes(p.px[oil], p.py[oil], dx))
+
+
 def _crowded_tank(per_side):
     """The SI tank's water as a block of per_side^2 particles per cell over
     12 x 12 cells: its tiles hold far more than one stage (the crowded path of
