@@ -115,10 +115,10 @@ constexpr int COUNTER_STAMP = 0;
 constexpr int COUNTER_PROGRESS = 1;
 constexpr int COUNTER_MAX_SPEED = 2;
 
-__device__ __forceinline__ bool finite_f(float v)
-{
-    return (__float_as_uint(v) & 0x7f800000u) != 0x7f800000u;
-}
+// |v| < infinity: false for both infinities and every NaN (one compare with
+// an absolute-value operand, where a test of the exponent bits takes two
+// instructions)
+__device__ __forceinline__ bool finite_f(float v) { return fabsf(v) < __int_as_float(0x7f800000); }
 __device__ __forceinline__ bool finite2(float2 v) { return finite_f(v.x) && finite_f(v.y); }
 __device__ __forceinline__ bool finite4(float4 v)
 {
